@@ -1,0 +1,370 @@
+#!/usr/bin/env python
+"""Benchmark of the GNOF orbital-gradient step (the per-iteration RI hot path).
+
+One step = one iteration of the orbital optimiser loop of DoNOF.jl
+(src/minimization.jl:387-422): AMSGrad-style update of the rotation y,
+C <- C exp(Y(y)), compute_Lagrange2 (three-index transform + Lagrangian),
+computeE_elec and the packed orbital gradient.
+
+Workload (synthetic; the reference publishes no data set and no basis data
+or integral engine exists here): nbf = 256, naux = 1024, nbf5 = 64
+(ndoc = 16, ncwo = 3), b ~ N(0, 1/sqrt(naux)) symmetrised, C = Q of a seeded
+QR, softmax occupations from N(0,1) logits, GNOF coefficients.  b (512 MiB
+FP64) exceeds the 126 MB L2, so no flush is needed between steps.
+
+  value   device-resident loop (donof_orbopt_dev, inputs in HBM)
+  e2e     the reference-facing host-buffer calls per step (donof_rotate +
+          donof_lagrange2 with host arrays, optimiser update on the host),
+          as DoNOF.jl's loop drives its GPU plugin
+  --impl reference   the CPU restatement of the reference path (C/OpenMP FP64
+          oracle, all host threads) on the same workload
+
+Multi-GPU: the optimiser loop of one job does not shard without a collective
+per step; --gpus N runs N independent replicas (one job per GPU, weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path[:0] = [str(ROOT), str(ROOT / "donof.jl_b200")]
+
+METRIC = "GNOF orbital-gradient steps/s"
+UNIT = "steps/s"
+WORKLOAD = dict(nbf=256, naux=1024, nbeta=16, ncwo=3)
+SEED = 1234
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--method", default="ADAM")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def config(args, world):
+    return {"workload": "synthetic-256 GNOF orbital step (nbf=256, naux=1024, nbf5=64)",
+            "nbf": WORKLOAD["nbf"], "naux": WORKLOAD["naux"], "nbf5": 64, "ndoc": 16, "ncwo": 3,
+            "orb_method": args.method, "precision": args.precision,
+            "parallelism": f"replicas x{world}", "l2": "inputs > L2 (b = 512 MiB FP64)"}
+
+
+class ClockSampler:
+    """nvidia-smi samples (200 ms) of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax = float(parts[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower() in ("active", "1"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_dgemm_tflops(torch, dev):
+    """FP64 tensor-core ceiling for the plain form: cuBLAS DGEMM 8192^3, best of 5
+    (the driver's peak file carries HBM and BF16 figures only)."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    for _ in range(2):
+        torch.matmul(a, b)
+    best = 1e30
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        torch.cuda.synchronize()
+        best = min(best, s.elapsed_time(e) / 1e3)
+    del a, b
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def load_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text())
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "fallback": True}
+
+
+def traffic_from_profiles(kernel_key):
+    """DRAM bytes per launch of the transform from the committed ncu summary, if present."""
+    p = ROOT / "profiles" / "traffic.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text()).get(kernel_key)
+        except Exception:
+            return None
+    return None
+
+
+def host_adam(state, g, i, alpha, beta1=0.5, beta2=0.9):
+    m, v, vmax = state
+    m[:] = beta1 * m + (1 - beta1) * g
+    v[:] = beta2 * v + (1 - beta2) * g * g
+    vmax[:] = np.maximum(vmax, v / (1 - beta2 ** i))
+    return -alpha * (m / (1 - beta1 ** i)) / np.sqrt(vmax + 1e-16)
+
+
+def pack(elag, nbf5):
+    g = 4.0 * (elag - elag.T)
+    iu = np.triu_indices(elag.shape[0], 1)
+    sel = iu[0] < nbf5
+    return g[iu[0][sel], iu[1][sel]]
+
+
+def run_cpu_steps(wl, steps, budget_s, threads=None):
+    """Orbital steps on the CPU oracle (C/OpenMP FP64): host update + rotate + Lagrangian."""
+    from oracle import native
+
+    if threads:
+        native.set_threads(threads)
+    p = wl.p
+    C = wl.C.copy(order="F")
+    elag, _ = native.lagrange2(C, wl.n, wl.H, wl.b, wl.cj12, wl.ck12, p.nalpha, p.nbeta)
+    st = (np.zeros(p.nvar), np.zeros(p.nvar), np.zeros(p.nvar))
+    done = 0
+    t0 = time.perf_counter()
+    for i in range(1, steps + 1):
+        y = host_adam(st, pack(elag, p.nbf5), i, 0.01)
+        C = native.rotate(y, C, p.nbf5)
+        elag, Hmat = native.lagrange2(C, wl.n, wl.H, wl.b, wl.cj12, wl.ck12, p.nalpha, p.nbeta)
+        done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    return done, dt, native.num_threads()
+
+
+def reference_arm(args, rank, world):
+    from donof_b200 import workload
+
+    if rank != 0:
+        return None
+    wl = workload.synthetic(**WORKLOAD, seed=SEED)
+    run_cpu_steps(wl, max(1, min(args.warmup, 1)), 60.0)  # warm caches / thread pool
+    done, dt, cores = run_cpu_steps(wl, args.steps, 150.0)
+    v = done / dt
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * dt / done, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": config(args, world),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"{done} of {args.steps} orbital steps (C/OpenMP FP64 restatement of "
+                                       "rotate_orbital + compute_Lagrange2, reference contraction order)"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    return line
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        if backend == "nccl":
+            import torch
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+
+    if args.impl == "reference":
+        line = reference_arm(args, rank, world)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    import torch
+    import donof_b200 as d
+    from donof_b200 import workload
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    wl = workload.synthetic(**WORKLOAD, seed=SEED)
+    p = wl.p
+    ctx = d.Context(local)
+    bt = d.eris_to_gpu(wl.b, args.precision, ctx)
+    tC0, tH, tn, tcj, tck = (d.to_device(x, dev) for x in (wl.C, wl.H, wl.n, wl.cj12, wl.ck12))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # ---- device-resident optimiser loop: warm-up, then exactly K steps
+    tC = tC0.clone()
+    d.orbopt_dev(args.method, tn, tcj, tck, tH, tC, bt, p, 0.01, args.warmup, 0.0)
+    tC.copy_(tC0)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    l0 = d.launch_count()
+    with ClockSampler(local) as clk:
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        E, nit, ok, _, _ = d.orbopt_dev(args.method, tn, tcj, tck, tH, tC, bt, p, 0.01, args.steps, 0.0)
+        ev1.record()
+        torch.cuda.synchronize()
+    launches = d.launch_count() - l0
+    barrier()
+    t = ev0.elapsed_time(ev1) / 1e3
+    assert nit == args.steps, (nit, args.steps)
+    if dist is not None:
+        tt = torch.tensor([t], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t = float(tt.item())
+    value = world * args.steps / t
+
+    # ---- roofline of the dominant kernel pair: the three-index transform (T1 + T2)
+    nbf, naux, nbf5 = p.nbf, p.nbfaux, p.nbf5
+    flops = 2.0 * nbf * nbf * nbf5 * naux + 2.0 * nbf * nbf5 * nbf5 * naux
+    for _ in range(3):
+        d.transform_dev(tC, bt, nbf5)
+    reps = 10
+    es = [torch.cuda.Event(enable_timing=True) for _ in range(reps + 1)]
+    es[0].record()
+    for r in range(reps):
+        d.transform_dev(tC, bt, nbf5)
+        es[r + 1].record()
+    torch.cuda.synchronize()
+    dur = [es[r].elapsed_time(es[r + 1]) / 1e3 for r in range(reps)]
+    tr = statistics.mean(dur)
+    peaks = load_peaks()
+    if args.precision == "fp64":
+        peak = measured_dgemm_tflops(torch, dev)
+        roof = {"bound": "tensor", "achieved": flops / tr / 1e12, "peak": peak, "unit": "TFLOP/s",
+                "frac": flops / tr / 1e12 / peak, "traffic": traffic_from_profiles("transform_f64"),
+                "kernel": "gemm_f64_kernel (T1: b_l C5, then T2: C5^T tmp_l), batched over naux",
+                "algorithmic": f"{flops:.4e} FLOP per transform", "ms": tr * 1e3,
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor pipe)"}
+    else:
+        byts = 4.0 * nbf * nbf * naux
+        roof = {"bound": "hbm", "achieved": byts / tr / 1e9, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": byts / tr / 1e9 / peaks["hbm_gbs"], "traffic": traffic_from_profiles("transform_mixed"),
+                "algorithmic": f"{byts:.4e} bytes (FP32 b read once) per transform", "ms": tr * 1e3,
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs" + (" (fallback)" if peaks.get("fallback") else "")}
+
+    # ---- end to end through the host-buffer C ABI (what a DoNOF.jl loop does per step)
+    e2e = None
+    if not args.no_e2e:
+        C = wl.C.copy(order="F")
+        st = (np.zeros(p.nvar), np.zeros(p.nvar), np.zeros(p.nvar))
+        elag, Hm = d.compute_Lagrange2(C, wl.n, wl.H, bt, wl.cj12, wl.ck12, p.nalpha, p.nbeta)
+
+        def host_step(i, C, elag):
+            y = host_adam(st, pack(elag, p.nbf5), i, 0.01)
+            C = d.rotate_orbital(y, C, p, ctx)
+            elag, Hm, E = d.compute_Lagrange2(C, wl.n, wl.H, bt, wl.cj12, wl.ck12, p.nalpha, p.nbeta,
+                                              return_energy=True)
+            return C, elag
+
+        for i in range(1, args.warmup + 1):
+            C, elag = host_step(i, C, elag)
+        C = wl.C.copy(order="F")
+        st = (np.zeros(p.nvar), np.zeros(p.nvar), np.zeros(p.nvar))
+        torch.cuda.synchronize()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for i in range(1, args.steps + 1):
+            C, elag = host_step(i, C, elag)
+        e1.record()
+        torch.cuda.synchronize()
+        te = e0.elapsed_time(e1) / 1e3
+        if dist is not None:
+            tt = torch.tensor([te], device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            te = float(tt.item())
+        nn, n55 = nbf * nbf, nbf5 * nbf5
+        h2d = 8 * (p.nvar + nn) + 8 * (nn + nn + nbf5 + 2 * n55)
+        d2h = 8 * nn + 8 * (nn + nbf * nbf5 + 1)
+        e2e = {"value": world * args.steps / te, "unit": UNIT, "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "path": "donof_rotate + donof_lagrange2 (host buffers), host update"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        done, dt, cores = run_cpu_steps(wl, 6, 20.0)
+        cpu = {"value": done / dt, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"{done} orbital steps of the same workload on the C/OpenMP FP64 oracle"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64" if args.precision == "fp64" else "tf32x3+f64", "data": "synthetic",
+                "config": config(args, world), "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": int(launches), "clocks": clk.summary(), "final_E": E}
+        print(json.dumps(line), flush=True)
+    bt.free()
+    ctx.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

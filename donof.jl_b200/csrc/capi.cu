@@ -1,0 +1,523 @@
+// C ABI of libdonofb200 (declarations and reference mapping in donof_b200.h).
+#include <stdarg.h>
+#include <string.h>
+
+#include <atomic>
+#include <new>
+
+#include "kernels.cuh"
+
+namespace donof {
+
+static thread_local std::string g_tls_error;
+static std::atomic<unsigned long long> g_launches{0};
+
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+void set_error(donof_ctx* ctx, const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (ctx) ctx->last_error = buf;
+    g_tls_error = buf;
+}
+
+int DevBuf::ensure(donof_ctx* ctx, size_t want) {
+    if (want <= bytes && ptr != nullptr) return DONOF_OK;
+    if (ptr) {
+        cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+    if (want == 0) want = 256;
+    cudaError_t e = cudaMalloc(&ptr, want);
+    if (e != cudaSuccess) {
+        ptr = nullptr;
+        set_error(ctx, "cudaMalloc(%zu bytes): %s", want, cudaGetErrorString(e));
+        return e == cudaErrorMemoryAllocation ? DONOF_ERR_OOM : DONOF_ERR_CUDA;
+    }
+    bytes = want;
+    return DONOF_OK;
+}
+
+void DevBuf::release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+}
+
+int orbopt_run(donof_job* job, int method, const double* n, const double* cj12, const double* ck12,
+               const double* H, int nbf5, int nalpha, int nbeta, double* alpha, int* maxloop,
+               double threshgorb, double* C, double* E_out, int* nit_out, int* success_out,
+               int precision);
+int convert_b_f32(donof_job* job);
+
+}  // namespace donof
+
+using namespace donof;
+
+namespace {
+
+int use_device(donof_ctx* ctx) {
+    DONOF_CUDA(ctx, cudaSetDevice(ctx->device));
+    return DONOF_OK;
+}
+
+int check_sizes(donof_ctx* ctx, int nbf, int nbf5, int nalpha, int nbeta) {
+    if (nbf <= 0 || nbf5 <= 0 || nbf5 > nbf) {
+        set_error(ctx, "invalid sizes nbf=%d nbf5=%d", nbf, nbf5);
+        return DONOF_ERR_ARG;
+    }
+    if (nbeta < 0 || nalpha < nbeta || nalpha > nbf5) {
+        set_error(ctx, "invalid occupations nalpha=%d nbeta=%d nbf5=%d", nalpha, nbeta, nbf5);
+        return DONOF_ERR_ARG;
+    }
+    return DONOF_OK;
+}
+
+#define REQUIRE(ctx, cond, msg)                 \
+    do {                                        \
+        if (!(cond)) {                          \
+            set_error((ctx), "%s", (msg));      \
+            return DONOF_ERR_ARG;               \
+        }                                       \
+    } while (0)
+
+// Copies `count` doubles host -> device staging slot.
+struct Stager {
+    donof_ctx* ctx;
+    cudaStream_t st;
+    char* base;
+    size_t off = 0;
+    double* put(const double* h, size_t count) {
+        double* d = reinterpret_cast<double*>(base + off);
+        off += ((count * sizeof(double) + 255) / 256) * 256;
+        if (h != nullptr) cudaMemcpyAsync(d, h, count * sizeof(double), cudaMemcpyHostToDevice, st);
+        return d;
+    }
+    static size_t bytes(size_t count) { return ((count * sizeof(double) + 255) / 256) * 256; }
+};
+
+int effective_precision(donof_job* job, int precision) {
+    if (precision != DONOF_PREC_FP64 && precision != DONOF_PREC_MIXED) {
+        set_error(job->ctx, "unknown precision %d", precision);
+        return -1;
+    }
+    if (precision == DONOF_PREC_MIXED && job->b32 == nullptr) {
+        set_error(job->ctx, "mixed precision requested but the job holds no FP32 copy of b");
+        return -1;
+    }
+    return precision;
+}
+
+}  // namespace
+
+extern "C" {
+
+int donof_version(void) { return 1; }
+
+unsigned long long donof_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+
+int donof_transform_dev(donof_job* job, int precision, const double* C, int nbf5, double* b_pq) {
+    if (!job) return DONOF_ERR_ARG;
+    donof_ctx* ctx = job->ctx;
+    REQUIRE(ctx, C != nullptr, "null C");
+    REQUIRE(ctx, nbf5 > 0 && nbf5 <= job->nbf, "invalid nbf5");
+    const int prec = effective_precision(job, precision);
+    if (prec < 0) return DONOF_ERR_ARG;
+    DONOF_CHECK(use_device(ctx));
+    if (prec == DONOF_PREC_MIXED) {
+        DONOF_CHECK(transforms_mixed(job, ctx->stream, C, nbf5));
+    } else {
+        DONOF_CHECK(transforms_f64(job, ctx->stream, C, nbf5));
+    }
+    if (b_pq != nullptr)
+        DONOF_CUDA(ctx, cudaMemcpyAsync(b_pq, job->bpq.ptr, sizeof(double) * (size_t)nbf5 * nbf5 * job->naux,
+                                        cudaMemcpyDeviceToDevice, ctx->stream));
+    return DONOF_OK;
+}
+
+const char* donof_status_string(int s) {
+    switch (s) {
+        case DONOF_OK: return "ok";
+        case DONOF_ERR_ARG: return "invalid argument";
+        case DONOF_ERR_CUDA: return "CUDA error";
+        case DONOF_ERR_OOM: return "out of device memory";
+        case DONOF_ERR_STATE: return "invalid state";
+        case DONOF_ERR_NOT_CONVERGED: return "not converged";
+        default: return "unknown status";
+    }
+}
+
+const char* donof_last_error(const donof_ctx* ctx) {
+    if (ctx) return ctx->last_error.c_str();
+    return g_tls_error.c_str();
+}
+
+int donof_create(int device, donof_ctx** out) {
+    if (out == nullptr) {
+        set_error(nullptr, "donof_create: null output pointer");
+        return DONOF_ERR_ARG;
+    }
+    *out = nullptr;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || device < 0 || device >= count) {
+        set_error(nullptr, "donof_create: device %d not available (%d devices, %s)", device, count,
+                  cudaGetErrorString(e));
+        return e != cudaSuccess ? DONOF_ERR_CUDA : DONOF_ERR_ARG;
+    }
+    donof_ctx* ctx = new (std::nothrow) donof_ctx();
+    if (!ctx) return DONOF_ERR_OOM;
+    ctx->device = device;
+    if (cudaSetDevice(device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        set_error(nullptr, "donof_create: cannot create a stream on device %d", device);
+        delete ctx;
+        return DONOF_ERR_CUDA;
+    }
+    ctx->own_stream = true;
+    cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device);
+    *out = ctx;
+    return DONOF_OK;
+}
+
+int donof_destroy(donof_ctx* ctx) {
+    if (!ctx) return DONOF_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    ctx->stage_in.release();
+    ctx->stage_out.release();
+    ctx->rot.release();
+    if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return DONOF_OK;
+}
+
+int donof_set_stream(donof_ctx* ctx, void* stream) {
+    if (!ctx) return DONOF_ERR_ARG;
+    DONOF_CHECK(use_device(ctx));
+    if (ctx->own_stream && ctx->stream) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaStreamDestroy(ctx->stream);
+    }
+    ctx->stream = static_cast<cudaStream_t>(stream);
+    ctx->own_stream = false;
+    return DONOF_OK;
+}
+
+void* donof_get_stream(donof_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int donof_synchronize(donof_ctx* ctx) {
+    if (!ctx) return DONOF_ERR_ARG;
+    DONOF_CHECK(use_device(ctx));
+    DONOF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return DONOF_OK;
+}
+
+static int make_job(donof_ctx* ctx, int nbf, int naux, int precision, donof_job** job) {
+    REQUIRE(ctx, job != nullptr, "null job pointer");
+    REQUIRE(ctx, nbf > 0 && naux > 0, "nbf and naux must be positive");
+    REQUIRE(ctx, precision == DONOF_PREC_FP64 || precision == DONOF_PREC_MIXED, "unknown precision");
+    donof_job* j = new (std::nothrow) donof_job();
+    if (!j) return DONOF_ERR_OOM;
+    j->ctx = ctx;
+    j->nbf = nbf;
+    j->naux = naux;
+    j->precision = precision;
+    *job = j;
+    return DONOF_OK;
+}
+
+int donof_b_upload(donof_ctx* ctx, const double* b_host, int nbf, int naux, int precision,
+                   donof_job** job) {
+    if (!ctx) return DONOF_ERR_ARG;
+    REQUIRE(ctx, b_host != nullptr, "null b");
+    DONOF_CHECK(use_device(ctx));
+    donof_job* j = nullptr;
+    DONOF_CHECK(make_job(ctx, nbf, naux, precision, &j));
+    const size_t bytes = sizeof(double) * (size_t)nbf * nbf * naux;
+    void* d = nullptr;
+    cudaError_t e = cudaMalloc(&d, bytes);
+    if (e != cudaSuccess) {
+        delete j;
+        set_error(ctx, "cudaMalloc(b, %zu bytes): %s", bytes, cudaGetErrorString(e));
+        return DONOF_ERR_OOM;
+    }
+    e = cudaMemcpyAsync(d, b_host, bytes, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+        cudaFree(d);
+        delete j;
+        set_error(ctx, "upload of b: %s", cudaGetErrorString(e));
+        return DONOF_ERR_CUDA;
+    }
+    j->b = static_cast<const double*>(d);
+    j->own_b = true;
+    if (precision == DONOF_PREC_MIXED) {
+        int s = convert_b_f32(j);
+        if (s != DONOF_OK) {
+            donof_job_free(j);
+            return s;
+        }
+    }
+    *job = j;
+    return DONOF_OK;
+}
+
+int donof_b_attach(donof_ctx* ctx, const double* b_dev, int nbf, int naux, int precision,
+                   donof_job** job) {
+    if (!ctx) return DONOF_ERR_ARG;
+    REQUIRE(ctx, b_dev != nullptr, "null b");
+    DONOF_CHECK(use_device(ctx));
+    donof_job* j = nullptr;
+    DONOF_CHECK(make_job(ctx, nbf, naux, precision, &j));
+    j->b = b_dev;
+    j->own_b = false;
+    if (precision == DONOF_PREC_MIXED) {
+        int s = convert_b_f32(j);
+        if (s != DONOF_OK) {
+            donof_job_free(j);
+            return s;
+        }
+    }
+    *job = j;
+    return DONOF_OK;
+}
+
+int donof_job_free(donof_job* job) {
+    if (!job) return DONOF_OK;
+    cudaSetDevice(job->ctx->device);
+    cudaStreamSynchronize(job->ctx->stream);
+    if (job->own_b && job->b) cudaFree((void*)job->b);
+    if (job->own_b32 && job->b32) cudaFree((void*)job->b32);
+    job->tmp.release();
+    job->bpq.release();
+    job->W.release();
+    job->part.release();
+    job->small.release();
+    job->orb.release();
+    job->io.release();
+    delete job;
+    return DONOF_OK;
+}
+
+size_t donof_job_device_bytes(const donof_job* job) {
+    if (!job) return 0;
+    size_t s = job->tmp.bytes + job->bpq.bytes + job->W.bytes + job->part.bytes + job->small.bytes +
+               job->orb.bytes + job->io.bytes;
+    if (job->own_b) s += sizeof(double) * (size_t)job->nbf * job->nbf * job->naux;
+    if (job->own_b32) s += sizeof(float) * (size_t)job->nbf * job->nbf * job->naux;
+    return s;
+}
+
+int donof_lagrange2_prec_dev(donof_job* job, int precision, const double* C, const double* n,
+                             const double* H, const double* cj12, const double* ck12, int nbf5,
+                             int nalpha, int nbeta, double* elag, double* H_mat, double* E_elec) {
+    if (!job) return DONOF_ERR_ARG;
+    donof_ctx* ctx = job->ctx;
+    DONOF_CHECK(check_sizes(ctx, job->nbf, nbf5, nalpha, nbeta));
+    REQUIRE(ctx, C && n && H && cj12 && ck12 && elag && H_mat, "null array argument");
+    const int prec = effective_precision(job, precision);
+    if (prec < 0) return DONOF_ERR_ARG;
+    DONOF_CHECK(use_device(ctx));
+    if (prec == DONOF_PREC_MIXED)
+        return lagrange2_mixed(job, ctx->stream, C, n, H, cj12, ck12, nbf5, nalpha, nbeta, elag, H_mat,
+                               E_elec);
+    return lagrange2_f64(job, ctx->stream, C, n, H, cj12, ck12, nbf5, nalpha, nbeta, elag, H_mat,
+                         E_elec);
+}
+
+int donof_lagrange2_dev(donof_job* job, const double* C, const double* n, const double* H,
+                        const double* cj12, const double* ck12, int nbf5, int nalpha, int nbeta,
+                        double* elag, double* H_mat, double* E_elec) {
+    if (!job) return DONOF_ERR_ARG;
+    return donof_lagrange2_prec_dev(job, job->precision, C, n, H, cj12, ck12, nbf5, nalpha, nbeta,
+                                    elag, H_mat, E_elec);
+}
+
+int donof_lagrange2(donof_job* job, const double* C, const double* n, const double* H,
+                    const double* cj12, const double* ck12, int nbf5, int nalpha, int nbeta,
+                    double* elag, double* H_mat, double* E_elec) {
+    if (!job) return DONOF_ERR_ARG;
+    donof_ctx* ctx = job->ctx;
+    DONOF_CHECK(check_sizes(ctx, job->nbf, nbf5, nalpha, nbeta));
+    REQUIRE(ctx, C && n && H && cj12 && ck12 && elag && H_mat, "null array argument");
+    DONOF_CHECK(use_device(ctx));
+    const size_t nbf = job->nbf, nn = nbf * nbf, n55 = (size_t)nbf5 * nbf5;
+    const size_t need = Stager::bytes(nn) * 3 + Stager::bytes(nbf5) + Stager::bytes(n55) * 2 +
+                        Stager::bytes(nbf * nbf5) + Stager::bytes(1);
+    DONOF_CHECK(job->io.ensure(ctx, need));
+    Stager sg{ctx, ctx->stream, job->io.as<char>()};
+    const double* dC = sg.put(C, nn);
+    const double* dH = sg.put(H, nn);
+    const double* dn = sg.put(n, nbf5);
+    const double* dcj = sg.put(cj12, n55);
+    const double* dck = sg.put(ck12, n55);
+    double* del = sg.put(nullptr, nn);
+    double* dHm = sg.put(nullptr, nbf * nbf5);
+    double* dE = sg.put(nullptr, 1);
+    DONOF_CUDA(ctx, cudaGetLastError());
+    DONOF_CHECK(donof_lagrange2_dev(job, dC, dn, dH, dcj, dck, nbf5, nalpha, nbeta, del, dHm, dE));
+    DONOF_CUDA(ctx, cudaMemcpyAsync(elag, del, nn * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    DONOF_CUDA(ctx, cudaMemcpyAsync(H_mat, dHm, nbf * nbf5 * sizeof(double), cudaMemcpyDeviceToHost,
+                                    ctx->stream));
+    if (E_elec)
+        DONOF_CUDA(ctx, cudaMemcpyAsync(E_elec, dE, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    DONOF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return DONOF_OK;
+}
+
+int donof_jkh_mo_prec_dev(donof_job* job, int precision, const double* C, const double* H, int nbf5,
+                          double* J_MO, double* K_MO, double* H_core) {
+    if (!job) return DONOF_ERR_ARG;
+    donof_ctx* ctx = job->ctx;
+    REQUIRE(ctx, nbf5 > 0 && nbf5 <= job->nbf, "invalid nbf5");
+    REQUIRE(ctx, C && H && J_MO && K_MO && H_core, "null array argument");
+    const int prec = effective_precision(job, precision);
+    if (prec < 0) return DONOF_ERR_ARG;
+    DONOF_CHECK(use_device(ctx));
+    if (prec == DONOF_PREC_MIXED) return jkh_mo_mixed(job, ctx->stream, C, H, nbf5, J_MO, K_MO, H_core);
+    return jkh_mo_f64(job, ctx->stream, C, H, nbf5, J_MO, K_MO, H_core);
+}
+
+int donof_jkh_mo_dev(donof_job* job, const double* C, const double* H, int nbf5, double* J_MO,
+                     double* K_MO, double* H_core) {
+    if (!job) return DONOF_ERR_ARG;
+    return donof_jkh_mo_prec_dev(job, job->precision, C, H, nbf5, J_MO, K_MO, H_core);
+}
+
+int donof_jkh_mo(donof_job* job, const double* C, const double* H, int nbf5, double* J_MO,
+                 double* K_MO, double* H_core) {
+    if (!job) return DONOF_ERR_ARG;
+    donof_ctx* ctx = job->ctx;
+    REQUIRE(ctx, nbf5 > 0 && nbf5 <= job->nbf, "invalid nbf5");
+    REQUIRE(ctx, C && H && J_MO && K_MO && H_core, "null array argument");
+    DONOF_CHECK(use_device(ctx));
+    const size_t nbf = job->nbf, nn = nbf * nbf, n55 = (size_t)nbf5 * nbf5;
+    DONOF_CHECK(job->io.ensure(ctx, Stager::bytes(nn) * 2 + Stager::bytes(n55) * 2 + Stager::bytes(nbf5)));
+    Stager sg{ctx, ctx->stream, job->io.as<char>()};
+    const double* dC = sg.put(C, nn);
+    const double* dH = sg.put(H, nn);
+    double* dJ = sg.put(nullptr, n55);
+    double* dK = sg.put(nullptr, n55);
+    double* dh = sg.put(nullptr, nbf5);
+    DONOF_CUDA(ctx, cudaGetLastError());
+    DONOF_CHECK(donof_jkh_mo_dev(job, dC, dH, nbf5, dJ, dK, dh));
+    DONOF_CUDA(ctx, cudaMemcpyAsync(J_MO, dJ, n55 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    DONOF_CUDA(ctx, cudaMemcpyAsync(K_MO, dK, n55 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    DONOF_CUDA(ctx, cudaMemcpyAsync(H_core, dh, nbf5 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    DONOF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return DONOF_OK;
+}
+
+int donof_rotate_dev(donof_ctx* ctx, const double* y, int nbf, int nbf5, const double* C,
+                     double* C_new) {
+    if (!ctx) return DONOF_ERR_ARG;
+    REQUIRE(ctx, nbf > 0 && nbf5 > 0 && nbf5 <= nbf, "invalid sizes");
+    REQUIRE(ctx, y && C && C_new, "null array argument");
+    REQUIRE(ctx, C != C_new, "C_new must not alias C");
+    DONOF_CHECK(use_device(ctx));
+    return rotate_f64(ctx, ctx->stream, y, nbf, nbf5, C, C_new);
+}
+
+int donof_rotate(donof_ctx* ctx, const double* y, int nbf, int nbf5, const double* C, double* C_new) {
+    if (!ctx) return DONOF_ERR_ARG;
+    REQUIRE(ctx, nbf > 0 && nbf5 > 0 && nbf5 <= nbf, "invalid sizes");
+    REQUIRE(ctx, y && C && C_new, "null array argument");
+    DONOF_CHECK(use_device(ctx));
+    const size_t nn = (size_t)nbf * nbf, nvar = (size_t)nvar_of(nbf, nbf5);
+    DONOF_CHECK(ctx->stage_in.ensure(ctx, Stager::bytes(nvar) + Stager::bytes(nn) * 2));
+    Stager sg{ctx, ctx->stream, ctx->stage_in.as<char>()};
+    const double* dy = sg.put(y, nvar);
+    const double* dC = sg.put(C, nn);
+    double* dCn = sg.put(nullptr, nn);
+    DONOF_CUDA(ctx, cudaGetLastError());
+    DONOF_CHECK(rotate_f64(ctx, ctx->stream, dy, nbf, nbf5, dC, dCn));
+    DONOF_CUDA(ctx, cudaMemcpyAsync(C_new, dCn, nn * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    DONOF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return DONOF_OK;
+}
+
+int donof_orbgrad(donof_job* job, const double* y, const double* C, const double* n, const double* H,
+                  const double* cj12, const double* ck12, int nbf5, int nalpha, int nbeta,
+                  double* grad) {
+    if (!job) return DONOF_ERR_ARG;
+    donof_ctx* ctx = job->ctx;
+    DONOF_CHECK(check_sizes(ctx, job->nbf, nbf5, nalpha, nbeta));
+    REQUIRE(ctx, C && n && H && cj12 && ck12 && grad, "null array argument");
+    DONOF_CHECK(use_device(ctx));
+    const size_t nbf = job->nbf, nn = nbf * nbf, n55 = (size_t)nbf5 * nbf5;
+    const size_t nvar = (size_t)nvar_of((int)nbf, nbf5);
+    const size_t need = Stager::bytes(nvar) * 2 + Stager::bytes(nn) * 4 + Stager::bytes(nbf5) +
+                        Stager::bytes(n55) * 2 + Stager::bytes(nbf * nbf5);
+    DONOF_CHECK(job->io.ensure(ctx, need));
+    Stager sg{ctx, ctx->stream, job->io.as<char>()};
+    const double* dy = sg.put(y, nvar);
+    const double* dC = sg.put(C, nn);
+    const double* dH = sg.put(H, nn);
+    const double* dn = sg.put(n, nbf5);
+    const double* dcj = sg.put(cj12, n55);
+    const double* dck = sg.put(ck12, n55);
+    double* dCr = sg.put(nullptr, nn);
+    double* del = sg.put(nullptr, nn);
+    double* dHm = sg.put(nullptr, nbf * nbf5);
+    double* dg = sg.put(nullptr, nvar);
+    DONOF_CUDA(ctx, cudaGetLastError());
+    const double* Cuse = dC;
+    if (y != nullptr) {
+        DONOF_CHECK(rotate_f64(ctx, ctx->stream, dy, (int)nbf, nbf5, dC, dCr));
+        Cuse = dCr;
+    }
+    DONOF_CHECK(donof_lagrange2_dev(job, Cuse, dn, dH, dcj, dck, nbf5, nalpha, nbeta, del, dHm, nullptr));
+    DONOF_CHECK(pack_grad(ctx, ctx->stream, del, (int)nbf, nbf5, dg, nullptr));
+    DONOF_CUDA(ctx, cudaMemcpyAsync(grad, dg, nvar * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    DONOF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return DONOF_OK;
+}
+
+int donof_orbopt(donof_job* job, int method, const double* n, const double* cj12, const double* ck12,
+                 const double* H, int nbf5, int nalpha, int nbeta, double* alpha, int* maxloop,
+                 double threshgorb, double* C_inout, double* E, int* nit, int* success) {
+    if (!job) return DONOF_ERR_ARG;
+    donof_ctx* ctx = job->ctx;
+    DONOF_CHECK(check_sizes(ctx, job->nbf, nbf5, nalpha, nbeta));
+    REQUIRE(ctx, n && cj12 && ck12 && H && C_inout && alpha && maxloop && E && nit && success,
+            "null argument");
+    REQUIRE(ctx, method >= DONOF_ORB_ADAM && method <= DONOF_ORB_DEMON, "unknown optimiser");
+    REQUIRE(ctx, *maxloop >= 1, "maxloop must be >= 1");
+    DONOF_CHECK(use_device(ctx));
+    const size_t nbf = job->nbf, nn = nbf * nbf, n55 = (size_t)nbf5 * nbf5;
+    DONOF_CHECK(job->io.ensure(ctx, Stager::bytes(nn) * 2 + Stager::bytes(nbf5) + Stager::bytes(n55) * 2));
+    Stager sg{ctx, ctx->stream, job->io.as<char>()};
+    double* dC = sg.put(C_inout, nn);
+    const double* dH = sg.put(H, nn);
+    const double* dn = sg.put(n, nbf5);
+    const double* dcj = sg.put(cj12, n55);
+    const double* dck = sg.put(ck12, n55);
+    DONOF_CUDA(ctx, cudaGetLastError());
+    DONOF_CHECK(orbopt_run(job, method, dn, dcj, dck, dH, nbf5, nalpha, nbeta, alpha, maxloop, threshgorb,
+                           dC, E, nit, success, job->precision));
+    DONOF_CUDA(ctx, cudaMemcpyAsync(C_inout, dC, nn * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    DONOF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return DONOF_OK;
+}
+
+int donof_orbopt_dev(donof_job* job, int method, const double* n, const double* cj12, const double* ck12,
+                     const double* H, int nbf5, int nalpha, int nbeta, double* alpha, int* maxloop,
+                     double threshgorb, double* C_inout, double* E, int* nit, int* success) {
+    if (!job) return DONOF_ERR_ARG;
+    donof_ctx* ctx = job->ctx;
+    DONOF_CHECK(check_sizes(ctx, job->nbf, nbf5, nalpha, nbeta));
+    REQUIRE(ctx, n && cj12 && ck12 && H && C_inout && alpha && maxloop && E && nit && success,
+            "null argument");
+    REQUIRE(ctx, method >= DONOF_ORB_ADAM && method <= DONOF_ORB_DEMON, "unknown optimiser");
+    REQUIRE(ctx, *maxloop >= 1, "maxloop must be >= 1");
+    DONOF_CHECK(use_device(ctx));
+    return orbopt_run(job, method, n, cj12, ck12, H, nbf5, nalpha, nbeta, alpha, maxloop, threshgorb, C_inout,
+                      E, nit, success, job->precision);
+}
+
+}  // extern "C"

@@ -1,0 +1,75 @@
+// Shared definitions for libdonofb200: status codes, context and job objects.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string>
+
+#include "../../include/donof_b200.h"
+
+namespace donof {
+
+// Count of kernel launches made by the library (diagnostics; see
+// donof_launch_count).  Every launch site calls count_launch().
+void count_launch();
+
+// Last error text is kept per context (and in a thread-local fallback for
+// calls that fail before a context exists).
+void set_error(donof_ctx* ctx, const char* fmt, ...);
+
+#define DONOF_CUDA(ctx, call)                                                    \
+    do {                                                                         \
+        cudaError_t _e = (call);                                                 \
+        if (_e != cudaSuccess) {                                                 \
+            ::donof::set_error((ctx), "%s:%d %s: %s", __FILE__, __LINE__, #call, \
+                               cudaGetErrorString(_e));                          \
+            return (_e == cudaErrorMemoryAllocation) ? DONOF_ERR_OOM             \
+                                                     : DONOF_ERR_CUDA;           \
+        }                                                                        \
+    } while (0)
+
+#define DONOF_CHECK(x)                 \
+    do {                               \
+        int _s = (x);                  \
+        if (_s != DONOF_OK) return _s; \
+    } while (0)
+
+// A device buffer that grows on demand (never shrinks until freed).
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    int ensure(donof_ctx* ctx, size_t want);
+    void release();
+    template <class T>
+    T* as() const { return static_cast<T*>(ptr); }
+};
+
+}  // namespace donof
+
+struct donof_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::string last_error;
+    int sm_count = 148;
+    // host-pointer staging (device side) shared by the host-buffer entry points
+    donof::DevBuf stage_in, stage_out;
+    // scratch for the rotation (exp of the generator)
+    donof::DevBuf rot;
+};
+
+struct donof_job {
+    donof_ctx* ctx = nullptr;
+    int nbf = 0, naux = 0, precision = DONOF_PREC_FP64;
+    const double* b = nullptr;  // device [m + nbf*n + nbf*nbf*l]
+    bool own_b = false;
+    const float* b32 = nullptr;  // FP32 copy for the mixed-precision form
+    bool own_b32 = false;
+    // per-call scratch, sized for the largest nbf5 seen
+    donof::DevBuf tmp, bpq, W, part, small;
+    // device-resident orbital-optimiser state
+    donof::DevBuf orb;
+    // host-API staging
+    donof::DevBuf io;
+};

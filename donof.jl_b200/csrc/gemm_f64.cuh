@@ -1,0 +1,262 @@
+// FP64 tensor-core GEMM for sm_100a (DMMA, mma.sync m16n8k4 .f64).
+//
+// tcgen05.mma has no f64 kind, so the plain FP64 form of the hot path runs on
+// the FP64 MMA pipe through warp-level mma.sync.  The kernel is a strided,
+// batched, optionally split-K GEMM
+//     C_z(i,j) = alpha * sum_k A_z(i,k) B_z(k,j) + beta * C_z(i,j)
+// with either operand K-contiguous or M/N-contiguous, so every contraction of
+// the path (three-index transforms, the Lagrangian GEMM, the small C^T X
+// products, the exponential of the rotation generator) uses the same kernel
+// without transposing copies in HBM.
+//
+// Operand addressing (0-based):
+//   A(i,k) = AK ? A[i*lda + k] : A[i + k*lda]
+//   B(k,j) = BK ? B[k + j*ldb] : B[k*ldb + j]
+//   C(i,j) = C[i + j*ldc]                  (column-major output)
+// Batch z = blockIdx.z / splits adds z*stride{A,B,C}; split s = blockIdx.z %
+// splits covers K range [s*kchunk, min(K, (s+1)*kchunk)) and, when splits > 1,
+// writes its partial result to C + s*strideSplit (beta is then ignored).
+//
+// Staging: a STAGES-deep cp.async ring (16-byte copies when the operand is
+// 16-byte aligned with even strides, 8-byte otherwise), zero-filled outside
+// the matrix; shared-memory rows are padded so the fragment reads of a warp
+// hit every bank pair exactly twice (the minimum for 256 bytes).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace donof {
+
+struct GemmF64Args {
+    int M, N, K;
+    const double* A;
+    long long lda, strideA;
+    const double* B;
+    long long ldb, strideB;
+    double* C;
+    long long ldc, strideC;
+    double alpha, beta;
+    int batch;
+    int splits;
+    int kchunk;
+    long long strideSplit;
+    // Optional device-side gates, read at kernel start (so that data-dependent
+    // control flow needs no host round trip and survives graph capture):
+    //   skip when skip_le != nullptr and *skip_le <= skip_level
+    //   skip when skip_nz != nullptr and *skip_nz != 0
+    const int* skip_le;
+    int skip_level;
+    const int* skip_nz;
+    // Optional indirect B operand: when B_ptr != nullptr, B = *B_ptr.
+    const double* const* B_ptr;
+};
+
+namespace gemm_detail {
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* dst, const void* src, bool valid) {
+    const uint32_t d = smem_u32(dst);
+    const int sz = valid ? BYTES : 0;  // src-size 0 zero-fills the destination
+    if constexpr (BYTES == 16) {
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(sz));
+    } else {
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(sz));
+    }
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+__device__ __forceinline__ void mma_f64_16x8x4(double (&c)[4], double a0, double a1, double b0) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, "
+        "{%0,%1,%2,%3};\n"
+        : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+        : "d"(a0), "d"(a1), "d"(b0));
+}
+
+}  // namespace gemm_detail
+
+template <int BM, int BN, int BK, int WARPS_M, int WARPS_N, int STAGES, bool AK, bool BKM, bool VEC>
+struct GemmF64Cfg {
+    static constexpr int THREADS = 32 * WARPS_M * WARPS_N;
+    static constexpr int WTM = BM / WARPS_M;  // warp tile rows
+    static constexpr int WTN = BN / WARPS_N;  // warp tile cols
+    static constexpr int MI = WTM / 16;
+    static constexpr int NI = WTN / 8;
+    // padded shared-memory strides (in doubles)
+    static constexpr int SA = AK ? (BK + 4) : (BM + 8);
+    static constexpr int SB = BKM ? (BK + 4) : (BN + 8);
+    static constexpr int A_ELEMS = AK ? BM * SA : BK * SA;
+    static constexpr int B_ELEMS = BKM ? BN * SB : BK * SB;
+    static constexpr int STAGE_ELEMS = A_ELEMS + B_ELEMS;
+    static constexpr size_t SMEM_BYTES = sizeof(double) * (size_t)STAGES * STAGE_ELEMS;
+    static constexpr int VW = VEC ? 2 : 1;  // doubles per copy
+    static_assert(WTM % 16 == 0 && WTN % 8 == 0, "warp tile must be a multiple of 16x8");
+    static_assert(BK % 4 == 0, "BK must be a multiple of 4");
+};
+
+template <int BM, int BN, int BK, int WARPS_M, int WARPS_N, int STAGES, bool AK, bool BKM, bool VEC>
+__global__ void __launch_bounds__(32 * WARPS_M * WARPS_N)
+gemm_f64_kernel(const GemmF64Args p) {
+    using Cfg = GemmF64Cfg<BM, BN, BK, WARPS_M, WARPS_N, STAGES, AK, BKM, VEC>;
+    extern __shared__ __align__(16) double smem[];
+
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const int wm = warp % WARPS_M;
+    const int wn = warp / WARPS_M;
+    const int g = lane >> 2;  // groupID
+    const int t = lane & 3;   // threadID_in_group
+
+    const int z = blockIdx.z / p.splits;
+    const int split = blockIdx.z % p.splits;
+    const int m0 = blockIdx.x * BM;
+    const int n0 = blockIdx.y * BN;
+    const int kbeg = split * p.kchunk;
+    const int kend = min(p.K, kbeg + p.kchunk);
+    const double* __restrict__ A = p.A + (long long)z * p.strideA;
+    const double* __restrict__ B = (p.B_ptr != nullptr ? *p.B_ptr : p.B) + (long long)z * p.strideB;
+    double* __restrict__ Cout = p.C + (long long)z * p.strideC +
+                                (p.splits > 1 ? (long long)split * p.strideSplit : 0LL);
+
+    if (p.skip_le != nullptr && *p.skip_le <= p.skip_level) return;
+    if (p.skip_nz != nullptr && *p.skip_nz != 0) return;
+
+    auto As = [&](int s) { return smem + (size_t)s * Cfg::STAGE_ELEMS; };
+    auto Bs = [&](int s) { return smem + (size_t)s * Cfg::STAGE_ELEMS + Cfg::A_ELEMS; };
+
+    auto load_tile = [&](int stage, int k0) {
+        double* as = As(stage);
+        double* bs = Bs(stage);
+        // ---- A tile: BM x BK
+        if constexpr (AK) {
+            constexpr int CPR = BK / Cfg::VW;  // copies per row
+            for (int c = tid; c < BM * CPR; c += Cfg::THREADS) {
+                const int i = c / CPR, kk = (c % CPR) * Cfg::VW;
+                const int gi = m0 + i, gk = k0 + kk;
+                const bool ok = (gi < p.M) && (gk < kend);
+                const double* src = ok ? (A + (long long)gi * p.lda + gk) : A;
+                gemm_detail::cp_async<8 * Cfg::VW>(as + i * Cfg::SA + kk, src, ok);
+            }
+        } else {
+            constexpr int CPR = BM / Cfg::VW;
+            for (int c = tid; c < BK * CPR; c += Cfg::THREADS) {
+                const int kk = c / CPR, i = (c % CPR) * Cfg::VW;
+                const int gi = m0 + i, gk = k0 + kk;
+                const bool ok = (gi < p.M) && (gk < kend);
+                const double* src = ok ? (A + gi + (long long)gk * p.lda) : A;
+                gemm_detail::cp_async<8 * Cfg::VW>(as + kk * Cfg::SA + i, src, ok);
+            }
+        }
+        // ---- B tile: BK x BN
+        if constexpr (BKM) {
+            constexpr int CPR = BK / Cfg::VW;
+            for (int c = tid; c < BN * CPR; c += Cfg::THREADS) {
+                const int j = c / CPR, kk = (c % CPR) * Cfg::VW;
+                const int gj = n0 + j, gk = k0 + kk;
+                const bool ok = (gj < p.N) && (gk < kend);
+                const double* src = ok ? (B + gk + (long long)gj * p.ldb) : B;
+                gemm_detail::cp_async<8 * Cfg::VW>(bs + j * Cfg::SB + kk, src, ok);
+            }
+        } else {
+            constexpr int CPR = BN / Cfg::VW;
+            for (int c = tid; c < BK * CPR; c += Cfg::THREADS) {
+                const int kk = c / CPR, j = (c % CPR) * Cfg::VW;
+                const int gj = n0 + j, gk = k0 + kk;
+                const bool ok = (gj < p.N) && (gk < kend);
+                const double* src = ok ? (B + (long long)gk * p.ldb + gj) : B;
+                gemm_detail::cp_async<8 * Cfg::VW>(bs + kk * Cfg::SB + j, src, ok);
+            }
+        }
+    };
+
+    double acc[Cfg::MI][Cfg::NI][4];
+#pragma unroll
+    for (int a = 0; a < Cfg::MI; ++a)
+#pragma unroll
+        for (int b = 0; b < Cfg::NI; ++b)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) acc[a][b][e] = 0.0;
+
+    const int nk = (kend > kbeg) ? (kend - kbeg + BK - 1) / BK : 0;
+
+#pragma unroll
+    for (int s = 0; s < STAGES - 1; ++s) {
+        if (s < nk) load_tile(s, kbeg + s * BK);
+        gemm_detail::cp_async_commit();
+    }
+
+    const int wrow = wm * Cfg::WTM;
+    const int wcol = wn * Cfg::WTN;
+
+    for (int kt = 0; kt < nk; ++kt) {
+        gemm_detail::cp_async_wait<STAGES - 2>();
+        __syncthreads();
+        {
+            const int nt = kt + STAGES - 1;
+            if (nt < nk) load_tile(nt % STAGES, kbeg + nt * BK);
+            gemm_detail::cp_async_commit();
+        }
+        const double* as = As(kt % STAGES);
+        const double* bs = Bs(kt % STAGES);
+#pragma unroll
+        for (int kk = 0; kk < BK; kk += 4) {
+            double af[Cfg::MI][2];
+            double bf[Cfg::NI];
+#pragma unroll
+            for (int a = 0; a < Cfg::MI; ++a) {
+                const int r = wrow + a * 16 + g;
+                if constexpr (AK) {
+                    af[a][0] = as[r * Cfg::SA + kk + t];
+                    af[a][1] = as[(r + 8) * Cfg::SA + kk + t];
+                } else {
+                    af[a][0] = as[(kk + t) * Cfg::SA + r];
+                    af[a][1] = as[(kk + t) * Cfg::SA + r + 8];
+                }
+            }
+#pragma unroll
+            for (int b = 0; b < Cfg::NI; ++b) {
+                const int cidx = wcol + b * 8 + g;
+                if constexpr (BKM) {
+                    bf[b] = bs[cidx * Cfg::SB + kk + t];
+                } else {
+                    bf[b] = bs[(kk + t) * Cfg::SB + cidx];
+                }
+            }
+#pragma unroll
+            for (int a = 0; a < Cfg::MI; ++a)
+#pragma unroll
+                for (int b = 0; b < Cfg::NI; ++b) gemm_detail::mma_f64_16x8x4(acc[a][b], af[a][0], af[a][1], bf[b]);
+        }
+    }
+    gemm_detail::cp_async_wait<0>();
+
+    // ---- epilogue
+    const bool use_beta = (p.splits == 1) && (p.beta != 0.0);
+#pragma unroll
+    for (int a = 0; a < Cfg::MI; ++a) {
+#pragma unroll
+        for (int b = 0; b < Cfg::NI; ++b) {
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int i = m0 + wrow + a * 16 + g + ((e >= 2) ? 8 : 0);
+                const int j = n0 + wcol + b * 8 + 2 * t + (e & 1);
+                if (i < p.M && j < p.N) {
+                    double* dst = Cout + i + (long long)j * p.ldc;
+                    double v = p.alpha * acc[a][b][e];
+                    if (use_beta) v += p.beta * (*dst);
+                    *dst = v;
+                }
+            }
+        }
+    }
+}
+
+}  // namespace donof

@@ -1,0 +1,248 @@
+// Plain FP64 form of the RI hot path: compute_Lagrange2 and JKH_MO.
+//
+// Restructured contraction (exact in exact arithmetic):
+//   T1   tmp_l  = B_l C5                  (per aux index l; nbf x nbf5)
+//   T2   b_pq^l = C5^T tmp_l              (nbf5 x nbf5)
+//   W[q,l,b]    = delta_qb (n'_b d_b^l + sum_q' cj12[b,q'] d_q'^l) - ck12[b,q] b_bq^l
+//                 with d_q^l = b_qq^l and n'_b = n_b on the beta/alpha-virtual
+//                 blocks (src/utils.jl:42-47), 0 elsewhere
+//   Y[m,b]      = sum_{q,l} tmp_l[m,q] W[q,l,b]          (one GEMM, K = nbf5*naux)
+//   elag[:, :nbf5] = C^T Y + n_b H_mat[:, b]
+// which equals src/utils.jl:17-55 term by term: every elag term there is
+// sum_k b_MO[a,.,k] X[.,k,b] with b_MO = C^T tmp, so C^T factors out and the
+// full nbf x nbf second transform of the reference is never formed.
+// JKH_MO (src/integrals.jl:144-172) reuses T1/T2: J = D D^T with D[p,l] = d_p^l
+// and K = sum_l (b_pq^l)^2.
+#include <math.h>
+
+#include "kernels.cuh"
+
+namespace donof {
+
+namespace {
+
+// W builder: one CTA per aux index l, 32x32 tiles transposed through shared
+// memory so that the reads of b_pq^l / ck12 ([b + nbf5*q]) and the writes of
+// W ([q + nbf5*l + Kt*b]) are both coalesced.
+__global__ void build_w_kernel(const double* __restrict__ bpq, const double* __restrict__ n,
+                               const double* __restrict__ cj12, const double* __restrict__ ck12,
+                               int nbf5, int naux, int nalpha, int nbeta,
+                               double* __restrict__ W) {
+    extern __shared__ double sh[];
+    double* d = sh;             // nbf5
+    double* tv = sh + nbf5;     // nbf5
+    __shared__ double tb[32][33];
+    __shared__ double tk[32][33];
+    const int l = blockIdx.x;
+    const long long n55 = (long long)nbf5 * nbf5;
+    const double* B = bpq + n55 * l;
+    const long long Kt = (long long)nbf5 * naux;
+    for (int q = threadIdx.x; q < nbf5; q += blockDim.x) d[q] = B[(long long)q * (nbf5 + 1)];
+    __syncthreads();
+    for (int b = threadIdx.x; b < nbf5; b += blockDim.x) {
+        double s = 0.0;
+        for (int q = 0; q < nbf5; ++q) s += cj12[b + (long long)nbf5 * q] * d[q];
+        const bool dj = (nbeta > 0) && (b < nbeta || b >= nalpha);
+        tv[b] = (dj ? n[b] * d[b] : 0.0) + s;
+    }
+    __syncthreads();
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x (blockDim/32)
+    const int rows = blockDim.x >> 5;
+    const int nt = (nbf5 + 31) / 32;
+    for (int tile = 0; tile < nt * nt; ++tile) {
+        const int b0 = (tile % nt) * 32, q0 = (tile / nt) * 32;
+        for (int r = ty; r < 32; r += rows) {
+            const int b = b0 + tx, q = q0 + r;
+            double vb = 0.0, vk = 0.0;
+            if (b < nbf5 && q < nbf5) {
+                vb = B[b + (long long)nbf5 * q];
+                vk = ck12[b + (long long)nbf5 * q];
+            }
+            tb[r][tx] = vb;  // [q - q0][b - b0]
+            tk[r][tx] = vk;
+        }
+        __syncthreads();
+        for (int r = ty; r < 32; r += rows) {
+            const int q = q0 + tx, b = b0 + r;
+            if (b < nbf5 && q < nbf5) {
+                double v = -tk[tx][r] * tb[tx][r];
+                if (q == b) v += tv[b];
+                W[q + (long long)nbf5 * l + Kt * b] = v;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// elag[a, b] = n_b H_mat[a, b] for b < nbf5 (the 2ndH/dy_ab term,
+// src/utils.jl:39), columns >= nbf5 set to zero.
+__global__ void elag_init_kernel(const double* __restrict__ Hmat, const double* __restrict__ n,
+                                 int nbf, int nbf5, double* __restrict__ elag) {
+    const long long total = (long long)nbf * nbf;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int b = (int)(i / nbf);
+        elag[i] = (b < nbf5) ? n[b] * Hmat[i] : 0.0;
+    }
+}
+
+// E_elec = sum_{i<nbf5} elag[i,i] + sum_i n_i H_mat[i,i]   (src/utils.jl:216-227)
+__global__ void e_elec_kernel(const double* __restrict__ elag, const double* __restrict__ Hmat,
+                              const double* __restrict__ n, int nbf, int nbf5, double* E) {
+    __shared__ double red[32];
+    double s = 0.0;
+    for (int i = threadIdx.x; i < nbf5; i += blockDim.x)
+        s += elag[i + (long long)nbf * i] + n[i] * Hmat[i + (long long)nbf * i];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        s = (threadIdx.x < (blockDim.x >> 5)) ? red[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (threadIdx.x == 0) *E = s;
+    }
+}
+
+// J/K partial sums over a chunk of aux indices; thread per (p, q).
+__global__ void jk_partial_kernel(const double* __restrict__ bpq, int nbf5, int naux, int lchunk,
+                                  double* __restrict__ part) {
+    const long long n55 = (long long)nbf5 * nbf5;
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const int c = blockIdx.y;
+    if (idx >= n55) return;
+    const int p = (int)(idx % nbf5), q = (int)(idx / nbf5);
+    const int l0 = c * lchunk, l1 = min(naux, l0 + lchunk);
+    double sj = 0.0, sk = 0.0;
+    for (int l = l0; l < l1; ++l) {
+        const double* B = bpq + n55 * l;
+        const double v = B[idx];
+        sj += B[(long long)p * (nbf5 + 1)] * B[(long long)q * (nbf5 + 1)];
+        sk += v * v;
+    }
+    part[(long long)c * 2 * n55 + idx] = sj;
+    part[(long long)c * 2 * n55 + n55 + idx] = sk;
+}
+
+// H_core[i] = sum_m C[m,i] (H C5)[m,i]; one warp per i.
+__global__ void hcore_kernel(const double* __restrict__ C, const double* __restrict__ HC, int nbf,
+                             int nbf5, double* __restrict__ Hcore) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= nbf5) return;
+    double s = 0.0;
+    for (int m = lane; m < nbf; m += 32) s += C[m + (long long)nbf * warp] * HC[m + (long long)nbf * warp];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) Hcore[warp] = s;
+}
+
+int grid_for(long long total, int threads, int sm) {
+    long long b = (total + threads - 1) / threads;
+    if (b > 8LL * sm) b = 8LL * sm;
+    return (int)(b < 1 ? 1 : b);
+}
+
+}  // namespace
+
+// T1 + T2 into the job scratch: tmp (nbf x nbf5 x naux) and bpq (nbf5^2 x naux).
+int transforms_f64(donof_job* job, cudaStream_t st, const double* C, int nbf5) {
+    donof_ctx* ctx = job->ctx;
+    const int nbf = job->nbf, naux = job->naux;
+    DONOF_CHECK(job->tmp.ensure(ctx, sizeof(double) * (size_t)nbf * nbf5 * naux));
+    DONOF_CHECK(job->bpq.ensure(ctx, sizeof(double) * (size_t)nbf5 * nbf5 * naux));
+    double* tmp = job->tmp.as<double>();
+    double* bpq = job->bpq.as<double>();
+    // T1: tmp_l(m,q) = sum_n b[m,n,l] C[n,q]; A(i=m,k=n) = b[m + nbf*n] (M-contiguous)
+    {
+        GemmF64Args p{};
+        p.M = nbf; p.N = nbf5; p.K = nbf;
+        p.A = job->b; p.lda = nbf; p.strideA = (long long)nbf * nbf;
+        p.B = C; p.ldb = nbf; p.strideB = 0;
+        p.C = tmp; p.ldc = nbf; p.strideC = (long long)nbf * nbf5;
+        p.alpha = 1.0; p.beta = 0.0; p.batch = naux; p.splits = 1;
+        DONOF_CHECK(gemm_f64(ctx, st, false, true, p, nbf >= 128 ? GemmTile::Large : GemmTile::Small));
+    }
+    // T2: bpq_l(p,q) = sum_m C[m,p] tmp_l[m,q]
+    {
+        GemmF64Args p{};
+        p.M = nbf5; p.N = nbf5; p.K = nbf;
+        p.A = C; p.lda = nbf; p.strideA = 0;
+        p.B = tmp; p.ldb = nbf; p.strideB = (long long)nbf * nbf5;
+        p.C = bpq; p.ldc = nbf5; p.strideC = (long long)nbf5 * nbf5;
+        p.alpha = 1.0; p.beta = 0.0; p.batch = naux; p.splits = 1;
+        DONOF_CHECK(gemm_f64(ctx, st, true, true, p, nbf5 > 64 ? GemmTile::Large : GemmTile::Small));
+    }
+    return DONOF_OK;
+}
+
+int lagrange2_f64(donof_job* job, cudaStream_t st, const double* C, const double* n,
+                  const double* H, const double* cj12, const double* ck12, int nbf5, int nalpha,
+                  int nbeta, double* elag, double* Hmat, double* E) {
+    donof_ctx* ctx = job->ctx;
+    const int nbf = job->nbf, naux = job->naux;
+    const long long Kt = (long long)nbf5 * naux;
+    DONOF_CHECK(job->small.ensure(ctx, sizeof(double) * (size_t)nbf * nbf5 * 2));
+    double* HC = job->small.as<double>();
+    double* Y = HC + (size_t)nbf * nbf5;
+
+    // H_mat = C^T (H C5)       (src/utils.jl:17-18)
+    DONOF_CHECK(gemm_f64_auto(ctx, st, false, true, nbf, nbf5, nbf, H, nbf, C, nbf, HC, nbf, 1.0,
+                              0.0, &job->part));
+    DONOF_CHECK(gemm_f64_auto(ctx, st, true, true, nbf, nbf5, nbf, C, nbf, HC, nbf, Hmat, nbf, 1.0,
+                              0.0, &job->part));
+
+    DONOF_CHECK(transforms_f64(job, st, C, nbf5));
+
+    DONOF_CHECK(job->W.ensure(ctx, sizeof(double) * (size_t)Kt * nbf5));
+    double* W = job->W.as<double>();
+    build_w_kernel<<<naux, 256, sizeof(double) * 2 * nbf5, st>>>(job->bpq.as<double>(), n, cj12,
+                                                                 ck12, nbf5, naux, nalpha, nbeta, W); count_launch();
+    DONOF_CUDA(ctx, cudaGetLastError());
+
+    // Y = sum_{q,l} tmp[m, q + nbf5*l] W[q + nbf5*l, b]
+    DONOF_CHECK(gemm_f64_auto(ctx, st, false, true, nbf, nbf5, (int)Kt, job->tmp.as<double>(), nbf,
+                              W, Kt, Y, nbf, 1.0, 0.0, &job->part));
+
+    // elag = n o H_mat (cols < nbf5), 0 elsewhere; then elag[:, :nbf5] += C^T Y
+    elag_init_kernel<<<grid_for((long long)nbf * nbf, 256, ctx->sm_count), 256, 0, st>>>(Hmat, n, nbf,
+                                                                                      nbf5, elag); count_launch();
+    DONOF_CUDA(ctx, cudaGetLastError());
+    DONOF_CHECK(gemm_f64_auto(ctx, st, true, true, nbf, nbf5, nbf, C, nbf, Y, nbf, elag, nbf, 1.0,
+                              1.0, &job->part));
+    if (E != nullptr) {
+        e_elec_kernel<<<1, 256, 0, st>>>(elag, Hmat, n, nbf, nbf5, E); count_launch();
+        DONOF_CUDA(ctx, cudaGetLastError());
+    }
+    return DONOF_OK;
+}
+
+int jkh_mo_f64(donof_job* job, cudaStream_t st, const double* C, const double* H, int nbf5,
+               double* J, double* K, double* Hcore) {
+    donof_ctx* ctx = job->ctx;
+    const int nbf = job->nbf, naux = job->naux;
+    DONOF_CHECK(transforms_f64(job, st, C, nbf5));
+    const long long n55 = (long long)nbf5 * nbf5;
+    // chunk the aux index so that about 2 CTAs per SM are busy
+    const int xblocks = (int)((n55 + 255) / 256);
+    int chunks = (2 * ctx->sm_count + xblocks - 1) / xblocks;
+    if (chunks > naux) chunks = naux;
+    if (chunks < 1) chunks = 1;
+    const int lchunk = (naux + chunks - 1) / chunks;
+    chunks = (naux + lchunk - 1) / lchunk;
+    DONOF_CHECK(job->part.ensure(ctx, sizeof(double) * (size_t)chunks * 2 * n55));
+    double* part = job->part.as<double>();
+    jk_partial_kernel<<<dim3(xblocks, chunks), 256, 0, st>>>(job->bpq.as<double>(), nbf5, naux, lchunk,
+                                                             part); count_launch();
+    DONOF_CUDA(ctx, cudaGetLastError());
+    DONOF_CHECK(splitk_reduce(ctx, st, part, 2 * n55, chunks, n55, J, 0.0));
+    DONOF_CHECK(splitk_reduce(ctx, st, part + n55, 2 * n55, chunks, n55, K, 0.0));
+    // H_core
+    DONOF_CHECK(job->small.ensure(ctx, sizeof(double) * (size_t)nbf * nbf5 * 2));
+    double* HC = job->small.as<double>();
+    DONOF_CHECK(gemm_f64_auto(ctx, st, false, true, nbf, nbf5, nbf, H, nbf, C, nbf, HC, nbf, 1.0,
+                              0.0, nullptr));
+    hcore_kernel<<<(nbf5 * 32 + 255) / 256, 256, 0, st>>>(C, HC, nbf, nbf5, Hcore); count_launch();
+    DONOF_CUDA(ctx, cudaGetLastError());
+    return DONOF_OK;
+}
+
+}  // namespace donof

@@ -1,0 +1,199 @@
+// Orbital optimisers on the device: gradient packing and the AMSGrad-style
+// updates of orbopt_adam / orbopt_adabelief / orbopt_yogi / orbopt_demon
+// (src/minimization.jl:242-630), plus the optimiser loop itself.
+#include <math.h>
+#include <string.h>
+
+#include <vector>
+
+#include "kernels.cuh"
+
+namespace donof {
+
+namespace {
+
+__device__ __forceinline__ long long packed_row_start(int i, int nbf) {
+    return (long long)i * (nbf - 1) - (long long)i * (i - 1) / 2;
+}
+
+// g[k] = 4 elag[i,j] - 4 elag[j,i] for the k-th pair (i < nbf5, j > i),
+// row-wise (src/pnof.jl:1395-1403).  One thread per packed entry; the pair
+// is recovered from k by walking rows (nbf5 <= a few hundred).
+__global__ void pack_grad_kernel(const double* __restrict__ elag, int nbf, int nbf5,
+                                 double* __restrict__ g, unsigned long long* maxabs,
+                                 const int* done) {
+    if (done != nullptr && *done) return;
+    const long long nvar = (long long)nbf5 * nbf - (long long)nbf5 * (nbf5 + 1) / 2;
+    double local = 0.0;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nvar;
+         k += (long long)gridDim.x * blockDim.x) {
+        // row i: largest i with packed_row_start(i) <= k
+        int lo = 0, hi = nbf5 - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (packed_row_start(mid, nbf) <= k) lo = mid; else hi = mid - 1;
+        }
+        const int i = lo;
+        const int j = (int)(k - packed_row_start(i, nbf)) + i + 1;
+        const double v = 4.0 * elag[i + (long long)nbf * j] - 4.0 * elag[j + (long long)nbf * i];
+        g[k] = v;
+        local = fmax(local, fabs(v));
+    }
+    if (maxabs != nullptr) {
+        for (int o = 16; o > 0; o >>= 1) local = fmax(local, __shfl_xor_sync(0xffffffffu, local, o));
+        if ((threadIdx.x & 31) == 0) atomicMax(maxabs, (unsigned long long)__double_as_longlong(local));
+    }
+}
+
+struct UpdCoef {
+    double beta1, beta2, bc1, bc2, alpha;  // bc = 1 - beta^i
+};
+
+// AMSGrad-style update shared by the four methods; `method` picks the second
+// moment rule (src/minimization.jl:310-316, 406-411, 503-508, 598-603).
+__global__ void update_kernel(int method, long long nvar, const double* __restrict__ g,
+                              double* __restrict__ m, double* __restrict__ v,
+                              double* __restrict__ vmax, double* __restrict__ y, UpdCoef c,
+                              const int* done) {
+    if (done != nullptr && *done) return;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nvar;
+         k += (long long)gridDim.x * blockDim.x) {
+        const double gk = g[k];
+        const double mk = c.beta1 * m[k] + (1.0 - c.beta1) * gk;
+        double vk;
+        if (method == DONOF_ORB_ADABELIEF) {
+            const double d = gk - mk;
+            vk = c.beta2 * v[k] + (1.0 - c.beta2) * (d * d);
+        } else if (method == DONOF_ORB_YOGI) {
+            const double g2 = gk * gk;
+            const double dv = v[k] - g2;
+            const double sg = (dv > 0.0) ? 1.0 : ((dv < 0.0) ? -1.0 : 0.0);
+            vk = v[k] - (1.0 - c.beta2) * sg * g2;
+        } else {
+            vk = c.beta2 * v[k] + (1.0 - c.beta2) * (gk * gk);
+        }
+        const double mhat = mk / c.bc1;
+        const double vhat = vk / c.bc2;
+        const double vm = fmax(vmax[k], vhat);
+        m[k] = mk;
+        v[k] = vk;
+        vmax[k] = vm;
+        y[k] = -c.alpha * mhat / sqrt(vm + 1e-16);
+    }
+}
+
+int nblocks(long long total, int sm) {
+    long long b = (total + 255) / 256;
+    if (b > 4LL * sm) b = 4LL * sm;
+    return (int)(b < 1 ? 1 : b);
+}
+
+}  // namespace
+
+int pack_grad(donof_ctx* ctx, cudaStream_t st, const double* elag, int nbf, int nbf5, double* g,
+              unsigned long long* maxabs_bits) {
+    const long long nvar = nvar_of(nbf, nbf5);
+    pack_grad_kernel<<<nblocks(nvar, ctx->sm_count), 256, 0, st>>>(elag, nbf, nbf5, g, maxabs_bits,
+                                                                   nullptr); count_launch();
+    DONOF_CUDA(ctx, cudaGetLastError());
+    return DONOF_OK;
+}
+
+// Device-resident optimiser loop; the host only reads one 16-byte status
+// (E, max|g|) per iteration to take the reference's branch decisions.
+int orbopt_run(donof_job* job, int method, const double* n, const double* cj12, const double* ck12,
+               const double* H, int nbf5, int nalpha, int nbeta, double* alpha, int* maxloop,
+               double threshgorb, double* C, double* E_out, int* nit_out, int* success_out,
+               int precision) {
+    donof_ctx* ctx = job->ctx;
+    cudaStream_t st = ctx->stream;
+    const int nbf = job->nbf;
+    const long long nvar = nvar_of(nbf, nbf5);
+    const long long nn = (long long)nbf * nbf;
+    // layout of the optimiser state
+    size_t off = 0;
+    auto take = [&](size_t count) { size_t o = off; off += ((count * sizeof(double) + 255) / 256) * 256; return o; };
+    const size_t o_m = take(nvar), o_v = take(nvar), o_vm = take(nvar), o_y = take(nvar), o_g = take(nvar);
+    const size_t o_C = take(nn), o_Cn = take(nn), o_best = take(nn), o_elag = take(nn);
+    const size_t o_H = take((size_t)nbf * nbf5), o_stat = take(4);
+    DONOF_CHECK(job->orb.ensure(ctx, off));
+    char* base = job->orb.as<char>();
+    double* m = (double*)(base + o_m);
+    double* v = (double*)(base + o_v);
+    double* vm = (double*)(base + o_vm);
+    double* y = (double*)(base + o_y);
+    double* g = (double*)(base + o_g);
+    double* Ccur = (double*)(base + o_C);
+    double* Cnew = (double*)(base + o_Cn);
+    double* Cbest = (double*)(base + o_best);
+    double* elag = (double*)(base + o_elag);
+    double* Hmat = (double*)(base + o_H);
+    double* stat = (double*)(base + o_stat);  // [0] = E, [1] = max|g| bits
+    DONOF_CUDA(ctx, cudaMemsetAsync(base + o_m, 0, o_y - o_m, st));  // m, v, vmax = 0
+
+    auto lagr = [&](const double* Cin) -> int {
+        if (precision == DONOF_PREC_MIXED)
+            return lagrange2_mixed(job, st, Cin, n, H, cj12, ck12, nbf5, nalpha, nbeta, elag, Hmat, stat);
+        return lagrange2_f64(job, st, Cin, n, H, cj12, ck12, nbf5, nalpha, nbeta, elag, Hmat, stat);
+    };
+    auto eval = [&](const double* Cin, double* E, double* gmax) -> int {
+        DONOF_CHECK(lagr(Cin));
+        DONOF_CUDA(ctx, cudaMemsetAsync(stat + 1, 0, sizeof(double), st));
+        DONOF_CHECK(pack_grad(ctx, st, elag, nbf, nbf5, g, (unsigned long long*)(stat + 1)));
+        double h[2];
+        DONOF_CUDA(ctx, cudaMemcpyAsync(h, stat, sizeof(h), cudaMemcpyDeviceToHost, st));
+        DONOF_CUDA(ctx, cudaStreamSynchronize(st));
+        *E = h[0];
+        *gmax = h[1];
+        return DONOF_OK;
+    };
+
+    DONOF_CUDA(ctx, cudaMemcpyAsync(Ccur, C, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st));
+    double E = 0.0, gmax = 0.0;
+    DONOF_CHECK(eval(Ccur, &E, &gmax));
+    double bestE = E;
+    DONOF_CUDA(ctx, cudaMemcpyAsync(Cbest, Ccur, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st));
+
+    const double a = *alpha;
+    double beta1 = (method == DONOF_ORB_DEMON) ? 0.6 : 0.5;
+    const double beta2 = (method == DONOF_ORB_DEMON) ? 0.999 : 0.9;
+    const double binit = beta1;
+    const int loops = *maxloop;
+    bool improved = false, success = false;
+    int nit = 0;
+    for (int i = 1; i <= loops; ++i) {
+        ++nit;
+        if (2.0 * gmax < threshgorb && improved) {
+            success = true;
+            break;
+        }
+        if (method == DONOF_ORB_DEMON) {
+            const double rate = (i - 1.0) / (loops - 1.0);
+            beta1 = binit * (1.0 - rate) / ((1.0 - binit) + binit * (1.0 - rate));
+        }
+        UpdCoef c{beta1, beta2, 1.0 - pow(beta1, i), 1.0 - pow(beta2, i), a};
+        update_kernel<<<nblocks(nvar, ctx->sm_count), 256, 0, st>>>(method, nvar, g, m, v, vm, y, c, nullptr); count_launch();
+        DONOF_CUDA(ctx, cudaGetLastError());
+        DONOF_CHECK(rotate_f64(ctx, st, y, nbf, nbf5, Ccur, Cnew));
+        double* t = Ccur; Ccur = Cnew; Cnew = t;
+        DONOF_CHECK(eval(Ccur, &E, &gmax));
+        if (E < bestE) {
+            bestE = E;
+            DONOF_CUDA(ctx, cudaMemcpyAsync(Cbest, Ccur, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st));
+            improved = true;
+        }
+    }
+    if (!improved) {
+        *alpha = 0.3 * (*alpha);
+        *maxloop = *maxloop + 10;
+    }
+    const bool return_best = (*maxloop < 100);
+    DONOF_CUDA(ctx, cudaMemcpyAsync(C, return_best ? Cbest : Ccur, sizeof(double) * nn,
+                                    cudaMemcpyDeviceToDevice, st));
+    *E_out = return_best ? bestE : E;
+    *nit_out = nit;
+    *success_out = success ? 1 : 0;
+    return DONOF_OK;
+}
+
+}  // namespace donof

@@ -1,0 +1,289 @@
+"""Host-side mirror of DoNOF.jl's GPU plugin interface (ext/DoNOFGPUExt.jl),
+driving libdonofb200 through its C ABI.
+
+Function names, argument order and meaning follow the reference methods they
+replace; arrays are FP64 in Julia (column-major) layout:
+
+  numpy inputs   : Fortran-ordered arrays indexed like Julia, e.g. C[m, p],
+                   b[m, n, l] (any order is accepted and converted).
+  torch inputs   : CUDA tensors holding the same column-major memory, i.e.
+                   with the index order reversed (b as (naux, nbf, nbf)),
+                   see ``to_device`` / ``from_device``.
+
+Every call goes to the CUDA library; there is no CPU code path for the hot
+contractions, and a missing library raises at import of ``_lib``.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from .param import Param
+
+try:  # torch is optional for the host-buffer entry points
+    import torch
+except Exception:  # pragma: no cover
+    torch = None
+
+
+def _ptr(a) -> int:
+    if a is None:
+        return None
+    if torch is not None and isinstance(a, torch.Tensor):
+        if not a.is_cuda or a.dtype != torch.float64 or not a.is_contiguous():
+            raise ValueError("device arrays must be contiguous float64 CUDA tensors")
+        return a.data_ptr()
+    return a.ctypes.data
+
+
+def _f64(a) -> np.ndarray:
+    return np.asfortranarray(np.asarray(a, dtype=np.float64))
+
+
+def to_device(a: np.ndarray, device="cuda"):
+    """Julia-layout numpy array -> CUDA tensor with the same memory order."""
+    a = _f64(a)
+    return torch.from_numpy(np.ascontiguousarray(a.T)).to(device)
+
+
+def from_device(t) -> np.ndarray:
+    """Inverse of ``to_device``."""
+    return np.asfortranarray(t.detach().cpu().numpy().T)
+
+
+class Context:
+    """One libdonofb200 context (device + CUDA stream)."""
+
+    def __init__(self, device: int = 0, torch_stream: bool = True):
+        self.lib = _lib.load()
+        h = ct.c_void_p()
+        _lib.check(self.lib.donof_create(int(device), ct.byref(h)), None)
+        self.handle = h
+        self.device = device
+        if torch_stream and torch is not None and torch.cuda.is_available():
+            # share torch's current stream so torch events time the work
+            self.set_stream(torch.cuda.current_stream(device).cuda_stream)
+
+    def set_stream(self, stream_handle: int) -> None:
+        self.check(self.lib.donof_set_stream(self.handle, ct.c_void_p(stream_handle)))
+
+    def check(self, status: int) -> None:
+        _lib.check(status, self.handle)
+
+    def synchronize(self) -> None:
+        self.check(self.lib.donof_synchronize(self.handle))
+
+    def close(self) -> None:
+        if getattr(self, "handle", None):
+            self.lib.donof_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default_ctx: Optional[Context] = None
+
+
+def default_context() -> Context:
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(0)
+    return _default_ctx
+
+
+class BTensor:
+    """The RI tensor b[m, n, l] resident on the device (a libdonofb200 job);
+    the counterpart of the CuArray that eris_to_gpu returns."""
+
+    def __init__(self, ctx: Context, handle, nbf: int, naux: int, precision: int, keep=None):
+        self.ctx, self.handle, self.nbf, self.naux, self.precision = ctx, handle, nbf, naux, precision
+        self._keep = keep  # keeps an attached device tensor alive
+
+    @property
+    def shape(self):
+        return (self.nbf, self.nbf, self.naux)
+
+    def device_bytes(self) -> int:
+        return int(self.ctx.lib.donof_job_device_bytes(self.handle))
+
+    def free(self) -> None:
+        if self.handle:
+            self.ctx.lib.donof_job_free(self.handle)
+            self.handle = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def _prec(precision) -> int:
+    if precision in ("fp64", _lib.PREC_FP64, None):
+        return _lib.PREC_FP64
+    if precision in ("mixed", _lib.PREC_MIXED):
+        return _lib.PREC_MIXED
+    raise ValueError(f"unknown precision {precision!r}")
+
+
+def eris_to_gpu(b, precision="fp64", ctx: Optional[Context] = None) -> BTensor:
+    """Upload (numpy) or attach (CUDA tensor) the RI tensor b
+    (ext/DoNOFGPUExt.jl:36-50)."""
+    ctx = ctx or default_context()
+    prec = _prec(precision)
+    h = ct.c_void_p()
+    if torch is not None and isinstance(b, torch.Tensor):
+        naux, nbf, nbf2 = b.shape
+        assert nbf == nbf2
+        ctx.check(ctx.lib.donof_b_attach(ctx.handle, ct.c_void_p(_ptr(b)), nbf, naux, prec, ct.byref(h)))
+        return BTensor(ctx, h, nbf, naux, prec, keep=b)
+    b = _f64(b)
+    nbf, nbf2, naux = b.shape
+    assert nbf == nbf2
+    ctx.check(ctx.lib.donof_b_upload(ctx.handle, ct.c_void_p(b.ctypes.data), nbf, naux, prec, ct.byref(h)))
+    return BTensor(ctx, h, nbf, naux, prec)
+
+
+def compute_Lagrange2(C, n, H, b: BTensor, cj12, ck12, nalpha: int, nbeta: int, return_energy=False):
+    """elag, H_mat = compute_Lagrange2(C, n, H, b, cj12, ck12, nalpha, nbeta)
+    (src/utils.jl:1-59; ext/DoNOFGPUExt.jl:150-245).  Host arrays in and out."""
+    C, n, H, cj12, ck12 = _f64(C), _f64(n), _f64(H), _f64(cj12), _f64(ck12)
+    nbf, nbf5 = b.nbf, n.shape[0]
+    elag = np.zeros((nbf, nbf), order="F")
+    Hmat = np.zeros((nbf, nbf5), order="F")
+    E = np.zeros(1)
+    b.ctx.check(b.ctx.lib.donof_lagrange2(b.handle, _ptr(C), _ptr(n), _ptr(H), _ptr(cj12), _ptr(ck12),
+                                          nbf5, int(nalpha), int(nbeta), _ptr(elag), _ptr(Hmat), _ptr(E)))
+    if return_energy:
+        return elag, Hmat, float(E[0])
+    return elag, Hmat
+
+
+def compute_Lagrange2_dev(C, n, H, b: BTensor, cj12, ck12, nalpha: int, nbeta: int, elag, Hmat, E=None,
+                          precision=None):
+    """Device-pointer form: all arrays are CUDA tensors in Julia layout; only
+    enqueues work on the context stream."""
+    prec = b.precision if precision is None else _prec(precision)
+    nbf5 = n.shape[0]
+    b.ctx.check(b.ctx.lib.donof_lagrange2_prec_dev(b.handle, prec, _ptr(C), _ptr(n), _ptr(H), _ptr(cj12),
+                                                   _ptr(ck12), nbf5, int(nalpha), int(nbeta), _ptr(elag),
+                                                   _ptr(Hmat), _ptr(E)))
+
+
+def JKH_MO(C, H, b: BTensor, nbf: int, nbf5: int, nbfaux: int):
+    """J_MO, K_MO, H_core = JKH_MO(C, H, b, nbf, nbf5, nbfaux)
+    (src/integrals.jl:144-172; ext/DoNOFGPUExt.jl:63-94)."""
+    if nbf != b.nbf or nbfaux != b.naux:
+        raise ValueError("nbf/nbfaux do not match the b tensor")
+    C, H = _f64(C), _f64(H)
+    J = np.zeros((nbf5, nbf5), order="F")
+    K = np.zeros((nbf5, nbf5), order="F")
+    Hc = np.zeros(nbf5)
+    b.ctx.check(b.ctx.lib.donof_jkh_mo(b.handle, _ptr(C), _ptr(H), int(nbf5), _ptr(J), _ptr(K), _ptr(Hc)))
+    return J, K, Hc
+
+
+def JKH_MO_dev(C, H, b: BTensor, nbf5: int, J, K, Hcore, precision=None):
+    prec = b.precision if precision is None else _prec(precision)
+    b.ctx.check(b.ctx.lib.donof_jkh_mo_prec_dev(b.handle, prec, _ptr(C), _ptr(H), int(nbf5), _ptr(J), _ptr(K),
+                                                _ptr(Hcore)))
+
+
+def computeJKH_MO(C, H, b: BTensor, p: Param):
+    """src/integrals.jl:131-140 (RI branch); ext/DoNOFGPUExt.jl:52-61."""
+    return JKH_MO(C, H, b, p.nbf, p.nbf5, p.nbfaux)
+
+
+def rotate_orbital(y, C, p: Param, ctx: Optional[Context] = None):
+    """C exp(Y(y)) in FP64 (src/utils.jl:499-521; replaces ext/DoNOFGPUExt.jl:355-382)."""
+    ctx = ctx or default_context()
+    y, C = _f64(y), _f64(C)
+    if y.shape[0] != p.nvar:
+        raise ValueError(f"y has {y.shape[0]} entries, nvar = {p.nvar}")
+    Cn = np.zeros_like(C, order="F")
+    ctx.check(ctx.lib.donof_rotate(ctx.handle, _ptr(y), p.nbf, p.nbf5, _ptr(C), _ptr(Cn)))
+    return Cn
+
+
+def rotate_orbital_dev(y, C, Cnew, nbf: int, nbf5: int, ctx: Optional[Context] = None):
+    ctx = ctx or default_context()
+    ctx.check(ctx.lib.donof_rotate_dev(ctx.handle, _ptr(y), nbf, nbf5, _ptr(C), _ptr(Cnew)))
+
+
+def calcorbg(y, n, cj12, ck12, C, H, b: BTensor, p: Param):
+    """Packed orbital gradient at y (src/pnof.jl:1389-1407)."""
+    n, cj12, ck12, C, H = _f64(n), _f64(cj12), _f64(ck12), _f64(C), _f64(H)
+    yv = None if y is None else _f64(y)
+    g = np.zeros(p.nvar)
+    b.ctx.check(b.ctx.lib.donof_orbgrad(b.handle, _ptr(yv), _ptr(C), _ptr(n), _ptr(H), _ptr(cj12), _ptr(ck12),
+                                        p.nbf5, p.nalpha, p.nbeta, _ptr(g)))
+    return g
+
+
+def orbopt(gamma, C, H, b: BTensor, p: Param, method: Optional[str] = None):
+    """One orbital-optimiser call, device resident (src/minimization.jl:242-630).
+    Returns (E, C, nit, success) and updates p.alpha / p.maxloop like the reference."""
+    from . import gnof
+
+    method = method or p.orb_method
+    n, _ = gnof.occupations(gamma, p)
+    cj12, ck12 = gnof.coupling(n, p)
+    Cio = np.array(_f64(C), copy=True, order="F")
+    alpha = ct.c_double(p.alpha)
+    maxloop = ct.c_int(p.maxloop)
+    E = ct.c_double()
+    nit = ct.c_int()
+    ok = ct.c_int()
+    n, cj12, ck12, H = _f64(n), _f64(cj12), _f64(ck12), _f64(H)
+    b.ctx.check(b.ctx.lib.donof_orbopt(b.handle, _lib.ORB_METHODS[method], _ptr(n), _ptr(cj12), _ptr(ck12),
+                                       _ptr(H), p.nbf5, p.nalpha, p.nbeta, ct.byref(alpha), ct.byref(maxloop),
+                                       float(p.threshgorb), _ptr(Cio), ct.byref(E), ct.byref(nit),
+                                       ct.byref(ok)))
+    p.alpha = alpha.value
+    p.maxloop = maxloop.value
+    return E.value, Cio, nit.value, bool(ok.value)
+
+
+def orbopt_dev(method: str, n, cj12, ck12, H, C, b: BTensor, p: Param, alpha: float, maxloop: int,
+               threshgorb: float):
+    """Device-pointer optimiser call: n, cj12, ck12, H, C are CUDA tensors in
+    Julia layout; C is updated in place.  Returns (E, nit, success, alpha, maxloop)."""
+    a, ml = ct.c_double(alpha), ct.c_int(maxloop)
+    E, nit, ok = ct.c_double(), ct.c_int(), ct.c_int()
+    b.ctx.check(b.ctx.lib.donof_orbopt_dev(b.handle, _lib.ORB_METHODS[method], _ptr(n), _ptr(cj12), _ptr(ck12),
+                                           _ptr(H), n.shape[0], p.nalpha, p.nbeta, ct.byref(a), ct.byref(ml),
+                                           float(threshgorb), _ptr(C), ct.byref(E), ct.byref(nit), ct.byref(ok)))
+    return E.value, nit.value, bool(ok.value), a.value, ml.value
+
+
+def transform_dev(C, b: BTensor, nbf5: int, out=None, precision=None):
+    """b_pq^l = C5^T b_l C5 on the device (out: CUDA tensor or None)."""
+    prec = b.precision if precision is None else _prec(precision)
+    b.ctx.check(b.ctx.lib.donof_transform_dev(b.handle, prec, _ptr(C), int(nbf5), _ptr(out)))
+
+
+def launch_count() -> int:
+    return int(_lib.load().donof_launch_count())
+
+
+def orbopt_adam(gamma, C, H, b, p):
+    return orbopt(gamma, C, H, b, p, "ADAM")
+
+
+def orbopt_adabelief(gamma, C, H, b, p):
+    return orbopt(gamma, C, H, b, p, "ADABelief")
+
+
+def orbopt_yogi(gamma, C, H, b, p):
+    return orbopt(gamma, C, H, b, p, "YOGI")
+
+
+def orbopt_demon(gamma, C, H, b, p):
+    return orbopt(gamma, C, H, b, p, "Demon")

@@ -1,0 +1,66 @@
+"""Seeded synthetic inputs with the shapes and value distributions of the
+benchmark workloads (the reference publishes no data set for this path and
+no integral engine or basis data is available, so every workload is
+synthetic):
+
+  b[m,n,l] ~ N(0, 1/sqrt(naux)) symmetrised in (m, n)  -- the RI tensor
+  C        = Q of the QR of a seeded N(0,1) nbf x nbf matrix
+  H        = seeded symmetric N(0,1)/sqrt(nbf) matrix
+  gamma    ~ N(0,1) softmax parameters, pairs then sorted by
+             order_occupations_softmax (which also permutes C)
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import gnof
+from .param import Param
+
+
+@dataclass
+class Workload:
+    p: Param
+    b: np.ndarray      # (nbf, nbf, naux), Fortran order (Julia layout)
+    C: np.ndarray      # (nbf, nbf), Fortran order
+    H: np.ndarray
+    gamma: np.ndarray
+    n: np.ndarray
+    cj12: np.ndarray
+    ck12: np.ndarray
+
+
+def make_b(nbf: int, naux: int, rng: np.random.Generator) -> np.ndarray:
+    # generated as (l, n, m) in C order, i.e. b[m, n, l] in Julia's column-major order
+    raw = rng.standard_normal((naux, nbf, nbf)) * (1.0 / np.sqrt(naux))
+    raw += raw.transpose(0, 2, 1)
+    raw *= 0.5
+    return raw.T  # Fortran-ordered view with shape (nbf, nbf, naux)
+
+
+def synthetic(nbf: int = 256, naux: int = 1024, nbeta: int = 16, ncwo: int = 3, seed: int = 1234,
+              occ_method: str = "Softmax", with_b: bool = True, **param_kw) -> Workload:
+    rng = np.random.default_rng(seed)
+    p = Param(nbf=nbf, nbfaux=naux, nalpha=nbeta, nbeta=nbeta, ncwo=ncwo, occ_method=occ_method, **param_kw)
+    if p.nbf5 > nbf:
+        raise ValueError(f"nbf5 = {p.nbf5} exceeds nbf = {nbf}")
+    b = make_b(nbf, naux, rng) if with_b else None
+    Q, _ = np.linalg.qr(rng.standard_normal((nbf, nbf)))
+    C = np.asfortranarray(Q)
+    A = rng.standard_normal((nbf, nbf))
+    H = np.asfortranarray((A + A.T) * (0.5 / np.sqrt(nbf)))
+    gamma = rng.standard_normal(p.nv)
+    if occ_method == "Softmax":
+        C, gamma = gnof.order_occupations_softmax(C, gamma, p)
+    n, _ = gnof.occupations(gamma, p)
+    cj12, ck12 = gnof.coupling(n, p)
+    return Workload(p, b, C, H, gamma, n, np.asfortranarray(cj12), np.asfortranarray(ck12))
+
+
+# Named workloads (sizes of the molecule-shaped surrogates: nbf, naux, nbeta, ncwo)
+CONFIGS = {
+    "water-ccpvdz-surrogate": dict(nbf=24, naux=116, nbeta=5, ncwo=3),
+    "synthetic-256": dict(nbf=256, naux=1024, nbeta=16, ncwo=3),
+    "n-octane-ccpvdz-surrogate": dict(nbf=202, naux=974, nbeta=33, ncwo=5),
+}

@@ -1,0 +1,171 @@
+/*
+ * libdonofb200 -- C ABI of the B200 (sm_100a) RI hot path for GNOF natural
+ * orbital functional energies.
+ *
+ * The entry points replace the methods that DoNOF.jl's GPU package extension
+ * (ext/DoNOFGPUExt.jl) adds for CuArray arguments; a Julia extension binds
+ * them with ccall (one call per reference method, same argument meaning).
+ *
+ * Conventions
+ *   - Every matrix is FP64, column-major (Julia layout), 0-based indices in the
+ *     descriptions below:  C[m + nbf*p], b[m + nbf*n + nbf*nbf*l],
+ *     H[m + nbf*n], n[p], cj12/ck12[p + nbf5*q], elag[a + nbf*b] (nbf x nbf),
+ *     H_mat[i + nbf*j] (nbf x nbf5), J_MO/K_MO[p + nbf5*q], H_core[p].
+ *   - Entry points without a suffix take HOST pointers, copy inputs to the
+ *     device, run on the context stream and return when the outputs are back
+ *     in host memory (the reference's per-call CuArray(...) / Array(...)).
+ *   - Entry points with the _dev suffix take DEVICE pointers, only enqueue
+ *     work on the context stream and return immediately.
+ *   - Every call returns a status code (DONOF_OK = 0); donof_last_error()
+ *     gives the text of the last failure on that context.
+ *   - One context per host thread; a context owns one CUDA stream.
+ */
+#ifndef DONOF_B200_H
+#define DONOF_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+/* status codes */
+#define DONOF_OK 0
+#define DONOF_ERR_ARG 1       /* invalid argument (size, null pointer, mode) */
+#define DONOF_ERR_CUDA 2      /* CUDA runtime error */
+#define DONOF_ERR_OOM 3       /* device allocation failed */
+#define DONOF_ERR_STATE 4     /* object in the wrong state for this call */
+#define DONOF_ERR_NOT_CONVERGED 5
+
+/* precision of the b tensor held by a job and of the bulk contractions */
+#define DONOF_PREC_FP64 0   /* all contractions in FP64 (plain form) */
+#define DONOF_PREC_MIXED 1  /* tensor-core TF32x3 bulk contractions, FP32 accumulation */
+
+/* orbital optimisers (src/minimization.jl:242-630) */
+#define DONOF_ORB_ADAM 0
+#define DONOF_ORB_ADABELIEF 1
+#define DONOF_ORB_YOGI 2
+#define DONOF_ORB_DEMON 3
+
+typedef struct donof_ctx donof_ctx;
+typedef struct donof_job donof_job;
+
+/* --- context ------------------------------------------------------------ */
+int donof_create(int device, donof_ctx** ctx);
+int donof_destroy(donof_ctx* ctx);
+/* use an existing cudaStream_t (passed as void*) instead of the own stream */
+int donof_set_stream(donof_ctx* ctx, void* stream);
+void* donof_get_stream(donof_ctx* ctx);
+int donof_synchronize(donof_ctx* ctx);
+const char* donof_last_error(const donof_ctx* ctx);
+const char* donof_status_string(int status);
+int donof_version(void);
+
+/* --- the b tensor ---------------------------------------------------------
+ * donof_b_upload replaces eris_to_gpu (ext/DoNOFGPUExt.jl:36-50, called at
+ * src/integrals.jl:59-62): copies the host RI tensor b[m,n,l] (nbf x nbf x
+ * naux, FP64) to the device once per job.  precision = DONOF_PREC_MIXED also
+ * keeps an FP32 copy for the mixed-precision form (the FP64 copy stays, for
+ * refinement steps).
+ * donof_b_attach wraps an existing device buffer without copying (the job
+ * does not own it and it must outlive the job).                            */
+int donof_b_upload(donof_ctx* ctx, const double* b_host, int nbf, int naux, int precision,
+                   donof_job** job);
+int donof_b_attach(donof_ctx* ctx, const double* b_dev, int nbf, int naux, int precision,
+                   donof_job** job);
+int donof_job_free(donof_job* job);
+/* device bytes held by the job (b copies + scratch) */
+size_t donof_job_device_bytes(const donof_job* job);
+
+/* --- compute_Lagrange2, RI method -------------------------------------------
+ * Replaces compute_Lagrange2(C,n,H,b::CuArray{T,3},cj12,ck12,nalpha,nbeta)
+ * (ext/DoNOFGPUExt.jl:150-245); CPU definition src/utils.jl:1-59.
+ * Outputs elag (nbf x nbf; columns >= nbf5 are zero) and H_mat = C^T H C5
+ * (nbf x nbf5).  The job's precision selects the plain FP64 or the mixed form.
+ * E_elec, if not NULL, receives computeE_elec(H_mat, n, elag)
+ * (src/utils.jl:216-227).                                                  */
+int donof_lagrange2(donof_job* job, const double* C, const double* n, const double* H,
+                    const double* cj12, const double* ck12, int nbf5, int nalpha, int nbeta,
+                    double* elag, double* H_mat, double* E_elec);
+int donof_lagrange2_dev(donof_job* job, const double* C, const double* n, const double* H,
+                        const double* cj12, const double* ck12, int nbf5, int nalpha,
+                        int nbeta, double* elag, double* H_mat, double* E_elec);
+/* Same as donof_lagrange2_dev with an explicit precision (overrides the job's;
+ * DONOF_PREC_MIXED needs a job uploaded with DONOF_PREC_MIXED).            */
+int donof_lagrange2_prec_dev(donof_job* job, int precision, const double* C, const double* n,
+                             const double* H, const double* cj12, const double* ck12,
+                             int nbf5, int nalpha, int nbeta, double* elag, double* H_mat,
+                             double* E_elec);
+
+/* --- JKH_MO, RI method ----------------------------------------------------
+ * Replaces computeJKH_MO / JKH_MO(C,H,b::CuArray{T,3},nbf,nbf5,nbfaux)
+ * (ext/DoNOFGPUExt.jl:52-94); CPU definition src/integrals.jl:131-172.
+ * J_MO[p,q] = sum_l b_pp^l b_qq^l, K_MO[p,q] = sum_l (b_pq^l)^2,
+ * H_core[p] = C_p^T H C_p, with b_pq^l = sum_mn C[m,p] b[m,n,l] C[n,q].     */
+int donof_jkh_mo(donof_job* job, const double* C, const double* H, int nbf5, double* J_MO,
+                 double* K_MO, double* H_core);
+int donof_jkh_mo_dev(donof_job* job, const double* C, const double* H, int nbf5, double* J_MO,
+                     double* K_MO, double* H_core);
+int donof_jkh_mo_prec_dev(donof_job* job, int precision, const double* C, const double* H,
+                          int nbf5, double* J_MO, double* K_MO, double* H_core);
+
+/* --- three-index transform ---------------------------------------------------
+ * b_pq^l = sum_mn C[m,p] b[m,n,l] C[n,q] for p, q < nbf5: the b_mnl -> b_pnl ->
+ * b_pql transform of JKH_MO / compute_eris_full (src/integrals.jl:159-160,
+ * 287-288; ext/DoNOFGPUExt.jl:71-72).  b_pq (device, may be NULL) receives
+ * b_pq[p + nbf5*q + nbf5*nbf5*l].                                            */
+int donof_transform_dev(donof_job* job, int precision, const double* C, int nbf5, double* b_pq);
+
+/* --- rotate_orbital ------------------------------------------------------
+ * Replaces rotate_orbital(y,C,p) (ext/DoNOFGPUExt.jl:355-382, which runs in
+ * FP32); CPU definition src/utils.jl:499-521, followed here in FP64:
+ * y (nvar = nbf5*nbf - nbf5*(nbf5+1)/2) is unpacked row-wise over i < nbf5,
+ * j > i into the antisymmetric Y, and C_new = C exp(Y).                      */
+int donof_rotate(donof_ctx* ctx, const double* y, int nbf, int nbf5, const double* C,
+                 double* C_new);
+int donof_rotate_dev(donof_ctx* ctx, const double* y, int nbf, int nbf5, const double* C,
+                     double* C_new);
+
+/* --- calcorbg --------------------------------------------------------------
+ * Orbital gradient at y (src/pnof.jl:1389-1407): C' = rotate_orbital(y, C),
+ * elag = compute_Lagrange2(C', ...), grad = 4 elag - 4 elag^T packed over
+ * i < nbf5, j > i.  y may be NULL for y = 0 (the call at src/energy.jl:188). */
+int donof_orbgrad(donof_job* job, const double* y, const double* C, const double* n,
+                  const double* H, const double* cj12, const double* ck12, int nbf5, int nalpha,
+                  int nbeta, double* grad);
+
+/* --- orbital optimiser -----------------------------------------------------
+ * One call of orbopt_adam / orbopt_adabelief / orbopt_yogi / orbopt_demon
+ * (src/minimization.jl:242-630) with the whole loop resident on the device:
+ * gradient packing, the AMSGrad-style update, rotation, Lagrangian, energy
+ * and best-(E, C) tracking.  C is read from and written back to C_inout.
+ * *alpha and *maxloop are read and updated like p.alpha / p.maxloop (step
+ * back-off when no iteration improved E).                                  */
+int donof_orbopt(donof_job* job, int method, const double* n, const double* cj12,
+                 const double* ck12, const double* H, int nbf5, int nalpha, int nbeta,
+                 double* alpha, int* maxloop, double threshgorb, double* C_inout, double* E,
+                 int* nit, int* success);
+/* Same with n, cj12, ck12, H and C_inout in device memory (C_inout is updated
+ * in place on the context stream; the call returns after the loop ends).     */
+int donof_orbopt_dev(donof_job* job, int method, const double* n, const double* cj12,
+                     const double* ck12, const double* H, int nbf5, int nalpha, int nbeta,
+                     double* alpha, int* maxloop, double threshgorb, double* C_inout, double* E,
+                     int* nit, int* success);
+
+/* --- diagnostics -------------------------------------------------------------
+ * Number of CUDA kernels this library has launched in the process so far.    */
+unsigned long long donof_launch_count(void);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DONOF_B200_H */
