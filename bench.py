@@ -82,7 +82,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
         except Exception:
@@ -92,6 +92,16 @@ class ClockSampler:
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
+
+    def wait_samples(self, k: int, timeout: float = 3.0):
+        """Block until k more samples have arrived (so the sampled window brackets
+        a short timed region on both sides)."""
+        if not self.proc:
+            return
+        want = len(self.lines) + k
+        t0 = time.time()
+        while len(self.lines) < want and time.time() - t0 < timeout:
+            time.sleep(0.02)
 
     def __exit__(self, *a):
         if self.proc:
@@ -265,11 +275,13 @@ def main():
     torch.cuda.synchronize()
     l0 = d.launch_count()
     with ClockSampler(local) as clk:
+        clk.wait_samples(2)
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev0.record()
         E, nit, ok, _, _ = d.orbopt_dev(args.method, tn, tcj, tck, tH, tC, bt, p, 0.01, args.steps, 0.0)
         ev1.record()
         torch.cuda.synchronize()
+        clk.wait_samples(1)
     launches = d.launch_count() - l0
     barrier()
     t = ev0.elapsed_time(ev1) / 1e3
