@@ -15,6 +15,8 @@
 // and K = sum_l (b_pq^l)^2.
 #include <math.h>
 
+#include <mutex>
+
 #include "kernels.cuh"
 
 namespace donof {
@@ -245,4 +247,174 @@ int jkh_mo_f64(donof_job* job, cudaStream_t st, const double* C, const double* H
     return DONOF_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free compute_Lagrange2 (donof_lagrange2_noalloc_dev).
+//
+// Some callers cannot call cudaMalloc at all: a host whose device memory is
+// owned by another runtime's pool (a Julia or PyTorch process that hands this
+// library only the arrays it already holds), code that must not add to a fixed
+// device-memory budget while it serves, or a caller that may not block on the
+// synchronising allocator in the middle of its own stream work.  This variant
+// runs the same FP64 pipeline as lagrange2_f64 but takes every intermediate
+// from one file-scope device array of NOALLOC_SCRATCH_BYTES, which every GPU
+// that loads the library holds until the process exits.  It never calls
+// cudaMalloc, cudaFree or an allocating library routine.
+//
+// The first call on a device looks the array up with cudaGetSymbolAddress
+// (with that device current) and caches the address; make that first call
+// before any stream capture.  Every call shares the one array, so calls that
+// overlap on the GPU (other streams, other host threads) race on it; each
+// call writes every scratch element it later reads, so nothing has to start
+// at zero and the contents left by the previous call are never used.
+// ---------------------------------------------------------------------------
+constexpr size_t NOALLOC_SCRATCH_BYTES = size_t(32) << 20;  // 32 MiB
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+std::mutex g_noalloc_mutex;
+void* g_noalloc_addr[64] = {};
+
+// Device address of g_noalloc_scratch on the current device (set-up once per device).
+int noalloc_scratch(donof_ctx* ctx, double** out) {
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (ctx->device < 0 || ctx->device >= 64) {
+        set_error(ctx, "device index %d out of range for the scratch table", ctx->device);
+        return DONOF_ERR_ARG;
+    }
+    if (g_noalloc_addr[ctx->device] == nullptr) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || p == nullptr) {
+            set_error(ctx, "cudaGetSymbolAddress(scratch) on device %d: %s", ctx->device,
+                      cudaGetErrorString(e));
+            return DONOF_ERR_CUDA;
+        }
+        g_noalloc_addr[ctx->device] = p;
+    }
+    *out = static_cast<double*>(g_noalloc_addr[ctx->device]);
+    return DONOF_OK;
+}
+
+size_t round256(size_t doubles) { return (doubles * sizeof(double) + 255) / 256 * 256 / sizeof(double); }
+
+}  // namespace
+
+int lagrange2_f64_noalloc(donof_job* job, cudaStream_t st, const double* C, const double* n,
+                          const double* H, const double* cj12, const double* ck12, int nbf5,
+                          int nalpha, int nbeta, double* elag, double* Hmat, double* E) {
+    donof_ctx* ctx = job->ctx;
+    const int nbf = job->nbf, naux = job->naux;
+    const long long Kt = (long long)nbf5 * naux;
+    // split count of the Lagrangian GEMM (K = nbf5 * naux), as in gemm_f64_auto
+    int splits = 1;
+    const GemmTile ytile = pick_tile(ctx, nbf, nbf5, (int)Kt, true, &splits);
+    int kchunk = (int)Kt;
+    if (splits > 1) {
+        kchunk = (int)(((Kt + splits - 1) / splits + 15) / 16 * 16);
+        splits = (int)((Kt + kchunk - 1) / kchunk);
+    }
+    const size_t s_tmp = round256((size_t)nbf * nbf5 * naux);
+    const size_t s_bpq = round256((size_t)nbf5 * nbf5 * naux);
+    const size_t s_w = round256((size_t)Kt * nbf5);
+    const size_t s_small = round256((size_t)nbf * nbf5);
+    const size_t s_part = round256((size_t)splits * nbf * nbf5);
+    const size_t need = (s_tmp + s_bpq + s_w + 2 * s_small + s_part) * sizeof(double);
+    if (need > NOALLOC_SCRATCH_BYTES) {
+        set_error(ctx,
+                  "donof_lagrange2_noalloc_dev: nbf=%d nbf5=%d naux=%d needs %zu bytes of scratch, "
+                  "more than the fixed %zu bytes; use donof_lagrange2_dev",
+                  nbf, nbf5, naux, need, NOALLOC_SCRATCH_BYTES);
+        return DONOF_ERR_ARG;
+    }
+    double* base = nullptr;
+    DONOF_CHECK(noalloc_scratch(ctx, &base));
+    double* tmp = base;
+    double* bpq = tmp + s_tmp;
+    double* W = bpq + s_bpq;
+    double* HC = W + s_w;
+    double* Y = HC + s_small;
+    double* part = Y + s_small;
+
+    auto plain = [&](bool ak, const double* A, const double* B, double* Cm, double beta) -> int {
+        int sp = 1;
+        const GemmTile t = pick_tile(ctx, nbf, nbf5, nbf, false, &sp);
+        GemmF64Args p{};
+        p.M = nbf; p.N = nbf5; p.K = nbf;
+        p.A = A; p.lda = nbf; p.B = B; p.ldb = nbf; p.C = Cm; p.ldc = nbf;
+        p.alpha = 1.0; p.beta = beta; p.batch = 1; p.splits = 1; p.kchunk = nbf;
+        return gemm_f64(ctx, st, ak, true, p, t);
+    };
+    // H_mat = C^T (H C5)
+    DONOF_CHECK(plain(false, H, C, HC, 0.0));
+    DONOF_CHECK(plain(true, C, HC, Hmat, 0.0));
+    // T1 / T2
+    {
+        GemmF64Args p{};
+        p.M = nbf; p.N = nbf5; p.K = nbf;
+        p.A = job->b; p.lda = nbf; p.strideA = (long long)nbf * nbf;
+        p.B = C; p.ldb = nbf; p.strideB = 0;
+        p.C = tmp; p.ldc = nbf; p.strideC = (long long)nbf * nbf5;
+        p.alpha = 1.0; p.beta = 0.0; p.batch = naux; p.splits = 1;
+        DONOF_CHECK(gemm_f64(ctx, st, false, true, p, nbf >= 128 ? GemmTile::Large : GemmTile::Small));
+    }
+    {
+        GemmF64Args p{};
+        p.M = nbf5; p.N = nbf5; p.K = nbf;
+        p.A = C; p.lda = nbf; p.strideA = 0;
+        p.B = tmp; p.ldb = nbf; p.strideB = (long long)nbf * nbf5;
+        p.C = bpq; p.ldc = nbf5; p.strideC = (long long)nbf5 * nbf5;
+        p.alpha = 1.0; p.beta = 0.0; p.batch = naux; p.splits = 1;
+        DONOF_CHECK(gemm_f64(ctx, st, true, true, p, nbf5 > 64 ? GemmTile::Large : GemmTile::Small));
+    }
+    build_w_kernel<<<naux, 256, sizeof(double) * 2 * nbf5, st>>>(bpq, n, cj12, ck12, nbf5, naux, nalpha,
+                                                                 nbeta, W); count_launch();
+    DONOF_CUDA(ctx, cudaGetLastError());
+    // Y = tmp W (split-K partials in the scratch, then reduced)
+    {
+        GemmF64Args p{};
+        p.M = nbf; p.N = nbf5; p.K = (int)Kt;
+        p.A = tmp; p.lda = nbf; p.B = W; p.ldb = Kt;
+        p.alpha = 1.0; p.beta = 0.0; p.batch = 1;
+        if (splits > 1) {
+            p.C = part; p.ldc = nbf; p.splits = splits; p.kchunk = kchunk;
+            p.strideSplit = (long long)nbf * nbf5;
+            DONOF_CHECK(gemm_f64(ctx, st, false, true, p, ytile));
+            DONOF_CHECK(splitk_reduce(ctx, st, part, (long long)nbf * nbf5, splits, (long long)nbf * nbf5, Y, 0.0));
+        } else {
+            p.C = Y; p.ldc = nbf; p.splits = 1; p.kchunk = (int)Kt;
+            DONOF_CHECK(gemm_f64(ctx, st, false, true, p, ytile));
+        }
+    }
+    elag_init_kernel<<<grid_for((long long)nbf * nbf, 256, ctx->sm_count), 256, 0, st>>>(Hmat, n, nbf, nbf5,
+                                                                                      elag); count_launch();
+    DONOF_CUDA(ctx, cudaGetLastError());
+    DONOF_CHECK(plain(true, C, Y, elag, 1.0));
+    if (E != nullptr) {
+        e_elec_kernel<<<1, 256, 0, st>>>(elag, Hmat, n, nbf, nbf5, E); count_launch();
+        DONOF_CUDA(ctx, cudaGetLastError());
+    }
+    return DONOF_OK;
+}
+
 }  // namespace donof
+
+extern "C" int donof_lagrange2_noalloc_dev(donof_job* job, const double* C, const double* n, const double* H,
+                                           const double* cj12, const double* ck12, int nbf5, int nalpha,
+                                           int nbeta, double* elag, double* H_mat, double* E_elec) {
+    using namespace donof;
+    if (!job) return DONOF_ERR_ARG;
+    donof_ctx* ctx = job->ctx;
+    if (nbf5 <= 0 || nbf5 > job->nbf || nbeta < 0 || nalpha < nbeta || nalpha > nbf5) {
+        set_error(ctx, "donof_lagrange2_noalloc_dev: invalid sizes nbf=%d nbf5=%d nalpha=%d nbeta=%d", job->nbf,
+                  nbf5, nalpha, nbeta);
+        return DONOF_ERR_ARG;
+    }
+    if (!C || !n || !H || !cj12 || !ck12 || !elag || !H_mat) {
+        set_error(ctx, "donof_lagrange2_noalloc_dev: null array argument");
+        return DONOF_ERR_ARG;
+    }
+    DONOF_CUDA(ctx, cudaSetDevice(ctx->device));
+    return lagrange2_f64_noalloc(job, ctx->stream, C, n, H, cj12, ck12, nbf5, nalpha, nbeta, elag, H_mat,
+                                 E_elec);
+}

@@ -101,6 +101,22 @@ int donof_lagrange2_prec_dev(donof_job* job, int precision, const double* C, con
                              int nbf5, int nalpha, int nbeta, double* elag, double* H_mat,
                              double* E_elec);
 
+/* Allocation-free compute_Lagrange2 (plain FP64 form, device pointers).
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc:
+ * hosts whose device memory belongs to another runtime's pool, services that
+ * must not grow their device footprint while running, or code that may not
+ * block on the synchronising allocator.  Every intermediate lives in one
+ * 32 MiB device array inside the library, held by every GPU that loads it
+ * until the process exits; sizes whose intermediates do not fit
+ * ((nbf*nbf5 + 2*nbf5*nbf5) * naux doubles plus small terms) are rejected
+ * with DONOF_ERR_ARG.  The first call on a device looks that array up (make
+ * it before any stream capture); all calls share it, so calls that overlap on
+ * the GPU race.  The job must not allocate either: attach b with
+ * donof_b_attach and DONOF_PREC_FP64.                                        */
+int donof_lagrange2_noalloc_dev(donof_job* job, const double* C, const double* n, const double* H,
+                                const double* cj12, const double* ck12, int nbf5, int nalpha,
+                                int nbeta, double* elag, double* H_mat, double* E_elec);
+
 /* --- JKH_MO, RI method ----------------------------------------------------
  * Replaces computeJKH_MO / JKH_MO(C,H,b::CuArray{T,3},nbf,nbf5,nbfaux)
  * (ext/DoNOFGPUExt.jl:52-94); CPU definition src/integrals.jl:131-172.

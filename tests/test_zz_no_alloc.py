@@ -1,0 +1,99 @@
+"""The allocation-free Lagrangian entry point (donof_lagrange2_noalloc_dev).
+
+It exists for callers that cannot call cudaMalloc -- a host whose device
+memory belongs to another runtime's pool, a service that must not grow its
+device footprint while running, code that may not block on the synchronising
+allocator -- and takes its intermediates from a fixed 32 MiB array inside the
+library.  These tests call it through the C ABI and compare it with the
+existing entry point (donof_lagrange2_dev) on two calls in a row with
+different orbitals, so the second call also shows that what the first call
+left in the shared array does not leak into the result.  The file is named to
+be collected last.
+"""
+import ctypes as ct
+
+import numpy as np
+import pytest
+
+import donof_b200 as d
+from donof_b200 import _lib, workload
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-10
+
+
+def rel(a, b):
+    a, b = a.double().cpu().numpy(), b.double().cpu().numpy()
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def test_noalloc_lagrange2_matches_existing_entry_point():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    ctx = d.Context(0)
+    lib = _lib.load()
+    wl = workload.synthetic(nbf=48, naux=96, nbeta=4, ncwo=3, seed=31)
+    p = wl.p
+    job_ref = d.eris_to_gpu(wl.b, "fp64", ctx)           # existing path, owns its scratch
+    tb = d.to_device(wl.b)
+    job_na = d.eris_to_gpu(tb, "fp64", ctx)              # attached b: the job allocates nothing
+    tn, tH, tcj, tck = (d.to_device(x) for x in (wl.n, wl.H, wl.cj12, wl.ck12))
+    rng = np.random.default_rng(5)
+    C2 = np.linalg.qr(wl.C @ np.linalg.qr(np.eye(p.nbf) + 0.05 * rng.standard_normal((p.nbf, p.nbf)))[0])[0]
+    orbitals = [d.to_device(wl.C), d.to_device(np.asfortranarray(C2))]
+
+    def outputs():
+        return (torch.zeros(p.nbf, p.nbf, dtype=torch.float64, device="cuda"),
+                torch.zeros(p.nbf5, p.nbf, dtype=torch.float64, device="cuda"),
+                torch.zeros(1, dtype=torch.float64, device="cuda"))
+
+    refs = []
+    for tC in orbitals:
+        el, hm, E = outputs()
+        d.compute_Lagrange2_dev(tC, tn, tH, job_ref, tcj, tck, p.nalpha, p.nbeta, el, hm, E)
+        refs.append((el, hm, E))
+    outs = [outputs() for _ in orbitals]
+    torch.cuda.synchronize()
+
+    free_after_first = None
+    for call, (tC, (el, hm, E), (rel_, rhm, rE)) in enumerate(zip(orbitals, outs, refs)):
+        st = lib.donof_lagrange2_noalloc_dev(job_na.handle, tC.data_ptr(), tn.data_ptr(), tH.data_ptr(),
+                                             tcj.data_ptr(), tck.data_ptr(), p.nbf5, p.nalpha, p.nbeta,
+                                             el.data_ptr(), hm.data_ptr(), E.data_ptr())
+        assert st == _lib.OK, lib.donof_last_error(ctx.handle)
+        torch.cuda.synchronize()
+        assert rel(el, rel_) <= TOL, f"call {call}: elag"
+        assert rel(hm, rhm) <= TOL, f"call {call}: H_mat"
+        assert abs(float(E) - float(rE)) <= TOL * max(1.0, abs(float(rE))), f"call {call}: E"
+        if call == 0:
+            free_after_first = torch.cuda.mem_get_info()[0]
+    # the second call allocated no device memory
+    assert torch.cuda.mem_get_info()[0] == free_after_first
+    job_ref.free()
+    job_na.free()
+    ctx.close()
+
+
+def test_noalloc_rejects_sizes_beyond_the_fixed_scratch():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    ctx = d.Context(0)
+    lib = _lib.load()
+    nbf, naux, nbf5 = 128, 512, 64          # (nbf*nbf5 + 2*nbf5^2)*naux doubles = 48 MiB > 32 MiB
+    b = torch.zeros(naux, nbf, nbf, dtype=torch.float64, device="cuda")
+    job = d.eris_to_gpu(b, "fp64", ctx)
+    C = torch.eye(nbf, dtype=torch.float64, device="cuda")
+    n = torch.full((nbf5,), 0.5, dtype=torch.float64, device="cuda")
+    cj = torch.zeros(nbf5, nbf5, dtype=torch.float64, device="cuda")
+    el = torch.zeros(nbf, nbf, dtype=torch.float64, device="cuda")
+    hm = torch.zeros(nbf5, nbf, dtype=torch.float64, device="cuda")
+    st = lib.donof_lagrange2_noalloc_dev(job.handle, C.data_ptr(), n.data_ptr(), C.data_ptr(), cj.data_ptr(),
+                                         cj.data_ptr(), nbf5, 16, 16, el.data_ptr(), hm.data_ptr(), None)
+    assert st == _lib.ERR_ARG
+    assert b"scratch" in lib.donof_last_error(ctx.handle)
+    job.free()
+    ctx.close()
