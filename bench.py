@@ -25,6 +25,7 @@ per step; --gpus N runs N independent replicas (one job per GPU, weak scaling).
 from __future__ import annotations
 
 import argparse
+import ctypes as ct
 import json
 import math
 import os
@@ -292,34 +293,41 @@ def main():
         t = float(tt.item())
     value = world * args.steps / t
 
-    # ---- roofline of the dominant kernel pair: the three-index transform (T1 + T2)
+    # ---- roofline of the dominant kernel, timed by the library's events on the launching stream
     nbf, naux, nbf5 = p.nbf, p.nbfaux, p.nbf5
-    flops = 2.0 * nbf * nbf * nbf5 * naux + 2.0 * nbf * nbf5 * nbf5 * naux
-    for _ in range(3):
-        d.transform_dev(tC, bt, nbf5)
-    reps = 10
-    es = [torch.cuda.Event(enable_timing=True) for _ in range(reps + 1)]
-    es[0].record()
-    for r in range(reps):
-        d.transform_dev(tC, bt, nbf5)
-        es[r + 1].record()
-    torch.cuda.synchronize()
-    dur = [es[r].elapsed_time(es[r + 1]) / 1e3 for r in range(reps)]
-    tr = statistics.mean(dur)
+    lib = ctx.lib
+    ctx.check(lib.donof_profile_enable(ctx.handle, 1))
+    el = torch.zeros(nbf, nbf, dtype=torch.float64, device=dev)
+    hm = torch.zeros(nbf5, nbf, dtype=torch.float64, device=dev)
+    Eb = torch.zeros(1, dtype=torch.float64, device=dev)
+    durs = []
+    for r in range(13):
+        d.compute_Lagrange2_dev(tC, tn, tH, bt, tcj, tck, p.nalpha, p.nbeta, el, hm, Eb)
+        ms = ct.c_float()
+        ctx.check(lib.donof_profile_last_ms(ctx.handle, ct.byref(ms)))
+        if r >= 3:
+            durs.append(ms.value / 1e3)
+    ctx.check(lib.donof_profile_enable(ctx.handle, 0))
+    tr = statistics.mean(durs)
     peaks = load_peaks()
     if args.precision == "fp64":
+        flops = 2.0 * nbf * nbf * nbf5 * naux
         peak = measured_dgemm_tflops(torch, dev)
         roof = {"bound": "tensor", "achieved": flops / tr / 1e12, "peak": peak, "unit": "TFLOP/s",
-                "frac": flops / tr / 1e12 / peak, "traffic": traffic_from_profiles("transform_f64"),
-                "kernel": "gemm_f64_kernel (T1: b_l C5, then T2: C5^T tmp_l), batched over naux",
-                "algorithmic": f"{flops:.4e} FLOP per transform", "ms": tr * 1e3,
-                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor pipe)"}
+                "frac": flops / tr / 1e12 / peak, "traffic": traffic_from_profiles("t1_f64"),
+                "kernel": "gemm_f64_kernel<128,64> T1: tmp_l = b_l C5, batched over naux (DMMA)",
+                "algorithmic": f"2*nbf^2*nbf5*naux = {flops:.4e} FLOP per launch", "ms": tr * 1e3,
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor pipe); of measured"}
     else:
         byts = 4.0 * nbf * nbf * naux
+        # MMA work actually issued per launch: T1 (hi and lo b), T2, Y (hi and lo tmp), M = 128 rows
+        flops = naux * (2 * 2.0 * 128 * nbf * nbf + 2.0 * 128 * 128 * nbf + 2 * 2.0 * 128 * nbf * 64)
         roof = {"bound": "hbm", "achieved": byts / tr / 1e9, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                "frac": byts / tr / 1e9 / peaks["hbm_gbs"], "traffic": traffic_from_profiles("transform_mixed"),
-                "algorithmic": f"{byts:.4e} bytes (FP32 b read once) per transform", "ms": tr * 1e3,
-                "peak_source": "MEASURED_PEAKS.json hbm_gbs" + (" (fallback)" if peaks.get("fallback") else "")}
+                "frac": byts / tr / 1e9 / peaks["hbm_gbs"], "traffic": traffic_from_profiles("lag_mixed"),
+                "kernel": "lag_mixed_kernel (fused T1, T2, W, Y on tcgen05, bf16 hi/lo)",
+                "algorithmic": f"b_hi + b_lo read once = 4*nbf^2*naux = {byts:.4e} bytes per launch",
+                "tensor_tflops": flops / tr / 1e12, "ms": tr * 1e3,
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs, of measured" + (" (fallback)" if peaks.get("fallback") else "")}
 
     # ---- end to end through the host-buffer C ABI (what a DoNOF.jl loop does per step)
     e2e = None
@@ -368,7 +376,7 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None,
-                "dtype": "f64" if args.precision == "fp64" else "tf32x3+f64", "data": "synthetic",
+                "dtype": "f64" if args.precision == "fp64" else "bf16x2-split+f64", "data": "synthetic",
                 "config": config(args, world), "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": int(launches), "clocks": clk.summary(), "final_E": E}
         print(json.dumps(line), flush=True)

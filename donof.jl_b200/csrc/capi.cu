@@ -53,6 +53,8 @@ int orbopt_run(donof_job* job, int method, const double* n, const double* cj12, 
                double threshgorb, double* C, double* E_out, int* nit_out, int* success_out,
                int precision);
 int convert_b_f32(donof_job* job);
+int mixed_status(donof_job* job, int* out);
+int mixed_t1_debug(donof_job* job, cudaStream_t st, const double* C, int nbf5, float* tmp_out);
 
 }  // namespace donof
 
@@ -105,8 +107,8 @@ int effective_precision(donof_job* job, int precision) {
         set_error(job->ctx, "unknown precision %d", precision);
         return -1;
     }
-    if (precision == DONOF_PREC_MIXED && job->b32 == nullptr) {
-        set_error(job->ctx, "mixed precision requested but the job holds no FP32 copy of b");
+    if (precision == DONOF_PREC_MIXED && job->b16hi == nullptr) {
+        set_error(job->ctx, "mixed precision requested but the job holds no bf16 split of b");
         return -1;
     }
     return precision;
@@ -119,6 +121,43 @@ extern "C" {
 int donof_version(void) { return 1; }
 
 unsigned long long donof_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+
+int donof_profile_enable(donof_ctx* ctx, int enable) {
+    if (!ctx) return DONOF_ERR_ARG;
+    DONOF_CHECK(use_device(ctx));
+    if (enable && !ctx->prof_ev[0]) {
+        DONOF_CUDA(ctx, cudaEventCreate(&ctx->prof_ev[0]));
+        DONOF_CUDA(ctx, cudaEventCreate(&ctx->prof_ev[1]));
+    }
+    ctx->profile = enable != 0;
+    ctx->prof_recorded = false;
+    return DONOF_OK;
+}
+
+int donof_profile_last_ms(donof_ctx* ctx, float* ms) {
+    if (!ctx || !ms) return DONOF_ERR_ARG;
+    if (!ctx->profile || !ctx->prof_recorded) {
+        set_error(ctx, "no profiled kernel recorded");
+        return DONOF_ERR_STATE;
+    }
+    DONOF_CHECK(use_device(ctx));
+    DONOF_CUDA(ctx, cudaEventSynchronize(ctx->prof_ev[1]));
+    DONOF_CUDA(ctx, cudaEventElapsedTime(ms, ctx->prof_ev[0], ctx->prof_ev[1]));
+    return DONOF_OK;
+}
+
+int donof_job_error_flag(donof_job* job, int* flag) {
+    if (!job || !flag) return DONOF_ERR_ARG;
+    DONOF_CHECK(use_device(job->ctx));
+    DONOF_CUDA(job->ctx, cudaStreamSynchronize(job->ctx->stream));
+    return mixed_status(job, flag);
+}
+
+int donof_mixed_tmp_dev(donof_job* job, const double* C, int nbf5, float* tmp) {
+    if (!job || !C || !tmp) return DONOF_ERR_ARG;
+    DONOF_CHECK(use_device(job->ctx));
+    return mixed_t1_debug(job, job->ctx->stream, C, nbf5, tmp);
+}
 
 int donof_transform_dev(donof_job* job, int precision, const double* C, int nbf5, double* b_pq) {
     if (!job) return DONOF_ERR_ARG;
@@ -192,6 +231,8 @@ int donof_destroy(donof_ctx* ctx) {
     ctx->stage_out.release();
     ctx->rot.release();
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+    if (ctx->prof_ev[0]) cudaEventDestroy(ctx->prof_ev[0]);
+    if (ctx->prof_ev[1]) cudaEventDestroy(ctx->prof_ev[1]);
     delete ctx;
     return DONOF_OK;
 }
@@ -292,7 +333,8 @@ int donof_job_free(donof_job* job) {
     cudaSetDevice(job->ctx->device);
     cudaStreamSynchronize(job->ctx->stream);
     if (job->own_b && job->b) cudaFree((void*)job->b);
-    if (job->own_b32 && job->b32) cudaFree((void*)job->b32);
+    if (job->b16hi) cudaFree(job->b16hi);
+    if (job->b16lo) cudaFree(job->b16lo);
     job->tmp.release();
     job->bpq.release();
     job->W.release();
@@ -309,7 +351,7 @@ size_t donof_job_device_bytes(const donof_job* job) {
     size_t s = job->tmp.bytes + job->bpq.bytes + job->W.bytes + job->part.bytes + job->small.bytes +
                job->orb.bytes + job->io.bytes;
     if (job->own_b) s += sizeof(double) * (size_t)job->nbf * job->nbf * job->naux;
-    if (job->own_b32) s += sizeof(float) * (size_t)job->nbf * job->nbf * job->naux;
+    if (job->b16hi) s += 4 * (size_t)((job->nbf + 7) / 8 * 8) * job->nbf * job->naux;
     return s;
 }
 

@@ -57,15 +57,35 @@ struct donof_ctx {
     donof::DevBuf stage_in, stage_out;
     // scratch for the rotation (exp of the generator)
     donof::DevBuf rot;
+    // optional timing of the dominant kernel of each call (donof_profile_*):
+    // events recorded on the launching stream around that kernel
+    bool profile = false;
+    cudaEvent_t prof_ev[2] = {nullptr, nullptr};
+    bool prof_recorded = false;
 };
+
+namespace donof {
+// Bracket the dominant kernel of a call with the context's profiling events.
+inline void prof_begin(donof_ctx* ctx, cudaStream_t st) {
+    if (ctx->profile && ctx->prof_ev[0]) cudaEventRecord(ctx->prof_ev[0], st);
+}
+inline void prof_end(donof_ctx* ctx, cudaStream_t st) {
+    if (ctx->profile && ctx->prof_ev[1]) {
+        cudaEventRecord(ctx->prof_ev[1], st);
+        ctx->prof_recorded = true;
+    }
+}
+}  // namespace donof
 
 struct donof_job {
     donof_ctx* ctx = nullptr;
     int nbf = 0, naux = 0, precision = DONOF_PREC_FP64;
     const double* b = nullptr;  // device [m + nbf*n + nbf*nbf*l]
     bool own_b = false;
-    const float* b32 = nullptr;  // FP32 copy for the mixed-precision form
-    bool own_b32 = false;
+    // bf16 split of b for the mixed-precision form: b = hi + lo, layout
+    // [m + ldm*n + ldm*nbf*l] with ldm = nbf rounded up to a multiple of 8
+    void* b16hi = nullptr;
+    void* b16lo = nullptr;
     // per-call scratch, sized for the largest nbf5 seen
     donof::DevBuf tmp, bpq, W, part, small;
     // device-resident orbital-optimiser state

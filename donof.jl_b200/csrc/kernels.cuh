@@ -33,6 +33,12 @@ int lagrange2_f64(donof_job* job, cudaStream_t st, const double* C, const double
 int jkh_mo_f64(donof_job* job, cudaStream_t st, const double* C, const double* H, int nbf5,
                double* J, double* K, double* Hcore);
 
+// Shared tails of the Lagrangian / JKH_MO (lagrange.cu): elag = n o H_mat + C^T Y
+// (columns >= nbf5 zero) and E_elec; H_core from HC = H C5.
+int elag_finish_f64(donof_job* job, cudaStream_t st, const double* C, const double* n, const double* Hmat,
+                    const double* Y, int nbf5, double* elag, double* E);
+int hcore_f64(donof_job* job, cudaStream_t st, const double* C, const double* HC, int nbf5, double* Hcore);
+
 // Mixed-precision pipelines (mixed.cu)
 int transforms_mixed(donof_job* job, cudaStream_t st, const double* C, int nbf5);
 int lagrange2_mixed(donof_job* job, cudaStream_t st, const double* C, const double* n,

@@ -161,7 +161,9 @@ int transforms_f64(donof_job* job, cudaStream_t st, const double* C, int nbf5) {
         p.B = C; p.ldb = nbf; p.strideB = 0;
         p.C = tmp; p.ldc = nbf; p.strideC = (long long)nbf * nbf5;
         p.alpha = 1.0; p.beta = 0.0; p.batch = naux; p.splits = 1;
+        prof_begin(ctx, st);
         DONOF_CHECK(gemm_f64(ctx, st, false, true, p, nbf >= 128 ? GemmTile::Large : GemmTile::Small));
+        prof_end(ctx, st);
     }
     // T2: bpq_l(p,q) = sum_m C[m,p] tmp_l[m,q]
     {
@@ -214,6 +216,27 @@ int lagrange2_f64(donof_job* job, cudaStream_t st, const double* C, const double
         e_elec_kernel<<<1, 256, 0, st>>>(elag, Hmat, n, nbf, nbf5, E); count_launch();
         DONOF_CUDA(ctx, cudaGetLastError());
     }
+    return DONOF_OK;
+}
+
+int elag_finish_f64(donof_job* job, cudaStream_t st, const double* C, const double* n, const double* Hmat,
+                    const double* Y, int nbf5, double* elag, double* E) {
+    donof_ctx* ctx = job->ctx;
+    const int nbf = job->nbf;
+    elag_init_kernel<<<grid_for((long long)nbf * nbf, 256, ctx->sm_count), 256, 0, st>>>(Hmat, n, nbf, nbf5,
+                                                                                      elag); count_launch();
+    DONOF_CUDA(ctx, cudaGetLastError());
+    DONOF_CHECK(gemm_f64_auto(ctx, st, true, true, nbf, nbf5, nbf, C, nbf, Y, nbf, elag, nbf, 1.0, 1.0, &job->part));
+    if (E != nullptr) {
+        e_elec_kernel<<<1, 256, 0, st>>>(elag, Hmat, n, nbf, nbf5, E); count_launch();
+        DONOF_CUDA(ctx, cudaGetLastError());
+    }
+    return DONOF_OK;
+}
+
+int hcore_f64(donof_job* job, cudaStream_t st, const double* C, const double* HC, int nbf5, double* Hcore) {
+    hcore_kernel<<<(nbf5 * 32 + 255) / 256, 256, 0, st>>>(C, HC, job->nbf, nbf5, Hcore); count_launch();
+    DONOF_CUDA(job->ctx, cudaGetLastError());
     return DONOF_OK;
 }
 

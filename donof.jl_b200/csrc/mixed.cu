@@ -1,52 +1,969 @@
-// Mixed-precision form of the RI hot path (tensor-core TF32x3 contractions
-// with FP32 accumulation).  FP32 copy of b kept next to the FP64 one.
+// Mixed-precision form of the RI hot path on the 5th-generation tensor cores.
+//
+// b is kept on the device as two bf16 arrays, b = b_hi + b_lo (both rounded
+// to nearest, 16 significant bits together); C5, the intermediates and the
+// functional weights are split the same way, and every product is formed from
+// all four hi/lo pairs with FP32 accumulation in tensor memory (TMEM).  The
+// hi and lo halves of the small operand are stacked as the 128 rows of one
+// MMA, so one tcgen05.mma (M = 128) yields both partial products.
+//
+// One persistent kernel (lag_mixed_kernel) walks the aux index l and, per l,
+// without leaving the SM:
+//   T1  D1[j, m] = sum_n Cs[j, n] b_x[n, m]      (x = hi, lo; j = q | 64+q)
+//       tmp[m, q] = D1[q, m] + D1[64+q, m]
+//   T2  D2[j, j'] = sum_m tmp_x[m, q] Cs[j', m]  -> b_pq = sum of 4 quadrants
+//   W   W[q, b] = delta_qb (n'_b d_b + sum_q' cj12[b,q'] d_q') - ck12[b,q] b_bq
+//   Y   D3[j, m] += sum_q W_x[q, b] tmp_y[m, q]   (accumulated over all l of the CTA)
+// and emits d_q^l = b_qq^l (for J_MO = D D^T) and per-CTA partial sums of
+// K_MO[p,q] = sum_l (b_pq^l)^2 and of Y.  b is read from HBM exactly once.
+//
+// Warp roles (192 threads): warps 0-3 epilogue (TMEM lane quarters), warp 4
+// TMA producer, warp 5 TMEM allocator + MMA issuer.  Operands are staged by
+// TMA (cp.async.bulk.tensor, no multicast) with 128-byte swizzle; every wait
+// on an mbarrier is bounded by a clock budget after which the CTA records an
+// error in the status word, drains its in-flight copies, frees TMEM and exits.
+//
+// Supported shapes: nbf <= 256, nbf5 <= 64 (one MMA tile per aux index);
+// other shapes are rejected with DONOF_ERR_ARG.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_bf16.h>
+#include <math.h>
+
 #include "kernels.cuh"
 
 namespace donof {
 
-namespace {
+namespace mx {
 
-__global__ void to_f32_kernel(const double* __restrict__ in, long long count, float* __restrict__ out) {
+constexpr int NTHREADS = 192;
+constexpr int RING = 2;               // b stages
+constexpr int KB = 32;                // n rows per b stage
+constexpr int BOX_M = 64;             // m per TMA box (128 B of bf16)
+constexpr int MAXNB = 4;              // up to 4 boxes -> N = 256
+constexpr int BOX_BYTES = KB * BOX_M * 2;           // 4 KB
+constexpr int STAGE_BYTES = 2 * MAXNB * BOX_BYTES;  // hi + lo, 32 KB
+constexpr int CS_BOX_BYTES = 128 * 64 * 2;          // 16 KB: 128 rows x 64 k
+constexpr int CS_BYTES = 4 * CS_BOX_BYTES;          // K up to 256 -> 64 KB
+constexpr int A2_BYTES = 4 * CS_BOX_BYTES;          // tmp split, 64 KB
+constexpr int A3_BYTES = CS_BOX_BYTES;              // W split, 16 KB
+constexpr int XS_STRIDE = 36;                       // floats per staging row
+constexpr int XS_BYTES = 64 * XS_STRIDE * 4;        // 9216 B
+constexpr int XH_STRIDE = 20;                       // floats per half-exchange row (16 + pad)
+constexpr int CK_BYTES = 64 * 64 * 4;                // ck12 (transposed, FP32), 16 KB
+// shared-memory map (offsets from a 1024-aligned base).  The hi/lo exchange
+// buffer of the epilogue aliases the W operand (A3): A3 is idle whenever the
+// exchange is used (before W is written, and after the last Y MMA completed).
+constexpr int OFF_CS = 0;
+constexpr int OFF_RING = OFF_CS + CS_BYTES;
+constexpr int OFF_A2 = OFF_RING + RING * STAGE_BYTES;
+constexpr int OFF_A3 = OFF_A2 + A2_BYTES;
+constexpr int OFF_XS = OFF_A3;
+static_assert(XS_BYTES <= A3_BYTES && 2 * 64 * XH_STRIDE * 4 <= A3_BYTES, "exchange buffers must fit in A3");
+constexpr int OFF_CK = OFF_A3 + A3_BYTES;
+constexpr int OFF_DS = OFF_CK + CK_BYTES;            // 64 floats d
+constexpr int OFF_TS = OFF_DS + 256;                 // 128 floats: partial sums of t
+constexpr int OFF_BAR = OFF_TS + 512 + 256;
+constexpr int NBAR = 16;
+constexpr int OFF_MISC = OFF_BAR + NBAR * 8;         // tmem base, abort flag
+constexpr int SMEM_USED = OFF_MISC + 64;
+constexpr int SMEM_ALLOC = SMEM_USED + 1024;         // slack for 1024-B alignment
+static_assert(SMEM_ALLOC <= 227 * 1024, "shared memory budget");
+
+// barrier indices
+constexpr int B_FULL = 0;      // +s, RING of them
+constexpr int B_EMPTY = 2;     // +s
+constexpr int B_CS = 4;
+constexpr int B_T1 = 5;
+constexpr int B_A2 = 6;
+constexpr int B_T2 = 7;
+constexpr int B_A3 = 8;
+constexpr int B_Y = 9;
+
+constexpr long long WAIT_CYCLES = 4000000000LL;  // ~2 s of SM clock
+
+struct Params {
+    int nbf, nbf5, naux, nalpha, nbeta;
+    int nb;                  // 64-wide m boxes (N = 64 * nb)
+    int nkb;                 // b stages per l (ceil(nbf / 32))
+    int ncs;                 // 64-wide k boxes of Cs (ceil(nbf / 64))
+    int mode;                // 1: write tmp; 2: write b_pq; 3: full Lagrangian
+    const float* n32;        // n (nbf5)
+    const float* cj32;       // cj12 (nbf5 x nbf5)
+    const float* ck32t;      // ck12 transposed: ck32t[q + nbf5*b] = ck12[b, q]
+    float* tmp_out;          // mode 1: tmp[m + nbf*q + nbf*nbf5*l]
+    float* bpq_out;          // mode 2: b_pq[p + nbf5*q + nbf5^2*l]
+    float* d_out;            // d[q + nbf5*l]
+    float* y_part;           // per CTA: Y[m + nbf*b]
+    float* k_part;           // per CTA: K[p + nbf5*q]
+    int* status;             // nonzero on timeout
+};
+
+__device__ __forceinline__ uint32_t saddr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, int count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait: false (and the abort flag set) if the phase does not complete
+// within WAIT_CYCLES or another role aborted.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
+    const long long t0 = clock64();
+    while (!mbar_try(bar, parity)) {
+        if (*abort_flag) return false;
+        if (clock64() - t0 > WAIT_CYCLES) {
+            *abort_flag = 1;
+            return false;
+        }
+    }
+    return true;
+}
+
+// Bounded wait that ignores the abort flag: used to drain in-flight copies and
+// MMAs before the CTA frees its resources.
+__device__ __forceinline__ bool mbar_drain(uint32_t bar, uint32_t parity) {
+    const long long t0 = clock64();
+    while (!mbar_try(bar, parity))
+        if (clock64() - t0 > WAIT_CYCLES) return false;
+    return true;
+}
+
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, uint32_t bar, int c0, int c1,
+                                            int c2) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(
+            dst),
+        "l"(map), "r"(bar), "r"(c0), "r"(c1), "r"(c2)
+        : "memory");
+}
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, uint32_t bar, int c0, int c1) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(dst),
+        "l"(map), "r"(bar), "r"(c0), "r"(c1)
+        : "memory");
+}
+
+// UMMA shared-memory descriptor, 128-byte swizzle, sm100 version bits.
+__device__ __forceinline__ uint64_t sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46) | (2ull << 61);
+}
+// instruction descriptor: bf16 x bf16 -> f32
+__host__ __device__ constexpr uint32_t idesc(int M, int N, int a_mn, int b_mn) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)a_mn << 15) | ((uint32_t)b_mn << 16) |
+           ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t id, uint32_t accum) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(a), "l"(b), "r"(id), "r"(accum));
+}
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Issue a 32-column TMEM load without waiting; the registers are valid only
+// after tmem_wait_ld().
+__device__ __forceinline__ void tmem_issue32(uint32_t taddr, uint32_t (&r)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// Byte offset of bf16 element k (0..63) of row r inside a K-major 128B-swizzled
+// tile whose rows are 128 bytes (8-row atoms of 1024 B).
+__device__ __forceinline__ uint32_t sw128(int r, int k) {
+    const int chunk = (k >> 3) ^ (r & 7);
+    return (uint32_t)(r * 128 + chunk * 16 + (k & 7) * 2);
+}
+
+__device__ __forceinline__ void split_bf16(float v, __nv_bfloat16& hi, __nv_bfloat16& lo) {
+    hi = __float2bfloat16_rn(v);
+    lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+}
+
+// Write 32 consecutive K values (k0..k0+31, k0 % 32 == 0) of rows rh (hi) and
+// rl (lo) into a K-major swizzled operand made of 64-wide boxes of box_bytes.
+__device__ __forceinline__ void put_split_row32(unsigned char* base, int box_bytes, int rh, int rl, int k0,
+                                                const float (&v)[32]) {
+    unsigned char* box = base + (k0 >> 6) * box_bytes;
+    const int kin = k0 & 63;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        __align__(16) __nv_bfloat16 h[8], l[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) split_bf16(v[c * 8 + e], h[e], l[e]);
+        *reinterpret_cast<uint4*>(box + sw128(rh, kin + c * 8)) = *reinterpret_cast<const uint4*>(h);
+        *reinterpret_cast<uint4*>(box + sw128(rl, kin + c * 8)) = *reinterpret_cast<const uint4*>(l);
+    }
+}
+
+// Finish 16 columns (OFF .. OFF+15 of the 32-column chunk c) of tmp row q:
+// mode 1 writes FP32 to global, otherwise the bf16 hi/lo split goes to A2.
+template <int OFF>
+__device__ __forceinline__ void finish_tmp16(const Params& P, unsigned char* sm, const float (&v)[32], int q, int c,
+                                             int l) {
+    if (P.mode == 1) {
+        if (q < P.nbf5) {
+            float* dst = P.tmp_out + (size_t)P.nbf * P.nbf5 * l + (size_t)P.nbf * q + c * 32 + OFF;
+#pragma unroll
+            for (int i = 0; i < 16; ++i)
+                if (c * 32 + OFF + i < P.nbf) dst[i] = v[OFF + i];
+        }
+        return;
+    }
+    const int k0 = c * 32 + OFF;
+    unsigned char* box = sm + OFF_A2 + (k0 >> 6) * CS_BOX_BYTES;
+    const int kin = k0 & 63;
+#pragma unroll
+    for (int cc = 0; cc < 2; ++cc) {
+        __align__(16) __nv_bfloat16 h[8], lo[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) split_bf16(v[OFF + cc * 8 + e], h[e], lo[e]);
+        *reinterpret_cast<uint4*>(box + sw128(q, kin + cc * 8)) = *reinterpret_cast<const uint4*>(h);
+        *reinterpret_cast<uint4*>(box + sw128(64 + q, kin + cc * 8)) = *reinterpret_cast<const uint4*>(lo);
+    }
+}
+
+__global__ void __launch_bounds__(NTHREADS, 1)
+lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_constant__ CUtensorMap map_blo,
+                 const __grid_constant__ CUtensorMap map_cs, const Params P) {
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const uint32_t sbase = saddr(sm);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sm + OFF_BAR);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(sm + OFF_MISC);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + OFF_MISC + 16);
+    float* xs = reinterpret_cast<float*>(sm + OFF_XS);
+    float* ds = reinterpret_cast<float*>(sm + OFF_DS);
+    auto bar = [&](int i) { return saddr(&bars[i]); };
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int G = gridDim.x;
+    const int my_count = (P.naux - (int)blockIdx.x + G - 1) / G;  // l = blockIdx.x + k*G
+    const int ncol = 64 * P.nb;
+
+    if (threadIdx.x == 0) {
+        *abort_flag = 0;
+        for (int s = 0; s < RING; ++s) {
+            mbar_init(bar(B_FULL + s), 1);
+            mbar_init(bar(B_EMPTY + s), 1);
+        }
+        mbar_init(bar(B_CS), 1);
+        mbar_init(bar(B_T1), 1);
+        mbar_init(bar(B_A2), 1);
+        mbar_init(bar(B_T2), 1);
+        mbar_init(bar(B_A3), 1);
+        mbar_init(bar(B_Y), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 5) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(saddr(tmem_slot)));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t R1 = tmem, R2 = tmem + 256;
+
+    if (warp == 4) {
+        // ------------------------------------------------------------ producer
+        if (lane == 0 && my_count > 0) {
+            mbar_expect_tx(bar(B_CS), (uint32_t)(P.ncs * CS_BOX_BYTES));
+            for (int kb = 0; kb < P.ncs; ++kb)
+                tma_load_2d(sbase + OFF_CS + kb * CS_BOX_BYTES, &map_cs, bar(B_CS), kb * 64, 0);
+            int it = 0;
+            bool ok = true;
+            for (int li = 0; li < my_count && ok; ++li) {
+                const int l = blockIdx.x + li * G;
+                for (int kb = 0; kb < P.nkb && ok; ++kb, ++it) {
+                    const int s = it % RING;
+                    const uint32_t ph = (uint32_t)((it / RING) & 1);
+                    if (!mbar_wait(bar(B_EMPTY + s), ph ^ 1u, abort_flag)) { ok = false; break; }
+                    mbar_expect_tx(bar(B_FULL + s), (uint32_t)(2 * P.nb * BOX_BYTES));
+                    const uint32_t st = sbase + OFF_RING + s * STAGE_BYTES;
+                    for (int i = 0; i < P.nb; ++i) {
+                        tma_load_3d(st + i * BOX_BYTES, &map_bhi, bar(B_FULL + s), i * BOX_M, kb * KB, l);
+                        tma_load_3d(st + (MAXNB + i) * BOX_BYTES, &map_blo, bar(B_FULL + s), i * BOX_M, kb * KB, l);
+                    }
+                }
+            }
+            // drain: every issued stage must have landed before the CTA exits
+            const int issued = it;
+            for (int j = (issued > RING ? issued - RING : 0); j < issued; ++j) {
+                const int s = j % RING;
+                mbar_drain(bar(B_FULL + s), (uint32_t)((j / RING) & 1));
+            }
+            mbar_drain(bar(B_CS), 0);
+        }
+    } else if (warp == 5) {
+        // ------------------------------------------------------------ MMA issuer
+        if (lane == 0 && my_count > 0) {
+            const uint32_t id_t1 = idesc(128, ncol, 0, 1);
+            const uint32_t id_t2 = idesc(128, 128, 0, 0);
+            const uint32_t id_y = idesc(128, ncol, 0, 1);
+            bool ok = mbar_wait(bar(B_CS), 0, abort_flag);
+            fence_after();
+            int it = 0;
+            for (int li = 0; li < my_count && ok; ++li) {
+                const uint32_t lph = (uint32_t)(li & 1);
+                // T1: R1[j, m] = sum_n Cs[j, n] b_x[n, m]
+                for (int kb = 0; kb < P.nkb; ++kb, ++it) {
+                    const int s = it % RING;
+                    if (!mbar_wait(bar(B_FULL + s), (uint32_t)((it / RING) & 1), abort_flag)) { ok = false; break; }
+                    fence_after();
+                    const uint32_t st = sbase + OFF_RING + s * STAGE_BYTES;
+#pragma unroll
+                    for (int ks = 0; ks < KB / 16; ++ks) {
+                        const int k = kb * KB + ks * 16;  // n offset
+                        const uint64_t a = sdesc(sbase + OFF_CS + (k >> 6) * CS_BOX_BYTES + (k & 63) * 2, 16, 1024);
+                        const uint64_t bh = sdesc(st + ks * 2048, BOX_BYTES, 1024);
+                        const uint64_t bl = sdesc(st + MAXNB * BOX_BYTES + ks * 2048, BOX_BYTES, 1024);
+                        umma(R1, a, bh, id_t1, (kb | ks) ? 1u : 0u);
+                        umma(R1, a, bl, id_t1, 1u);
+                    }
+                    umma_commit(bar(B_EMPTY + s));
+                }
+                if (!ok) break;
+                umma_commit(bar(B_T1));
+                if (P.mode == 1) {
+                    // the epilogue writes tmp and hands R1 back through B_A2
+                    if (!mbar_wait(bar(B_A2), lph, abort_flag)) { ok = false; break; }
+                    fence_after();
+                    continue;
+                }
+                // T2: R1[j, j'] = sum_m A2[j, m] Cs[j', m]
+                if (!mbar_wait(bar(B_A2), lph, abort_flag)) { ok = false; break; }
+                fence_after();
+                for (int ks = 0; ks < ncol / 16; ++ks) {
+                    const int k = ks * 16;  // m offset
+                    const uint64_t a = sdesc(sbase + OFF_A2 + (k >> 6) * CS_BOX_BYTES + (k & 63) * 2, 16, 1024);
+                    const uint64_t b = sdesc(sbase + OFF_CS + (k >> 6) * CS_BOX_BYTES + (k & 63) * 2, 16, 1024);
+                    umma(R1, a, b, id_t2, ks ? 1u : 0u);
+                }
+                umma_commit(bar(B_T2));
+                if (!mbar_wait(bar(B_A3), lph, abort_flag)) { ok = false; break; }
+                fence_after();
+                if (P.mode == 2) continue;
+                // Y: R2[j, m] += sum_q A3[j, q] tmp_x[q, m]  (A2 read as an MN-major operand)
+#pragma unroll
+                for (int ks = 0; ks < 4; ++ks) {
+                    const uint64_t a = sdesc(sbase + OFF_A3 + ks * 32, 16, 1024);
+                    const uint64_t bh = sdesc(sbase + OFF_A2 + ks * 2048, CS_BOX_BYTES, 1024);
+                    const uint64_t bl = sdesc(sbase + OFF_A2 + 8192 + ks * 2048, CS_BOX_BYTES, 1024);
+                    umma(R2, a, bh, id_y, (li | ks) ? 1u : 0u);
+                    umma(R2, a, bl, id_y, 1u);
+                }
+            }
+            umma_commit(bar(B_Y));
+            mbar_drain(bar(B_Y), 0);  // every MMA of this CTA has completed
+        }
+    } else {
+        // ------------------------------------------------------------ epilogue (warps 0-3)
+        const int row = warp * 32 + lane;     // TMEM lane = accumulator row
+        const int q = row & 63;               // q (T1/T2 rows) or b (Y rows)
+        const bool lo_half = row >= 64;
+        const uint32_t lane_addr = (uint32_t)(warp * 32) << 16;
+        volatile int* epi_ok = reinterpret_cast<volatile int*>(sm + OFF_MISC + 32);
+        // one thread waits, the 128 epilogue threads agree on the outcome
+        auto epi_wait = [&](int b, uint32_t parity) -> bool {
+            if (threadIdx.x == 0) *epi_ok = mbar_wait(bar(b), parity, abort_flag) ? 1 : 0;
+            epi_sync();
+            const bool r = *epi_ok != 0;
+            epi_sync();
+            if (r) fence_after();
+            return r;
+        };
+        // ck12 (transposed) staged once per CTA: cks[b * 64 + q] = ck12[b, q]
+        float* cks = reinterpret_cast<float*>(sm + OFF_CK);
+        for (int i = threadIdx.x; i < 64 * 64; i += 128) {
+            const int qq = i & 63, bb = i >> 6;
+            cks[i] = (qq < P.nbf5 && bb < P.nbf5) ? P.ck32t[qq + (size_t)P.nbf5 * bb] : 0.f;
+        }
+        epi_sync();
+        // exchange halves: xh receives the hi rows' columns 16..31, xl the lo rows' columns 0..15
+        float* xh = xs;
+        float* xl = xs + 64 * XH_STRIDE;
+        // T2 exchange: rows of 32 floats, 8 KB per side (the two fill A3 exactly)
+        float* x2h = xs;
+        float* x2l = xs + 64 * 32;
+        float* ts = reinterpret_cast<float*>(sm + OFF_TS);
+        // row q of cj12 restricted to this thread's half of the columns, kept in registers
+        float cjr[32];
+        {
+            const int coff = lo_half ? 32 : 0;
+#pragma unroll
+            for (int i = 0; i < 32; ++i)
+                cjr[i] = (q < P.nbf5 && coff + i < P.nbf5) ? __ldg(P.cj32 + q + (size_t)P.nbf5 * (coff + i)) : 0.f;
+        }
+        bool ok = true;
+        for (int li = 0; li < my_count && ok; ++li) {
+            const int l = blockIdx.x + li * G;
+            const uint32_t lph = (uint32_t)(li & 1);
+            // ---- T1 drain: tmp[m, q] = D1[q, m] + D1[64+q, m]; the hi-row thread finishes
+            // columns 0..15 of each 32-column chunk, the lo-row thread columns 16..31
+            if (!epi_wait(B_T1, lph)) { ok = false; break; }
+            auto drain_chunk = [&](const uint32_t (&r)[32], int c) {
+                float v[32];
+#pragma unroll
+                for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+                if (lo_half) {
+#pragma unroll
+                    for (int i = 0; i < 16; i += 4)
+                        *reinterpret_cast<float4*>(&xl[q * XH_STRIDE + i]) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 16; i += 4)
+                        *reinterpret_cast<float4*>(&xh[q * XH_STRIDE + i]) =
+                            make_float4(v[16 + i], v[17 + i], v[18 + i], v[19 + i]);
+                }
+                epi_sync();
+                if (lo_half) {
+#pragma unroll
+                    for (int i = 0; i < 16; i += 4) {
+                        const float4 w = *reinterpret_cast<const float4*>(&xh[q * XH_STRIDE + i]);
+                        v[16 + i] += w.x; v[17 + i] += w.y; v[18 + i] += w.z; v[19 + i] += w.w;
+                    }
+                    finish_tmp16<16>(P, sm, v, q, c, l);
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 16; i += 4) {
+                        const float4 w = *reinterpret_cast<const float4*>(&xl[q * XH_STRIDE + i]);
+                        v[i] += w.x; v[i + 1] += w.y; v[i + 2] += w.z; v[i + 3] += w.w;
+                    }
+                    finish_tmp16<0>(P, sm, v, q, c, l);
+                }
+                epi_sync();
+            };
+            {
+                // software pipeline: the TMEM load of the next chunk is in flight while the
+                // current one is exchanged, split and stored (ncol / 32 is even)
+                const int nch = ncol / 32;
+                uint32_t ra[32], rb[32];
+                tmem_issue32(R1 + lane_addr, ra);
+                for (int c = 0; c < nch; c += 2) {
+                    tmem_wait_ld();
+                    tmem_issue32(R1 + lane_addr + (c + 1) * 32, rb);
+                    drain_chunk(ra, c);
+                    tmem_wait_ld();
+                    if (c + 2 < nch) tmem_issue32(R1 + lane_addr + (c + 2) * 32, ra);
+                    drain_chunk(rb, c + 1);
+                }
+            }
+            fence_async_smem();
+            fence_before();
+            epi_sync();
+            if (threadIdx.x == 0) mbar_arrive(bar(B_A2));
+            if (P.mode == 1) continue;
+            // ---- T2 drain: b_pq[p, q] = sum of the four quadrants of D2[q | 64+q, p | 64+p]
+            if (!epi_wait(B_T2, lph)) { ok = false; break; }
+            // The hi-row thread of column q finishes b_pq[p, q] for p in [0, 32),
+            // the lo-row thread for p in [32, 64) (off = first p of the range).
+            float bq[32];
+            {
+                float a[32], b2[32], u[32];
+                tmem_ld32(R1 + lane_addr + 0, a);
+                tmem_ld32(R1 + lane_addr + 64, u);
+#pragma unroll
+                for (int i = 0; i < 32; ++i) a[i] += u[i];      // p in [0, 32)
+                tmem_ld32(R1 + lane_addr + 32, b2);
+                tmem_ld32(R1 + lane_addr + 96, u);
+#pragma unroll
+                for (int i = 0; i < 32; ++i) b2[i] += u[i];     // p in [32, 64)
+                // exchange: each side sends the range it does not finish (rows of 32
+                // floats, float4 index swizzled by q to spread the banks)
+                float* send = lo_half ? x2l : x2h;
+                const float* recv = lo_half ? x2h : x2l;
+#pragma unroll
+                for (int i4 = 0; i4 < 8; ++i4) {
+                    const int sw = (i4 ^ (q & 7)) * 4;
+                    float4 s4;
+                    if (lo_half) s4 = make_float4(a[i4 * 4], a[i4 * 4 + 1], a[i4 * 4 + 2], a[i4 * 4 + 3]);
+                    else s4 = make_float4(b2[i4 * 4], b2[i4 * 4 + 1], b2[i4 * 4 + 2], b2[i4 * 4 + 3]);
+                    *reinterpret_cast<float4*>(&send[q * 32 + sw]) = s4;
+                }
+                epi_sync();
+#pragma unroll
+                for (int i4 = 0; i4 < 8; ++i4) {
+                    const int sw = (i4 ^ (q & 7)) * 4;
+                    const float4 r4 = *reinterpret_cast<const float4*>(&recv[q * 32 + sw]);
+                    if (lo_half) {
+                        bq[i4 * 4] = b2[i4 * 4] + r4.x; bq[i4 * 4 + 1] = b2[i4 * 4 + 1] + r4.y;
+                        bq[i4 * 4 + 2] = b2[i4 * 4 + 2] + r4.z; bq[i4 * 4 + 3] = b2[i4 * 4 + 3] + r4.w;
+                    } else {
+                        bq[i4 * 4] = a[i4 * 4] + r4.x; bq[i4 * 4 + 1] = a[i4 * 4 + 1] + r4.y;
+                        bq[i4 * 4 + 2] = a[i4 * 4 + 2] + r4.z; bq[i4 * 4 + 3] = a[i4 * 4 + 3] + r4.w;
+                    }
+                }
+            }
+            // R1 is free again once every thread's loads are done
+            fence_before();
+            const int off = lo_half ? 32 : 0;
+            const bool own_diag = (q >= off) && (q < off + 32);   // this thread holds b_pq[q, q]
+            {
+                float dq = 0.f;
+#pragma unroll
+                for (int i = 0; i < 32; ++i)
+                    if (off + i == q) dq = bq[i];
+                if (own_diag) {
+                    if (q >= P.nbf5) dq = 0.f;
+                    ds[q] = dq;
+                    if (q < P.nbf5 && P.mode == 2) P.d_out[q + (size_t)P.nbf5 * l] = dq;
+                }
+                if (q < P.nbf5 && P.mode == 2) {   // J/K ingredients are only needed by JKH_MO
+                    if (P.mode == 2) {
+                        float* dst = P.bpq_out + (size_t)P.nbf5 * P.nbf5 * l + (size_t)P.nbf5 * q + off;
+#pragma unroll
+                        for (int i = 0; i < 32; ++i)
+                            if (off + i < P.nbf5) dst[i] = bq[i];
+                    }
+                    // K_MO partial sums of this CTA, stored transposed (kp[q + nbf5*p]) so that
+                    // the reductions of a warp are coalesced; each address has one writer
+                    float* kp = P.k_part + (size_t)blockIdx.x * P.nbf5 * P.nbf5 + q;
+#pragma unroll
+                    for (int i = 0; i < 32; ++i)
+                        if (off + i < P.nbf5) atomicAdd(kp + (size_t)P.nbf5 * (off + i), bq[i] * bq[i]);
+                }
+            }
+            epi_sync();
+            if (P.mode != 2) {
+                // W[q, b] = delta_qb (n'_q d_q + t_q) - ck12[b, q] b_pq[b, q],  t_q = sum_q' cj12[q, q'] d_q'
+                float tpart = 0.f;
+#pragma unroll
+                for (int i = 0; i < 32; ++i) tpart += cjr[i] * ds[off + i];
+                ts[row] = tpart;
+                epi_sync();
+                float diag = 0.f;
+                if (own_diag && q < P.nbf5) {
+                    const float t = ts[q] + ts[64 + q];
+                    const bool dj = (P.nbeta > 0) && (q < P.nbeta || q >= P.nalpha);
+                    diag = (dj ? P.n32[q] * ds[q] : 0.f) + t;
+                }
+                // A3 row b (hi) / 64+b (lo), K = q, for b in this thread's range
+#pragma unroll
+                for (int i = 0; i < 32; ++i) {
+                    const int b = off + i;
+                    float w = 0.f;
+                    if (q < P.nbf5 && b < P.nbf5) w = -cks[b * 64 + q] * bq[i] + (b == q ? diag : 0.f);
+                    __nv_bfloat16 h, lo;
+                    split_bf16(w, h, lo);
+                    *reinterpret_cast<__nv_bfloat16*>(sm + OFF_A3 + sw128(b, q)) = h;
+                    *reinterpret_cast<__nv_bfloat16*>(sm + OFF_A3 + sw128(64 + b, q)) = lo;
+                }
+            }
+            fence_async_smem();
+            fence_before();
+            epi_sync();
+            if (threadIdx.x == 0) mbar_arrive(bar(B_A3));
+        }
+        // ---- final: Y partial (mode 3) and K partial
+        if (ok && my_count > 0 && P.mode == 3) {
+            if (epi_wait(B_Y, 0)) {
+                for (int c = 0; c < ncol / 32; ++c) {
+                    float v[32];
+                    tmem_ld32(R2 + lane_addr + c * 32, v);
+                    if (lo_half) {
+#pragma unroll
+                        for (int i = 0; i < 32; i += 4)
+                            *reinterpret_cast<float4*>(&xs[q * XS_STRIDE + i]) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+                    }
+                    epi_sync();
+                    if (!lo_half && q < P.nbf5) {
+                        float* dst = P.y_part + (size_t)blockIdx.x * P.nbf * P.nbf5 + (size_t)P.nbf * q + c * 32;
+                        for (int i = 0; i < 32; ++i)
+                            if (c * 32 + i < P.nbf) dst[i] = v[i] + xs[q * XS_STRIDE + i];
+                    }
+                    epi_sync();
+                }
+            }
+        }
+    }
+
+    fence_before();
+    __syncthreads();
+    if (threadIdx.x == 0 && *abort_flag) atomicExch(P.status, 1);
+    if (warp == 5) {
+        fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem));
+    }
+}
+
+// ---------------------------------------------------------------- helpers
+__global__ void split_b_kernel(const double* __restrict__ b, int nbf, int ldm, long long nl,
+                               __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo) {
+    // nl = nbf * naux columns (n, l) of length nbf (m)
+    const long long total = (long long)ldm * nl;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int m = (int)(i % ldm);
+        const long long col = i / ldm;
+        double v = (m < nbf) ? b[m + (long long)nbf * col] : 0.0;
+        const __nv_bfloat16 h = __double2bfloat16(v);
+        const __nv_bfloat16 l = __double2bfloat16(v - (double)__bfloat162float(h));
+        hi[i] = h;
+        lo[i] = l;
+    }
+}
+
+// Cs[k + ldk*j], j < 64: C_hi[k, j]; 64 <= j < 128: C_lo[k, j-64]; zero beyond nbf5 / nbf.
+__global__ void split_c_kernel(const double* __restrict__ C, int nbf, int nbf5, int ldk,
+                               __nv_bfloat16* __restrict__ cs) {
+    const int total = ldk * 128;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        const int k = i % ldk, j = i / ldk;
+        const int q = j & 63;
+        double v = (k < nbf && q < nbf5) ? C[k + (long long)nbf * q] : 0.0;
+        const __nv_bfloat16 h = __double2bfloat16(v);
+        cs[i] = (j < 64) ? h : __double2bfloat16(v - (double)__bfloat162float(h));
+    }
+}
+
+// out[j + n*i] = a[i + n*j] (n x n transpose to FP32)
+__global__ void to_f32_transpose(const double* __restrict__ a, int n, float* __restrict__ out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n * n; i += gridDim.x * blockDim.x) {
+        const int r = i % n, c = i / n;
+        out[c + n * r] = (float)a[i];
+    }
+}
+
+__global__ void to_f32_small(const double* __restrict__ a, int count, float* __restrict__ out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) out[i] = (float)a[i];
+}
+
+// out[i] = sum_g part[g*stride + i] in FP64
+__global__ void reduce_f32_to_f64(const float* __restrict__ part, long long stride, int parts, long long count,
+                                  double* __restrict__ out) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
+         i += (long long)gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int g = 0; g < parts; ++g) s += (double)part[i + g * stride];
+        out[i] = s;
+    }
+}
+
+// Same for an n x n matrix stored transposed in the partials: out[c + n*r] = sum_g part[r + n*c + g*stride]
+__global__ void reduce_f32_to_f64_t(const float* __restrict__ part, long long stride, int parts, int n,
+                                    double* __restrict__ out) {
+    const long long count = (long long)n * n;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
+         i += (long long)gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int g = 0; g < parts; ++g) s += (double)part[i + g * stride];
+        const long long r = i % n, c = i / n;
+        out[c + n * r] = s;
+    }
+}
+
+__global__ void f32_to_f64(const float* __restrict__ a, long long count, double* __restrict__ out) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
          i += (long long)gridDim.x * blockDim.x)
-        out[i] = (float)in[i];
+        out[i] = (double)a[i];
+}
+
+}  // namespace mx
+
+namespace {
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+int make_map(donof_ctx* ctx, CUtensorMap* map, const void* base, int rank, const cuuint64_t* dims,
+             const cuuint64_t* strides_bytes, const cuuint32_t* box) {
+    auto fn = encode_fn();
+    if (!fn) {
+        set_error(ctx, "cuTensorMapEncodeTiled is not available");
+        return DONOF_ERR_CUDA;
+    }
+    cuuint32_t es[3] = {1, 1, 1};
+    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, rank, const_cast<void*>(base), dims, strides_bytes, box, es,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error(ctx, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+        return DONOF_ERR_CUDA;
+    }
+    return DONOF_OK;
+}
+
+int ldm_of(int nbf) { return (nbf + 7) / 8 * 8; }
+
+bool mixed_shape_ok(int nbf, int nbf5) { return nbf >= 1 && nbf <= 256 && nbf5 >= 1 && nbf5 <= 64; }
+
+// Scratch of the mixed form inside the job: [status | Cs | n32 | cj32 | ck32 | d | y_part | k_part | tmp/bpq out]
+struct MixedScratch {
+    int* status;
+    __nv_bfloat16* cs;
+    float *n32, *cj32, *ck32, *d, *ypart, *kpart;
+    double *Y, *Kd, *dd;
+};
+
+int mixed_prepare(donof_job* job, cudaStream_t st, const double* C, int nbf5, MixedScratch* S, int grid) {
+    donof_ctx* ctx = job->ctx;
+    const int nbf = job->nbf, naux = job->naux;
+    const int ldk = ldm_of(nbf);
+    size_t off = 0;
+    auto take = [&](size_t bytes) { size_t o = off; off += (bytes + 255) / 256 * 256; return o; };
+    const size_t o_status = take(sizeof(int) * 4);
+    const size_t o_cs = take(sizeof(__nv_bfloat16) * (size_t)ldk * 128);
+    const size_t o_n = take(sizeof(float) * 64);
+    const size_t o_cj = take(sizeof(float) * 64 * 64);
+    const size_t o_ck = take(sizeof(float) * 64 * 64);
+    const size_t o_d = take(sizeof(float) * (size_t)nbf5 * naux);
+    const size_t o_y = take(sizeof(float) * (size_t)grid * nbf * nbf5);
+    const size_t o_k = take(sizeof(float) * (size_t)grid * nbf5 * nbf5);
+    const size_t o_Y = take(sizeof(double) * (size_t)nbf * nbf5);
+    const size_t o_K = take(sizeof(double) * (size_t)nbf5 * nbf5);
+    const size_t o_dd = take(sizeof(double) * (size_t)nbf5 * naux);
+    DONOF_CHECK(job->W.ensure(ctx, off));  // the FP64 form's W buffer doubles as the mixed scratch
+    char* base = job->W.as<char>();
+    S->status = reinterpret_cast<int*>(base + o_status);
+    S->cs = reinterpret_cast<__nv_bfloat16*>(base + o_cs);
+    S->n32 = reinterpret_cast<float*>(base + o_n);
+    S->cj32 = reinterpret_cast<float*>(base + o_cj);
+    S->ck32 = reinterpret_cast<float*>(base + o_ck);
+    S->d = reinterpret_cast<float*>(base + o_d);
+    S->ypart = reinterpret_cast<float*>(base + o_y);
+    S->kpart = reinterpret_cast<float*>(base + o_k);
+    S->Y = reinterpret_cast<double*>(base + o_Y);
+    S->Kd = reinterpret_cast<double*>(base + o_K);
+    S->dd = reinterpret_cast<double*>(base + o_dd);
+    DONOF_CUDA(ctx, cudaMemsetAsync(S->status, 0, sizeof(int) * 4, st));
+    // the kernel accumulates its K_MO partial sums into these
+    DONOF_CUDA(ctx, cudaMemsetAsync(S->kpart, 0, sizeof(float) * (size_t)grid * nbf5 * nbf5, st));
+    mx::split_c_kernel<<<(ldk * 128 + 255) / 256, 256, 0, st>>>(C, nbf, nbf5, ldk, S->cs); count_launch();
+    DONOF_CUDA(ctx, cudaGetLastError());
+    return DONOF_OK;
+}
+
+int launch_mixed(donof_job* job, cudaStream_t st, int nbf5, int nalpha, int nbeta, int mode, const MixedScratch& S,
+                 float* tmp_out, float* bpq_out, int grid) {
+    donof_ctx* ctx = job->ctx;
+    const int nbf = job->nbf, naux = job->naux;
+    const int ldm = ldm_of(nbf);
+    CUtensorMap mhi, mlo, mcs;
+    {
+        cuuint64_t dims[3] = {(cuuint64_t)nbf, (cuuint64_t)nbf, (cuuint64_t)naux};
+        cuuint64_t strides[2] = {(cuuint64_t)ldm * 2, (cuuint64_t)ldm * nbf * 2};
+        cuuint32_t box[3] = {mx::BOX_M, mx::KB, 1};
+        DONOF_CHECK(make_map(ctx, &mhi, job->b16hi, 3, dims, strides, box));
+        DONOF_CHECK(make_map(ctx, &mlo, job->b16lo, 3, dims, strides, box));
+    }
+    {
+        cuuint64_t dims[2] = {(cuuint64_t)nbf, 128};
+        cuuint64_t strides[1] = {(cuuint64_t)ldm * 2};
+        cuuint32_t box[2] = {64, 128};
+        DONOF_CHECK(make_map(ctx, &mcs, S.cs, 2, dims, strides, box));
+    }
+    mx::Params P{};
+    P.nbf = nbf; P.nbf5 = nbf5; P.naux = naux; P.nalpha = nalpha; P.nbeta = nbeta;
+    P.nb = (nbf + 63) / 64;
+    P.nkb = (nbf + mx::KB - 1) / mx::KB;
+    P.ncs = (nbf + 63) / 64;
+    P.mode = mode;
+    P.n32 = S.n32; P.cj32 = S.cj32; P.ck32t = S.ck32;
+    P.tmp_out = tmp_out; P.bpq_out = bpq_out; P.d_out = S.d; P.y_part = S.ypart; P.k_part = S.kpart;
+    P.status = S.status;
+    static unsigned long long attr_mask = 0;
+    const unsigned long long bit = 1ull << (ctx->device & 63);
+    if (!(attr_mask & bit)) {
+        DONOF_CUDA(ctx, cudaFuncSetAttribute(mx::lag_mixed_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             mx::SMEM_ALLOC));
+        attr_mask |= bit;
+    }
+    prof_begin(ctx, st);
+    mx::lag_mixed_kernel<<<grid, mx::NTHREADS, mx::SMEM_ALLOC, st>>>(mhi, mlo, mcs, P); count_launch();
+    prof_end(ctx, st);
+    DONOF_CUDA(ctx, cudaGetLastError());
+    return DONOF_OK;
+}
+
+int mixed_grid(donof_job* job) { return job->naux < job->ctx->sm_count ? job->naux : job->ctx->sm_count; }
+
+int check_mixed(donof_job* job, int nbf5) {
+    if (job->b16hi == nullptr) {
+        set_error(job->ctx, "mixed precision requested but the job holds no bf16 split of b");
+        return DONOF_ERR_ARG;
+    }
+    if (!mixed_shape_ok(job->nbf, nbf5)) {
+        set_error(job->ctx, "the mixed-precision kernel supports nbf <= 256 and nbf5 <= 64 (got nbf=%d nbf5=%d)",
+                  job->nbf, nbf5);
+        return DONOF_ERR_ARG;
+    }
+    return DONOF_OK;
+}
+
+int read_status(donof_job* job, cudaStream_t st, const MixedScratch& S) {
+    (void)job; (void)st; (void)S;
+    return DONOF_OK;
 }
 
 }  // namespace
 
 int convert_b_f32(donof_job* job) {
+    // b split into bf16 hi + lo (the mixed form's copy of b)
     donof_ctx* ctx = job->ctx;
-    const long long count = (long long)job->nbf * job->nbf * job->naux;
-    void* d = nullptr;
-    DONOF_CUDA(ctx, cudaMalloc(&d, sizeof(float) * (size_t)count));
-    to_f32_kernel<<<8 * ctx->sm_count, 256, 0, ctx->stream>>>(job->b, count, static_cast<float*>(d)); count_launch();
-    cudaError_t e = cudaGetLastError();
+    const int nbf = job->nbf, ldm = ldm_of(nbf);
+    const size_t count = (size_t)ldm * nbf * job->naux;
+    void* hi = nullptr;
+    void* lo = nullptr;
+    DONOF_CUDA(ctx, cudaMalloc(&hi, sizeof(__nv_bfloat16) * count));
+    cudaError_t e = cudaMalloc(&lo, sizeof(__nv_bfloat16) * count);
+    if (e != cudaSuccess) {
+        cudaFree(hi);
+        set_error(ctx, "cudaMalloc(b split): %s", cudaGetErrorString(e));
+        return DONOF_ERR_OOM;
+    }
+    mx::split_b_kernel<<<8 * ctx->sm_count, 256, 0, ctx->stream>>>(job->b, nbf, ldm, (long long)nbf * job->naux,
+                                                                   static_cast<__nv_bfloat16*>(hi),
+                                                                   static_cast<__nv_bfloat16*>(lo)); count_launch();
+    e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) {
-        cudaFree(d);
-        set_error(ctx, "FP32 conversion of b: %s", cudaGetErrorString(e));
+        cudaFree(hi);
+        cudaFree(lo);
+        set_error(ctx, "bf16 split of b: %s", cudaGetErrorString(e));
         return DONOF_ERR_CUDA;
     }
-    job->b32 = static_cast<const float*>(d);
-    job->own_b32 = true;
+    job->b16hi = hi;
+    job->b16lo = lo;
     return DONOF_OK;
 }
 
-int transforms_mixed(donof_job* job, cudaStream_t, const double*, int) {
-    set_error(job->ctx, "mixed-precision transform not available in this build");
-    return DONOF_ERR_STATE;
+int transforms_mixed(donof_job* job, cudaStream_t st, const double* C, int nbf5) {
+    DONOF_CHECK(check_mixed(job, nbf5));
+    donof_ctx* ctx = job->ctx;
+    const int nbf = job->nbf, naux = job->naux, grid = mixed_grid(job);
+    MixedScratch S;
+    DONOF_CHECK(mixed_prepare(job, st, C, nbf5, &S, grid));
+    DONOF_CHECK(job->tmp.ensure(ctx, sizeof(float) * (size_t)nbf5 * nbf5 * naux));
+    float* bpq32 = job->tmp.as<float>();
+    DONOF_CHECK(launch_mixed(job, st, nbf5, nbf5, nbf5, 2, S, nullptr, bpq32, grid));
+    DONOF_CHECK(job->bpq.ensure(ctx, sizeof(double) * (size_t)nbf5 * nbf5 * naux));
+    const long long cnt = (long long)nbf5 * nbf5 * naux;
+    mx::f32_to_f64<<<4 * ctx->sm_count, 256, 0, st>>>(bpq32, cnt, job->bpq.as<double>()); count_launch();
+    DONOF_CUDA(ctx, cudaGetLastError());
+    return DONOF_OK;
 }
 
-int lagrange2_mixed(donof_job* job, cudaStream_t, const double*, const double*, const double*,
-                    const double*, const double*, int, int, int, double*, double*, double*) {
-    set_error(job->ctx, "mixed-precision Lagrangian not available in this build");
-    return DONOF_ERR_STATE;
+int mixed_t1_debug(donof_job* job, cudaStream_t st, const double* C, int nbf5, float* tmp_out) {
+    DONOF_CHECK(check_mixed(job, nbf5));
+    const int grid = mixed_grid(job);
+    MixedScratch S;
+    DONOF_CHECK(mixed_prepare(job, st, C, nbf5, &S, grid));
+    return launch_mixed(job, st, nbf5, nbf5, nbf5, 1, S, tmp_out, nullptr, grid);
 }
 
-int jkh_mo_mixed(donof_job* job, cudaStream_t, const double*, const double*, int, double*, double*,
-                 double*) {
-    set_error(job->ctx, "mixed-precision JKH_MO not available in this build");
-    return DONOF_ERR_STATE;
+int mixed_status(donof_job* job, int* out) {
+    if (job->W.ptr == nullptr) { *out = 0; return DONOF_OK; }
+    DONOF_CUDA(job->ctx, cudaMemcpy(out, job->W.ptr, sizeof(int), cudaMemcpyDeviceToHost));
+    return DONOF_OK;
+}
+
+int lagrange2_mixed(donof_job* job, cudaStream_t st, const double* C, const double* n, const double* H,
+                    const double* cj12, const double* ck12, int nbf5, int nalpha, int nbeta, double* elag,
+                    double* Hmat, double* E) {
+    DONOF_CHECK(check_mixed(job, nbf5));
+    donof_ctx* ctx = job->ctx;
+    const int nbf = job->nbf, grid = mixed_grid(job);
+    MixedScratch S;
+    DONOF_CHECK(mixed_prepare(job, st, C, nbf5, &S, grid));
+    mx::to_f32_small<<<1, 256, 0, st>>>(n, nbf5, S.n32); count_launch();
+    mx::to_f32_small<<<16, 256, 0, st>>>(cj12, nbf5 * nbf5, S.cj32); count_launch();
+    mx::to_f32_transpose<<<16, 256, 0, st>>>(ck12, nbf5, S.ck32); count_launch();
+    DONOF_CUDA(ctx, cudaGetLastError());
+    DONOF_CHECK(launch_mixed(job, st, nbf5, nalpha, nbeta, 3, S, nullptr, nullptr, grid));
+    // Y (FP64) = sum over CTAs of the FP32 partials
+    const long long ny = (long long)nbf * nbf5;
+    mx::reduce_f32_to_f64<<<(int)((ny + 255) / 256), 256, 0, st>>>(S.ypart, ny, grid, ny, S.Y); count_launch();
+    DONOF_CUDA(ctx, cudaGetLastError());
+    // H_mat = C^T (H C5) and elag = n o H_mat + C^T Y in FP64
+    DONOF_CHECK(job->small.ensure(ctx, sizeof(double) * (size_t)nbf * nbf5 * 2));
+    double* HC = job->small.as<double>();
+    DONOF_CHECK(gemm_f64_auto(ctx, st, false, true, nbf, nbf5, nbf, H, nbf, C, nbf, HC, nbf, 1.0, 0.0, &job->part));
+    DONOF_CHECK(gemm_f64_auto(ctx, st, true, true, nbf, nbf5, nbf, C, nbf, HC, nbf, Hmat, nbf, 1.0, 0.0, &job->part));
+    DONOF_CHECK(elag_finish_f64(job, st, C, n, Hmat, S.Y, nbf5, elag, E));
+    return DONOF_OK;
+}
+
+int jkh_mo_mixed(donof_job* job, cudaStream_t st, const double* C, const double* H, int nbf5, double* J, double* K,
+                 double* Hcore) {
+    DONOF_CHECK(check_mixed(job, nbf5));
+    donof_ctx* ctx = job->ctx;
+    const int nbf = job->nbf, naux = job->naux, grid = mixed_grid(job);
+    MixedScratch S;
+    DONOF_CHECK(mixed_prepare(job, st, C, nbf5, &S, grid));
+    // mode 2 also emits d and the K partials; b_pq itself goes to a scratch
+    DONOF_CHECK(job->tmp.ensure(ctx, sizeof(float) * (size_t)nbf5 * nbf5 * naux));
+    DONOF_CHECK(launch_mixed(job, st, nbf5, nbf5, nbf5, 2, S, nullptr, job->tmp.as<float>(), grid));
+    const long long n55 = (long long)nbf5 * nbf5;
+    mx::reduce_f32_to_f64_t<<<(int)((n55 + 255) / 256), 256, 0, st>>>(S.kpart, n55, grid, nbf5, K); count_launch();
+    // J = D D^T with D[p, l] = d_p^l (FP64 GEMM on the FP32 diagonals)
+    const long long nd = (long long)nbf5 * naux;
+    mx::f32_to_f64<<<4 * ctx->sm_count, 256, 0, st>>>(S.d, nd, S.dd); count_launch();
+    DONOF_CUDA(ctx, cudaGetLastError());
+    DONOF_CHECK(gemm_f64_auto(ctx, st, false, false, nbf5, nbf5, naux, S.dd, nbf5, S.dd, nbf5, J, nbf5, 1.0, 0.0,
+                              &job->part));
+    DONOF_CHECK(job->small.ensure(ctx, sizeof(double) * (size_t)nbf * nbf5 * 2));
+    double* HC = job->small.as<double>();
+    DONOF_CHECK(gemm_f64_auto(ctx, st, false, true, nbf, nbf5, nbf, H, nbf, C, nbf, HC, nbf, 1.0, 0.0, nullptr));
+    DONOF_CHECK(hcore_f64(job, st, C, HC, nbf5, Hcore));
+    return DONOF_OK;
 }
 
 }  // namespace donof

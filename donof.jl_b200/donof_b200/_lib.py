@@ -61,6 +61,10 @@ SIGNATURES = {
                               _ip, _ip]),
     "donof_transform_dev": (_i, [_vp, _i, _vp, _i, _vp]),
     "donof_launch_count": (ct.c_ulonglong, []),
+    "donof_job_error_flag": (_i, [_vp, _ip]),
+    "donof_profile_enable": (_i, [_vp, _i]),
+    "donof_profile_last_ms": (_i, [_vp, ct.POINTER(ct.c_float)]),
+    "donof_mixed_tmp_dev": (_i, [_vp, _vp, _i, _vp]),
     "donof_orbopt": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _i, _i, _i, _dp, _ip, ct.c_double, _vp, _dp,
                           _ip, _ip]),
 }

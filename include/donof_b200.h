@@ -175,6 +175,19 @@ int donof_orbopt_dev(donof_job* job, int method, const double* n, const double* 
 /* --- diagnostics -------------------------------------------------------------
  * Number of CUDA kernels this library has launched in the process so far.    */
 unsigned long long donof_launch_count(void);
+/* With profiling enabled, each call brackets its dominant kernel (the first
+ * three-index transform of the FP64 form, the fused tensor-core kernel of the
+ * mixed form) with CUDA events on the context stream; donof_profile_last_ms
+ * waits for and returns the duration of the most recent one.                 */
+int donof_profile_enable(donof_ctx* ctx, int enable);
+int donof_profile_last_ms(donof_ctx* ctx, float* ms);
+/* Reads (synchronising the context stream) the job's device error flag: 1 if
+ * a mixed-precision kernel gave up on a bounded wait since the last call that
+ * reset it (each mixed-precision call resets it).                            */
+int donof_job_error_flag(donof_job* job, int* flag);
+/* First contraction of the mixed form alone, for checking it:
+ * tmp[m + nbf*q + nbf*nbf5*l] = sum_n b[m,n,l] C[n,q] (FP32, device).        */
+int donof_mixed_tmp_dev(donof_job* job, const double* C, int nbf5, float* tmp);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

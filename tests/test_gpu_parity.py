@@ -183,5 +183,5 @@ def test_invalid_arguments_raise(cuda_ctx):
     hm = np.zeros((p.nbf, p.nbf5), order="F")
     with pytest.raises(_lib.DonofError) as e:  # mixed form needs a job uploaded for it
         d.compute_Lagrange2_dev(C, n, H, bt, cj, ck, p.nalpha, p.nbeta, out, hm, precision="mixed")
-    assert e.value.status == _lib.ERR_ARG and "FP32" in str(e.value)
+    assert e.value.status == _lib.ERR_ARG and "bf16 split" in str(e.value)
     bt.free()
