@@ -346,6 +346,14 @@ int donof_job_free(donof_job* job) {
     return DONOF_OK;
 }
 
+int donof_job_set_precision(donof_job* job, int precision) {
+    if (!job) return DONOF_ERR_ARG;
+    const int prec = effective_precision(job, precision);
+    if (prec < 0) return DONOF_ERR_ARG;
+    job->precision = prec;
+    return DONOF_OK;
+}
+
 size_t donof_job_device_bytes(const donof_job* job) {
     if (!job) return 0;
     size_t s = job->tmp.bytes + job->bpq.bytes + job->W.bytes + job->part.bytes + job->small.bytes +

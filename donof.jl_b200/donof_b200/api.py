@@ -77,9 +77,19 @@ class Context:
         self.check(self.lib.donof_synchronize(self.handle))
 
     def close(self) -> None:
+        """Free every job of this context, then the context itself (a job must
+        never outlive its context: the library dereferences it on free)."""
         if getattr(self, "handle", None):
+            for job in list(getattr(self, "_jobs", ())):
+                job.free()
             self.lib.donof_destroy(self.handle)
             self.handle = None
+
+    def _register(self, job) -> None:
+        if not hasattr(self, "_jobs"):
+            import weakref
+            self._jobs = weakref.WeakSet()
+        self._jobs.add(job)
 
     def __del__(self):  # pragma: no cover
         try:
@@ -105,18 +115,27 @@ class BTensor:
     def __init__(self, ctx: Context, handle, nbf: int, naux: int, precision: int, keep=None):
         self.ctx, self.handle, self.nbf, self.naux, self.precision = ctx, handle, nbf, naux, precision
         self._keep = keep  # keeps an attached device tensor alive
+        ctx._register(self)
 
     @property
     def shape(self):
         return (self.nbf, self.nbf, self.naux)
 
+    def set_precision(self, precision) -> None:
+        """Switch the precision of the calls that take none explicitly ("fp64" is
+        always allowed; "mixed" needs a job uploaded as mixed)."""
+        prec = _prec(precision)
+        self.ctx.check(self.ctx.lib.donof_job_set_precision(self.handle, prec))
+        self.precision = prec
+
     def device_bytes(self) -> int:
         return int(self.ctx.lib.donof_job_device_bytes(self.handle))
 
     def free(self) -> None:
-        if self.handle:
+        # the context frees its jobs before it is destroyed; after that the handle is gone
+        if self.handle and getattr(self.ctx, "handle", None):
             self.ctx.lib.donof_job_free(self.handle)
-            self.handle = None
+        self.handle = None
 
     def __del__(self):  # pragma: no cover
         try:

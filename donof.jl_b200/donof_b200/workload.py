@@ -58,6 +58,31 @@ def synthetic(nbf: int = 256, naux: int = 1024, nbeta: int = 16, ncwo: int = 3, 
     return Workload(p, b, C, H, gamma, n, np.asfortranarray(cj12), np.asfortranarray(ck12))
 
 
+def molecule_like(nbf: int = 256, naux: int = 1024, nbeta: int = 16, ncwo: int = 3, seed: int = 1234,
+                  two_e_scale: float = 0.5, occ_method: str = "Softmax", **param_kw) -> Workload:
+    """Seeded inputs with a molecule-like energy landscape for full optimisations:
+    H = Q diag(eps) Q^T with nbeta bound levels in [-3, -0.8] Eh and the rest in
+    [0.1, 2.5] Eh, b ~ N(0, two_e_scale/sqrt(naux)) symmetrised (a two-electron part
+    weaker than the one-electron one), starting orbitals close to those of H, and
+    the reference's initial gamma (src/guess.jl:200-213).  The purely random
+    workload of ``synthetic`` has an occupation landscape with several stationary
+    points, which makes converged energies depend on the optimiser's path."""
+    rng = np.random.default_rng(seed)
+    p = Param(nbf=nbf, nbfaux=naux, nalpha=nbeta, nbeta=nbeta, ncwo=ncwo, occ_method=occ_method, **param_kw)
+    Q, _ = np.linalg.qr(rng.standard_normal((nbf, nbf)))
+    eps = np.sort(np.concatenate([-np.linspace(3.0, 0.8, nbeta), np.linspace(0.1, 2.5, nbf - nbeta)]))
+    H = np.asfortranarray((Q * eps) @ Q.T)
+    raw = rng.standard_normal((naux, nbf, nbf)) * (two_e_scale / np.sqrt(naux))
+    raw += raw.transpose(0, 2, 1)
+    raw *= 0.5
+    b = raw.T
+    C = np.asfortranarray(np.linalg.qr(Q + 0.05 * rng.standard_normal((nbf, nbf)))[0])
+    gamma = gnof.guess_gamma(p)
+    n, _ = gnof.occupations(gamma, p)
+    cj12, ck12 = gnof.coupling(n, p)
+    return Workload(p, b, C, H, gamma, n, np.asfortranarray(cj12), np.asfortranarray(ck12))
+
+
 # Named workloads (sizes of the molecule-shaped surrogates: nbf, naux, nbeta, ncwo)
 CONFIGS = {
     "water-ccpvdz-surrogate": dict(nbf=24, naux=116, nbeta=5, ncwo=3),

@@ -78,6 +78,10 @@ int donof_b_upload(donof_ctx* ctx, const double* b_host, int nbf, int naux, int 
 int donof_b_attach(donof_ctx* ctx, const double* b_dev, int nbf, int naux, int precision,
                    donof_job** job);
 int donof_job_free(donof_job* job);
+/* Precision used by the calls without an explicit one (DONOF_PREC_MIXED needs
+ * a job created with DONOF_PREC_MIXED; switching to FP64 is always allowed,
+ * e.g. for the closing refinement iterations of a mixed-precision run).      */
+int donof_job_set_precision(donof_job* job, int precision);
 /* device bytes held by the job (b copies + scratch) */
 size_t donof_job_device_bytes(const donof_job* job);
 
