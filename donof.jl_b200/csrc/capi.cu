@@ -13,6 +13,9 @@ static thread_local std::string g_tls_error;
 static std::atomic<unsigned long long> g_launches{0};
 
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void g_launch_adjust(long long delta) {
+    g_launches.fetch_add((unsigned long long)delta, std::memory_order_relaxed);
+}
 
 void set_error(donof_ctx* ctx, const char* fmt, ...) {
     char buf[1024];
@@ -31,6 +34,7 @@ int DevBuf::ensure(donof_ctx* ctx, size_t want) {
         ptr = nullptr;
         bytes = 0;
     }
+    ++gen;
     if (want == 0) want = 256;
     cudaError_t e = cudaMalloc(&ptr, want);
     if (e != cudaSuccess) {
@@ -231,6 +235,7 @@ int donof_destroy(donof_ctx* ctx) {
     ctx->stage_out.release();
     ctx->rot.release();
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+    if (ctx->aux_stream) cudaStreamDestroy(ctx->aux_stream);
     if (ctx->prof_ev[0]) cudaEventDestroy(ctx->prof_ev[0]);
     if (ctx->prof_ev[1]) cudaEventDestroy(ctx->prof_ev[1]);
     delete ctx;
@@ -341,6 +346,8 @@ int donof_job_free(donof_job* job) {
     job->part.release();
     job->small.release();
     job->orb.release();
+    if (job->orb_exec) cudaGraphExecDestroy(job->orb_exec);
+    if (job->orb_graph) cudaGraphDestroy(job->orb_graph);
     job->io.release();
     delete job;
     return DONOF_OK;

@@ -11,8 +11,10 @@
 namespace donof {
 
 // Count of kernel launches made by the library (diagnostics; see
-// donof_launch_count).  Every launch site calls count_launch().
+// donof_launch_count).  Every launch site calls count_launch(); graph
+// replays add their kernel count through g_launch_adjust.
 void count_launch();
+void g_launch_adjust(long long delta);
 
 // Last error text is kept per context (and in a thread-local fallback for
 // calls that fail before a context exists).
@@ -39,6 +41,7 @@ void set_error(donof_ctx* ctx, const char* fmt, ...);
 struct DevBuf {
     void* ptr = nullptr;
     size_t bytes = 0;
+    unsigned gen = 0;  // bumped on every reallocation (captured graphs check it)
     int ensure(donof_ctx* ctx, size_t want);
     void release();
     template <class T>
@@ -62,6 +65,8 @@ struct donof_ctx {
     bool profile = false;
     cudaEvent_t prof_ev[2] = {nullptr, nullptr};
     bool prof_recorded = false;
+    // private stream for graph capture when the context uses the legacy default stream
+    cudaStream_t aux_stream = nullptr;
 };
 
 namespace donof {
@@ -92,4 +97,10 @@ struct donof_job {
     donof::DevBuf orb;
     // host-API staging
     donof::DevBuf io;
+    // captured optimiser loop (graph with a conditional WHILE node) and the
+    // inputs it was captured for
+    cudaGraph_t orb_graph = nullptr;
+    cudaGraphExec_t orb_exec = nullptr;
+    unsigned long long orb_key[10] = {};
+    int orb_per_iter = 0;
 };

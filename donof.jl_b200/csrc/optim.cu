@@ -99,12 +99,258 @@ int pack_grad(donof_ctx* ctx, cudaStream_t st, const double* elag, int nbf, int 
     return DONOF_OK;
 }
 
-// Device-resident optimiser loop; the host only reads one 16-byte status
-// (E, max|g|) per iteration to take the reference's branch decisions.
+// ---------------------------------------------------------------------------
+// Graph form of the optimiser loop: one CUDA graph whose conditional WHILE
+// node repeats the iteration body (update, rotation, Lagrangian, gradient,
+// best-E bookkeeping) on the device; the body's last kernel evaluates the
+// reference's stopping rule and clears the loop condition.  The host launches
+// the graph once per orbopt call and reads the final state once.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct OrbState {
+    double E, bestE, alpha, thresh;
+    unsigned long long gmax_bits;  // max|g| of the latest gradient, as the bits of a non-negative double
+    int it, maxloop, method, improved, improved_now, success, nit, pad;
+};
+
+// update of the AMSGrad family with the iteration count and step size read
+// from the device state (src/minimization.jl:307-316, 406-411, 503-508, 598-603)
+__global__ void orb_update_kernel(const OrbState* __restrict__ s, long long nvar, const double* __restrict__ g,
+                                  double* __restrict__ m, double* __restrict__ v, double* __restrict__ vmax,
+                                  double* __restrict__ y) {
+    const int i = s->it + 1;
+    const int method = s->method;
+    double beta1 = (method == DONOF_ORB_DEMON) ? 0.6 : 0.5;
+    const double beta2 = (method == DONOF_ORB_DEMON) ? 0.999 : 0.9;
+    if (method == DONOF_ORB_DEMON) {
+        const double binit = beta1;
+        const double rate = (i - 1.0) / (s->maxloop - 1.0);
+        beta1 = binit * (1.0 - rate) / ((1.0 - binit) + binit * (1.0 - rate));
+    }
+    const double bc1 = 1.0 - pow(beta1, (double)i), bc2 = 1.0 - pow(beta2, (double)i);
+    const double alpha = s->alpha;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nvar;
+         k += (long long)gridDim.x * blockDim.x) {
+        const double gk = g[k];
+        const double mk = beta1 * m[k] + (1.0 - beta1) * gk;
+        double vk;
+        if (method == DONOF_ORB_ADABELIEF) {
+            const double dd = gk - mk;
+            vk = beta2 * v[k] + (1.0 - beta2) * (dd * dd);
+        } else if (method == DONOF_ORB_YOGI) {
+            const double g2 = gk * gk;
+            const double dv = v[k] - g2;
+            const double sg = (dv > 0.0) ? 1.0 : ((dv < 0.0) ? -1.0 : 0.0);
+            vk = v[k] - (1.0 - beta2) * sg * g2;
+        } else {
+            vk = beta2 * v[k] + (1.0 - beta2) * (gk * gk);
+        }
+        const double vm = fmax(vmax[k], vk / bc2);
+        m[k] = mk;
+        v[k] = vk;
+        vmax[k] = vm;
+        y[k] = -alpha * (mk / bc1) / sqrt(vm + 1e-16);
+    }
+}
+
+// End of iteration it+1: best-E tracking and the stopping rule evaluated at the
+// start of the next iteration in the reference (src/minimization.jl:387-422).
+__global__ void orb_end_kernel(OrbState* s, cudaGraphConditionalHandle h) {
+    s->it += 1;
+    const int i = s->it;
+    const double E = s->E;
+    int now = 0;
+    if (E < s->bestE) {
+        s->bestE = E;
+        s->improved = 1;
+        now = 1;
+    }
+    s->improved_now = now;
+    const double gmax = __longlong_as_double((long long)s->gmax_bits);
+    int stop = 0;
+    if (i >= s->maxloop) {
+        stop = 1;
+        s->nit = i;
+    } else if (2.0 * gmax < s->thresh && s->improved) {
+        stop = 1;
+        s->success = 1;
+        s->nit = i + 1;
+    }
+    cudaGraphSetConditional(h, stop ? 0u : 1u);
+}
+
+__global__ void copy_if_kernel(const double* __restrict__ src, double* __restrict__ dst, long long count,
+                               const int* flag) {
+    if (*flag == 0) return;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
+         i += (long long)gridDim.x * blockDim.x)
+        dst[i] = src[i];
+}
+
+}  // namespace
+
+int orbopt_run_host(donof_job* job, int method, const double* n, const double* cj12, const double* ck12,
+                    const double* H, int nbf5, int nalpha, int nbeta, double* alpha, int* maxloop,
+                    double threshgorb, double* C, double* E_out, int* nit_out, int* success_out, int precision);
+
 int orbopt_run(donof_job* job, int method, const double* n, const double* cj12, const double* ck12,
                const double* H, int nbf5, int nalpha, int nbeta, double* alpha, int* maxloop,
                double threshgorb, double* C, double* E_out, int* nit_out, int* success_out,
                int precision) {
+    const char* env = getenv("DONOF_ORBOPT_HOST_LOOP");
+    if (env && env[0] == '1')
+        return orbopt_run_host(job, method, n, cj12, ck12, H, nbf5, nalpha, nbeta, alpha, maxloop, threshgorb, C,
+                               E_out, nit_out, success_out, precision);
+    donof_ctx* ctx = job->ctx;
+    cudaStream_t st = ctx->stream;
+    if (st == nullptr || st == cudaStreamLegacy) {
+        // the legacy default stream cannot be captured: run this synchronous
+        // call on a private stream, ordered after the work already queued
+        if (!ctx->aux_stream) DONOF_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->aux_stream, cudaStreamNonBlocking));
+        DONOF_CUDA(ctx, cudaStreamSynchronize(st));
+        st = ctx->aux_stream;
+    }
+    struct ProfileOff {  // event records are not allowed in a conditional body
+        donof_ctx* c;
+        bool was;
+        ~ProfileOff() { c->profile = was; }
+    } profile_off{ctx, ctx->profile};
+    ctx->profile = false;
+    const int nbf = job->nbf;
+    const long long nvar = nvar_of(nbf, nbf5);
+    const long long nn = (long long)nbf * nbf;
+    size_t off = 0;
+    auto take = [&](size_t bytes) { size_t o = off; off += (bytes + 255) / 256 * 256; return o; };
+    const size_t o_m = take(8 * nvar), o_v = take(8 * nvar), o_vm = take(8 * nvar), o_y = take(8 * nvar),
+                 o_g = take(8 * nvar);
+    const size_t o_C = take(8 * nn), o_Cn = take(8 * nn), o_best = take(8 * nn), o_elag = take(8 * nn);
+    const size_t o_H = take(8 * (size_t)nbf * nbf5), o_st = take(sizeof(OrbState));
+    DONOF_CHECK(job->orb.ensure(ctx, off));
+    DONOF_CHECK(ctx->rot.ensure(ctx, rotate_scratch_bytes(nbf)));
+    char* base = job->orb.as<char>();
+    double* m = (double*)(base + o_m);
+    double* v = (double*)(base + o_v);
+    double* vm = (double*)(base + o_vm);
+    double* y = (double*)(base + o_y);
+    double* g = (double*)(base + o_g);
+    double* Ccur = (double*)(base + o_C);
+    double* Cnew = (double*)(base + o_Cn);
+    double* Cbest = (double*)(base + o_best);
+    double* elag = (double*)(base + o_elag);
+    double* Hmat = (double*)(base + o_H);
+    OrbState* S = (OrbState*)(base + o_st);
+
+    auto lagr = [&](const double* Cin) -> int {
+        if (precision == DONOF_PREC_MIXED)
+            return lagrange2_mixed(job, st, Cin, n, H, cj12, ck12, nbf5, nalpha, nbeta, elag, Hmat, &S->E);
+        return lagrange2_f64(job, st, Cin, n, H, cj12, ck12, nbf5, nalpha, nbeta, elag, Hmat, &S->E);
+    };
+    auto grad = [&]() -> int {
+        DONOF_CUDA(ctx, cudaMemsetAsync(&S->gmax_bits, 0, sizeof(unsigned long long), st));
+        return pack_grad(ctx, st, elag, nbf, nbf5, g, &S->gmax_bits);
+    };
+
+    // initial evaluation (also sizes every scratch buffer the graph will use)
+    DONOF_CUDA(ctx, cudaMemsetAsync(base + o_m, 0, o_y - o_m, st));  // m, v, vmax = 0
+    DONOF_CUDA(ctx, cudaMemcpyAsync(Ccur, C, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st));
+    DONOF_CHECK(lagr(Ccur));
+    DONOF_CHECK(grad());
+    DONOF_CUDA(ctx, cudaMemcpyAsync(Cbest, Ccur, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st));
+    OrbState hs{};
+    DONOF_CUDA(ctx, cudaMemcpyAsync(&hs, S, sizeof(OrbState), cudaMemcpyDeviceToHost, st));
+    DONOF_CUDA(ctx, cudaStreamSynchronize(st));
+    const double E0 = hs.E;
+    hs.bestE = E0;
+    hs.alpha = *alpha;
+    hs.thresh = threshgorb;
+    hs.it = 0;
+    hs.maxloop = *maxloop;
+    hs.method = method;
+    hs.improved = hs.improved_now = hs.success = hs.nit = 0;
+    DONOF_CUDA(ctx, cudaMemcpyAsync(S, &hs, sizeof(OrbState), cudaMemcpyHostToDevice, st));
+
+    if (*maxloop >= 1) {
+        // (re)build the graph when its inputs or any buffer it references changed
+        const unsigned long long gens = (unsigned long long)job->tmp.gen + job->bpq.gen + job->W.gen + job->part.gen +
+                                        job->small.gen + job->orb.gen + ctx->rot.gen;
+        const unsigned long long key[10] = {(unsigned long long)(uintptr_t)n, (unsigned long long)(uintptr_t)cj12,
+                                            (unsigned long long)(uintptr_t)ck12, (unsigned long long)(uintptr_t)H,
+                                            (unsigned long long)nbf5 | ((unsigned long long)nalpha << 20) |
+                                                ((unsigned long long)nbeta << 40),
+                                            (unsigned long long)method, (unsigned long long)precision, gens,
+                                            (unsigned long long)(uintptr_t)base, (unsigned long long)(uintptr_t)st};
+        bool valid = job->orb_exec != nullptr;
+        for (int k = 0; k < 10 && valid; ++k) valid = (job->orb_key[k] == key[k]);
+        if (!valid) {
+            if (job->orb_exec) cudaGraphExecDestroy(job->orb_exec);
+            if (job->orb_graph) cudaGraphDestroy(job->orb_graph);
+            job->orb_exec = nullptr;
+            job->orb_graph = nullptr;
+            cudaGraph_t graph = nullptr;
+            DONOF_CUDA(ctx, cudaGraphCreate(&graph, 0));
+            job->orb_graph = graph;
+            cudaGraphConditionalHandle handle;
+            DONOF_CUDA(ctx, cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault));
+            cudaGraphNodeParams cp = {};
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = handle;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            cudaGraphNode_t node;
+            DONOF_CUDA(ctx, cudaGraphAddNode(&node, graph, nullptr, 0, &cp));
+            cudaGraph_t body = cp.conditional.phGraph_out[0];
+            const unsigned long long l0 = donof_launch_count();
+            DONOF_CUDA(ctx, cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0,
+                                                          cudaStreamCaptureModeThreadLocal));
+            int rc = DONOF_OK;
+            do {
+                orb_update_kernel<<<nblocks(nvar, ctx->sm_count), 256, 0, st>>>(S, nvar, g, m, v, vm, y); count_launch();
+                if ((rc = rotate_f64(ctx, st, y, nbf, nbf5, Ccur, Cnew)) != DONOF_OK) break;
+                if ((rc = lagr(Cnew)) != DONOF_OK) break;
+                if ((rc = grad()) != DONOF_OK) break;
+                orb_end_kernel<<<1, 1, 0, st>>>(S, handle); count_launch();
+                copy_if_kernel<<<nblocks(nn, ctx->sm_count), 256, 0, st>>>(Cnew, Cbest, nn, &S->improved_now); count_launch();
+                if (cudaMemcpyAsync(Ccur, Cnew, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st) != cudaSuccess) rc = DONOF_ERR_CUDA;
+            } while (false);
+            cudaGraph_t captured = nullptr;
+            const cudaError_t ce = cudaStreamEndCapture(st, &captured);
+            if (rc != DONOF_OK) return rc;
+            if (ce != cudaSuccess) {
+                set_error(ctx, "capture of the optimiser body: %s", cudaGetErrorString(ce));
+                return DONOF_ERR_CUDA;
+            }
+            job->orb_per_iter = (int)(donof_launch_count() - l0);
+            // the capture counted the body's launches once; replays are counted below
+            g_launch_adjust(-(long long)job->orb_per_iter);
+            cudaGraphExec_t exec = nullptr;
+            DONOF_CUDA(ctx, cudaGraphInstantiate(&exec, graph, 0));
+            job->orb_exec = exec;
+            for (int k = 0; k < 10; ++k) job->orb_key[k] = key[k];
+        }
+        DONOF_CUDA(ctx, cudaGraphLaunch(job->orb_exec, st));
+        DONOF_CUDA(ctx, cudaMemcpyAsync(&hs, S, sizeof(OrbState), cudaMemcpyDeviceToHost, st));
+        DONOF_CUDA(ctx, cudaStreamSynchronize(st));
+        g_launch_adjust((long long)job->orb_per_iter * hs.it);
+    }
+    if (!hs.improved) {
+        *alpha = 0.3 * (*alpha);
+        *maxloop = *maxloop + 10;
+    }
+    const bool return_best = (*maxloop < 100);
+    DONOF_CUDA(ctx, cudaMemcpyAsync(C, return_best ? Cbest : Ccur, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st));
+    *E_out = return_best ? hs.bestE : hs.E;
+    *nit_out = hs.nit;
+    *success_out = hs.success;
+    return DONOF_OK;
+}
+
+// Host-driven form of the same loop (one 16-byte read per iteration); kept as
+// a reference execution mode, selected with DONOF_ORBOPT_HOST_LOOP=1.
+int orbopt_run_host(donof_job* job, int method, const double* n, const double* cj12, const double* ck12,
+                    const double* H, int nbf5, int nalpha, int nbeta, double* alpha, int* maxloop,
+                    double threshgorb, double* C, double* E_out, int* nit_out, int* success_out,
+                    int precision) {
     donof_ctx* ctx = job->ctx;
     cudaStream_t st = ctx->stream;
     const int nbf = job->nbf;
