@@ -366,7 +366,7 @@ size_t donof_job_device_bytes(const donof_job* job) {
     size_t s = job->tmp.bytes + job->bpq.bytes + job->W.bytes + job->part.bytes + job->small.bytes +
                job->orb.bytes + job->io.bytes;
     if (job->own_b) s += sizeof(double) * (size_t)job->nbf * job->nbf * job->naux;
-    if (job->b16hi) s += 4 * (size_t)((job->nbf + 7) / 8 * 8) * job->nbf * job->naux;
+    if (job->b16hi) s += 4 * (size_t)64 * ((job->nbf + 63) / 64) * job->nbf * job->naux;
     return s;
 }
 

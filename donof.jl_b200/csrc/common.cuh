@@ -87,8 +87,8 @@ struct donof_job {
     int nbf = 0, naux = 0, precision = DONOF_PREC_FP64;
     const double* b = nullptr;  // device [m + nbf*n + nbf*nbf*l]
     bool own_b = false;
-    // bf16 split of b for the mixed-precision form: b = hi + lo, layout
-    // [m + ldm*n + ldm*nbf*l] with ldm = nbf rounded up to a multiple of 8
+    // bf16 split of b for the mixed-precision form: b = hi + lo, quarter-major
+    // layout [mi + 64*n + 64*nbf*qb + 64*nbf*nb*l] with m = 64*qb + mi, nb = ceil(nbf/64)
     void* b16hi = nullptr;
     void* b16lo = nullptr;
     // per-call scratch, sized for the largest nbf5 seen

@@ -37,48 +37,49 @@ namespace donof {
 namespace mx {
 
 constexpr int NTHREADS = 192;
-constexpr int RING = 2;               // b stages
-constexpr int KB = 32;                // n rows per b stage
-constexpr int BOX_M = 64;             // m per TMA box (128 B of bf16)
-constexpr int MAXNB = 4;              // up to 4 boxes -> N = 256
-constexpr int BOX_BYTES = KB * BOX_M * 2;           // 4 KB
-constexpr int STAGE_BYTES = 2 * MAXNB * BOX_BYTES;  // hi + lo, 32 KB
+constexpr int KB = 64;                // n rows per b stage (8 KB TMA boxes)
+constexpr int BOX_M = 64;             // m per TMA box (128 B of bf16) = one T1 quarter
+constexpr int MAXNB = 4;              // up to 4 boxes -> nbf <= 256
+constexpr int BOX_BYTES = KB * BOX_M * 2;           // 8 KB
+constexpr int STAGE_BYTES = 2 * BOX_BYTES;          // hi + lo, 16 KB
+constexpr int RING = 4;                             // b stages in shared memory (64 KB)
 constexpr int CS_BOX_BYTES = 128 * 64 * 2;          // 16 KB: 128 rows x 64 k
 constexpr int CS_BYTES = 4 * CS_BOX_BYTES;          // K up to 256 -> 64 KB
 constexpr int A2_BYTES = 4 * CS_BOX_BYTES;          // tmp split, 64 KB
 constexpr int A3_BYTES = CS_BOX_BYTES;              // W split, 16 KB
-constexpr int XS_STRIDE = 36;                       // floats per staging row
-constexpr int XS_BYTES = 64 * XS_STRIDE * 4;        // 9216 B
-constexpr int XH_STRIDE = 20;                       // floats per half-exchange row (16 + pad)
 constexpr int CK_BYTES = 64 * 64 * 4;                // ck12 (transposed, FP32), 16 KB
-// shared-memory map (offsets from a 1024-aligned base).  The hi/lo exchange
-// buffer of the epilogue aliases the W operand (A3): A3 is idle whenever the
-// exchange is used (before W is written, and after the last Y MMA completed).
+// shared-memory map (offsets from a 1024-aligned base)
 constexpr int OFF_CS = 0;
 constexpr int OFF_RING = OFF_CS + CS_BYTES;
 constexpr int OFF_A2 = OFF_RING + RING * STAGE_BYTES;
 constexpr int OFF_A3 = OFF_A2 + A2_BYTES;
-constexpr int OFF_XS = OFF_A3;
-static_assert(XS_BYTES <= A3_BYTES && 2 * 64 * XH_STRIDE * 4 <= A3_BYTES, "exchange buffers must fit in A3");
 constexpr int OFF_CK = OFF_A3 + A3_BYTES;
 constexpr int OFF_DS = OFF_CK + CK_BYTES;            // 64 floats d
-constexpr int OFF_TS = OFF_DS + 256;                 // 128 floats: partial sums of t
-constexpr int OFF_BAR = OFF_TS + 512 + 256;
-constexpr int NBAR = 16;
+constexpr int OFF_BAR = OFF_DS + 256;
+constexpr int NBAR = 32;
 constexpr int OFF_MISC = OFF_BAR + NBAR * 8;         // tmem base, abort flag
 constexpr int SMEM_USED = OFF_MISC + 64;
 constexpr int SMEM_ALLOC = SMEM_USED + 1024;         // slack for 1024-B alignment
 static_assert(SMEM_ALLOC <= 227 * 1024, "shared memory budget");
 
 // barrier indices
-constexpr int B_FULL = 0;      // +s, RING of them
-constexpr int B_EMPTY = 2;     // +s
-constexpr int B_CS = 4;
-constexpr int B_T1 = 5;
-constexpr int B_A2 = 6;
-constexpr int B_T2 = 7;
-constexpr int B_A3 = 8;
-constexpr int B_Y = 9;
+constexpr int B_FULL = 0;          // +s, RING of them: stage s landed
+constexpr int B_EMPTY = RING;      // +s: stage s consumed by the MMAs
+constexpr int B_CS = 2 * RING;     // Cs landed
+constexpr int B_T1 = B_CS + 1;     // +slot (2): T1 quarter in TMEM slot complete
+constexpr int B_T1FREE = B_T1 + 2; // +slot (2): the four epilogue warps read the slot (count 4)
+constexpr int B_A2 = B_T1FREE + 2; // tmp split of the aux index written (one phase per index)
+constexpr int B_T2 = B_A2 + 1;     // T2 complete
+constexpr int B_A3 = B_T2 + 1;     // W split written, T2 region drained
+constexpr int B_Y = B_A3 + 1;      // Y MMAs of the aux index complete
+constexpr int B_END = B_Y + 1;     // every MMA of the CTA complete
+static_assert(B_END < NBAR, "barrier count");
+
+// TMEM columns (512 allocated): Y accumulator [0, 256), two T1 quarter slots
+// of 64 columns [256, 384), T2 [384, 512)
+constexpr int TM_Y = 0;
+constexpr int TM_T1 = 256;
+constexpr int TM_T2 = 384;
 
 constexpr long long WAIT_CYCLES = 4000000000LL;  // ~2 s of SM clock
 
@@ -89,8 +90,8 @@ struct Params {
     int ncs;                 // 64-wide k boxes of Cs (ceil(nbf / 64))
     int mode;                // 1: write tmp; 2: write b_pq; 3: full Lagrangian
     const float* n32;        // n (nbf5)
-    const float* cj32;       // cj12 (nbf5 x nbf5)
-    const float* ck32t;      // ck12 transposed: ck32t[q + nbf5*b] = ck12[b, q]
+    const float* cj32;       // cj12 zero-padded to 64 x 64: cj32[q + 64*c] = cj12[q, c]
+    const float* ck32t;      // ck12 transposed, zero-padded: ck32t[q + 64*b] = ck12[b, q]
     float* tmp_out;          // mode 1: tmp[m + nbf*q + nbf*nbf5*l]
     float* bpq_out;          // mode 2: b_pq[p + nbf5*q + nbf5^2*l]
     float* d_out;            // d[q + nbf5*l]
@@ -117,6 +118,19 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Non-blocking test (try_wait may suspend the thread until a time limit when the
+// phase is incomplete, which would delay a loop that watches two barriers).
+__device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(ok)
         : "r"(bar), "r"(parity)
@@ -152,6 +166,14 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map
         "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(
             dst),
         "l"(map), "r"(bar), "r"(c0), "r"(c1), "r"(c2)
+        : "memory");
+}
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap* map, uint32_t bar, int c0, int c1,
+                                            int c2, int c3) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5, %6}], [%2];" ::"r"(
+            dst),
+        "l"(map), "r"(bar), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
         : "memory");
 }
 __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, uint32_t bar, int c0, int c1) {
@@ -228,46 +250,34 @@ __device__ __forceinline__ void split_bf16(float v, __nv_bfloat16& hi, __nv_bflo
     lo = __float2bfloat16_rn(v - __bfloat162float(hi));
 }
 
-// Write 32 consecutive K values (k0..k0+31, k0 % 32 == 0) of rows rh (hi) and
-// rl (lo) into a K-major swizzled operand made of 64-wide boxes of box_bytes.
-__device__ __forceinline__ void put_split_row32(unsigned char* base, int box_bytes, int rh, int rl, int k0,
-                                                const float (&v)[32]) {
-    unsigned char* box = base + (k0 >> 6) * box_bytes;
-    const int kin = k0 & 63;
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-        __align__(16) __nv_bfloat16 h[8], l[8];
-#pragma unroll
-        for (int e = 0; e < 8; ++e) split_bf16(v[c * 8 + e], h[e], l[e]);
-        *reinterpret_cast<uint4*>(box + sw128(rh, kin + c * 8)) = *reinterpret_cast<const uint4*>(h);
-        *reinterpret_cast<uint4*>(box + sw128(rl, kin + c * 8)) = *reinterpret_cast<const uint4*>(l);
-    }
-}
+// Row of the stacked (hi, lo) operands and accumulators that holds part x
+// (0 hi, 1 lo) of index q: r = 32 (q / 16) + 16 x + q % 16, so that a warp's
+// 32 TMEM lanes hold the hi and lo rows of the same 16 indices.
+__device__ __forceinline__ int prow(int q, int x) { return 32 * (q >> 4) + 16 * x + (q & 15); }
 
-// Finish 16 columns (OFF .. OFF+15 of the 32-column chunk c) of tmp row q:
-// mode 1 writes FP32 to global, otherwise the bf16 hi/lo split goes to A2.
-template <int OFF>
-__device__ __forceinline__ void finish_tmp16(const Params& P, unsigned char* sm, const float (&v)[32], int q, int c,
+// Finish columns m0 .. m0+15 of tmp row q: mode 1 writes FP32 to global,
+// otherwise the bf16 hi/lo split goes to A2 (rows prow(q, 0), prow(q, 1)).
+__device__ __forceinline__ void finish_tmp16(const Params& P, unsigned char* sm, const float (&v)[16], int q, int m0,
                                              int l) {
     if (P.mode == 1) {
         if (q < P.nbf5) {
-            float* dst = P.tmp_out + (size_t)P.nbf * P.nbf5 * l + (size_t)P.nbf * q + c * 32 + OFF;
+            float* dst = P.tmp_out + (size_t)P.nbf * P.nbf5 * l + (size_t)P.nbf * q + m0;
 #pragma unroll
             for (int i = 0; i < 16; ++i)
-                if (c * 32 + OFF + i < P.nbf) dst[i] = v[OFF + i];
+                if (m0 + i < P.nbf) dst[i] = v[i];
         }
         return;
     }
-    const int k0 = c * 32 + OFF;
-    unsigned char* box = sm + OFF_A2 + (k0 >> 6) * CS_BOX_BYTES;
-    const int kin = k0 & 63;
+    unsigned char* box = sm + OFF_A2 + (m0 >> 6) * CS_BOX_BYTES;
+    const int kin = m0 & 63;
+    const int rh = prow(q, 0), rl = prow(q, 1);
 #pragma unroll
     for (int cc = 0; cc < 2; ++cc) {
         __align__(16) __nv_bfloat16 h[8], lo[8];
 #pragma unroll
-        for (int e = 0; e < 8; ++e) split_bf16(v[OFF + cc * 8 + e], h[e], lo[e]);
-        *reinterpret_cast<uint4*>(box + sw128(q, kin + cc * 8)) = *reinterpret_cast<const uint4*>(h);
-        *reinterpret_cast<uint4*>(box + sw128(64 + q, kin + cc * 8)) = *reinterpret_cast<const uint4*>(lo);
+        for (int e = 0; e < 8; ++e) split_bf16(v[cc * 8 + e], h[e], lo[e]);
+        *reinterpret_cast<uint4*>(box + sw128(rh, kin + cc * 8)) = *reinterpret_cast<const uint4*>(h);
+        *reinterpret_cast<uint4*>(box + sw128(rl, kin + cc * 8)) = *reinterpret_cast<const uint4*>(lo);
     }
 }
 
@@ -280,8 +290,6 @@ lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_const
     uint64_t* bars = reinterpret_cast<uint64_t*>(sm + OFF_BAR);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(sm + OFF_MISC);
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + OFF_MISC + 16);
-    float* xs = reinterpret_cast<float*>(sm + OFF_XS);
-    float* ds = reinterpret_cast<float*>(sm + OFF_DS);
     auto bar = [&](int i) { return saddr(&bars[i]); };
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -291,16 +299,7 @@ lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_const
 
     if (threadIdx.x == 0) {
         *abort_flag = 0;
-        for (int s = 0; s < RING; ++s) {
-            mbar_init(bar(B_FULL + s), 1);
-            mbar_init(bar(B_EMPTY + s), 1);
-        }
-        mbar_init(bar(B_CS), 1);
-        mbar_init(bar(B_T1), 1);
-        mbar_init(bar(B_A2), 1);
-        mbar_init(bar(B_T2), 1);
-        mbar_init(bar(B_A3), 1);
-        mbar_init(bar(B_Y), 1);
+        for (int i = 0; i <= B_END; ++i) mbar_init(bar(i), (i == B_T1FREE || i == B_T1FREE + 1) ? 4 : 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 5) {
@@ -311,10 +310,12 @@ lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_const
     __syncthreads();
     fence_after();
     const uint32_t tmem = *tmem_slot;
-    const uint32_t R1 = tmem, R2 = tmem + 256;
+    const uint32_t RY = tmem + TM_Y, RT1 = tmem + TM_T1, RT2 = tmem + TM_T2;
 
     if (warp == 4) {
         // ------------------------------------------------------------ producer
+        // stages in the order the MMAs consume them: per aux index, per 64-column
+        // quarter of m, per 32 rows of n (hi and lo box of the same rows)
         if (lane == 0 && my_count > 0) {
             mbar_expect_tx(bar(B_CS), (uint32_t)(P.ncs * CS_BOX_BYTES));
             for (int kb = 0; kb < P.ncs; ++kb)
@@ -323,15 +324,15 @@ lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_const
             bool ok = true;
             for (int li = 0; li < my_count && ok; ++li) {
                 const int l = blockIdx.x + li * G;
-                for (int kb = 0; kb < P.nkb && ok; ++kb, ++it) {
-                    const int s = it % RING;
-                    const uint32_t ph = (uint32_t)((it / RING) & 1);
-                    if (!mbar_wait(bar(B_EMPTY + s), ph ^ 1u, abort_flag)) { ok = false; break; }
-                    mbar_expect_tx(bar(B_FULL + s), (uint32_t)(2 * P.nb * BOX_BYTES));
-                    const uint32_t st = sbase + OFF_RING + s * STAGE_BYTES;
-                    for (int i = 0; i < P.nb; ++i) {
-                        tma_load_3d(st + i * BOX_BYTES, &map_bhi, bar(B_FULL + s), i * BOX_M, kb * KB, l);
-                        tma_load_3d(st + (MAXNB + i) * BOX_BYTES, &map_blo, bar(B_FULL + s), i * BOX_M, kb * KB, l);
+                for (int qb = 0; qb < P.nb && ok; ++qb) {
+                    for (int kb = 0; kb < P.nkb; ++kb, ++it) {
+                        const int s = it % RING;
+                        const uint32_t ph = (uint32_t)((it / RING) & 1);
+                        if (!mbar_wait(bar(B_EMPTY + s), ph ^ 1u, abort_flag)) { ok = false; break; }
+                        mbar_expect_tx(bar(B_FULL + s), (uint32_t)STAGE_BYTES);
+                        const uint32_t st = sbase + OFF_RING + s * STAGE_BYTES;
+                        tma_load_4d(st, &map_bhi, bar(B_FULL + s), 0, kb * KB, qb, l);
+                        tma_load_4d(st + BOX_BYTES, &map_blo, bar(B_FULL + s), 0, kb * KB, qb, l);
                     }
                 }
             }
@@ -345,19 +346,58 @@ lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_const
         }
     } else if (warp == 5) {
         // ------------------------------------------------------------ MMA issuer
+        // Issue order per aux index l: its T1 quarters, T2(l), then (while the
+        // epilogue drains T2(l) and builds W(l)) up to two T1 quarters of l+1 into
+        // the free slots, and Y(l) as soon as W(l) is ready.
         if (lane == 0 && my_count > 0) {
-            const uint32_t id_t1 = idesc(128, ncol, 0, 1);
+            const uint32_t id_t1 = idesc(128, BOX_M, 0, 1);
             const uint32_t id_t2 = idesc(128, 128, 0, 0);
             const uint32_t id_y = idesc(128, ncol, 0, 1);
             bool ok = mbar_wait(bar(B_CS), 0, abort_flag);
             fence_after();
-            int it = 0;
-            for (int li = 0; li < my_count && ok; ++li) {
-                const uint32_t lph = (uint32_t)(li & 1);
-                // T1: R1[j, m] = sum_n Cs[j, n] b_x[n, m]
+            int it = 0;          // ring stages consumed
+            int tq = 0;          // T1 quarters issued (slot = tq & 1)
+            int y_li = -1;       // aux index whose Y MMAs are still to be issued
+            auto issue_y = [&]() {
+                // Y: RY[j, m] += sum_q A3[j, q] tmp_x[q, m]  (A2 read as an MN-major operand)
+#pragma unroll
+                for (int ks = 0; ks < 4; ++ks) {
+                    const uint64_t a = sdesc(sbase + OFF_A3 + ks * 32, 16, 1024);
+                    // K rows q = 16 ks + i of the hi part are A2 rows 32 ks + i, the lo part 32 ks + 16 + i
+                    const uint64_t bh = sdesc(sbase + OFF_A2 + ks * 4096, CS_BOX_BYTES, 1024);
+                    const uint64_t bl = sdesc(sbase + OFF_A2 + ks * 4096 + 2048, CS_BOX_BYTES, 1024);
+                    umma(RY, a, bh, id_y, (y_li | ks) ? 1u : 0u);
+                    umma(RY, a, bl, id_y, 1u);
+                }
+                umma_commit(bar(B_Y));
+                y_li = -1;
+            };
+            // Bounded wait that issues the pending Y MMAs as soon as W is ready.
+            auto wait_poll = [&](uint32_t b, uint32_t parity) -> bool {
+                const long long t0 = clock64();
+                while (!mbar_test(b, parity)) {
+                    if (y_li >= 0 && mbar_test(bar(B_A3), (uint32_t)(y_li & 1))) {
+                        fence_after();
+                        issue_y();
+                    }
+                    if (*abort_flag) return false;
+                    if (clock64() - t0 > WAIT_CYCLES) { *abort_flag = 1; return false; }
+                }
+                return true;
+            };
+            // T1 quarter: slot[j, m'] = sum_n Cs[j, n] b_x[n, m'] over one 64-column box of m
+            auto t1_quarter = [&]() -> bool {
+                const int slot = tq & 1;
+                if (!wait_poll(bar(B_T1FREE + slot), (uint32_t)(((tq >> 1) & 1) ^ 1))) return false;
+                fence_after();
+                const uint32_t d = RT1 + slot * BOX_M;
                 for (int kb = 0; kb < P.nkb; ++kb, ++it) {
                     const int s = it % RING;
-                    if (!mbar_wait(bar(B_FULL + s), (uint32_t)((it / RING) & 1), abort_flag)) { ok = false; break; }
+                    if (y_li >= 0 && mbar_test(bar(B_A3), (uint32_t)(y_li & 1))) {
+                        fence_after();
+                        issue_y();
+                    }
+                    if (!wait_poll(bar(B_FULL + s), (uint32_t)((it / RING) & 1))) return false;
                     fence_after();
                     const uint32_t st = sbase + OFF_RING + s * STAGE_BYTES;
 #pragma unroll
@@ -365,51 +405,55 @@ lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_const
                         const int k = kb * KB + ks * 16;  // n offset
                         const uint64_t a = sdesc(sbase + OFF_CS + (k >> 6) * CS_BOX_BYTES + (k & 63) * 2, 16, 1024);
                         const uint64_t bh = sdesc(st + ks * 2048, BOX_BYTES, 1024);
-                        const uint64_t bl = sdesc(st + MAXNB * BOX_BYTES + ks * 2048, BOX_BYTES, 1024);
-                        umma(R1, a, bh, id_t1, (kb | ks) ? 1u : 0u);
-                        umma(R1, a, bl, id_t1, 1u);
+                        const uint64_t bl = sdesc(st + BOX_BYTES + ks * 2048, BOX_BYTES, 1024);
+                        umma(d, a, bh, id_t1, (kb | ks) ? 1u : 0u);
+                        umma(d, a, bl, id_t1, 1u);
                     }
                     umma_commit(bar(B_EMPTY + s));
                 }
+                umma_commit(bar(B_T1 + slot));
+                ++tq;
+                return true;
+            };
+            const int ahead_max = P.nb < 2 ? P.nb : 2;
+            int ahead = 0;  // quarters of the current index issued early
+            for (int li = 0; li < my_count && ok; ++li) {
+                const uint32_t lph = (uint32_t)(li & 1);
+                for (int qb = ahead; qb < P.nb && ok; ++qb) ok = t1_quarter();
+                ahead = 0;
                 if (!ok) break;
-                umma_commit(bar(B_T1));
-                if (P.mode == 1) {
-                    // the epilogue writes tmp and hands R1 back through B_A2
-                    if (!mbar_wait(bar(B_A2), lph, abort_flag)) { ok = false; break; }
-                    fence_after();
-                    continue;
-                }
-                // T2: R1[j, j'] = sum_m A2[j, m] Cs[j', m]
-                if (!mbar_wait(bar(B_A2), lph, abort_flag)) { ok = false; break; }
+                if (P.mode == 1) continue;
+                // T2: RT2[j, j'] = sum_m A2[j, m] Cs[j', m]
+                if (!wait_poll(bar(B_A2), lph)) { ok = false; break; }
                 fence_after();
                 for (int ks = 0; ks < ncol / 16; ++ks) {
                     const int k = ks * 16;  // m offset
                     const uint64_t a = sdesc(sbase + OFF_A2 + (k >> 6) * CS_BOX_BYTES + (k & 63) * 2, 16, 1024);
                     const uint64_t b = sdesc(sbase + OFF_CS + (k >> 6) * CS_BOX_BYTES + (k & 63) * 2, 16, 1024);
-                    umma(R1, a, b, id_t2, ks ? 1u : 0u);
+                    umma(RT2, a, b, id_t2, ks ? 1u : 0u);
                 }
                 umma_commit(bar(B_T2));
+                if (P.mode == 3) y_li = li;
+                // T1 of the next index into the slots the epilogue has already drained
+                if (li + 1 < my_count)
+                    for (; ahead < ahead_max && ok; ++ahead) ok = t1_quarter();
+                if (!ok) break;
+                // W(l) ready (and the T2 region drained)
                 if (!mbar_wait(bar(B_A3), lph, abort_flag)) { ok = false; break; }
                 fence_after();
-                if (P.mode == 2) continue;
-                // Y: R2[j, m] += sum_q A3[j, q] tmp_x[q, m]  (A2 read as an MN-major operand)
-#pragma unroll
-                for (int ks = 0; ks < 4; ++ks) {
-                    const uint64_t a = sdesc(sbase + OFF_A3 + ks * 32, 16, 1024);
-                    const uint64_t bh = sdesc(sbase + OFF_A2 + ks * 2048, CS_BOX_BYTES, 1024);
-                    const uint64_t bl = sdesc(sbase + OFF_A2 + 8192 + ks * 2048, CS_BOX_BYTES, 1024);
-                    umma(R2, a, bh, id_y, (li | ks) ? 1u : 0u);
-                    umma(R2, a, bl, id_y, 1u);
-                }
+                if (y_li >= 0) issue_y();
             }
-            umma_commit(bar(B_Y));
-            mbar_drain(bar(B_Y), 0);  // every MMA of this CTA has completed
+            umma_commit(bar(B_END));
+            mbar_drain(bar(B_END), 0);  // every MMA of this CTA has completed
         }
     } else {
         // ------------------------------------------------------------ epilogue (warps 0-3)
-        const int row = warp * 32 + lane;     // TMEM lane = accumulator row
-        const int q = row & 63;               // q (T1/T2 rows) or b (Y rows)
-        const bool lo_half = row >= 64;
+        // Accumulator rows are stacked as prow(q, x): warp g holds q in [16 g, 16 g + 16),
+        // the hi part in lanes 0-15 and the lo part in lanes 16-31, so every hi + lo sum
+        // is a shuffle between lanes i and i + 16 of one warp.
+        const int q = 16 * warp + (lane & 15);  // q (T1/T2 rows) or b (Y rows)
+        const int x = lane >> 4;                 // 0: hi row, 1: lo row
+        const int off = 32 * x;                  // T2/W: this thread finishes p (or b) in [off, off + 32)
         const uint32_t lane_addr = (uint32_t)(warp * 32) << 16;
         volatile int* epi_ok = reinterpret_cast<volatile int*>(sm + OFF_MISC + 32);
         // one thread waits, the 128 epilogue threads agree on the outcome
@@ -421,132 +465,112 @@ lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_const
             if (r) fence_after();
             return r;
         };
+        // one warp waits on its own (lane 0 polls, the warp agrees)
+        auto warp_wait = [&](int b, uint32_t parity) -> bool {
+            int r = 1;
+            if (lane == 0) r = mbar_wait(bar(b), parity, abort_flag) ? 1 : 0;
+            r = __shfl_sync(0xffffffffu, r, 0);
+            if (r) fence_after();
+            return r != 0;
+        };
+        // the four warps agree to go on unless a wait failed somewhere (every failed
+        // wait sets the abort flag)
+        auto agree = [&](bool mine) -> bool {
+            if (!mine) *abort_flag = 1;
+            epi_sync();
+            if (threadIdx.x == 0) *epi_ok = *abort_flag ? 0 : 1;
+            epi_sync();
+            const bool r = *epi_ok != 0;
+            epi_sync();
+            return r;
+        };
         // ck12 (transposed) staged once per CTA: cks[b * 64 + q] = ck12[b, q]
         float* cks = reinterpret_cast<float*>(sm + OFF_CK);
-        for (int i = threadIdx.x; i < 64 * 64; i += 128) {
-            const int qq = i & 63, bb = i >> 6;
-            cks[i] = (qq < P.nbf5 && bb < P.nbf5) ? P.ck32t[qq + (size_t)P.nbf5 * bb] : 0.f;
-        }
-        epi_sync();
-        // exchange halves: xh receives the hi rows' columns 16..31, xl the lo rows' columns 0..15
-        float* xh = xs;
-        float* xl = xs + 64 * XH_STRIDE;
-        // T2 exchange: rows of 32 floats, 8 KB per side (the two fill A3 exactly)
-        float* x2h = xs;
-        float* x2l = xs + 64 * 32;
-        float* ts = reinterpret_cast<float*>(sm + OFF_TS);
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+            reinterpret_cast<float4*>(cks)[threadIdx.x + 128 * i] =
+                __ldg(reinterpret_cast<const float4*>(P.ck32t) + threadIdx.x + 128 * i);
         // row q of cj12 restricted to this thread's half of the columns, kept in registers
         float cjr[32];
-        {
-            const int coff = lo_half ? 32 : 0;
 #pragma unroll
-            for (int i = 0; i < 32; ++i)
-                cjr[i] = (q < P.nbf5 && coff + i < P.nbf5) ? __ldg(P.cj32 + q + (size_t)P.nbf5 * (coff + i)) : 0.f;
-        }
+        for (int i = 0; i < 32; ++i) cjr[i] = __ldg(P.cj32 + q + 64 * (off + i));
+        epi_sync();
+        float* ds = reinterpret_cast<float*>(sm + OFF_DS);
+
+        // columns 32 c .. 32 c + 31 of tmp row q: the hi lane finishes the first 16,
+        // the lo lane the last 16
+        auto drain32 = [&](const uint32_t (&r)[32], int c, int l) {
+            float v[16];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                const float send = __uint_as_float(x ? r[i] : r[16 + i]);
+                const float keep = __uint_as_float(x ? r[16 + i] : r[i]);
+                v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+            }
+            finish_tmp16(P, sm, v, q, 32 * c + 16 * x, l);
+        };
+
         bool ok = true;
+        int tq = 0;  // T1 quarters drained (slot = tq & 1)
         for (int li = 0; li < my_count && ok; ++li) {
             const int l = blockIdx.x + li * G;
             const uint32_t lph = (uint32_t)(li & 1);
-            // ---- T1 drain: tmp[m, q] = D1[q, m] + D1[64+q, m]; the hi-row thread finishes
-            // columns 0..15 of each 32-column chunk, the lo-row thread columns 16..31
-            if (!epi_wait(B_T1, lph)) { ok = false; break; }
-            auto drain_chunk = [&](const uint32_t (&r)[32], int c) {
-                float v[32];
-#pragma unroll
-                for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
-                if (lo_half) {
-#pragma unroll
-                    for (int i = 0; i < 16; i += 4)
-                        *reinterpret_cast<float4*>(&xl[q * XH_STRIDE + i]) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
-                } else {
-#pragma unroll
-                    for (int i = 0; i < 16; i += 4)
-                        *reinterpret_cast<float4*>(&xh[q * XH_STRIDE + i]) =
-                            make_float4(v[16 + i], v[17 + i], v[18 + i], v[19 + i]);
-                }
-                epi_sync();
-                if (lo_half) {
-#pragma unroll
-                    for (int i = 0; i < 16; i += 4) {
-                        const float4 w = *reinterpret_cast<const float4*>(&xh[q * XH_STRIDE + i]);
-                        v[16 + i] += w.x; v[17 + i] += w.y; v[18 + i] += w.z; v[19 + i] += w.w;
-                    }
-                    finish_tmp16<16>(P, sm, v, q, c, l);
-                } else {
-#pragma unroll
-                    for (int i = 0; i < 16; i += 4) {
-                        const float4 w = *reinterpret_cast<const float4*>(&xl[q * XH_STRIDE + i]);
-                        v[i] += w.x; v[i + 1] += w.y; v[i + 2] += w.z; v[i + 3] += w.w;
-                    }
-                    finish_tmp16<0>(P, sm, v, q, c, l);
-                }
-                epi_sync();
-            };
-            {
-                // software pipeline: the TMEM load of the next chunk is in flight while the
-                // current one is exchanged, split and stored (ncol / 32 is even)
-                const int nch = ncol / 32;
+            // ---- T1 drain, one 64-column quarter of m at a time, each warp on its own:
+            // tmp[m, q] = D1[prow(q, 0), m] + D1[prow(q, 1), m]
+            bool wok = true;
+            for (int qb = 0; qb < P.nb; ++qb) {
+                const int t = tq + qb, slot = t & 1;
+                if (!warp_wait(B_T1 + slot, (uint32_t)((t >> 1) & 1))) { wok = false; break; }
+                // A2 is read by the Y MMAs of the previous index
+                if (qb == 0 && li > 0 && P.mode == 3 && !warp_wait(B_Y, (uint32_t)((li - 1) & 1))) { wok = false; break; }
+                const uint32_t src = RT1 + slot * BOX_M + lane_addr;
                 uint32_t ra[32], rb[32];
-                tmem_issue32(R1 + lane_addr, ra);
-                for (int c = 0; c < nch; c += 2) {
-                    tmem_wait_ld();
-                    tmem_issue32(R1 + lane_addr + (c + 1) * 32, rb);
-                    drain_chunk(ra, c);
-                    tmem_wait_ld();
-                    if (c + 2 < nch) tmem_issue32(R1 + lane_addr + (c + 2) * 32, ra);
-                    drain_chunk(rb, c + 1);
-                }
+                tmem_issue32(src, ra);
+                tmem_issue32(src + 32, rb);
+                tmem_wait_ld();
+                // the slot can take the next quarter while this one is finished
+                fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(bar(B_T1FREE + slot));
+                drain32(ra, 2 * qb, l);
+                drain32(rb, 2 * qb + 1, l);
             }
-            fence_async_smem();
-            fence_before();
-            epi_sync();
-            if (threadIdx.x == 0) mbar_arrive(bar(B_A2));
+            tq += P.nb;
+            if (P.mode != 1) fence_async_smem();  // A2 written by the generic proxy, read by the MMAs
+            if (!agree(wok)) { ok = false; break; }
             if (P.mode == 1) continue;
-            // ---- T2 drain: b_pq[p, q] = sum of the four quadrants of D2[q | 64+q, p | 64+p]
+            if (threadIdx.x == 0) mbar_arrive(bar(B_A2));
+            // ---- T2 drain: b_pq[p, q] = sum over x, x' of D2[prow(q, x), prow(p, x')]
             if (!epi_wait(B_T2, lph)) { ok = false; break; }
-            // The hi-row thread of column q finishes b_pq[p, q] for p in [0, 32),
-            // the lo-row thread for p in [32, 64) (off = first p of the range).
-            float bq[32];
+            float bq[32];  // b_pq for p = off + i
             {
-                float a[32], b2[32], u[32];
-                tmem_ld32(R1 + lane_addr + 0, a);
-                tmem_ld32(R1 + lane_addr + 64, u);
+                float lowp[32], highp[32];  // this row's sums over x' for p in [0, 32) and [32, 64)
+                uint32_t r0[32], r1[32];
+                tmem_issue32(RT2 + lane_addr + 0, r0);
+                tmem_issue32(RT2 + lane_addr + 32, r1);
+                tmem_wait_ld();
 #pragma unroll
-                for (int i = 0; i < 32; ++i) a[i] += u[i];      // p in [0, 32)
-                tmem_ld32(R1 + lane_addr + 32, b2);
-                tmem_ld32(R1 + lane_addr + 96, u);
-#pragma unroll
-                for (int i = 0; i < 32; ++i) b2[i] += u[i];     // p in [32, 64)
-                // exchange: each side sends the range it does not finish (rows of 32
-                // floats, float4 index swizzled by q to spread the banks)
-                float* send = lo_half ? x2l : x2h;
-                const float* recv = lo_half ? x2h : x2l;
-#pragma unroll
-                for (int i4 = 0; i4 < 8; ++i4) {
-                    const int sw = (i4 ^ (q & 7)) * 4;
-                    float4 s4;
-                    if (lo_half) s4 = make_float4(a[i4 * 4], a[i4 * 4 + 1], a[i4 * 4 + 2], a[i4 * 4 + 3]);
-                    else s4 = make_float4(b2[i4 * 4], b2[i4 * 4 + 1], b2[i4 * 4 + 2], b2[i4 * 4 + 3]);
-                    *reinterpret_cast<float4*>(&send[q * 32 + sw]) = s4;
+                for (int i = 0; i < 16; ++i) {
+                    lowp[i] = __uint_as_float(r0[i]) + __uint_as_float(r0[16 + i]);
+                    lowp[16 + i] = __uint_as_float(r1[i]) + __uint_as_float(r1[16 + i]);
                 }
-                epi_sync();
+                tmem_issue32(RT2 + lane_addr + 64, r0);
+                tmem_issue32(RT2 + lane_addr + 96, r1);
+                tmem_wait_ld();
 #pragma unroll
-                for (int i4 = 0; i4 < 8; ++i4) {
-                    const int sw = (i4 ^ (q & 7)) * 4;
-                    const float4 r4 = *reinterpret_cast<const float4*>(&recv[q * 32 + sw]);
-                    if (lo_half) {
-                        bq[i4 * 4] = b2[i4 * 4] + r4.x; bq[i4 * 4 + 1] = b2[i4 * 4 + 1] + r4.y;
-                        bq[i4 * 4 + 2] = b2[i4 * 4 + 2] + r4.z; bq[i4 * 4 + 3] = b2[i4 * 4 + 3] + r4.w;
-                    } else {
-                        bq[i4 * 4] = a[i4 * 4] + r4.x; bq[i4 * 4 + 1] = a[i4 * 4 + 1] + r4.y;
-                        bq[i4 * 4 + 2] = a[i4 * 4 + 2] + r4.z; bq[i4 * 4 + 3] = a[i4 * 4 + 3] + r4.w;
-                    }
+                for (int i = 0; i < 16; ++i) {
+                    highp[i] = __uint_as_float(r0[i]) + __uint_as_float(r0[16 + i]);
+                    highp[16 + i] = __uint_as_float(r1[i]) + __uint_as_float(r1[16 + i]);
+                }
+#pragma unroll
+                for (int i = 0; i < 32; ++i) {
+                    const float send = x ? lowp[i] : highp[i];
+                    bq[i] = (x ? highp[i] : lowp[i]) + __shfl_xor_sync(0xffffffffu, send, 16);
                 }
             }
-            // R1 is free again once every thread's loads are done
+            // the T2 region is free again once every thread's loads are done
             fence_before();
-            const int off = lo_half ? 32 : 0;
-            const bool own_diag = (q >= off) && (q < off + 32);   // this thread holds b_pq[q, q]
+            const bool own_diag = (q >= off) && (q < off + 32);  // this thread holds b_pq[q, q]
             {
                 float dq = 0.f;
 #pragma unroll
@@ -557,13 +581,11 @@ lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_const
                     ds[q] = dq;
                     if (q < P.nbf5 && P.mode == 2) P.d_out[q + (size_t)P.nbf5 * l] = dq;
                 }
-                if (q < P.nbf5 && P.mode == 2) {   // J/K ingredients are only needed by JKH_MO
-                    if (P.mode == 2) {
-                        float* dst = P.bpq_out + (size_t)P.nbf5 * P.nbf5 * l + (size_t)P.nbf5 * q + off;
+                if (q < P.nbf5 && P.mode == 2) {  // J/K ingredients are only needed by JKH_MO
+                    float* dst = P.bpq_out + (size_t)P.nbf5 * P.nbf5 * l + (size_t)P.nbf5 * q + off;
 #pragma unroll
-                        for (int i = 0; i < 32; ++i)
-                            if (off + i < P.nbf5) dst[i] = bq[i];
-                    }
+                    for (int i = 0; i < 32; ++i)
+                        if (off + i < P.nbf5) dst[i] = bq[i];
                     // K_MO partial sums of this CTA, stored transposed (kp[q + nbf5*p]) so that
                     // the reductions of a warp are coalesced; each address has one writer
                     float* kp = P.k_part + (size_t)blockIdx.x * P.nbf5 * P.nbf5 + q;
@@ -578,15 +600,13 @@ lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_const
                 float tpart = 0.f;
 #pragma unroll
                 for (int i = 0; i < 32; ++i) tpart += cjr[i] * ds[off + i];
-                ts[row] = tpart;
-                epi_sync();
+                const float t = tpart + __shfl_xor_sync(0xffffffffu, tpart, 16);
                 float diag = 0.f;
                 if (own_diag && q < P.nbf5) {
-                    const float t = ts[q] + ts[64 + q];
                     const bool dj = (P.nbeta > 0) && (q < P.nbeta || q >= P.nalpha);
                     diag = (dj ? P.n32[q] * ds[q] : 0.f) + t;
                 }
-                // A3 row b (hi) / 64+b (lo), K = q, for b in this thread's range
+                // A3 rows prow(b, 0) (hi) / prow(b, 1) (lo), K = q, for b in this thread's range
 #pragma unroll
                 for (int i = 0; i < 32; ++i) {
                     const int b = off + i;
@@ -594,8 +614,8 @@ lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_const
                     if (q < P.nbf5 && b < P.nbf5) w = -cks[b * 64 + q] * bq[i] + (b == q ? diag : 0.f);
                     __nv_bfloat16 h, lo;
                     split_bf16(w, h, lo);
-                    *reinterpret_cast<__nv_bfloat16*>(sm + OFF_A3 + sw128(b, q)) = h;
-                    *reinterpret_cast<__nv_bfloat16*>(sm + OFF_A3 + sw128(64 + b, q)) = lo;
+                    *reinterpret_cast<__nv_bfloat16*>(sm + OFF_A3 + sw128(prow(b, 0), q)) = h;
+                    *reinterpret_cast<__nv_bfloat16*>(sm + OFF_A3 + sw128(prow(b, 1), q)) = lo;
                 }
             }
             fence_async_smem();
@@ -603,24 +623,21 @@ lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_const
             epi_sync();
             if (threadIdx.x == 0) mbar_arrive(bar(B_A3));
         }
-        // ---- final: Y partial (mode 3) and K partial
+        // ---- final: Y partial (mode 3): Y[m, b] = D3[prow(b, 0), m] + D3[prow(b, 1), m]
         if (ok && my_count > 0 && P.mode == 3) {
-            if (epi_wait(B_Y, 0)) {
+            if (epi_wait(B_Y, (uint32_t)((my_count - 1) & 1))) {
                 for (int c = 0; c < ncol / 32; ++c) {
-                    float v[32];
-                    tmem_ld32(R2 + lane_addr + c * 32, v);
-                    if (lo_half) {
+                    uint32_t r[32];
+                    tmem_issue32(RY + lane_addr + c * 32, r);
+                    tmem_wait_ld();
+                    const int m0 = 32 * c + 16 * x;
+                    float* dst = P.y_part + (size_t)blockIdx.x * P.nbf * P.nbf5 + (size_t)P.nbf * q + m0;
 #pragma unroll
-                        for (int i = 0; i < 32; i += 4)
-                            *reinterpret_cast<float4*>(&xs[q * XS_STRIDE + i]) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+                    for (int i = 0; i < 16; ++i) {
+                        const float send = __uint_as_float(x ? r[i] : r[16 + i]);
+                        const float v = __uint_as_float(x ? r[16 + i] : r[i]) + __shfl_xor_sync(0xffffffffu, send, 16);
+                        if (q < P.nbf5 && m0 + i < P.nbf) dst[i] = v;
                     }
-                    epi_sync();
-                    if (!lo_half && q < P.nbf5) {
-                        float* dst = P.y_part + (size_t)blockIdx.x * P.nbf * P.nbf5 + (size_t)P.nbf * q + c * 32;
-                        for (int i = 0; i < 32; ++i)
-                            if (c * 32 + i < P.nbf) dst[i] = v[i] + xs[q * XS_STRIDE + i];
-                    }
-                    epi_sync();
                 }
             }
         }
@@ -636,45 +653,55 @@ lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_const
 }
 
 // ---------------------------------------------------------------- helpers
-__global__ void split_b_kernel(const double* __restrict__ b, int nbf, int ldm, long long nl,
+// b = hi + lo in the quarter-major layout the mixed kernel streams: element
+// (m, n, l) at [mi + 64 n + 64 nbf qb + 64 nbf nb l] with m = 64 qb + mi, so
+// that the 32-row stages of one 64-column quarter are contiguous 4 KB blocks;
+// m >= nbf is zero.
+__global__ void split_b_kernel(const double* __restrict__ b, int nbf, int nb, long long naux,
                                __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo) {
-    // nl = nbf * naux columns (n, l) of length nbf (m)
-    const long long total = (long long)ldm * nl;
+    const long long total = 64LL * nbf * nb * naux;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
          i += (long long)gridDim.x * blockDim.x) {
-        const int m = (int)(i % ldm);
-        const long long col = i / ldm;
-        double v = (m < nbf) ? b[m + (long long)nbf * col] : 0.0;
+        const int mi = (int)(i & 63);
+        const long long r = i >> 6;
+        const int n = (int)(r % nbf);
+        const long long r2 = r / nbf;
+        const int qb = (int)(r2 % nb);
+        const long long l = r2 / nb;
+        const int m = 64 * qb + mi;
+        double v = (m < nbf) ? b[m + (long long)nbf * n + (long long)nbf * nbf * l] : 0.0;
         const __nv_bfloat16 h = __double2bfloat16(v);
-        const __nv_bfloat16 l = __double2bfloat16(v - (double)__bfloat162float(h));
+        const __nv_bfloat16 lw = __double2bfloat16(v - (double)__bfloat162float(h));
         hi[i] = h;
-        lo[i] = l;
+        lo[i] = lw;
     }
 }
 
-// Cs[k + ldk*j], j < 64: C_hi[k, j]; 64 <= j < 128: C_lo[k, j-64]; zero beyond nbf5 / nbf.
+// Cs[k + ldk*j] = C_x[k, q] for j = prow(q, x) (x = 0: bf16 hi, 1: lo); zero beyond nbf5 / nbf.
 __global__ void split_c_kernel(const double* __restrict__ C, int nbf, int nbf5, int ldk,
                                __nv_bfloat16* __restrict__ cs) {
     const int total = ldk * 128;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
         const int k = i % ldk, j = i / ldk;
-        const int q = j & 63;
+        const int q = 16 * (j >> 5) + (j & 15), x = (j >> 4) & 1;  // j = prow(q, x)
         double v = (k < nbf && q < nbf5) ? C[k + (long long)nbf * q] : 0.0;
         const __nv_bfloat16 h = __double2bfloat16(v);
-        cs[i] = (j < 64) ? h : __double2bfloat16(v - (double)__bfloat162float(h));
+        cs[i] = (x == 0) ? h : __double2bfloat16(v - (double)__bfloat162float(h));
     }
 }
 
-// out[j + n*i] = a[i + n*j] (n x n transpose to FP32)
-__global__ void to_f32_transpose(const double* __restrict__ a, int n, float* __restrict__ out) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n * n; i += gridDim.x * blockDim.x) {
-        const int r = i % n, c = i / n;
-        out[c + n * r] = (float)a[i];
+// n, cj12 and ck12 of the functional in FP32, zero-padded to 64:
+// n32[q], cj32[q + 64 c] = cj12[q, c], ck32[q + 64 b] = ck12[b, q]
+__global__ void prep_coef_kernel(const double* __restrict__ n, const double* __restrict__ cj12,
+                                 const double* __restrict__ ck12, int nbf5, float* __restrict__ n32,
+                                 float* __restrict__ cj32, float* __restrict__ ck32) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 64 * 64; i += gridDim.x * blockDim.x) {
+        const int r = i & 63, c = i >> 6;
+        const bool in = r < nbf5 && c < nbf5;
+        cj32[i] = in ? (float)cj12[r + nbf5 * c] : 0.f;
+        ck32[i] = in ? (float)ck12[c + nbf5 * r] : 0.f;
+        if (i < 64) n32[i] = (i < nbf5) ? (float)n[i] : 0.f;
     }
-}
-
-__global__ void to_f32_small(const double* __restrict__ a, int count, float* __restrict__ out) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) out[i] = (float)a[i];
 }
 
 // out[i] = sum_g part[g*stride + i] in FP64
@@ -730,7 +757,7 @@ int make_map(donof_ctx* ctx, CUtensorMap* map, const void* base, int rank, const
         set_error(ctx, "cuTensorMapEncodeTiled is not available");
         return DONOF_ERR_CUDA;
     }
-    cuuint32_t es[3] = {1, 1, 1};
+    cuuint32_t es[5] = {1, 1, 1, 1, 1};
     CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, rank, const_cast<void*>(base), dims, strides_bytes, box, es,
                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
@@ -798,11 +825,13 @@ int launch_mixed(donof_job* job, cudaStream_t st, int nbf5, int nalpha, int nbet
     const int ldm = ldm_of(nbf);
     CUtensorMap mhi, mlo, mcs;
     {
-        cuuint64_t dims[3] = {(cuuint64_t)nbf, (cuuint64_t)nbf, (cuuint64_t)naux};
-        cuuint64_t strides[2] = {(cuuint64_t)ldm * 2, (cuuint64_t)ldm * nbf * 2};
-        cuuint32_t box[3] = {mx::BOX_M, mx::KB, 1};
-        DONOF_CHECK(make_map(ctx, &mhi, job->b16hi, 3, dims, strides, box));
-        DONOF_CHECK(make_map(ctx, &mlo, job->b16lo, 3, dims, strides, box));
+        // quarter-major split: [mi + 64 n + 64 nbf qb + 64 nbf nb l], m = 64 qb + mi
+        const int nb = (nbf + 63) / 64;
+        cuuint64_t dims[4] = {64, (cuuint64_t)nbf, (cuuint64_t)nb, (cuuint64_t)naux};
+        cuuint64_t strides[3] = {128, (cuuint64_t)128 * nbf, (cuuint64_t)128 * nbf * nb};
+        cuuint32_t box[4] = {mx::BOX_M, mx::KB, 1, 1};
+        DONOF_CHECK(make_map(ctx, &mhi, job->b16hi, 4, dims, strides, box));
+        DONOF_CHECK(make_map(ctx, &mlo, job->b16lo, 4, dims, strides, box));
     }
     {
         cuuint64_t dims[2] = {(cuuint64_t)nbf, 128};
@@ -858,8 +887,8 @@ int read_status(donof_job* job, cudaStream_t st, const MixedScratch& S) {
 int convert_b_f32(donof_job* job) {
     // b split into bf16 hi + lo (the mixed form's copy of b)
     donof_ctx* ctx = job->ctx;
-    const int nbf = job->nbf, ldm = ldm_of(nbf);
-    const size_t count = (size_t)ldm * nbf * job->naux;
+    const int nbf = job->nbf, nb = (nbf + 63) / 64;
+    const size_t count = (size_t)64 * nb * nbf * job->naux;
     void* hi = nullptr;
     void* lo = nullptr;
     DONOF_CUDA(ctx, cudaMalloc(&hi, sizeof(__nv_bfloat16) * count));
@@ -869,7 +898,7 @@ int convert_b_f32(donof_job* job) {
         set_error(ctx, "cudaMalloc(b split): %s", cudaGetErrorString(e));
         return DONOF_ERR_OOM;
     }
-    mx::split_b_kernel<<<8 * ctx->sm_count, 256, 0, ctx->stream>>>(job->b, nbf, ldm, (long long)nbf * job->naux,
+    mx::split_b_kernel<<<8 * ctx->sm_count, 256, 0, ctx->stream>>>(job->b, nbf, nb, (long long)job->naux,
                                                                    static_cast<__nv_bfloat16*>(hi),
                                                                    static_cast<__nv_bfloat16*>(lo)); count_launch();
     e = cudaGetLastError();
@@ -923,9 +952,7 @@ int lagrange2_mixed(donof_job* job, cudaStream_t st, const double* C, const doub
     const int nbf = job->nbf, grid = mixed_grid(job);
     MixedScratch S;
     DONOF_CHECK(mixed_prepare(job, st, C, nbf5, &S, grid));
-    mx::to_f32_small<<<1, 256, 0, st>>>(n, nbf5, S.n32); count_launch();
-    mx::to_f32_small<<<16, 256, 0, st>>>(cj12, nbf5 * nbf5, S.cj32); count_launch();
-    mx::to_f32_transpose<<<16, 256, 0, st>>>(ck12, nbf5, S.ck32); count_launch();
+    mx::prep_coef_kernel<<<16, 256, 0, st>>>(n, cj12, ck12, nbf5, S.n32, S.cj32, S.ck32); count_launch();
     DONOF_CUDA(ctx, cudaGetLastError());
     DONOF_CHECK(launch_mixed(job, st, nbf5, nalpha, nbeta, 3, S, nullptr, nullptr, grid));
     // Y (FP64) = sum over CTAs of the FP32 partials
