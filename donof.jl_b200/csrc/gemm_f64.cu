@@ -126,6 +126,33 @@ int gemm_f64_auto(donof_ctx* ctx, cudaStream_t st, bool a_kmajor, bool b_kmajor,
     return gemm_f64(ctx, st, a_kmajor, b_kmajor, p, tile);
 }
 
+int gemm_f64_partials(donof_ctx* ctx, cudaStream_t st, bool a_kmajor, bool b_kmajor, int M, int N, int K,
+                      const double* A, long long lda, const double* B, long long ldb, DevBuf* part,
+                      const double** out, int* nparts) {
+    GemmF64Args p{};
+    p.M = M; p.N = N; p.K = K;
+    p.A = A; p.lda = lda; p.B = B; p.ldb = ldb;
+    p.alpha = 1.0; p.beta = 0.0; p.batch = 1; p.splits = 1; p.kchunk = K;
+    int splits = 1, kchunk = K;
+    const GemmTile tile = pick_tile(ctx, M, N, K, true, &splits);
+    if (splits > 1) {
+        kchunk = ((K + splits - 1) / splits + 15) / 16 * 16;
+        splits = (K + kchunk - 1) / kchunk;
+    }
+    const long long per = (long long)M * N;
+    DONOF_CHECK(part->ensure(ctx, sizeof(double) * per * splits));
+    p.C = part->as<double>(); p.ldc = M;
+    if (splits > 1) {
+        p.splits = splits;
+        p.kchunk = kchunk;
+        p.strideSplit = per;
+    }
+    DONOF_CHECK(gemm_f64(ctx, st, a_kmajor, b_kmajor, p, tile));
+    *out = part->as<double>();
+    *nparts = splits;
+    return DONOF_OK;
+}
+
 __global__ void splitk_reduce_kernel(const double* __restrict__ part, long long stride, int splits,
                                      long long count, double* __restrict__ out, double beta) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;

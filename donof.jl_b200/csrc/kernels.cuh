@@ -25,6 +25,20 @@ int gemm_f64_auto(donof_ctx* ctx, cudaStream_t st, bool a_kmajor, bool b_kmajor,
                   int K, const double* A, long long lda, const double* B, long long ldb,
                   double* C, long long ldc, double alpha, double beta, DevBuf* part);
 
+// Like gemm_f64_auto with alpha = 1, beta = 0, but the split-K partial sums are
+// left in `part` for the caller to reduce: *out = partials (ld M, stride M*N),
+// *nparts = their count (1 when the product was not split).
+int gemm_f64_partials(donof_ctx* ctx, cudaStream_t st, bool a_kmajor, bool b_kmajor, int M, int N, int K,
+                      const double* A, long long lda, const double* B, long long ldb, DevBuf* part,
+                      const double** out, int* nparts);
+
+// Fused FP64 tail of the Lagrangian (tail.cu): Y = sum of nparts partials
+// (FP32 or FP64, part[g * pstride + m + nbf * b]), HC = H C5, H_mat = C^T HC,
+// elag = [n o H_mat + C^T Y | 0] and E_elec (when E != nullptr).
+int elag_tail_f64(donof_job* job, cudaStream_t st, const double* C, const double* H, const double* n, int nbf5,
+                  const void* part, bool part_f32, int nparts, long long pstride, double* Hmat, double* elag,
+                  double* E);
+
 // FP64 pipelines (lagrange.cu)
 int transforms_f64(donof_job* job, cudaStream_t st, const double* C, int nbf5);
 int lagrange2_f64(donof_job* job, cudaStream_t st, const double* C, const double* n,
@@ -33,10 +47,7 @@ int lagrange2_f64(donof_job* job, cudaStream_t st, const double* C, const double
 int jkh_mo_f64(donof_job* job, cudaStream_t st, const double* C, const double* H, int nbf5,
                double* J, double* K, double* Hcore);
 
-// Shared tails of the Lagrangian / JKH_MO (lagrange.cu): elag = n o H_mat + C^T Y
-// (columns >= nbf5 zero) and E_elec; H_core from HC = H C5.
-int elag_finish_f64(donof_job* job, cudaStream_t st, const double* C, const double* n, const double* Hmat,
-                    const double* Y, int nbf5, double* elag, double* E);
+// H_core from HC = H C5 (lagrange.cu).
 int hcore_f64(donof_job* job, cudaStream_t st, const double* C, const double* HC, int nbf5, double* Hcore);
 
 // Mixed-precision pipelines (mixed.cu)

@@ -184,15 +184,6 @@ int lagrange2_f64(donof_job* job, cudaStream_t st, const double* C, const double
     donof_ctx* ctx = job->ctx;
     const int nbf = job->nbf, naux = job->naux;
     const long long Kt = (long long)nbf5 * naux;
-    DONOF_CHECK(job->small.ensure(ctx, sizeof(double) * (size_t)nbf * nbf5 * 2));
-    double* HC = job->small.as<double>();
-    double* Y = HC + (size_t)nbf * nbf5;
-
-    // H_mat = C^T (H C5)       (src/utils.jl:17-18)
-    DONOF_CHECK(gemm_f64_auto(ctx, st, false, true, nbf, nbf5, nbf, H, nbf, C, nbf, HC, nbf, 1.0,
-                              0.0, &job->part));
-    DONOF_CHECK(gemm_f64_auto(ctx, st, true, true, nbf, nbf5, nbf, C, nbf, HC, nbf, Hmat, nbf, 1.0,
-                              0.0, &job->part));
 
     DONOF_CHECK(transforms_f64(job, st, C, nbf5));
 
@@ -202,36 +193,13 @@ int lagrange2_f64(donof_job* job, cudaStream_t st, const double* C, const double
                                                                  ck12, nbf5, naux, nalpha, nbeta, W); count_launch();
     DONOF_CUDA(ctx, cudaGetLastError());
 
-    // Y = sum_{q,l} tmp[m, q + nbf5*l] W[q + nbf5*l, b]
-    DONOF_CHECK(gemm_f64_auto(ctx, st, false, true, nbf, nbf5, (int)Kt, job->tmp.as<double>(), nbf,
-                              W, Kt, Y, nbf, 1.0, 0.0, &job->part));
-
-    // elag = n o H_mat (cols < nbf5), 0 elsewhere; then elag[:, :nbf5] += C^T Y
-    elag_init_kernel<<<grid_for((long long)nbf * nbf, 256, ctx->sm_count), 256, 0, st>>>(Hmat, n, nbf,
-                                                                                      nbf5, elag); count_launch();
-    DONOF_CUDA(ctx, cudaGetLastError());
-    DONOF_CHECK(gemm_f64_auto(ctx, st, true, true, nbf, nbf5, nbf, C, nbf, Y, nbf, elag, nbf, 1.0,
-                              1.0, &job->part));
-    if (E != nullptr) {
-        e_elec_kernel<<<1, 256, 0, st>>>(elag, Hmat, n, nbf, nbf5, E); count_launch();
-        DONOF_CUDA(ctx, cudaGetLastError());
-    }
-    return DONOF_OK;
-}
-
-int elag_finish_f64(donof_job* job, cudaStream_t st, const double* C, const double* n, const double* Hmat,
-                    const double* Y, int nbf5, double* elag, double* E) {
-    donof_ctx* ctx = job->ctx;
-    const int nbf = job->nbf;
-    elag_init_kernel<<<grid_for((long long)nbf * nbf, 256, ctx->sm_count), 256, 0, st>>>(Hmat, n, nbf, nbf5,
-                                                                                      elag); count_launch();
-    DONOF_CUDA(ctx, cudaGetLastError());
-    DONOF_CHECK(gemm_f64_auto(ctx, st, true, true, nbf, nbf5, nbf, C, nbf, Y, nbf, elag, nbf, 1.0, 1.0, &job->part));
-    if (E != nullptr) {
-        e_elec_kernel<<<1, 256, 0, st>>>(elag, Hmat, n, nbf, nbf5, E); count_launch();
-        DONOF_CUDA(ctx, cudaGetLastError());
-    }
-    return DONOF_OK;
+    // Y = sum_{q,l} tmp[m, q + nbf5*l] W[q + nbf5*l, b], left as split-K partials
+    const double* ypart = nullptr;
+    int nparts = 1;
+    DONOF_CHECK(gemm_f64_partials(ctx, st, false, true, nbf, nbf5, (int)Kt, job->tmp.as<double>(), nbf, W, Kt,
+                                  &job->part, &ypart, &nparts));
+    // H_mat = C^T (H C5) (src/utils.jl:17-18), elag = [n o H_mat + C^T Y | 0], E_elec
+    return elag_tail_f64(job, st, C, H, n, nbf5, ypart, false, nparts, (long long)nbf * nbf5, Hmat, elag, E);
 }
 
 int hcore_f64(donof_job* job, cudaStream_t st, const double* C, const double* HC, int nbf5, double* Hcore) {

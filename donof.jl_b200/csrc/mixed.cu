@@ -5,12 +5,16 @@
 // functional weights are split the same way, and every product is formed from
 // all four hi/lo pairs with FP32 accumulation in tensor memory (TMEM).  The
 // hi and lo halves of the small operand are stacked as the 128 rows of one
-// MMA, so one tcgen05.mma (M = 128) yields both partial products.
+// MMA, so one tcgen05.mma (M = 128) yields both partial products; the row of
+// part x (0 hi, 1 lo) of index q is prow(q, x) = 32 (q / 16) + 16 x + q % 16,
+// which puts both parts of q in one warp's TMEM lanes (i and i + 16), so the
+// hi + lo sums are warp shuffles.
 //
 // One persistent kernel (lag_mixed_kernel) walks the aux index l and, per l,
 // without leaving the SM:
-//   T1  D1[j, m] = sum_n Cs[j, n] b_x[n, m]      (x = hi, lo; j = q | 64+q)
-//       tmp[m, q] = D1[q, m] + D1[64+q, m]
+//   T1  D1[j, m] = sum_n Cs[j, n] b_x[n, m]      (x = hi, lo; j = prow(q, x)),
+//       one 64-column quarter of m at a time into two ping-pong TMEM slots
+//       tmp[m, q] = D1[prow(q, 0), m] + D1[prow(q, 1), m]
 //   T2  D2[j, j'] = sum_m tmp_x[m, q] Cs[j', m]  -> b_pq = sum of 4 quadrants
 //   W   W[q, b] = delta_qb (n'_b d_b + sum_q' cj12[b,q'] d_q') - ck12[b,q] b_bq
 //   Y   D3[j, m] += sum_q W_x[q, b] tmp_y[m, q]   (accumulated over all l of the CTA)
@@ -39,7 +43,6 @@ namespace mx {
 constexpr int NTHREADS = 192;
 constexpr int KB = 64;                // n rows per b stage (8 KB TMA boxes)
 constexpr int BOX_M = 64;             // m per TMA box (128 B of bf16) = one T1 quarter
-constexpr int MAXNB = 4;              // up to 4 boxes -> nbf <= 256
 constexpr int BOX_BYTES = KB * BOX_M * 2;           // 8 KB
 constexpr int STAGE_BYTES = 2 * BOX_BYTES;          // hi + lo, 16 KB
 constexpr int RING = 4;                             // b stages in shared memory (64 KB)
@@ -86,7 +89,7 @@ constexpr long long WAIT_CYCLES = 4000000000LL;  // ~2 s of SM clock
 struct Params {
     int nbf, nbf5, naux, nalpha, nbeta;
     int nb;                  // 64-wide m boxes (N = 64 * nb)
-    int nkb;                 // b stages per l (ceil(nbf / 32))
+    int nkb;                 // b stages per quarter of m (ceil(nbf / KB))
     int ncs;                 // 64-wide k boxes of Cs (ceil(nbf / 64))
     int mode;                // 1: write tmp; 2: write b_pq; 3: full Lagrangian
     const float* n32;        // n (nbf5)
@@ -606,16 +609,25 @@ lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_const
                     const bool dj = (P.nbeta > 0) && (q < P.nbeta || q >= P.nalpha);
                     diag = (dj ? P.n32[q] * ds[q] : 0.f) + t;
                 }
-                // A3 rows prow(b, 0) (hi) / prow(b, 1) (lo), K = q, for b in this thread's range
+                // This thread builds part of A3 row b = q (hi: prow(q, 0), lo: prow(q, 1)) over
+                // K = k in [off, off + 32), using the symmetry of b_pq (bq[i] = b_pq[off + i, q]):
+                // W[k, q] = delta_kq (n'_q d_q + t_q) - ck12[q, k] b_pq[q, k]
+                const float4* ckrow = reinterpret_cast<const float4*>(cks + q * 64 + off);  // ck12[q, off + i]
+                const int rh = prow(q, 0), rl = prow(q, 1);
 #pragma unroll
-                for (int i = 0; i < 32; ++i) {
-                    const int b = off + i;
-                    float w = 0.f;
-                    if (q < P.nbf5 && b < P.nbf5) w = -cks[b * 64 + q] * bq[i] + (b == q ? diag : 0.f);
-                    __nv_bfloat16 h, lo;
-                    split_bf16(w, h, lo);
-                    *reinterpret_cast<__nv_bfloat16*>(sm + OFF_A3 + sw128(prow(b, 0), q)) = h;
-                    *reinterpret_cast<__nv_bfloat16*>(sm + OFF_A3 + sw128(prow(b, 1), q)) = lo;
+                for (int c = 0; c < 4; ++c) {
+                    const float4 k0 = ckrow[2 * c], k1 = ckrow[2 * c + 1];
+                    const float ck8[8] = {k0.x, k0.y, k0.z, k0.w, k1.x, k1.y, k1.z, k1.w};
+                    __align__(16) __nv_bfloat16 h[8], lo[8];
+#pragma unroll
+                    for (int e = 0; e < 8; ++e) {
+                        const int i = 8 * c + e, k = off + i;
+                        float w = 0.f;
+                        if (q < P.nbf5 && k < P.nbf5) w = -ck8[e] * bq[i] + (k == q ? diag : 0.f);
+                        split_bf16(w, h[e], lo[e]);
+                    }
+                    *reinterpret_cast<uint4*>(sm + OFF_A3 + sw128(rh, off + 8 * c)) = *reinterpret_cast<const uint4*>(h);
+                    *reinterpret_cast<uint4*>(sm + OFF_A3 + sw128(rl, off + 8 * c)) = *reinterpret_cast<const uint4*>(lo);
                 }
             }
             fence_async_smem();
@@ -701,17 +713,6 @@ __global__ void prep_coef_kernel(const double* __restrict__ n, const double* __r
         cj32[i] = in ? (float)cj12[r + nbf5 * c] : 0.f;
         ck32[i] = in ? (float)ck12[c + nbf5 * r] : 0.f;
         if (i < 64) n32[i] = (i < nbf5) ? (float)n[i] : 0.f;
-    }
-}
-
-// out[i] = sum_g part[g*stride + i] in FP64
-__global__ void reduce_f32_to_f64(const float* __restrict__ part, long long stride, int parts, long long count,
-                                  double* __restrict__ out) {
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
-         i += (long long)gridDim.x * blockDim.x) {
-        double s = 0.0;
-        for (int g = 0; g < parts; ++g) s += (double)part[i + g * stride];
-        out[i] = s;
     }
 }
 
@@ -877,11 +878,6 @@ int check_mixed(donof_job* job, int nbf5) {
     return DONOF_OK;
 }
 
-int read_status(donof_job* job, cudaStream_t st, const MixedScratch& S) {
-    (void)job; (void)st; (void)S;
-    return DONOF_OK;
-}
-
 }  // namespace
 
 int convert_b_f32(donof_job* job) {
@@ -917,7 +913,7 @@ int convert_b_f32(donof_job* job) {
 int transforms_mixed(donof_job* job, cudaStream_t st, const double* C, int nbf5) {
     DONOF_CHECK(check_mixed(job, nbf5));
     donof_ctx* ctx = job->ctx;
-    const int nbf = job->nbf, naux = job->naux, grid = mixed_grid(job);
+    const int naux = job->naux, grid = mixed_grid(job);
     MixedScratch S;
     DONOF_CHECK(mixed_prepare(job, st, C, nbf5, &S, grid));
     DONOF_CHECK(job->tmp.ensure(ctx, sizeof(float) * (size_t)nbf5 * nbf5 * naux));
@@ -955,17 +951,8 @@ int lagrange2_mixed(donof_job* job, cudaStream_t st, const double* C, const doub
     mx::prep_coef_kernel<<<16, 256, 0, st>>>(n, cj12, ck12, nbf5, S.n32, S.cj32, S.ck32); count_launch();
     DONOF_CUDA(ctx, cudaGetLastError());
     DONOF_CHECK(launch_mixed(job, st, nbf5, nalpha, nbeta, 3, S, nullptr, nullptr, grid));
-    // Y (FP64) = sum over CTAs of the FP32 partials
-    const long long ny = (long long)nbf * nbf5;
-    mx::reduce_f32_to_f64<<<(int)((ny + 255) / 256), 256, 0, st>>>(S.ypart, ny, grid, ny, S.Y); count_launch();
-    DONOF_CUDA(ctx, cudaGetLastError());
-    // H_mat = C^T (H C5) and elag = n o H_mat + C^T Y in FP64
-    DONOF_CHECK(job->small.ensure(ctx, sizeof(double) * (size_t)nbf * nbf5 * 2));
-    double* HC = job->small.as<double>();
-    DONOF_CHECK(gemm_f64_auto(ctx, st, false, true, nbf, nbf5, nbf, H, nbf, C, nbf, HC, nbf, 1.0, 0.0, &job->part));
-    DONOF_CHECK(gemm_f64_auto(ctx, st, true, true, nbf, nbf5, nbf, C, nbf, HC, nbf, Hmat, nbf, 1.0, 0.0, &job->part));
-    DONOF_CHECK(elag_finish_f64(job, st, C, n, Hmat, S.Y, nbf5, elag, E));
-    return DONOF_OK;
+    // Y (FP64) = sum over CTAs of the FP32 partials; H_mat, elag and E_elec in FP64
+    return elag_tail_f64(job, st, C, H, n, nbf5, S.ypart, true, grid, (long long)nbf * nbf5, Hmat, elag, E);
 }
 
 int jkh_mo_mixed(donof_job* job, cudaStream_t st, const double* C, const double* H, int nbf5, double* J, double* K,

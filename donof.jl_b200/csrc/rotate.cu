@@ -15,6 +15,7 @@
 #include <math.h>
 #include <stdlib.h>
 
+#include "dtile.cuh"
 #include "kernels.cuh"
 
 namespace donof {
@@ -193,20 +194,18 @@ int rotate_f64_gated(donof_ctx* ctx, cudaStream_t st, const double* y, int nbf, 
 // Single-launch form: one cooperative kernel runs every stage of the same
 // algorithm (unpack + norm, X^2, X^3 and X^4, the Paterson-Stockmeyer
 // combinations, the two Horner products, the s squarings and C E^(2^s)) with
-// a grid barrier between stages, instead of ~25 separate launches.  Each CTA
-// computes 32 x 32 output tiles on the FP64 MMA pipe (mma.sync m16n8k4 .f64).
-// Every barrier wait is bounded; on a timeout the kernel records the error in
-// the rotation state and returns (its output is then not valid).
+// a bounded grid barrier between stages, instead of ~25 separate launches.
+// The products are split into 32 x 16 tiles (dtile.cuh) spread over the SMs.
+// On a barrier timeout the kernel records the error and returns (its output
+// is then not valid).
 // ---------------------------------------------------------------------------
 namespace {
 
-constexpr long long BARRIER_CYCLES = 2000000000LL;  // ~1 s
+constexpr int RT_TN = 16;  // tile width of the rotation products
 
 struct CoopState {
     unsigned long long norm_bits;
-    unsigned bar_count;
-    unsigned bar_gen;
-    int err;
+    dtile::GridSync gs;
 };
 
 struct CoopArgs {
@@ -218,107 +217,34 @@ struct CoopArgs {
     CoopState* cs;
 };
 
-// Bounded grid barrier for a co-resident (cooperatively launched) grid.
-__device__ bool coop_barrier(CoopState* cs) {
-    __shared__ int fail;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        fail = 0;
-        volatile unsigned* vgen = &cs->bar_gen;
-        const unsigned g0 = *vgen;
-        __threadfence();
-        if (atomicAdd(&cs->bar_count, 1u) == gridDim.x - 1) {
-            cs->bar_count = 0;
-            __threadfence();
-            atomicAdd(&cs->bar_gen, 1u);
-        } else {
-            const long long t0 = clock64();
-            while (*vgen == g0) {
-                if (clock64() - t0 > BARRIER_CYCLES || *(volatile int*)&cs->err) {
-                    atomicExch(&cs->err, 1);
-                    fail = 1;
-                    break;
-                }
-            }
-        }
-        __threadfence();
-    }
-    __syncthreads();
-    return fail == 0;
+__device__ __forceinline__ dtile::Gemm sq_gemm(int n, const double* A, const double* B, double* C, double alpha,
+                                               bool accumulate) {
+    dtile::Gemm g;
+    g.A = A; g.lda = n; g.ta = false;
+    g.B = B; g.ldb = n; g.tb = false;
+    g.C = C; g.ldc = n;
+    g.M = n; g.N = n; g.K = n;
+    g.alpha = alpha; g.accumulate = accumulate;
+    return g;
 }
 
-// C(i,j) = alpha * sum_k A[i + k*n] B[k + j*n] (+ C(i,j) when accumulate) for one
-// 32 x 32 output tile; 128 threads as 2 x 2 warps of 16 x 16.
-__device__ void tile_mm32(const double* __restrict__ A, const double* __restrict__ B, double* __restrict__ Cm,
-                          int n, int tile, double alpha, bool accumulate, double* sm) {
-    const int nt = (n + 31) / 32;
-    const int i0 = (tile % nt) * 32, j0 = (tile / nt) * 32;
-    double* As = sm;            // [k][i], stride 36 (conflict-free fragment reads)
-    double* Bs = sm + 16 * 36;  // [j][k], stride 20
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int g = lane >> 2, t = lane & 3;
-    const int wrow = (warp & 1) * 16, wcol = (warp >> 1) * 16;
-    double acc[2][4] = {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}};
-    double ra[4], rb[4];
-    auto fetch = [&](int k0) {
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            const int e = tid + 128 * r;
-            const int i = e & 31, k = e >> 5;  // A: 32 rows x 16 k
-            const int gi = i0 + i, gk = k0 + k;
-            ra[r] = (gi < n && gk < n) ? A[gi + (long long)gk * n] : 0.0;
-            const int kb = e & 15, j = e >> 4;  // B: 16 k x 32 cols
-            const int gkb = k0 + kb, gj = j0 + j;
-            rb[r] = (gkb < n && gj < n) ? B[gkb + (long long)gj * n] : 0.0;
-        }
-    };
-    fetch(0);
-    for (int k0 = 0; k0 < n; k0 += 16) {
-        __syncthreads();
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            const int e = tid + 128 * r;
-            As[(e >> 5) * 36 + (e & 31)] = ra[r];
-            Bs[(e >> 4) * 20 + (e & 15)] = rb[r];
-        }
-        __syncthreads();
-        if (k0 + 16 < n) fetch(k0 + 16);  // next block in flight during the MMAs
-#pragma unroll
-        for (int kk = 0; kk < 16; kk += 4) {
-            const double a0 = As[(kk + t) * 36 + wrow + g];
-            const double a1 = As[(kk + t) * 36 + wrow + g + 8];
-#pragma unroll
-            for (int ni = 0; ni < 2; ++ni) {
-                const double b0 = Bs[(wcol + ni * 8 + g) * 20 + kk + t];
-                gemm_detail::mma_f64_16x8x4(acc[ni], a0, a1, b0);
-            }
-        }
-    }
-#pragma unroll
-    for (int ni = 0; ni < 2; ++ni)
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            const int i = i0 + wrow + g + ((e >= 2) ? 8 : 0);
-            const int j = j0 + wcol + ni * 8 + 2 * t + (e & 1);
-            if (i < n && j < n) {
-                double* dst = Cm + i + (long long)j * n;
-                const double v = alpha * acc[ni][e];
-                *dst = accumulate ? *dst + v : v;
-            }
-        }
+__device__ __forceinline__ void run_tiles(const dtile::Gemm& g, double* sm) {
+    const int nt = dtile::tiles<RT_TN>(g);
+    for (int w = blockIdx.x; w < nt; w += gridDim.x) dtile::tile<RT_TN>(g, w, sm);
 }
 
-__global__ void __launch_bounds__(128) rotate_coop_kernel(const CoopArgs a) {
-    __shared__ __align__(16) double sm[16 * 36 + 32 * 20];
-    __shared__ double red[4];
+__global__ void __launch_bounds__(dtile::THREADS) rotate_coop_kernel(const CoopArgs a) {
+    extern __shared__ __align__(16) double sm[];
+    __shared__ double red[dtile::WARPS];
     const int n = a.nbf, G = gridDim.x, cta = blockIdx.x, tid = threadIdx.x;
     const long long nn = (long long)n * n;
-    const int nt = (n + 31) / 32, ntiles = nt * nt;
     CoopState* cs = a.cs;
+    dtile::GridSync* gs = &cs->gs;
+    unsigned epoch = 0;
     // S0: unpack y into Y, column sums of |Y| -> ||Y||_1
     for (int j = cta; j < n; j += G) {
         double s = 0.0;
-        for (int i = tid; i < n; i += 128) {
+        for (int i = tid; i < n; i += dtile::THREADS) {
             double v = 0.0;
             if (i < j && i < a.nbf5) v = a.y[packed_index(i, j, n)];
             else if (j < i && j < a.nbf5) v = -a.y[packed_index(j, i, n)];
@@ -328,51 +254,76 @@ __global__ void __launch_bounds__(128) rotate_coop_kernel(const CoopArgs a) {
         for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
         if ((tid & 31) == 0) red[tid >> 5] = s;
         __syncthreads();
-        if (tid == 0) atomicMax(&cs->norm_bits, (unsigned long long)__double_as_longlong(red[0] + red[1] + red[2] + red[3]));
+        if (tid == 0) {
+            double t = 0.0;
+            for (int w = 0; w < dtile::WARPS; ++w) t += red[w];
+            atomicMax(&cs->norm_bits, (unsigned long long)__double_as_longlong(t));
+        }
         __syncthreads();
     }
-    if (!coop_barrier(cs)) return;
+    if (!dtile::grid_barrier(gs, epoch)) return;
     const double norm = __longlong_as_double((long long)cs->norm_bits);
     int s = 0;
     if (norm > 0.25) s = (int)ceil(log2(norm / 0.25));
     if (s > SMAX) s = SMAX;
-    const double sc = ldexp(1.0, -s);  // X = sc * Y
+    const double sc = ldexp(1.0, -s);  // X = sc * Y (a power of two: exact)
     // S1: X2 = X X
-    for (int w = cta; w < ntiles; w += G) tile_mm32(a.Y, a.Y, a.X2, n, w, sc * sc, false, sm);
-    if (!coop_barrier(cs)) return;
+    run_tiles(sq_gemm(n, a.Y, a.Y, a.X2, sc * sc, false), sm);
+    if (!dtile::grid_barrier(gs, epoch)) return;
     // S2: X3 = X2 X, X4 = X2 X2
-    for (int w = cta; w < 2 * ntiles; w += G) {
-        if (w < ntiles) tile_mm32(a.X2, a.Y, a.X3, n, w, sc, false, sm);
-        else tile_mm32(a.X2, a.X2, a.X4, n, w - ntiles, 1.0, false, sm);
+    {
+        const dtile::Gemm g3 = sq_gemm(n, a.X2, a.Y, a.X3, sc, false);
+        const dtile::Gemm g4 = sq_gemm(n, a.X2, a.X2, a.X4, 1.0, false);
+        const int nt = dtile::tiles<RT_TN>(g3);
+        for (int w = cta; w < 2 * nt; w += G) {
+            if (w < nt) dtile::tile<RT_TN>(g3, w, sm);
+            else dtile::tile<RT_TN>(g4, w - nt, sm);
+        }
     }
-    if (!coop_barrier(cs)) return;
+    if (!dtile::grid_barrier(gs, epoch)) return;
     // S3: the three polynomial blocks of the degree-12 Taylor sum (1/k! coefficients)
     {
         double c[13];
         c[0] = 1.0;
         for (int k = 1; k <= 12; ++k) c[k] = c[k - 1] / k;
-        for (long long idx = cta * 128LL + tid; idx < nn; idx += (long long)G * 128) {
-            const double dg = ((idx % n) == (idx / n)) ? 1.0 : 0.0;
-            const double x = sc * a.Y[idx], x2 = a.X2[idx], x3 = a.X3[idx], x4 = a.X4[idx];
-            a.P[idx] = c[12] * x4 + c[11] * x3 + c[10] * x2 + c[9] * x + c[8] * dg;
-            a.E1[idx] = c[7] * x3 + c[6] * x2 + c[5] * x + c[4] * dg;
-            a.bufs[idx] = c[3] * x3 + c[2] * x2 + c[1] * x + c[0] * dg;
+        // four elements per thread and pass: every load is issued before the stores
+        constexpr int U = 4;
+        const long long stride = (long long)G * dtile::THREADS;
+        for (long long base = cta * (long long)dtile::THREADS + tid; base < nn; base += U * stride) {
+            double x[U], x2[U], x3[U], x4[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const long long idx = base + u * stride;
+                const bool in = idx < nn;
+                x[u] = in ? sc * a.Y[idx] : 0.0;
+                x2[u] = in ? a.X2[idx] : 0.0;
+                x3[u] = in ? a.X3[idx] : 0.0;
+                x4[u] = in ? a.X4[idx] : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const long long idx = base + u * stride;
+                if (idx >= nn) break;
+                const double dg = ((idx % n) == (idx / n)) ? 1.0 : 0.0;
+                a.P[idx] = c[12] * x4[u] + c[11] * x3[u] + c[10] * x2[u] + c[9] * x[u] + c[8] * dg;
+                a.E1[idx] = c[7] * x3[u] + c[6] * x2[u] + c[5] * x[u] + c[4] * dg;
+                a.bufs[idx] = c[3] * x3[u] + c[2] * x2[u] + c[1] * x[u] + c[0] * dg;
+            }
         }
     }
-    if (!coop_barrier(cs)) return;
+    if (!dtile::grid_barrier(gs, epoch)) return;
     // S4: E1 += P X4;  S5: E0 = bufs[0] += E1 X4
-    for (int w = cta; w < ntiles; w += G) tile_mm32(a.P, a.X4, a.E1, n, w, 1.0, true, sm);
-    if (!coop_barrier(cs)) return;
-    for (int w = cta; w < ntiles; w += G) tile_mm32(a.E1, a.X4, a.bufs, n, w, 1.0, true, sm);
-    if (!coop_barrier(cs)) return;
+    run_tiles(sq_gemm(n, a.P, a.X4, a.E1, 1.0, true), sm);
+    if (!dtile::grid_barrier(gs, epoch)) return;
+    run_tiles(sq_gemm(n, a.E1, a.X4, a.bufs, 1.0, true), sm);
+    if (!dtile::grid_barrier(gs, epoch)) return;
     // squarings: bufs[k+1] = bufs[k]^2
     for (int k = 0; k < s; ++k) {
-        for (int w = cta; w < ntiles; w += G) tile_mm32(a.bufs + k * nn, a.bufs + k * nn, a.bufs + (k + 1) * nn, n, w,
-                                                        1.0, false, sm);
-        if (!coop_barrier(cs)) return;
+        run_tiles(sq_gemm(n, a.bufs + k * nn, a.bufs + k * nn, a.bufs + (k + 1) * nn, 1.0, false), sm);
+        if (!dtile::grid_barrier(gs, epoch)) return;
     }
     // C_new = C E^(2^s)
-    for (int w = cta; w < ntiles; w += G) tile_mm32(a.C, a.bufs + s * nn, a.Cnew, n, w, 1.0, false, sm);
+    run_tiles(sq_gemm(n, a.C, a.bufs + s * nn, a.Cnew, 1.0, false), sm);
 }
 
 }  // namespace
@@ -395,18 +346,28 @@ int rotate_f64(donof_ctx* ctx, cudaStream_t st, const double* y, int nbf, int nb
     a.X2 = a.Y + nn; a.X3 = a.Y + 2 * nn; a.X4 = a.Y + 3 * nn; a.P = a.Y + 4 * nn;
     a.bufs = a.Y + 5 * nn;           // E^(2^k), k = 0..SMAX
     a.E1 = a.bufs + (SMAX + 1) * nn;  // extra slot
-    const int ntiles = ((nbf + 31) / 32) * ((nbf + 31) / 32);
+    const int smem = (int)sizeof(double) * dtile::smem_doubles<RT_TN>();
+    static unsigned long long attr_mask = 0;
+    const unsigned long long bit = 1ull << (ctx->device & 63);
+    if (!(attr_mask & bit)) {
+        DONOF_CUDA(ctx, cudaFuncSetAttribute(rotate_coop_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        attr_mask |= bit;
+    }
     int per_sm = 0;
-    DONOF_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rotate_coop_kernel, 128, 0));
-    int grid = ctx->sm_count * (per_sm > 0 ? per_sm : 1);
-    if (grid > 2 * ntiles) grid = 2 * ntiles;  // stage S2 has 2 * ntiles tiles
-    if (grid > ctx->sm_count) grid = ctx->sm_count;
+    DONOF_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rotate_coop_kernel, dtile::THREADS, smem));
+    if (per_sm < 1) {
+        set_error(ctx, "rotate_coop_kernel does not fit on an SM");
+        return DONOF_ERR_CUDA;
+    }
+    const int mt = (nbf + dtile::TM - 1) / dtile::TM, ntile = mt * ((nbf + RT_TN - 1) / RT_TN);
+    int grid = ctx->sm_count;                  // one CTA per SM (co-resident: the kernel has grid barriers)
+    if (grid > 2 * ntile) grid = 2 * ntile;    // stage S2 has 2 * ntile tiles
     if (grid < 1) grid = 1;
     DONOF_CUDA(ctx, cudaMemsetAsync(a.cs, 0, sizeof(CoopState), st));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);
-    cfg.blockDim = dim3(128);
-    cfg.dynamicSmemBytes = 0;
+    cfg.blockDim = dim3(dtile::THREADS);
+    cfg.dynamicSmemBytes = smem;
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeCooperative;

@@ -1,0 +1,184 @@
+// The FP64 tail of the orbital-gradient Lagrangian, in one cooperative launch
+// (src/utils.jl:17-18 and :39 for H_mat and elag, :216-227 for the energy):
+//
+//   Y      = sum_g part_g            partial sums of Y = sum_l tmp_l W_l (FP32 per-CTA
+//                                    partials of the mixed kernel, or FP64 split-K partials)
+//   HC     = H C5                    (nbf x nbf5)
+//   Bp     = HC diag(n) + Y
+//   H_mat  = C^T HC                  (nbf x nbf5)
+//   elag   = [C^T Bp | 0]            = n o H_mat + C^T Y on the first nbf5 columns
+//   E_elec = sum_{i < nbf5} elag[i, i] + n_i H_mat[i, i]
+//
+// Stage 1 runs the HC tiles and the reduction of the Y partials side by side,
+// stage 2 forms Bp, stage 3 the H_mat and elag tiles; the last CTA to finish
+// stage 3 sums the energy in a fixed order.  Bounded grid barriers separate
+// the stages.
+#include "dtile.cuh"
+#include "kernels.cuh"
+
+namespace donof {
+
+namespace {
+
+constexpr int TL_TN = 16;
+
+struct TailState {
+    dtile::GridSync gs;
+    unsigned done;
+    unsigned pad[3];
+};
+
+struct TailArgs {
+    const double* C;
+    const double* H;
+    const double* n;
+    int nbf, nbf5;
+    const void* part;  // part[g * pstride + m + nbf * b]
+    int part_f32;
+    int nparts;
+    long long pstride;
+    double *Y, *HC, *Bp;  // scratch, nbf x nbf5 each
+    double *Hmat, *elag, *E;
+    TailState* ts;
+};
+
+__global__ void __launch_bounds__(dtile::THREADS) elag_tail_kernel(const TailArgs a) {
+    extern __shared__ __align__(16) double sm[];
+    const int nbf = a.nbf, nbf5 = a.nbf5, G = gridDim.x, cta = blockIdx.x, tid = threadIdx.x;
+    const long long ny = (long long)nbf * nbf5;
+    dtile::GridSync* gs = &a.ts->gs;
+    unsigned epoch = 0;
+
+    // ---- stage 1: HC = H C5 (tiles on the first CTAs), Y = sum of partials (the rest)
+    dtile::Gemm ghc;
+    ghc.A = a.H; ghc.lda = nbf; ghc.ta = false;
+    ghc.B = a.C; ghc.ldb = nbf; ghc.tb = false;
+    ghc.C = a.HC; ghc.ldc = nbf;
+    ghc.M = nbf; ghc.N = nbf5; ghc.K = nbf;
+    ghc.alpha = 1.0; ghc.accumulate = false;
+    const int nt_hc = dtile::tiles<TL_TN>(ghc);
+    const int red_ctas = G > nt_hc ? G - nt_hc : G;  // CTAs that reduce Y
+    const int red_first = G > nt_hc ? nt_hc : 0;
+    for (int w = cta; w < nt_hc; w += G) dtile::tile<TL_TN>(ghc, w, sm);
+    if (cta >= red_first) {
+        const int r = cta - red_first;
+        for (long long i = (long long)r * dtile::THREADS + tid; i < ny; i += (long long)red_ctas * dtile::THREADS) {
+            double s = 0.0;
+            if (a.part_f32) {
+                const float* p = static_cast<const float*>(a.part) + i;
+#pragma unroll 8
+                for (int g = 0; g < a.nparts; ++g) s += (double)__ldg(p + g * a.pstride);
+            } else {
+                const double* p = static_cast<const double*>(a.part) + i;
+#pragma unroll 8
+                for (int g = 0; g < a.nparts; ++g) s += __ldg(p + g * a.pstride);
+            }
+            a.Y[i] = s;
+        }
+    }
+    // columns nbf5.. of elag are zero
+    {
+        const long long z0 = (long long)nbf * nbf5, zn = (long long)nbf * nbf;
+        for (long long i = z0 + (long long)cta * dtile::THREADS + tid; i < zn; i += (long long)G * dtile::THREADS)
+            a.elag[i] = 0.0;
+    }
+    if (!dtile::grid_barrier(gs, epoch)) return;
+
+    // ---- stage 2: Bp = HC diag(n) + Y
+    for (long long i = (long long)cta * dtile::THREADS + tid; i < ny; i += (long long)G * dtile::THREADS)
+        a.Bp[i] = a.HC[i] * a.n[i / nbf] + a.Y[i];
+    if (!dtile::grid_barrier(gs, epoch)) return;
+
+    // ---- stage 3: H_mat = C^T HC, elag[:, :nbf5] = C^T Bp
+    dtile::Gemm gh;
+    gh.A = a.C; gh.lda = nbf; gh.ta = true;
+    gh.B = a.HC; gh.ldb = nbf; gh.tb = false;
+    gh.C = a.Hmat; gh.ldc = nbf;
+    gh.M = nbf; gh.N = nbf5; gh.K = nbf;
+    gh.alpha = 1.0; gh.accumulate = false;
+    dtile::Gemm ge = gh;
+    ge.B = a.Bp;
+    ge.C = a.elag;
+    const int nt = dtile::tiles<TL_TN>(gh);
+    for (int w = cta; w < 2 * nt; w += G) {
+        if (w < nt) dtile::tile<TL_TN>(gh, w, sm);
+        else dtile::tile<TL_TN>(ge, w - nt, sm);
+    }
+    if (a.E == nullptr) return;
+    // ---- energy: the last CTA to finish sums the diagonals in a fixed order
+    __shared__ unsigned last;
+    __shared__ double red[dtile::WARPS];
+    __syncthreads();
+    if (tid == 0) {
+        __threadfence();
+        last = (atomicAdd(&a.ts->done, 1u) == (unsigned)G - 1) ? 1u : 0u;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double s = 0.0;
+    for (int i = tid; i < nbf5; i += dtile::THREADS) {
+        const volatile double* el = a.elag;
+        const volatile double* hm = a.Hmat;
+        s += el[i + (long long)nbf * i] + a.n[i] * hm[i + (long long)nbf * i];
+    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((tid & 31) == 0) red[tid >> 5] = s;
+    __syncthreads();
+    if (tid == 0) {
+        double t = 0.0;
+        for (int w = 0; w < dtile::WARPS; ++w) t += red[w];
+        *a.E = t;
+    }
+}
+
+}  // namespace
+
+int elag_tail_f64(donof_job* job, cudaStream_t st, const double* C, const double* H, const double* n, int nbf5,
+                  const void* part, bool part_f32, int nparts, long long pstride, double* Hmat, double* elag,
+                  double* E) {
+    donof_ctx* ctx = job->ctx;
+    const int nbf = job->nbf;
+    const size_t ny = (size_t)nbf * nbf5;
+    DONOF_CHECK(job->small.ensure(ctx, 256 + sizeof(double) * 3 * ny));
+    char* base = job->small.as<char>();
+    TailArgs a{};
+    a.C = C; a.H = H; a.n = n;
+    a.nbf = nbf; a.nbf5 = nbf5;
+    a.part = part; a.part_f32 = part_f32 ? 1 : 0; a.nparts = nparts; a.pstride = pstride;
+    a.ts = reinterpret_cast<TailState*>(base);
+    a.Y = reinterpret_cast<double*>(base + 256);
+    a.HC = a.Y + ny;
+    a.Bp = a.HC + ny;
+    a.Hmat = Hmat; a.elag = elag; a.E = E;
+    const int smem = (int)sizeof(double) * dtile::smem_doubles<TL_TN>();
+    static unsigned long long attr_mask = 0;
+    const unsigned long long bit = 1ull << (ctx->device & 63);
+    if (!(attr_mask & bit)) {
+        DONOF_CUDA(ctx, cudaFuncSetAttribute(elag_tail_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        attr_mask |= bit;
+    }
+    int per_sm = 0;
+    DONOF_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, elag_tail_kernel, dtile::THREADS, smem));
+    if (per_sm < 1) {
+        set_error(ctx, "elag_tail_kernel does not fit on an SM");
+        return DONOF_ERR_CUDA;
+    }
+    const int grid = ctx->sm_count;  // one CTA per SM (co-resident: the kernel has grid barriers)
+    DONOF_CUDA(ctx, cudaMemsetAsync(a.ts, 0, sizeof(TailState), st));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(dtile::THREADS);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    DONOF_CUDA(ctx, cudaLaunchKernelEx(&cfg, elag_tail_kernel, a));
+    count_launch();
+    return DONOF_OK;
+}
+
+}  // namespace donof
