@@ -149,6 +149,55 @@ __device__ __forceinline__ void load_panel(const Gemm& g, int i0, int j0, int k0
     cp_async_commit();
 }
 
+// Copies of the K panels of one tile, set up once per tile: interior tiles of
+// non-transposed, 16-byte aligned operands with even leading dimensions take
+// a precomputed per-thread pointer (every thread copies the same row pair of
+// A and the same k pair of B in every panel); everything else, and the last
+// panel when K is not a multiple of KC, goes through load_panel.
+template <int TN>
+struct PanelLoader {
+    bool fast;
+    const double* a_src;  // this thread's first A pair of panel 0
+    const double* b_src;  // this thread's first B pair of panel 0
+    long long a_kstep;    // A elements between two k rows copied by this thread
+    long long b_jstep;    // B elements between two columns copied by this thread
+    long long a_panel;    // A elements between panels (KC k rows)
+    int a_dst, b_dst;     // offsets in the panel buffers
+
+    static constexpr int APER = TM / 2, AKSTEP = THREADS / APER;  // A: pairs per k row, k rows per pass
+    static constexpr int BPER = KC / 2, BJSTEP = THREADS / BPER;  // B: pairs per column, columns per pass
+
+    __device__ __forceinline__ PanelLoader(const Gemm& g, int i0, int j0) {
+        const int tid = threadIdx.x;
+        fast = !g.ta && !g.tb && (g.lda & 1) == 0 && (g.ldb & 1) == 0 &&
+               ((reinterpret_cast<uintptr_t>(g.A) | reinterpret_cast<uintptr_t>(g.B)) & 15) == 0 &&
+               i0 + TM <= g.M && j0 + TN <= g.N;
+        const int ai = 2 * (tid % APER), ak = tid / APER;
+        const int bk = 2 * (tid % BPER), bj = tid / BPER;
+        a_src = g.A + (i0 + ai) + (long long)ak * g.lda;
+        b_src = g.B + bk + (long long)(j0 + bj) * g.ldb;
+        a_kstep = (long long)AKSTEP * g.lda;
+        b_jstep = (long long)BJSTEP * g.ldb;
+        a_panel = (long long)KC * g.lda;
+        a_dst = ak * AS + ai;
+        b_dst = bj * BS + bk;
+    }
+
+    __device__ __forceinline__ void load(const Gemm& g, int i0, int j0, int p, double* As, double* Bs) const {
+        if (fast && (p + 1) * KC <= g.K) {
+            const double* sa = a_src + p * a_panel;
+            const double* sb = b_src + p * KC;
+#pragma unroll
+            for (int r = 0; r < KC / AKSTEP; ++r) cp_async16(As + a_dst + r * AKSTEP * AS, sa + r * a_kstep);
+#pragma unroll
+            for (int r = 0; r < TN / BJSTEP; ++r) cp_async16(Bs + b_dst + r * BJSTEP * BS, sb + r * b_jstep);
+            cp_async_commit();
+        } else {
+            load_panel<TN>(g, i0, j0, p * KC, As, Bs);
+        }
+    }
+};
+
 // One 32 x TN output tile (index t of the GEMM's tiles, column-major over the
 // tile grid).  sm holds smem_doubles<TN>() doubles.  The caller's CTA has
 // THREADS threads; every thread must call this.
@@ -174,11 +223,12 @@ __device__ void tile(const Gemm& g, int t, double* sm) {
     auto Bs = [&](int buf) { return sm + buf * (KC * AS + TN * BS) + KC * AS; };
 
     const int npan = (g.K + KC - 1) / KC;
+    const PanelLoader<TN> ld(g, i0, j0);
     __syncthreads();  // the buffers may still be read by the previous tile
     // prologue: the first NBUF - 1 panels in flight (one commit group each, empty ones too)
 #pragma unroll
     for (int p = 0; p < NBUF - 1; ++p) {
-        if (p < npan) load_panel<TN>(g, i0, j0, p * KC, As(p), Bs(p));
+        if (p < npan) ld.load(g, i0, j0, p, As(p), Bs(p));
         else cp_async_commit();
     }
     for (int p = 0; p < npan; ++p) {
@@ -186,7 +236,7 @@ __device__ void tile(const Gemm& g, int t, double* sm) {
         cp_async_wait<NBUF - 2>();
         __syncthreads();  // panel p visible to all; buffer (p - 1) % NBUF no longer read
         const int pn = p + NBUF - 1;
-        if (pn < npan) load_panel<TN>(g, i0, j0, pn * KC, As(pn % NBUF), Bs(pn % NBUF));
+        if (pn < npan) ld.load(g, i0, j0, pn, As(pn % NBUF), Bs(pn % NBUF));
         else cp_async_commit();
         const double* A_ = As(p % NBUF);
         const double* B_ = Bs(p % NBUF);
@@ -228,20 +278,20 @@ __device__ void tile(const Gemm& g, int t, double* sm) {
         old[u] = (inb[u] && g.accumulate) ? *dst[u] : 0.0;
     }
     __syncthreads();  // every warp is done with the panels: the ring becomes the reduction buffer
-    double* red = sm;  // red[(warp * 32 + lane) * V + v]
+    double* red = sm;  // red[(v * WARPS + warp) * 32 + lane]: lane-contiguous, conflict-free
 #pragma unroll
     for (int mi = 0; mi < MI; ++mi)
 #pragma unroll
         for (int ni = 0; ni < NI; ++ni)
 #pragma unroll
-            for (int e = 0; e < 4; ++e) red[(warp * 32 + lane) * V + (mi * NI + ni) * 4 + e] = acc[mi][ni][e];
+            for (int e = 0; e < 4; ++e) red[(((mi * NI + ni) * 4 + e) * WARPS + warp) * 32 + lane] = acc[mi][ni][e];
     __syncthreads();
 #pragma unroll
     for (int u = 0; u < U; ++u) {
         const int v = warp + WARPS * u;
         double s = 0.0;
 #pragma unroll
-        for (int w = 0; w < WARPS; ++w) s += red[(w * 32 + lane) * V + v];
+        for (int w = 0; w < WARPS; ++w) s += red[(v * WARPS + w) * 32 + lane];
         if (inb[u]) *dst[u] = old[u] + g.alpha * s;
     }
 }
