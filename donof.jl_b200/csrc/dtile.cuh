@@ -20,16 +20,18 @@ namespace dtile {
 constexpr int TM = 32;        // tile rows
 constexpr int KC = 64;        // K panel depth
 constexpr int NBUF = 3;       // panel buffers (ring)
-constexpr int AS = 36;        // A panel stride ([k][i], doubles): conflict-free fragment reads
-constexpr int BS = KC + 4;    // B panel stride ([j][k], doubles): conflict-free fragment reads
+constexpr int AS = 36;        // A panel stride, [k][i] layout (doubles): conflict-free fragment reads
+constexpr int ATS = KC + 4;   // A panel stride, [i][k] layout (transposed A)
+constexpr int BS = KC + 4;    // B panel stride, [j][k] layout
 constexpr int THREADS = 256;  // 8 warps, each on an eighth of every K panel
 constexpr int WARPS = THREADS / 32;
+constexpr int APANEL = (KC * AS > TM * ATS) ? KC * AS : TM * ATS;  // doubles of one A panel
 
 // Shared memory (doubles) of one tile product with TN output columns: the ring
 // of A and B panels, which also holds the final cross-warp sum.
 template <int TN>
 constexpr int smem_doubles() {
-    return (NBUF * (KC * AS + TN * BS) > THREADS * TN) ? NBUF * (KC * AS + TN * BS) : THREADS * TN;
+    return (NBUF * (APANEL + TN * BS) > THREADS * TN) ? NBUF * (APANEL + TN * BS) : THREADS * TN;
 }
 
 // C(i, j) for i < M, j < N of one GEMM: C = alpha opA(A) opB(B) (+ C when accumulate)
@@ -66,120 +68,83 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
-// Stage the K panel [k0, k0 + KC) of the tile (i0, j0) into As[k][i], Bs[j][k]
-// (zeros outside the matrices) as one cp.async group.  Non-transposed operands
-// with an even leading dimension and a 16-byte aligned base move two doubles
-// per copy; interior panels skip the bounds checks.
-template <int TN>
+// Shared-memory offset of A element (i, k) of a panel: [k][i] for A as stored,
+// [i][k] for a transposed A (both contiguous along the stored fast index).
+template <bool TA>
+__device__ __forceinline__ int aoff(int i, int k) { return TA ? i * ATS + k : k * AS + i; }
+
+// Stage the K panel [k0, k0 + KC) of the tile (i0, j0) into the A and B panel
+// buffers (zeros outside the matrices) as one cp.async group; the general
+// path, used at the edges of the matrices and for unaligned operands.
+template <int TN, bool TA>
 __device__ __forceinline__ void load_panel(const Gemm& g, int i0, int j0, int k0, double* As, double* Bs) {
     const int tid = threadIdx.x;
-    const bool full_k = k0 + KC <= g.K;
-    const bool a16 = !g.ta && (g.lda & 1) == 0 && (reinterpret_cast<uintptr_t>(g.A) & 15) == 0;
-    const bool b16 = !g.tb && (g.ldb & 1) == 0 && (reinterpret_cast<uintptr_t>(g.B) & 15) == 0;
-    // A: TM x KC elements
-    if (a16 && full_k && i0 + TM <= g.M) {
-        // every thread copies the same row pair (i, i+1) of every KSTEP-th k row
-        constexpr int PER = TM / 2;           // pairs per k row
-        constexpr int KSTEP = THREADS / PER;  // k rows per pass
-        const int i = 2 * (tid % PER), k = tid / PER;
-        const double* src = g.A + (i0 + i) + (long long)(k0 + k) * g.lda;
-        double* dst = As + k * AS + i;
-#pragma unroll
-        for (int r = 0; r < KC / KSTEP; ++r) cp_async16(dst + r * KSTEP * AS, src + (long long)r * KSTEP * g.lda);
-    } else if (a16) {
-        for (int e = tid; e < TM * KC / 2; e += THREADS) {
-            const int i = 2 * (e % (TM / 2)), k = e / (TM / 2);  // pairs (i, i+1), contiguous in A and in As
-            double* dst = As + k * AS + i;
-            const int gi = i0 + i, gk = k0 + k;
-            if (gk < g.K && gi + 1 < g.M) {
-                cp_async16(dst, g.A + gi + (long long)gk * g.lda);
-            } else {
-                dst[0] = (gk < g.K && gi < g.M) ? g.A[gi + (long long)gk * g.lda] : 0.0;
-                dst[1] = 0.0;
-            }
-        }
-    } else {
-        for (int e = tid; e < TM * KC; e += THREADS) {
-            int i, k;
-            if (g.ta) { k = e % KC; i = e / KC; }  // consecutive threads: consecutive k (contiguous in A)
-            else { i = e % TM; k = e / TM; }       // consecutive threads: consecutive i
-            double* dst = As + k * AS + i;
-            const int gi = i0 + i, gk = k0 + k;
-            if (gi < g.M && gk < g.K)
-                cp_async8(dst, g.ta ? g.A + gk + (long long)gi * g.lda : g.A + gi + (long long)gk * g.lda);
-            else
-                *dst = 0.0;
-        }
+    for (int e = tid; e < TM * KC; e += THREADS) {
+        int i, k;
+        if (TA) { k = e % KC; i = e / KC; }  // consecutive threads: consecutive k (contiguous in A)
+        else { i = e % TM; k = e / TM; }     // consecutive threads: consecutive i
+        double* dst = As + aoff<TA>(i, k);
+        const int gi = i0 + i, gk = k0 + k;
+        if (gi < g.M && gk < g.K)
+            cp_async8(dst, TA ? g.A + gk + (long long)gi * g.lda : g.A + gi + (long long)gk * g.lda);
+        else
+            *dst = 0.0;
     }
-    // B: KC x TN elements
-    if (b16 && full_k && j0 + TN <= g.N) {
-        // every thread copies the same k pair of every JSTEP-th column
-        constexpr int PER = KC / 2;           // pairs per column
-        constexpr int JSTEP = THREADS / PER;  // columns per pass
-        const int k = 2 * (tid % PER), j = tid / PER;
-        const double* src = g.B + (k0 + k) + (long long)(j0 + j) * g.ldb;
+    for (int e = tid; e < KC * TN; e += THREADS) {
+        int j, k;
+        if (g.tb) { j = e % TN; k = e / TN; }  // consecutive j contiguous in B
+        else { k = e % KC; j = e / KC; }       // consecutive k contiguous in B
         double* dst = Bs + j * BS + k;
-#pragma unroll
-        for (int r = 0; r < TN / JSTEP; ++r) cp_async16(dst + r * JSTEP * BS, src + (long long)r * JSTEP * g.ldb);
-    } else if (b16) {
-        for (int e = tid; e < KC * TN / 2; e += THREADS) {
-            const int k = 2 * (e % (KC / 2)), j = e / (KC / 2);  // pairs (k, k+1), contiguous in B and in Bs
-            double* dst = Bs + j * BS + k;
-            const int gj = j0 + j, gk = k0 + k;
-            if (gj < g.N && gk + 1 < g.K) {
-                cp_async16(dst, g.B + gk + (long long)gj * g.ldb);
-            } else {
-                dst[0] = (gj < g.N && gk < g.K) ? g.B[gk + (long long)gj * g.ldb] : 0.0;
-                dst[1] = 0.0;
-            }
-        }
-    } else {
-        for (int e = tid; e < KC * TN; e += THREADS) {
-            int j, k;
-            if (g.tb) { j = e % TN; k = e / TN; }  // consecutive j contiguous in B
-            else { k = e % KC; j = e / KC; }       // consecutive k contiguous in B
-            double* dst = Bs + j * BS + k;
-            const int gj = j0 + j, gk = k0 + k;
-            if (gj < g.N && gk < g.K)
-                cp_async8(dst, g.tb ? g.B + gj + (long long)gk * g.ldb : g.B + gk + (long long)gj * g.ldb);
-            else
-                *dst = 0.0;
-        }
+        const int gj = j0 + j, gk = k0 + k;
+        if (gj < g.N && gk < g.K)
+            cp_async8(dst, g.tb ? g.B + gj + (long long)gk * g.ldb : g.B + gk + (long long)gj * g.ldb);
+        else
+            *dst = 0.0;
     }
     cp_async_commit();
 }
 
-// Copies of the K panels of one tile, set up once per tile: interior tiles of
-// non-transposed, 16-byte aligned operands with even leading dimensions take
-// a precomputed per-thread pointer (every thread copies the same row pair of
-// A and the same k pair of B in every panel); everything else, and the last
-// panel when K is not a multiple of KC, goes through load_panel.
-template <int TN>
+// Copies of the K panels of one tile, set up once per tile.  Interior tiles of
+// 16-byte aligned operands with even leading dimensions (B not transposed)
+// take a precomputed per-thread pointer: every thread copies the same pair of
+// doubles, contiguous in memory and in the panel, at fixed strides in every
+// panel.  Everything else, and the last panel when K is not a multiple of KC,
+// goes through load_panel.
+template <int TN, bool TA>
 struct PanelLoader {
+    // A as stored: pairs (i, i+1) along a k row; transposed A: pairs (k, k+1) along a row i
+    static constexpr int APER = TA ? KC / 2 : TM / 2;           // pairs per line
+    static constexpr int ALINES = THREADS / APER;                // lines per pass
+    static constexpr int APASS = (TA ? TM : KC) / ALINES;        // passes
+    static constexpr int BPER = KC / 2, BJSTEP = THREADS / BPER;  // B: pairs per column, columns per pass
+
     bool fast;
     const double* a_src;  // this thread's first A pair of panel 0
     const double* b_src;  // this thread's first B pair of panel 0
-    long long a_kstep;    // A elements between two k rows copied by this thread
+    long long a_line;     // A elements between two lines copied by this thread
+    long long a_panel;    // A elements between panels
     long long b_jstep;    // B elements between two columns copied by this thread
-    long long a_panel;    // A elements between panels (KC k rows)
     int a_dst, b_dst;     // offsets in the panel buffers
-
-    static constexpr int APER = TM / 2, AKSTEP = THREADS / APER;  // A: pairs per k row, k rows per pass
-    static constexpr int BPER = KC / 2, BJSTEP = THREADS / BPER;  // B: pairs per column, columns per pass
 
     __device__ __forceinline__ PanelLoader(const Gemm& g, int i0, int j0) {
         const int tid = threadIdx.x;
-        fast = !g.ta && !g.tb && (g.lda & 1) == 0 && (g.ldb & 1) == 0 &&
+        fast = !g.tb && (g.lda & 1) == 0 && (g.ldb & 1) == 0 &&
                ((reinterpret_cast<uintptr_t>(g.A) | reinterpret_cast<uintptr_t>(g.B)) & 15) == 0 &&
                i0 + TM <= g.M && j0 + TN <= g.N;
-        const int ai = 2 * (tid % APER), ak = tid / APER;
+        const int ap = 2 * (tid % APER), al = tid / APER;  // pair offset within the line, line
+        if (TA) {  // line = row i (k contiguous)
+            a_src = g.A + ap + (long long)(i0 + al) * g.lda;
+            a_panel = KC;
+            a_dst = aoff<true>(al, ap);
+        } else {   // line = k row (i contiguous)
+            a_src = g.A + (i0 + ap) + (long long)al * g.lda;
+            a_panel = (long long)KC * g.lda;
+            a_dst = aoff<false>(ap, al);
+        }
+        a_line = (long long)ALINES * g.lda;
         const int bk = 2 * (tid % BPER), bj = tid / BPER;
-        a_src = g.A + (i0 + ai) + (long long)ak * g.lda;
         b_src = g.B + bk + (long long)(j0 + bj) * g.ldb;
-        a_kstep = (long long)AKSTEP * g.lda;
         b_jstep = (long long)BJSTEP * g.ldb;
-        a_panel = (long long)KC * g.lda;
-        a_dst = ak * AS + ai;
         b_dst = bj * BS + bk;
     }
 
@@ -187,22 +152,24 @@ struct PanelLoader {
         if (fast && (p + 1) * KC <= g.K) {
             const double* sa = a_src + p * a_panel;
             const double* sb = b_src + p * KC;
+            constexpr int ADST = TA ? ALINES * ATS : ALINES * AS;  // panel offset between passes
 #pragma unroll
-            for (int r = 0; r < KC / AKSTEP; ++r) cp_async16(As + a_dst + r * AKSTEP * AS, sa + r * a_kstep);
+            for (int r = 0; r < APASS; ++r) cp_async16(As + a_dst + r * ADST, sa + r * a_line);
 #pragma unroll
             for (int r = 0; r < TN / BJSTEP; ++r) cp_async16(Bs + b_dst + r * BJSTEP * BS, sb + r * b_jstep);
             cp_async_commit();
         } else {
-            load_panel<TN>(g, i0, j0, p * KC, As, Bs);
+            load_panel<TN, TA>(g, i0, j0, p * KC, As, Bs);
         }
     }
 };
 
 // One 32 x TN output tile (index t of the GEMM's tiles, column-major over the
-// tile grid).  sm holds smem_doubles<TN>() doubles.  The caller's CTA has
+// tile grid) with A read as stored (TA = false) or transposed (TA = true; must
+// equal g.ta).  sm holds smem_doubles<TN>() doubles.  The caller's CTA has
 // THREADS threads; every thread must call this.
-template <int TN>
-__device__ void tile(const Gemm& g, int t, double* sm) {
+template <int TN, bool TA>
+__device__ void tile_t(const Gemm& g, int t, double* sm) {
     static_assert(TN == 16 || TN == 32, "tile width");
     constexpr int NI = TN / 8;      // n8 blocks
     constexpr int MI = TM / 16;     // m16 blocks
@@ -219,11 +186,11 @@ __device__ void tile(const Gemm& g, int t, double* sm) {
         for (int b = 0; b < NI; ++b)
 #pragma unroll
             for (int e = 0; e < 4; ++e) acc[a][b][e] = 0.0;
-    auto As = [&](int buf) { return sm + buf * (KC * AS + TN * BS); };
-    auto Bs = [&](int buf) { return sm + buf * (KC * AS + TN * BS) + KC * AS; };
+    auto As = [&](int buf) { return sm + buf * (APANEL + TN * BS); };
+    auto Bs = [&](int buf) { return sm + buf * (APANEL + TN * BS) + APANEL; };
 
     const int npan = (g.K + KC - 1) / KC;
-    const PanelLoader<TN> ld(g, i0, j0);
+    const PanelLoader<TN, TA> ld(g, i0, j0);
     __syncthreads();  // the buffers may still be read by the previous tile
     // prologue: the first NBUF - 1 panels in flight (one commit group each, empty ones too)
 #pragma unroll
@@ -246,8 +213,8 @@ __device__ void tile(const Gemm& g, int t, double* sm) {
             double af[MI][2], bf[NI];
 #pragma unroll
             for (int mi = 0; mi < MI; ++mi) {
-                af[mi][0] = A_[(kk + tq) * AS + mi * 16 + gq];
-                af[mi][1] = A_[(kk + tq) * AS + mi * 16 + gq + 8];
+                af[mi][0] = A_[aoff<TA>(mi * 16 + gq, kk + tq)];
+                af[mi][1] = A_[aoff<TA>(mi * 16 + gq + 8, kk + tq)];
             }
 #pragma unroll
             for (int ni = 0; ni < NI; ++ni) bf[ni] = B_[(ni * 8 + gq) * BS + kk + tq];
@@ -294,6 +261,13 @@ __device__ void tile(const Gemm& g, int t, double* sm) {
         for (int w = 0; w < WARPS; ++w) s += red[(v * WARPS + w) * 32 + lane];
         if (inb[u]) *dst[u] = old[u] + g.alpha * s;
     }
+}
+
+// One output tile of g (see tile_t).
+template <int TN>
+__device__ __forceinline__ void tile(const Gemm& g, int t, double* sm) {
+    if (g.ta) tile_t<TN, true>(g, t, sm);
+    else tile_t<TN, false>(g, t, sm);
 }
 
 // ---------------------------------------------------------------------------

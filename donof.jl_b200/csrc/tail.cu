@@ -61,19 +61,83 @@ __global__ void __launch_bounds__(dtile::THREADS) elag_tail_kernel(const TailArg
     const int red_first = G > nt_hc ? nt_hc : 0;
     for (int w = cta; w < nt_hc; w += G) dtile::tile<TL_TN>(ghc, w, sm);
     if (cta >= red_first) {
-        const int r = cta - red_first;
-        for (long long i = (long long)r * dtile::THREADS + tid; i < ny; i += (long long)red_ctas * dtile::THREADS) {
-            double s = 0.0;
-            if (a.part_f32) {
-                const float* p = static_cast<const float*>(a.part) + i;
-#pragma unroll 8
-                for (int g = 0; g < a.nparts; ++g) s += (double)__ldg(p + g * a.pstride);
-            } else {
-                const double* p = static_cast<const double*>(a.part) + i;
-#pragma unroll 8
-                for (int g = 0; g < a.nparts; ++g) s += __ldg(p + g * a.pstride);
+        // Warp w sums the partials g = w (mod WARPS) of a block of elements, then the
+        // warps' sums are added in a fixed order (the result does not depend on timing).
+        __shared__ double wsum[dtile::WARPS][128];
+        const int lane = tid & 31, warp = tid >> 5;
+        const bool vec = a.part_f32 && (a.pstride & 3) == 0 && (ny & 3) == 0 &&
+                         (reinterpret_cast<uintptr_t>(a.part) & 15) == 0;
+        if (vec) {
+            // FP32 partials, blocks of 128 elements: four consecutive elements per lane
+            const long long nblk = (ny + 127) / 128;
+            const float* p = static_cast<const float*>(a.part);
+            for (long long blk = cta - red_first; blk < nblk; blk += red_ctas) {
+                const long long e = blk * 128 + 4 * lane;
+                double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+                if (e < ny) {
+                    // up to PF partials per warp in flight at once
+                    constexpr int PF = 20;
+                    for (int g0 = warp; g0 < a.nparts; g0 += PF * dtile::WARPS) {
+                        float4 v[PF];
+#pragma unroll
+                        for (int i = 0; i < PF; ++i) {
+                            const int g = g0 + i * dtile::WARPS;
+                            v[i] = (g < a.nparts) ? __ldg(reinterpret_cast<const float4*>(p + g * a.pstride + e))
+                                                  : make_float4(0.f, 0.f, 0.f, 0.f);
+                        }
+#pragma unroll
+                        for (int i = 0; i < PF; ++i) {
+                            s0 += (double)v[i].x; s1 += (double)v[i].y; s2 += (double)v[i].z; s3 += (double)v[i].w;
+                        }
+                    }
+                }
+                wsum[warp][4 * lane] = s0;
+                wsum[warp][4 * lane + 1] = s1;
+                wsum[warp][4 * lane + 2] = s2;
+                wsum[warp][4 * lane + 3] = s3;
+                __syncthreads();
+                if (tid < 128 && blk * 128 + tid < ny) {
+                    double t = 0.0;
+#pragma unroll
+                    for (int w = 0; w < dtile::WARPS; ++w) t += wsum[w][tid];
+                    a.Y[blk * 128 + tid] = t;
+                }
+                __syncthreads();
             }
-            a.Y[i] = s;
+        } else {
+            // blocks of 64 elements, two per lane
+            const long long nblk = (ny + 63) / 64;
+            for (long long blk = cta - red_first; blk < nblk; blk += red_ctas) {
+                const long long e0 = blk * 64 + lane, e1 = e0 + 32;
+                double s0 = 0.0, s1 = 0.0;
+                if (a.part_f32) {
+                    const float* p = static_cast<const float*>(a.part);
+#pragma unroll 4
+                    for (int g = warp; g < a.nparts; g += dtile::WARPS) {
+                        const float* q = p + g * a.pstride;
+                        if (e0 < ny) s0 += (double)__ldg(q + e0);
+                        if (e1 < ny) s1 += (double)__ldg(q + e1);
+                    }
+                } else {
+                    const double* p = static_cast<const double*>(a.part);
+#pragma unroll 4
+                    for (int g = warp; g < a.nparts; g += dtile::WARPS) {
+                        const double* q = p + g * a.pstride;
+                        if (e0 < ny) s0 += __ldg(q + e0);
+                        if (e1 < ny) s1 += __ldg(q + e1);
+                    }
+                }
+                wsum[warp][lane] = s0;
+                wsum[warp][32 + lane] = s1;
+                __syncthreads();
+                if (tid < 64 && blk * 64 + tid < ny) {
+                    double t = 0.0;
+#pragma unroll
+                    for (int w = 0; w < dtile::WARPS; ++w) t += wsum[w][tid];
+                    a.Y[blk * 64 + tid] = t;
+                }
+                __syncthreads();
+            }
         }
     }
     // columns nbf5.. of elag are zero
