@@ -1,5 +1,6 @@
 // Host-side dispatch of the FP64 DMMA GEMM (tile shape, operand layout,
 // 16-byte vs 8-byte staging) and the split-K reduction.
+#include <atomic>
 #include "gemm_f64.cuh"
 #include "kernels.cuh"
 
@@ -13,16 +14,16 @@ cudaError_t launch_cfg(const GemmF64Args& p, cudaStream_t st) {
     using Cfg = GemmF64Cfg<BM, BN, BK, WM, WN, STAGES, AK, BKM, VEC>;
     auto kern = gemm_f64_kernel<BM, BN, BK, WM, WN, STAGES, AK, BKM, VEC>;
     // the shared-memory opt-in is per function and device; remember it per device
-    static unsigned long long attr_mask = 0;
+    static std::atomic<unsigned long long> attr_mask{0};
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     const unsigned long long bit = 1ull << (dev & 63);
-    if (!(attr_mask & bit)) {
+    if (!(attr_mask.load(std::memory_order_acquire) & bit)) {
         e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)Cfg::SMEM_BYTES);
         if (e != cudaSuccess) return e;
-        attr_mask |= bit;
+        attr_mask.fetch_or(bit, std::memory_order_acq_rel);
     }
     dim3 grid((p.M + BM - 1) / BM, (p.N + BN - 1) / BN, p.batch * p.splits);
     kern<<<grid, Cfg::THREADS, Cfg::SMEM_BYTES, st>>>(p); count_launch();

@@ -29,6 +29,7 @@
 //
 // Supported shapes: nbf <= 256, nbf5 <= 64 (one MMA tile per aux index);
 // other shapes are rejected with DONOF_ERR_ARG.
+#include <atomic>
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_bf16.h>
@@ -740,14 +741,15 @@ __global__ void f32_to_f64(const float* __restrict__ a, long long count, double*
 namespace {
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    if (!fn) {
+    // looked up once (thread-safe static initialisation)
+    static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
         void* p = nullptr;
         cudaDriverEntryPointQueryResult q;
         if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
             q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-    }
+            return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        return static_cast<PFN_cuTensorMapEncodeTiled_v12000>(nullptr);
+    }();
     return fn;
 }
 
@@ -849,12 +851,12 @@ int launch_mixed(donof_job* job, cudaStream_t st, int nbf5, int nalpha, int nbet
     P.n32 = S.n32; P.cj32 = S.cj32; P.ck32t = S.ck32;
     P.tmp_out = tmp_out; P.bpq_out = bpq_out; P.d_out = S.d; P.y_part = S.ypart; P.k_part = S.kpart;
     P.status = S.status;
-    static unsigned long long attr_mask = 0;
+    static std::atomic<unsigned long long> attr_mask{0};
     const unsigned long long bit = 1ull << (ctx->device & 63);
-    if (!(attr_mask & bit)) {
+    if (!(attr_mask.load(std::memory_order_acquire) & bit)) {
         DONOF_CUDA(ctx, cudaFuncSetAttribute(mx::lag_mixed_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              mx::SMEM_ALLOC));
-        attr_mask |= bit;
+        attr_mask.fetch_or(bit, std::memory_order_acq_rel);
     }
     prof_begin(ctx, st);
     mx::lag_mixed_kernel<<<grid, mx::NTHREADS, mx::SMEM_ALLOC, st>>>(mhi, mlo, mcs, P); count_launch();

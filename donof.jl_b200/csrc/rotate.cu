@@ -12,6 +12,7 @@
 // the matching buffer through a device-side pointer, so the whole sequence
 // has no host round trip and can be captured in a graph.  Norms beyond
 // 0.25 * 2^SMAX are flagged in the status word (accuracy would degrade).
+#include <atomic>
 #include <math.h>
 #include <stdlib.h>
 
@@ -347,11 +348,11 @@ int rotate_f64(donof_ctx* ctx, cudaStream_t st, const double* y, int nbf, int nb
     a.bufs = a.Y + 5 * nn;           // E^(2^k), k = 0..SMAX
     a.E1 = a.bufs + (SMAX + 1) * nn;  // extra slot
     const int smem = (int)sizeof(double) * dtile::smem_doubles<RT_TN>();
-    static unsigned long long attr_mask = 0;
+    static std::atomic<unsigned long long> attr_mask{0};
     const unsigned long long bit = 1ull << (ctx->device & 63);
-    if (!(attr_mask & bit)) {
+    if (!(attr_mask.load(std::memory_order_acquire) & bit)) {
         DONOF_CUDA(ctx, cudaFuncSetAttribute(rotate_coop_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-        attr_mask |= bit;
+        attr_mask.fetch_or(bit, std::memory_order_acq_rel);
     }
     int per_sm = 0;
     DONOF_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rotate_coop_kernel, dtile::THREADS, smem));

@@ -13,6 +13,7 @@
 // stage 2 forms Bp, stage 3 the H_mat and elag tiles; the last CTA to finish
 // stage 3 sums the energy in a fixed order.  Bounded grid barriers separate
 // the stages.
+#include <atomic>
 #include "dtile.cuh"
 #include "kernels.cuh"
 
@@ -216,11 +217,11 @@ int elag_tail_f64(donof_job* job, cudaStream_t st, const double* C, const double
     a.Bp = a.HC + ny;
     a.Hmat = Hmat; a.elag = elag; a.E = E;
     const int smem = (int)sizeof(double) * dtile::smem_doubles<TL_TN>();
-    static unsigned long long attr_mask = 0;
+    static std::atomic<unsigned long long> attr_mask{0};
     const unsigned long long bit = 1ull << (ctx->device & 63);
-    if (!(attr_mask & bit)) {
+    if (!(attr_mask.load(std::memory_order_acquire) & bit)) {
         DONOF_CUDA(ctx, cudaFuncSetAttribute(elag_tail_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-        attr_mask |= bit;
+        attr_mask.fetch_or(bit, std::memory_order_acq_rel);
     }
     int per_sm = 0;
     DONOF_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, elag_tail_kernel, dtile::THREADS, smem));

@@ -1,0 +1,249 @@
+"""Continuous batching of GNOF energy jobs on one GPU.
+
+Requests (core Hamiltonian, RI tensor b, starting orbitals and occupations,
+parameters, precision) are admitted while their device footprint fits the
+memory budget; each admitted job runs the energy loop of ``optimize.energy``
+(or the mixed-precision form with closing FP64 iterations) on its own library
+context, i.e. its own CUDA stream, so the device work of all jobs in flight
+overlaps on the GPU.  A job that arrives while others run is admitted as soon
+as a slot and enough memory are free; results are returned per ticket.
+
+Admission policy (``Admission``): first fit over the queue in arrival order,
+bounded by ``max_inflight`` slots and the memory budget; the head of the queue
+is never passed over more than ``max_bypass`` times, so a large job cannot be
+starved by a stream of small ones.  The policy is separate from the executor so
+that it can be exercised without a GPU.
+
+The device footprint of a job is its RI tensor (FP64, plus the bf16 split in the
+mixed form) and the per-call scratch of the transforms (tmp, b_pq, W), the
+orbital state and the partial sums (see ``footprint``).
+"""
+from __future__ import annotations
+
+import itertools
+import threading
+import time
+from collections import deque
+from dataclasses import dataclass, field
+from typing import Callable, Deque, Dict, List, Optional
+
+import numpy as np
+
+from .param import Param
+
+PRECISIONS = ("fp64", "mixed", "mixed_refined")
+
+
+@dataclass
+class Request:
+    """One energy job.  b is the host RI tensor b[m, n, P] (nbf x nbf x naux,
+    column-major); C the starting orbitals; gamma the starting occupation
+    parameters (the reference's guess when None)."""
+    H: np.ndarray
+    b: np.ndarray
+    C: np.ndarray
+    p: Param
+    gamma: Optional[np.ndarray] = None
+    precision: str = "fp64"
+    E_nuc: float = 0.0
+    maxit: Optional[int] = None
+    tag: object = None
+
+
+@dataclass
+class Result:
+    ticket: int
+    E_elec: float = float("nan")
+    E_tot: float = float("nan")
+    converged: bool = False
+    iterations: int = 0
+    C: Optional[np.ndarray] = None
+    n: Optional[np.ndarray] = None
+    error: Optional[str] = None
+    t_submit: float = 0.0
+    t_start: float = 0.0
+    t_done: float = 0.0
+    footprint: int = 0
+    tag: object = None
+
+    @property
+    def latency(self) -> float:
+        return self.t_done - self.t_submit
+
+
+def footprint(nbf: int, naux: int, nbf5: int, precision: str) -> int:
+    """Device bytes a job holds while it runs (upper estimate)."""
+    b = 8 * nbf * nbf * naux
+    nb = (nbf + 63) // 64
+    split = 4 * 64 * nb * nbf * naux if precision != "fp64" else 0
+    # FP64 transforms: tmp (nbf nbf5 naux), b_pq and W (nbf5^2 naux each)
+    scratch = 8 * (nbf * nbf5 * naux + 2 * nbf5 * nbf5 * naux)
+    small = 8 * (4 * nbf * nbf + 16 * nbf * nbf5) + (32 << 20)
+    return b + split + scratch + small
+
+
+class Admission:
+    """First-fit admission by memory budget and slots (no GPU involved)."""
+
+    def __init__(self, budget_bytes: int, max_inflight: int = 8, max_bypass: int = 4):
+        self.budget = int(budget_bytes)
+        self.max_inflight = max_inflight
+        self.max_bypass = max_bypass
+        self.used = 0
+        self.inflight = 0
+        self.queue: Deque[tuple] = deque()  # (ticket, bytes)
+        self._head_bypassed = 0
+
+    def push(self, ticket: int, nbytes: int) -> None:
+        if nbytes > self.budget:
+            raise ValueError(f"job needs {nbytes} bytes, more than the whole budget of {self.budget}")
+        self.queue.append((ticket, nbytes))
+
+    def take(self) -> List[tuple]:
+        """Tickets (with their bytes) to start now, in the order they start."""
+        started = []
+        while self.inflight < self.max_inflight and self.queue:
+            pick = None
+            for i, (t, nb) in enumerate(self.queue):
+                if self.used + nb <= self.budget:
+                    if i > 0 and self._head_bypassed >= self.max_bypass:
+                        break  # the head waits for memory; nobody passes it any more
+                    pick = i
+                    break
+            if pick is None:
+                break
+            t, nb = self.queue[pick]
+            del self.queue[pick]
+            if pick > 0:
+                self._head_bypassed += 1
+            else:
+                self._head_bypassed = 0
+            self.used += nb
+            self.inflight += 1
+            started.append((t, nb))
+        return started
+
+    def release(self, nbytes: int) -> None:
+        self.used -= nbytes
+        self.inflight -= 1
+
+
+def run_energy(req: Request, device: int) -> Result:
+    """Executor: the energy loop of one request on its own context and stream."""
+    from . import api
+    from .optimize import energy, energy_mixed_refined
+
+    ctx = api.Context(device, torch_stream=False)
+    b = None
+    try:
+        up = "fp64" if req.precision == "fp64" else "mixed"
+        b = api.eris_to_gpu(req.b, up, ctx)
+        if req.precision == "mixed_refined":
+            r, _ = energy_mixed_refined(req.H, b, req.p, req.C, req.gamma, E_nuc=req.E_nuc, maxit=req.maxit)
+        else:
+            r = energy(req.H, b, req.p, req.C, req.gamma, E_nuc=req.E_nuc, maxit=req.maxit)
+        return Result(ticket=-1, E_elec=r.E_elec, E_tot=r.E_tot, converged=r.converged, iterations=r.iterations,
+                      C=r.C, n=r.n)
+    finally:
+        if b is not None:
+            b.free()
+        ctx.close()
+
+
+class Server:
+    """Accepts requests at any time; runs admitted jobs concurrently, each on
+    its own stream.  ``executor(request, device) -> Result`` does the work
+    (``run_energy`` by default)."""
+
+    def __init__(self, device: int = 0, budget_bytes: Optional[int] = None, max_inflight: int = 8,
+                 max_bypass: int = 4, executor: Callable[[Request, int], Result] = run_energy):
+        if budget_bytes is None:
+            import torch
+            free, _ = torch.cuda.mem_get_info(device)
+            budget_bytes = int(0.85 * free)
+        self.device = device
+        self.admission = Admission(budget_bytes, max_inflight, max_bypass)
+        self.executor = executor
+        self._lock = threading.Condition()
+        self._tickets = itertools.count(1)
+        self._pending: Dict[int, Request] = {}
+        self._results: Dict[int, Result] = {}
+        self._submit_t: Dict[int, float] = {}
+        self._bytes: Dict[int, int] = {}
+        self._threads: List[threading.Thread] = []
+        self._closed = False
+
+    # ---- client side
+    def submit(self, req: Request) -> int:
+        if req.precision not in PRECISIONS:
+            raise ValueError(f"precision must be one of {PRECISIONS}")
+        nbf, naux = req.p.nbf, req.p.nbfaux
+        nb = footprint(nbf, naux, req.p.nbf5, req.precision)
+        with self._lock:
+            if self._closed:
+                raise RuntimeError("server is shut down")
+            t = next(self._tickets)
+            self.admission.push(t, nb)
+            self._pending[t] = req
+            self._submit_t[t] = time.perf_counter()
+            self._bytes[t] = nb
+            self._admit_locked()
+        return t
+
+    def poll(self, ticket: int) -> Optional[Result]:
+        with self._lock:
+            return self._results.get(ticket)
+
+    def wait(self, ticket: int, timeout: Optional[float] = None) -> Result:
+        end = None if timeout is None else time.perf_counter() + timeout
+        with self._lock:
+            while ticket not in self._results:
+                rem = None if end is None else end - time.perf_counter()
+                if rem is not None and rem <= 0:
+                    raise TimeoutError(f"ticket {ticket} not done")
+                self._lock.wait(rem)
+            return self._results[ticket]
+
+    def shutdown(self, wait: bool = True) -> None:
+        with self._lock:
+            self._closed = True
+        if wait:
+            for th in list(self._threads):
+                th.join()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.shutdown()
+
+    # ---- scheduling
+    def _admit_locked(self) -> None:
+        for t, nb in self.admission.take():
+            req = self._pending.pop(t)
+            th = threading.Thread(target=self._run, args=(t, req, nb), daemon=True)
+            self._threads.append(th)
+            th.start()
+
+    def _run(self, t: int, req: Request, nb: int) -> None:
+        t0 = time.perf_counter()
+        try:
+            r = self.executor(req, self.device)
+        except Exception as e:  # the job fails, the server goes on
+            r = Result(ticket=t, error=f"{type(e).__name__}: {e}")
+        r.ticket = t
+        r.t_start = t0
+        r.t_done = time.perf_counter()
+        r.footprint = nb
+        r.tag = req.tag
+        with self._lock:
+            r.t_submit = self._submit_t.pop(t)
+            self._results[t] = r
+            self.admission.release(self._bytes.pop(t))
+            self._admit_locked()
+            self._lock.notify_all()
+
+
+def percentiles(values, qs=(50, 99)) -> dict:
+    v = np.asarray(values, dtype=np.float64)
+    return {f"p{q}": float(np.percentile(v, q)) for q in qs} if v.size else {f"p{q}": None for q in qs}

@@ -1,0 +1,90 @@
+"""Host-side tests of the continuous-batching server: admission by memory budget
+and slots, no starvation of a large job, and the submit/poll/wait plumbing with
+a fake executor (no GPU)."""
+import threading
+import time
+
+import numpy as np
+import pytest
+
+from donof_b200.param import Param
+from donof_b200.serve import Admission, Request, Result, Server, footprint, percentiles
+
+
+def test_admission_fits_budget_and_slots():
+    a = Admission(budget_bytes=100, max_inflight=2)
+    for t, nb in ((1, 60), (2, 30), (3, 30)):
+        a.push(t, nb)
+    assert [t for t, _ in a.take()] == [1, 2]      # third: no slot left
+    a.release(60)
+    assert [t for t, _ in a.take()] == [3]
+    assert a.used == 60 and a.inflight == 2
+
+
+def test_admission_first_fit_then_head_protected():
+    a = Admission(budget_bytes=100, max_inflight=8, max_bypass=2)
+    a.push(1, 90)
+    assert [t for t, _ in a.take()] == [1]
+    a.push(2, 50)                                    # head: does not fit beside job 1
+    for t in (3, 4, 5):
+        a.push(t, 5)
+    started = [t for t, _ in a.take()]
+    assert started == [3, 4]                         # two small jobs pass the head, then it is protected
+    a.release(90)
+    assert [t for t, _ in a.take()] == [2, 5]
+
+
+def test_admission_rejects_oversize():
+    a = Admission(budget_bytes=10)
+    with pytest.raises(ValueError):
+        a.push(1, 11)
+
+
+def test_footprint_grows_with_precision_and_size():
+    f64 = footprint(64, 128, 16, "fp64")
+    mix = footprint(64, 128, 16, "mixed")
+    assert mix > f64 > 8 * 64 * 64 * 128
+    assert footprint(128, 128, 16, "fp64") > f64
+
+
+def _req(nbf, tag):
+    p = Param(nbf=nbf, nbfaux=8, nbeta=2, nalpha=2, ncwo=1)
+    return Request(H=np.eye(nbf), b=np.zeros((nbf, nbf, 8)), C=np.eye(nbf), p=p, tag=tag)
+
+
+def test_server_overlaps_and_returns_every_ticket():
+    live, peak = [0], [0]
+    lock = threading.Lock()
+
+    def fake(req, device):
+        with lock:
+            live[0] += 1
+            peak[0] = max(peak[0], live[0])
+        time.sleep(0.05)
+        with lock:
+            live[0] -= 1
+        return Result(ticket=-1, E_elec=float(req.p.nbf), converged=True)
+
+    with Server(budget_bytes=10**12, max_inflight=3, executor=fake) as s:
+        tickets = [s.submit(_req(8 + i, tag=i)) for i in range(7)]
+        res = [s.wait(t, timeout=10) for t in tickets]
+    assert [r.E_elec for r in res] == [8.0 + i for i in range(7)]
+    assert [r.tag for r in res] == list(range(7))
+    assert peak[0] == 3                                  # jobs ran side by side, never more than the slots
+    assert all(r.latency >= 0.05 for r in res)
+    q = percentiles([r.latency for r in res])
+    assert q["p50"] <= q["p99"]
+
+
+def test_server_reports_a_failing_job_and_goes_on():
+    def fake(req, device):
+        if req.tag == "bad":
+            raise RuntimeError("boom")
+        return Result(ticket=-1, E_elec=1.0)
+
+    with Server(budget_bytes=10**12, executor=fake) as s:
+        t1 = s.submit(_req(8, "bad"))
+        t2 = s.submit(_req(8, "good"))
+        r1, r2 = s.wait(t1, 5), s.wait(t2, 5)
+    assert r1.error and "boom" in r1.error
+    assert r2.error is None and r2.E_elec == 1.0
