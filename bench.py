@@ -16,6 +16,10 @@ FP64) exceeds the 126 MB L2, so no flush is needed between steps.
   e2e     the reference-facing host-buffer calls per step (donof_rotate +
           donof_lagrange2 with host arrays, optimiser update on the host),
           as DoNOF.jl's loop drives its GPU plugin
+          (e2e.latency_ms: p50/p99 of the per-step times of that loop)
+  energies  converged GNOF energies/s of the FP64 form and of the mixed form
+          with closing FP64 iterations, from the same start, on a molecule-
+          shaped surrogate (nbf = 96, naux = 384), with |dE| between them
   --impl reference   the CPU restatement of the reference path (C/OpenMP FP64
           oracle, all host threads) on the same workload
 
@@ -57,6 +61,7 @@ def parse():
     ap.add_argument("--method", default="ADAM")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-energies", action="store_true")
     ap.add_argument("--profile-case", action="store_true",
                     help="run the mixed and FP64 Lagrangian and the rotation three times each on the "
                          "benchmark workload and exit (the case the committed ncu captures use)")
@@ -230,6 +235,47 @@ def reference_arm(args, rank, world):
     return line
 
 
+ENERGY_CASE = dict(nbf=96, naux=384, nbeta=8, ncwo=3)
+
+
+def energies_bench(d, torch, ctx):
+    """Converged GNOF energies/s of the FP64 form and of the mixed form with
+    closing FP64 iterations, from the same start, on a molecule-shaped surrogate
+    (weak two-electron part: a single well-defined minimum), with the energy
+    difference between the two results."""
+    from donof_b200 import workload
+    from donof_b200.optimize import energy, energy_mixed_refined
+    out = {"workload": "molecule-like surrogate (nbf=96, naux=384, nbeta=8, ncwo=3, two_e_scale=0.2), "
+                       "max|g_orb|, |g_occ| < 1e-6",
+           "unit": "energies/s"}
+    res = {}
+    for form in ("fp64", "mixed_refined"):
+        wl = workload.molecule_like(**ENERGY_CASE, seed=5, two_e_scale=0.2)
+        p = wl.p
+        p.threshgorb = p.threshgocc = 1e-6
+        p.threshen = 1e-10
+        b = d.eris_to_gpu(wl.b, "fp64" if form == "fp64" else "mixed", ctx)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        if form == "fp64":
+            r = energy(wl.H, b, p, wl.C, wl.gamma, maxit=1000)
+            extra = {}
+        else:
+            r, rm = energy_mixed_refined(wl.H, b, p, wl.C, wl.gamma, maxit=1000)
+            extra = {"mixed_outer_iterations": rm.iterations, "mixed_orbital_steps": rm.tot_it_orb}
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        b.free()
+        res[form] = r
+        out[form] = {"value": 1.0 / dt, "seconds": dt, "E_elec": r.E_elec, "converged": r.converged,
+                     "outer_iterations": r.iterations, "orbital_steps": r.tot_it_orb,
+                     "occupation_cg_iterations": r.tot_it_occ, **extra}
+    out["abs_dE_Eh"] = abs(res["mixed_refined"].E_elec - res["fp64"].E_elec)
+    out["within_1uEh"] = out["abs_dE_Eh"] <= 1e-6
+    out["speedup"] = out["mixed_refined"]["value"] / out["fp64"]["value"]
+    return out
+
+
 def profile_case(d, torch, wl, ctx):
     """Three calls each of the mixed and FP64 Lagrangian and of the rotation."""
     import numpy as np
@@ -374,13 +420,14 @@ def main():
         st = (np.zeros(p.nvar), np.zeros(p.nvar), np.zeros(p.nvar))
         torch.cuda.synchronize()
         barrier()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
+        evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+        evs[0].record()
         for i in range(1, args.steps + 1):
             C, elag = host_step(i, C, elag)
-        e1.record()
+            evs[i].record()
         torch.cuda.synchronize()
-        te = e0.elapsed_time(e1) / 1e3
+        te = evs[0].elapsed_time(evs[-1]) / 1e3
+        per_step = [evs[i - 1].elapsed_time(evs[i]) for i in range(1, args.steps + 1)]
         if dist is not None:
             tt = torch.tensor([te], device=dev)
             dist.all_reduce(tt, op=dist.ReduceOp.MAX)
@@ -389,7 +436,13 @@ def main():
         h2d = 8 * (p.nvar + nn) + 8 * (nn + nn + nbf5 + 2 * n55)
         d2h = 8 * nn + 8 * (nn + nbf * nbf5 + 1)
         e2e = {"value": world * args.steps / te, "unit": UNIT, "h2d_bytes_per_step": h2d,
-               "d2h_bytes_per_step": d2h, "path": "donof_rotate + donof_lagrange2 (host buffers), host update"}
+               "d2h_bytes_per_step": d2h, "path": "donof_rotate + donof_lagrange2 (host buffers), host update",
+               "latency_ms": {"p50": float(np.percentile(per_step, 50)), "p99": float(np.percentile(per_step, 99)),
+                              "per": "orbital step through the host-buffer C ABI"}}
+
+    energies = None
+    if rank == 0 and world == 1 and not args.no_energies:
+        energies = energies_bench(d, torch, ctx)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -404,6 +457,8 @@ def main():
                 "dtype": "f64" if args.precision == "fp64" else "bf16x2-split+f64", "data": "synthetic",
                 "config": config(args, world), "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": int(launches), "clocks": clk.summary(), "final_E": E}
+        if energies is not None:
+            line["energies"] = energies
         print(json.dumps(line), flush=True)
     bt.free()
     ctx.close()

@@ -50,10 +50,10 @@ def _softmax(gamma, p: Param):
     n[strong] = inv
     w = e * inv[:, None]                      # weak occupations of each pair
     n[P] = w
-    for g in range(p.ndoc):
-        # src/pnof.jl:1152 multiplies by n[i] (1-based i), kept as is
-        dn[strong[g], G[g]] = -n[g] * w[g]
-        dn[np.ix_(P[g], G[g])] = np.diag(w[g]) - np.outer(w[g], w[g])
+    # src/pnof.jl:1152 multiplies by n[i] (1-based i, the pair index), kept as is
+    dn[strong[:, None], G] = -n[: p.ndoc][:, None] * w
+    eye = np.eye(p.ncwo)
+    dn[P[:, :, None], G[:, None, :]] = eye[None] * w[:, :, None] - w[:, :, None] * w[:, None, :]
     return n, dn
 
 
@@ -128,6 +128,11 @@ def _dynamic(n, p: Param):
     return nd, F, coc
 
 
+def _pairs(p: Param):
+    """Index arrays of the pairs: S (ndoc, 1) strong orbitals, W (ndoc, ncwo) their weak ones."""
+    return (p.no1 + np.arange(p.ndoc))[:, None], p.pair_table()
+
+
 def coupling(n, p: Param):
     """cj12, ck12 of GNOF (ipnof = 8) with zeroed diagonals (PNOFi_selector)."""
     if p.ipnof != 8:
@@ -155,15 +160,15 @@ def coupling(n, p: Param):
     ck[be, cw] += np.outer(nd12[be], nd12[cw]) - np.outer(nd[be], nd[cw])
     ck[cw, be] += np.outer(nd12[cw], nd12[be]) - np.outer(nd[cw], nd[be])
     ck[cw, cw] -= np.outer(nd12[cw], nd12[cw]) + np.outer(nd[cw], nd[cw])
-    strong = p.no1 + np.arange(p.ndoc)
-    for g, ws in zip(strong, p.pair_table()):
-        cj[g, ws] = 0.0
-        cj[ws, g] = 0.0
-        cj[np.ix_(ws, ws)] = 0.0
-        r = np.sqrt(n[g] * n[ws])
-        ck[g, ws] = r
-        ck[ws, g] = r
-        ck[np.ix_(ws, ws)] = -np.sqrt(np.outer(n[ws], n[ws]))
+    S, W = _pairs(p)  # every pair (strong s, weak ws) at once
+    cj[S, W] = 0.0
+    cj[W, S] = 0.0
+    cj[W[:, :, None], W[:, None, :]] = 0.0
+    r = np.sqrt(n[S] * n[W])
+    ck[S, W] = r
+    ck[W, S] = r
+    sw = np.sqrt(n[W])
+    ck[W[:, :, None], W[:, None, :]] = -(sw[:, :, None] * sw[:, None, :])
     np.fill_diagonal(cj, 0.0)
     np.fill_diagonal(ck, 0.0)
     return cj, ck
@@ -245,6 +250,90 @@ def coupling_derivatives(n, dn, p: Param):
 der_PNOFi_selector = coupling_derivatives
 
 
+def _derivative_factors(n, dn, p: Param):
+    """The derivatives of coupling_derivatives as sums of separable terms,
+        Dcj[i, j, :] = Mcj[i, j] dn[i, :],   Dck[i, j, :] = sum_t Mck[t][i, j] A[t][i, :],
+    with the per-row derivative arrays A = (dn, dfi, dnd12, dnd) (nbf5 x nv) and
+    the same blocks, masks and overwrites as coupling_derivatives (and
+    der_CJCKD8, src/pnof.jl:603-793) without the nv axis."""
+    nd, F, coc = _dynamic(n, p)
+    strong = p.no1 + np.arange(p.ndoc)
+    P = p.pair_table()
+    dnd = np.zeros((p.nbf5, p.nv))
+    for g in range(p.ndoc):
+        s, ws = strong[g], P[g]
+        k = 2.0 * coc[g] / p.h_cut
+        dnd[s] = F[g] * dn[s] * (1.0 + n[s] * k)
+        dnd[ws] = F[g] * dn[ws] + F[g] * k * np.outer(n[ws], dn[s])
+    nd12 = np.sqrt(nd)
+    dnd12 = 0.5 * dnd / np.maximum(nd12, 1e-15)[:, None]
+    f = np.clip(n * (1.0 - n), 0.0, None)
+    dfi = np.zeros((p.nbf5, p.nv))
+    act = slice(p.no1, p.nbf5)
+    if p.ista in (0, 1, 5, 2, 4):
+        fi = np.sqrt(f) * (0.9 if p.ista == 2 else 1.0)
+        a = np.maximum(fi[act], 1e-15)
+        scale = 0.81 if p.ista == 2 else 1.0
+        dfi[act] = (scale / (2.0 * a) * (1.0 - 2.0 * n[act]))[:, None] * dn[act]
+        if p.ista == 4:
+            e = np.exp(-(n[act] - 0.5) ** 2)
+            dfi[act] = dfi[act] * e[:, None] - (fi[act] * 2.0 * (n[act] - 0.5) * e)[:, None] * dn[act]
+            fi = fi * np.exp(-(n - 0.5) ** 2)
+    elif p.ista == 3:
+        al_ = 0.55
+        aa = (2.0 ** (2.0 * al_ - 1.0)) ** (1.0 / al_)
+        fi = (aa * f) ** al_
+        a = np.maximum(aa * n[act] * (1.0 - n[act]), 1e-15)
+        dfi[act] = (al_ * a ** (al_ - 1.0) * aa * (1.0 - 2.0 * n[act]))[:, None] * dn[act]
+    else:
+        raise ValueError(f"ista = {p.ista} is not a GNOF variant")
+    N = p.nbf5
+    be, al, cw = slice(p.no1, p.nbeta), slice(p.nbeta, p.nalpha), slice(p.nalpha, p.nbf5)
+    Mcj = np.tile(2.0 * n, (N, 1))
+    Mdn = np.tile(n, (N, 1))
+    Mdfi = np.zeros((N, N))
+    Mdnd12 = np.zeros((N, N))
+    Mdnd = np.zeros((N, N))
+    if p.ista == 0:
+        Mdfi[be, cw] += fi[cw][None, :]
+        Mdfi[cw, be] += fi[be][None, :]
+        Mdfi[cw, cw] += fi[cw][None, :]
+        if p.nsoc > 0:
+            Mdfi[be, al] += 0.25
+            Mdfi[cw, al] += 0.5
+    else:
+        Mdfi += fi[None, :]
+    Ms = (Mdn, Mdfi, Mdnd12, Mdnd)
+    if p.nsoc > 1:
+        for M in Ms:
+            M[al, al] = 0.0
+    Mdnd12[be, cw] += nd12[cw][None, :]
+    Mdnd[be, cw] -= nd[cw][None, :]
+    Mdnd12[cw, be] += nd12[be][None, :]
+    Mdnd[cw, be] -= nd[be][None, :]
+    Mdnd12[cw, cw] -= nd12[cw][None, :]
+    Mdnd[cw, cw] -= nd[cw][None, :]
+    S, W = _pairs(p)
+    WW = (W[:, :, None], W[:, None, :])
+    Mcj[S, W] = 0.0
+    Mcj[W, S] = 0.0
+    Mcj[WW] = 0.0
+    for M in Ms:
+        M[S, W] = 0.0
+        M[W, S] = 0.0
+        M[WW] = 0.0
+    sa = np.sqrt(np.maximum(n[S], 1e-15))  # (ndoc, 1)
+    sb = np.sqrt(np.maximum(n[W], 1e-15))  # (ndoc, ncwo)
+    Mdn[S, W] = 0.5 / sa * np.sqrt(n[W])
+    Mdn[W, S] = 0.5 / sb * np.sqrt(n[S])
+    Mdn[WW] = -0.5 * (1.0 / sb)[:, :, None] * np.sqrt(n[W])[:, None, :]
+    d = np.arange(N)
+    Mcj[d, d] = 0.0
+    for M in Ms:
+        M[d, d] = 0.0
+    return (dn, dfi, dnd12, dnd), Mcj, Ms
+
+
 def calce(n, cj12, ck12, J_MO, K_MO, H_core, p: Param) -> float:
     """Occupation-space energy (src/pnof.jl:1273-1300)."""
     dJ = np.diag(J_MO)
@@ -264,14 +353,20 @@ def calcocce(gamma, J_MO, K_MO, H_core, p: Param) -> float:
 
 
 def calcoccg(gamma, J_MO, K_MO, H_core, p: Param) -> np.ndarray:
-    """Occupation gradient (src/pnof.jl:1324-1377)."""
+    """Occupation gradient (src/pnof.jl:1324-1377).  The reference contracts the
+    nbf5 x nbf5 x nv derivative tensors of der_CJCKD8 with J_MO and K_MO; their
+    terms are separable (_derivative_factors), so the contraction runs over
+    (i, j) first and costs O(nbf5^2 + nbf5 nv) instead of O(nbf5^2 nv)."""
     n, dn = occupations(gamma, p)
-    Dcj, Dck = coupling_derivatives(n, dn, p)
+    A, Mcj, Mck = _derivative_factors(n, dn, p)
     w = 2.0 * H_core + np.diag(J_MO)
     rows = np.r_[np.arange(p.no1, p.nbeta), np.arange(p.nalpha, p.nbf5)]
     g = dn[rows].T @ w[rows]
-    g += 2.0 * np.einsum("ijk,ji->k", Dcj[rows], J_MO[:, rows])
-    g -= 2.0 * np.einsum("ijk,ji->k", Dck[rows], K_MO[:, rows])
+    vj = np.sum(Mcj * J_MO.T, axis=1)  # vj[i] = sum_j Mcj[i, j] J_MO[j, i]
+    g += 2.0 * A[0][rows].T @ vj[rows]
+    for a, M in zip(A, Mck):
+        vk = np.sum(M * K_MO.T, axis=1)
+        g -= 2.0 * a[rows].T @ vk[rows]
     return g
 
 

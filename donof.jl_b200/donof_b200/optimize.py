@@ -265,13 +265,21 @@ def energy(H, b: api.BTensor, p: Param, C, gamma=None, E_nuc: float = 0.0, freez
 
 
 def energy_mixed_refined(H, b: api.BTensor, p: Param, C, gamma=None, E_nuc: float = 0.0,
-                         maxit: Optional[int] = None, log: Optional[Callable[[dict], None]] = None):
-    """The mixed-precision form to convergence, then closing FP64 iterations from
-    its orbitals and occupations until the FP64 gradients meet the same
-    thresholds.  Returns (refined result, mixed-phase result); b must have been
-    uploaded with precision "mixed" and is left in FP64 mode."""
+                         maxit: Optional[int] = None, log: Optional[Callable[[dict], None]] = None,
+                         mixed_factor: float = 10.0):
+    """The mixed-precision form until its gradients are below mixed_factor times
+    the thresholds (the bf16-split gradients carry ~1e-5 relative rounding, so
+    driving them to the FP64 thresholds only adds iterations), then closing FP64
+    iterations from its orbitals and occupations until the FP64 gradients meet
+    p's thresholds.  Returns (refined result, mixed-phase result); b must have
+    been uploaded with precision "mixed" and is left in FP64 mode."""
+    import copy
+    pm = copy.copy(p)
+    pm.threshgorb = p.threshgorb * mixed_factor
+    pm.threshgocc = p.threshgocc * mixed_factor
     b.set_precision("mixed")
-    r_mixed = energy(H, b, p, C, gamma, E_nuc=E_nuc, maxit=maxit, log=log, order=False)
+    r_mixed = energy(H, b, pm, C, gamma, E_nuc=E_nuc, maxit=maxit, log=log, order=False)
+    p.maxloop = pm.maxloop
     b.set_precision("fp64")
     r = energy(H, b, p, r_mixed.C, r_mixed.gamma, E_nuc=E_nuc, maxit=maxit, log=log)
     return r, r_mixed
