@@ -48,6 +48,8 @@ SIGNATURES = {
     "donof_job_free": (_i, [_vp]),
     "donof_job_set_precision": (_i, [_vp, _i]),
     "donof_job_device_bytes": (ct.c_size_t, [_vp]),
+    "donof_occ_energy": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "donof_occ_cg": (_i, [_vp, _vp, _vp, _vp, _vp, ct.c_double, _i, _vp, _vp, _vp]),
     "donof_lagrange2": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp, _vp]),
     "donof_lagrange2_dev": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp, _vp]),
     "donof_lagrange2_prec_dev": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp, _vp]),

@@ -306,3 +306,46 @@ def orbopt_yogi(gamma, C, H, b, p):
 
 def orbopt_demon(gamma, C, H, b, p):
     return orbopt(gamma, C, H, b, p, "Demon")
+
+
+# ---------------------------------------------------------------- occupation layer (host, native)
+class _OccParams(ct.Structure):
+    _fields_ = [("nbf5", ct.c_int), ("no1", ct.c_int), ("nbeta", ct.c_int), ("nalpha", ct.c_int),
+                ("ncwo", ct.c_int), ("ista", ct.c_int), ("high_spin", ct.c_int), ("occ_method", ct.c_int),
+                ("h_cut", ct.c_double)]
+
+
+def _occ_params(p: Param) -> _OccParams:
+    methods = {"Softmax": 0, "Trigonometric": 1}
+    if p.occ_method not in methods:
+        raise ValueError(f"occupation method {p.occ_method!r} is not supported")
+    return _OccParams(p.nbf5, p.no1, p.nbeta, p.nalpha, p.ncwo, p.ista, int(bool(p.HighSpin)),
+                      methods[p.occ_method], float(p.h_cut))
+
+
+def occ_energy(gamma, J_MO, K_MO, H_core, p: Param, grad: bool = True):
+    """calcocce (and calcoccg) in the library's native host code: (E, gradient or None)."""
+    lib = _lib.load()
+    prm = _occ_params(p)
+    gamma = np.ascontiguousarray(gamma, dtype=np.float64)
+    J, K = _f64(J_MO), _f64(K_MO)
+    Hc = np.ascontiguousarray(H_core, dtype=np.float64)
+    E = ct.c_double()
+    g = np.zeros(p.nv) if grad else None
+    _lib.check(lib.donof_occ_energy(ct.byref(prm), _ptr(gamma), _ptr(J), _ptr(K), _ptr(Hc), ct.byref(E),
+                                    _ptr(g) if grad else None))
+    return E.value, g
+
+
+def occ_cg(gamma, J_MO, K_MO, H_core, p: Param, g_abstol: float, max_iter: int = 1000):
+    """The conjugate-gradient minimisation of occoptr over gamma in native host
+    code: (gamma, E, iterations, converged)."""
+    lib = _lib.load()
+    prm = _occ_params(p)
+    x = np.array(gamma, dtype=np.float64, copy=True)
+    J, K = _f64(J_MO), _f64(K_MO)
+    Hc = np.ascontiguousarray(H_core, dtype=np.float64)
+    E, nit, ok = ct.c_double(), ct.c_int(), ct.c_int()
+    _lib.check(lib.donof_occ_cg(ct.byref(prm), _ptr(J), _ptr(K), _ptr(Hc), _ptr(x), float(g_abstol), int(max_iter),
+                                ct.byref(E), ct.byref(nit), ct.byref(ok)))
+    return x, E.value, nit.value, bool(ok.value)

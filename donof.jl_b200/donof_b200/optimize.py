@@ -134,18 +134,16 @@ def cg_minimize(f: Callable, g: Callable, x0: np.ndarray, g_abstol: float, max_i
 # ---------------------------------------------------------------- occupation optimiser
 def occoptr(gamma, C, H, b: api.BTensor, p: Param, freeze_occ: bool = False):
     """src/minimization.jl:100-139.  J_MO, K_MO, H_core come from the device once;
-    the CG runs on the host over gamma.  Returns (E, nit, success, gamma, n, cj12, ck12)
-    and updates p.maxloop like the reference."""
+    the CG over gamma runs in the library's native host code (donof_occ_cg, the
+    same minimiser as cg_minimize).  Returns (E, nit, success, gamma, n, cj12,
+    ck12) and updates p.maxloop like the reference."""
     gamma = np.array(gamma, dtype=np.float64)
     E, nit, ok = -1.0, 0, True
     if p.ndoc > 0 and not freeze_occ:
         J, K, Hc = api.computeJKH_MO(C, H, b, p)
-        res = cg_minimize(lambda x: gnof.calcocce(x, J, K, Hc, p), lambda x: gnof.calcoccg(x, J, K, Hc, p),
-                          gamma, p.threshen)
-        gamma = res.minimizer
-        if res.iterations < 1:
+        gamma, E, nit, ok = api.occ_cg(gamma, J, K, Hc, p, p.threshen)
+        if nit < 1:
             p.maxloop = p.maxloop + 10
-        E, nit, ok = res.minimum, res.iterations, res.g_converged
     n, _ = gnof.occupations(gamma, p)
     cj12, ck12 = gnof.coupling(n, p)
     return E, nit, ok, gamma, n, cj12, ck12
@@ -250,7 +248,7 @@ def energy(H, b: api.BTensor, p: Param, C, gamma=None, E_nuc: float = 0.0, freez
         cj12, ck12 = gnof.coupling(n, p)
         grad_orb = api.calcorbg(None, n, cj12, ck12, C, H, b, p)
         J, K, Hc = api.computeJKH_MO(C, H, b, p)
-        grad_occ = gnof.calcoccg(gamma, J, K, Hc, p)
+        _, grad_occ = api.occ_energy(gamma, J, K, Hc, p)
         row = dict(it=it, nit_orb=nit_orb, nit_occ=nit_occ, E=E, E_tot=E + E_nuc, E_diff=E_diff, maxdiff=maxdiff,
                    max_grad_orb=float(np.max(np.abs(grad_orb))), norm_grad_occ=float(np.linalg.norm(grad_occ)))
         hist.append(row)

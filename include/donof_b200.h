@@ -176,6 +176,31 @@ int donof_orbopt_dev(donof_job* job, int method, const double* n, const double* 
                      double* alpha, int* maxloop, double threshgorb, double* C_inout, double* E,
                      int* nit, int* success);
 
+/* --- occupation layer and occupation optimiser (host, FP64) ------------------
+ * Native host code, no GPU: DoNOF.jl runs this part on the host too.
+ * Sizes and switches of the GNOF occupation layer (names of src/param.jl):
+ * nbf5, no1, nbeta, nalpha, ncwo, ista (0-5), HighSpin, occ_method
+ * (0 = Softmax, 1 = Trigonometric) and h_cut.  nv = ncwo * (nbeta - no1).   */
+typedef struct {
+    int nbf5, no1, nbeta, nalpha, ncwo, ista, high_spin, occ_method;
+    double h_cut;
+} donof_occ_params;
+/* Occupation energy at gamma from cached J_MO, K_MO (nbf5 x nbf5, column-
+ * major) and H_core (nbf5): calce / calcocce (src/pnof.jl:1273-1322) with the
+ * occupations of ocupacion_softmax / _trigonometric (:1047-1163) and the GNOF
+ * couplings of CJCKD8 (:488-601); with grad != NULL also its gamma-gradient
+ * (nv), calcoccg (:1324-1377, der_CJCKD8 :603-793).                          */
+int donof_occ_energy(const donof_occ_params* p, const double* gamma, const double* J_MO,
+                     const double* K_MO, const double* H_core, double* E, double* grad);
+/* Replaces the minimisation of occoptr (src/minimization.jl:100-139, Optim.jl
+ * ConjugateGradient with g_abstol): Hager-Zhang conjugate gradient with a
+ * strong-Wolfe line search over gamma (in/out, nv), stopped when
+ * max|grad| <= g_abstol or after max_iter iterations.  Returns the energy,
+ * the iteration count and whether the gradient test was met.               */
+int donof_occ_cg(const donof_occ_params* p, const double* J_MO, const double* K_MO,
+                 const double* H_core, double* gamma, double g_abstol, int max_iter, double* E,
+                 int* nit, int* converged);
+
 /* --- diagnostics -------------------------------------------------------------
  * Number of CUDA kernels this library has launched in the process so far.    */
 unsigned long long donof_launch_count(void);
