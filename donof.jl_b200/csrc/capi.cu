@@ -313,6 +313,41 @@ int donof_b_upload(donof_ctx* ctx, const double* b_host, int nbf, int naux, int 
     return DONOF_OK;
 }
 
+int donof_iaux(donof_ctx* ctx, const double* G, const double* I3c, int nbf, int naux, int precision,
+               donof_job** job) {
+    if (!ctx) return DONOF_ERR_ARG;
+    REQUIRE(ctx, G != nullptr && I3c != nullptr, "null G or I");
+    DONOF_CHECK(use_device(ctx));
+    donof_job* j = nullptr;
+    DONOF_CHECK(make_job(ctx, nbf, naux, precision, &j));
+    const size_t bytes = sizeof(double) * (size_t)nbf * nbf * naux;
+    void* d = nullptr;
+    cudaError_t e = cudaMalloc(&d, bytes);
+    if (e != cudaSuccess) {
+        delete j;
+        set_error(ctx, "cudaMalloc(b, %zu bytes): %s", bytes, cudaGetErrorString(e));
+        return DONOF_ERR_OOM;
+    }
+    int s = iaux_f64(ctx, ctx->stream, G, I3c, nbf, naux, static_cast<double*>(d), &j->part);
+    if (s != DONOF_OK) {
+        cudaFree(d);
+        j->part.release();
+        delete j;
+        return s;
+    }
+    j->b = static_cast<const double*>(d);
+    j->own_b = true;
+    if (precision == DONOF_PREC_MIXED) {
+        s = convert_b_f32(j);
+        if (s != DONOF_OK) {
+            donof_job_free(j);
+            return s;
+        }
+    }
+    *job = j;
+    return DONOF_OK;
+}
+
 int donof_b_attach(donof_ctx* ctx, const double* b_dev, int nbf, int naux, int precision,
                    donof_job** job) {
     if (!ctx) return DONOF_ERR_ARG;

@@ -39,6 +39,11 @@ int elag_tail_f64(donof_job* job, cudaStream_t st, const double* C, const double
                   const void* part, bool part_f32, int nparts, long long pstride, double* Hmat, double* elag,
                   double* E);
 
+// b = I G^{-1/2} on the device from host G (naux x naux) and I (nbf x nbf x naux)
+// (iaux.cu); part is scratch for the products.
+int iaux_f64(donof_ctx* ctx, cudaStream_t st, const double* G_host, const double* I_host, int nbf, int naux,
+             double* b, DevBuf* part);
+
 // FP64 pipelines (lagrange.cu)
 int transforms_f64(donof_job* job, cudaStream_t st, const double* C, int nbf5);
 int lagrange2_f64(donof_job* job, cudaStream_t st, const double* C, const double* n,

@@ -45,6 +45,7 @@ SIGNATURES = {
     "donof_synchronize": (_i, [_vp]),
     "donof_b_upload": (_i, [_vp, _vp, _i, _i, _i, ct.POINTER(_vp)]),
     "donof_b_attach": (_i, [_vp, _vp, _i, _i, _i, ct.POINTER(_vp)]),
+    "donof_iaux": (_i, [_vp, _vp, _vp, _i, _i, _i, ct.POINTER(_vp)]),
     "donof_job_free": (_i, [_vp]),
     "donof_job_set_precision": (_i, [_vp, _i]),
     "donof_job_device_bytes": (ct.c_size_t, [_vp]),

@@ -170,6 +170,28 @@ def eris_to_gpu(b, precision="fp64", ctx: Optional[Context] = None) -> BTensor:
     return BTensor(ctx, h, nbf, naux, prec)
 
 
+def Iaux_gpu(G, I, precision="fp64", ctx: Optional[Context] = None) -> BTensor:
+    """b = I G^{-1/2} built on the device from the two-centre integrals G
+    (naux x naux; its upper triangle, Symmetric(G)) and the three-centre
+    integrals I (nbf x nbf x naux), kept there as the job's RI tensor
+    (Iaux / Iaux_gpu, src/integrals.jl:68-91, ext/DoNOFGPUExt.jl:9-33,
+    followed by eris_to_gpu)."""
+    ctx = ctx or default_context()
+    prec = _prec(precision)
+    G = _f64(G)
+    I = _f64(I)
+    nbf, nbf2, naux = I.shape
+    if nbf != nbf2 or G.shape != (naux, naux):
+        raise ValueError(f"I must be nbf x nbf x naux and G naux x naux (got {I.shape}, {G.shape})")
+    h = ct.c_void_p()
+    ctx.check(ctx.lib.donof_iaux(ctx.handle, ct.c_void_p(G.ctypes.data), ct.c_void_p(I.ctypes.data), nbf, naux,
+                                 prec, ct.byref(h)))
+    return BTensor(ctx, h, nbf, naux, prec)
+
+
+Iaux = Iaux_gpu
+
+
 def compute_Lagrange2(C, n, H, b: BTensor, cj12, ck12, nalpha: int, nbeta: int, return_energy=False):
     """elag, H_mat = compute_Lagrange2(C, n, H, b, cj12, ck12, nalpha, nbeta)
     (src/utils.jl:1-59; ext/DoNOFGPUExt.jl:150-245).  Host arrays in and out."""

@@ -75,6 +75,14 @@ int donof_version(void);
  * does not own it and it must outlive the job).                            */
 int donof_b_upload(donof_ctx* ctx, const double* b_host, int nbf, int naux, int precision,
                    donof_job** job);
+/* donof_iaux replaces Iaux / Iaux_gpu (src/integrals.jl:68-91,
+ * ext/DoNOFGPUExt.jl:9-33) followed by eris_to_gpu: from the two-centre
+ * integrals G (naux x naux, host, the upper triangle is read as
+ * Symmetric(G)) and the three-centre integrals I (nbf x nbf x naux, host) it
+ * builds b = I G^{-1/2} on the device (negative eigenvalues of G give zero
+ * inverse square roots) and returns a job that owns it, as donof_b_upload. */
+int donof_iaux(donof_ctx* ctx, const double* G, const double* I3c, int nbf, int naux, int precision,
+               donof_job** job);
 int donof_b_attach(donof_ctx* ctx, const double* b_dev, int nbf, int naux, int precision,
                    donof_job** job);
 int donof_job_free(donof_job* job);
