@@ -20,7 +20,8 @@
 // Staging: a STAGES-deep cp.async ring (16-byte copies when the operand is
 // 16-byte aligned with even strides, 8-byte otherwise), zero-filled outside
 // the matrix; shared-memory rows are padded so the fragment reads of a warp
-// hit every bank pair exactly twice (the minimum for 256 bytes).
+// hit every bank pair exactly twice (the minimum for 256 bytes): row strides
+// are 4 (mod 16) doubles.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -80,6 +81,39 @@ __device__ __forceinline__ void mma_f64_16x8x4(double (&c)[4], double a0, double
         : "d"(a0), "d"(a1), "d"(b0));
 }
 
+// K depth of one FP64 MMA instruction (4, 8 or 16); sm_90 and later have the
+// m16n8k8 and m16n8k16 shapes, which move the same work in fewer instructions.
+constexpr int kMmaK = 8;
+
+// Fragment layouts (g = lane / 4, t = lane % 4), element e of a thread:
+//   A (16 x K, row):  row g + 8 (e % 2), column t + 4 (e / 2),  e < K / 2
+//   B (K x 8,  col):  row t + 4 e,       column g,              e < K / 4
+//   C/D (16 x 8):     row g + 8 (e / 2), column 2 t + e % 2,    e < 4
+template <int K>
+__device__ __forceinline__ void mma_f64(double (&c)[4], const double (&a)[K / 2], const double (&b)[K / 4]) {
+    if constexpr (K == 4) {
+        asm volatile(
+            "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, "
+            "{%0,%1,%2,%3};\n"
+            : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+            : "d"(a[0]), "d"(a[1]), "d"(b[0]));
+    } else if constexpr (K == 8) {
+        asm volatile(
+            "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+            "{%0,%1,%2,%3};\n"
+            : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+            : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+    } else {
+        static_assert(K == 16, "FP64 MMA depth must be 4, 8 or 16");
+        asm volatile(
+            "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, "
+            "{%4,%5,%6,%7,%8,%9,%10,%11}, {%12,%13,%14,%15}, {%0,%1,%2,%3};\n"
+            : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+            : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]),
+              "d"(b[0]), "d"(b[1]), "d"(b[2]), "d"(b[3]));
+    }
+}
+
 }  // namespace gemm_detail
 
 template <int BM, int BN, int BK, int WARPS_M, int WARPS_N, int STAGES, bool AK, bool BKM, bool VEC>
@@ -90,8 +124,10 @@ struct GemmF64Cfg {
     static constexpr int MI = WTM / 16;
     static constexpr int NI = WTN / 8;
     // padded shared-memory strides (in doubles)
-    static constexpr int SA = AK ? (BK + 4) : (BM + 8);
-    static constexpr int SB = BKM ? (BK + 4) : (BN + 8);
+    // (both forms: a half-warp's 16 fragment reads land on 16 distinct bank pairs,
+    // since the 4 threads of a group step the row by 4 doubles mod 16)
+    static constexpr int SA = AK ? (BK + 4) : (BM + 4);
+    static constexpr int SB = BKM ? (BK + 4) : (BN + 4);
     static constexpr int A_ELEMS = AK ? BM * SA : BK * SA;
     static constexpr int B_ELEMS = BKM ? BN * SB : BK * SB;
     static constexpr int STAGE_ELEMS = A_ELEMS + B_ELEMS;
@@ -105,6 +141,8 @@ template <int BM, int BN, int BK, int WARPS_M, int WARPS_N, int STAGES, bool AK,
 __global__ void __launch_bounds__(32 * WARPS_M * WARPS_N)
 gemm_f64_kernel(const GemmF64Args p) {
     using Cfg = GemmF64Cfg<BM, BN, BK, WARPS_M, WARPS_N, STAGES, AK, BKM, VEC>;
+    constexpr int KS = gemm_detail::kMmaK;
+    static_assert(BK % KS == 0, "BK must be a multiple of the MMA depth");
     extern __shared__ __align__(16) double smem[];
 
     const int tid = threadIdx.x;
@@ -207,33 +245,31 @@ gemm_f64_kernel(const GemmF64Args p) {
         const double* as = As(kt % STAGES);
         const double* bs = Bs(kt % STAGES);
 #pragma unroll
-        for (int kk = 0; kk < BK; kk += 4) {
-            double af[Cfg::MI][2];
-            double bf[Cfg::NI];
+        for (int kk = 0; kk < BK; kk += KS) {
+            double af[Cfg::MI][KS / 2];
+            double bf[Cfg::NI][KS / 4];
 #pragma unroll
             for (int a = 0; a < Cfg::MI; ++a) {
-                const int r = wrow + a * 16 + g;
-                if constexpr (AK) {
-                    af[a][0] = as[r * Cfg::SA + kk + t];
-                    af[a][1] = as[(r + 8) * Cfg::SA + kk + t];
-                } else {
-                    af[a][0] = as[(kk + t) * Cfg::SA + r];
-                    af[a][1] = as[(kk + t) * Cfg::SA + r + 8];
+#pragma unroll
+                for (int e = 0; e < KS / 2; ++e) {
+                    const int r = wrow + a * 16 + g + 8 * (e & 1);
+                    const int k = kk + t + 4 * (e >> 1);
+                    af[a][e] = AK ? as[r * Cfg::SA + k] : as[k * Cfg::SA + r];
                 }
             }
 #pragma unroll
             for (int b = 0; b < Cfg::NI; ++b) {
                 const int cidx = wcol + b * 8 + g;
-                if constexpr (BKM) {
-                    bf[b] = bs[cidx * Cfg::SB + kk + t];
-                } else {
-                    bf[b] = bs[(kk + t) * Cfg::SB + cidx];
+#pragma unroll
+                for (int e = 0; e < KS / 4; ++e) {
+                    const int k = kk + t + 4 * e;
+                    bf[b][e] = BKM ? bs[cidx * Cfg::SB + k] : bs[k * Cfg::SB + cidx];
                 }
             }
 #pragma unroll
             for (int a = 0; a < Cfg::MI; ++a)
 #pragma unroll
-                for (int b = 0; b < Cfg::NI; ++b) gemm_detail::mma_f64_16x8x4(acc[a][b], af[a][0], af[a][1], bf[b]);
+                for (int b = 0; b < Cfg::NI; ++b) gemm_detail::mma_f64<KS>(acc[a][b], af[a], bf[b]);
         }
     }
     gemm_detail::cp_async_wait<0>();
