@@ -63,6 +63,17 @@ int lagrange2_mixed(donof_job* job, cudaStream_t st, const double* C, const doub
 int jkh_mo_mixed(donof_job* job, cudaStream_t st, const double* C, const double* H, int nbf5,
                  double* J, double* K, double* Hcore);
 
+// General-shape mixed pipeline (mixed_general.cu), used when the fused kernel's
+// shape limits (nbf <= 256, nbf5 <= 64) do not hold.
+bool mixed_general_needed(int nbf, int nbf5);
+int transforms_mixed_general(donof_job* job, cudaStream_t st, const double* C, int nbf5);
+int lagrange2_mixed_general(donof_job* job, cudaStream_t st, const double* C, const double* n, const double* H,
+                            const double* cj12, const double* ck12, int nbf5, int nalpha, int nbeta, double* elag,
+                            double* Hmat, double* E);
+int jkh_mo_mixed_general(donof_job* job, cudaStream_t st, const double* C, const double* H, int nbf5, double* J,
+                         double* K, double* Hcore);
+int mixed_t1_general(donof_job* job, cudaStream_t st, const double* C, int nbf5, float* tmp_out);
+
 // Rotation C_new = C exp(Y(y)) (rotate.cu)
 int rotate_f64(donof_ctx* ctx, cudaStream_t st, const double* y, int nbf, int nbf5,
                const double* C, double* Cnew);

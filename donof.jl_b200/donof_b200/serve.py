@@ -78,6 +78,10 @@ def footprint(nbf: int, naux: int, nbf5: int, precision: str) -> int:
     split = 4 * 64 * nb * nbf * naux if precision != "fp64" else 0
     # FP64 transforms: tmp (nbf nbf5 naux), b_pq and W (nbf5^2 naux each)
     scratch = 8 * (nbf * nbf5 * naux + 2 * nbf5 * nbf5 * naux)
+    if precision != "fp64" and (nbf > 256 or nbf5 > 64):
+        # general-shape mixed pipeline: tmp split, FP32 b_pq, W split, Y partials
+        ldm, ldq = -(-nbf // 8) * 8, -(-nbf5 // 8) * 8
+        scratch += 4 * (ldm * nbf5 * naux + nbf5 * nbf5 * naux + ldq * nbf5 * naux + 148 * nbf * nbf5)
     small = 8 * (4 * nbf * nbf + 16 * nbf * nbf5) + (32 << 20)
     return b + split + scratch + small
 

@@ -5,7 +5,8 @@ The tolerance is the one of the split representation, not of FP64: b and
 every operand are stored as two bf16 numbers (16 significant bits), so each
 contraction carries a relative error of order 1e-5 of its largest output;
 the tests bound the max-norm relative error by 2e-4 (T1 / b_pq / J / K /
-elag) and the energy by 1e-5 relative.
+elag) and the energy by 1e-5 relative.  Shapes beyond the fused kernel
+(nbf5 > 64 or nbf > 256) exercise the general-shape pipeline.
 """
 import ctypes as ct
 
@@ -29,6 +30,11 @@ SIZES = [
     dict(nbf=64, naux=40, nbeta=4, ncwo=3),       # nbf5 = 16
     dict(nbf=130, naux=70, nbeta=8, ncwo=3),      # three boxes, nbf not a multiple of 32
     dict(nbf=256, naux=1024, nbeta=16, ncwo=3),   # benchmark workload
+    # general-shape pipeline (nbf5 > 64 or nbf > 256)
+    dict(nbf=96, naux=60, nbeta=20, ncwo=3),      # nbf5 = 80: one row tile
+    dict(nbf=202, naux=120, nbeta=33, ncwo=5),    # n-octane shape, nbf5 = 198: two row tiles
+    dict(nbf=300, naux=40, nbeta=20, ncwo=3),     # nbf > 256: two column tiles in T1 and Y
+    dict(nbf=330, naux=24, nbeta=65, ncwo=3),     # nbf5 = 260 > 256: two column tiles in T2
 ]
 
 
@@ -117,10 +123,14 @@ def test_mixed_lagrangian_matches_fp64(jobs, kw):
     assert abs(E1 - E0) <= 1e-5 * abs(E0)
 
 
-def test_mixed_rejects_unsupported_shapes(cuda_ctx):
-    wl = workload.synthetic(nbf=300, naux=4, nbeta=20, ncwo=3, seed=1)   # nbf > 256
+def test_mixed_rejects_bad_nbf5(cuda_ctx):
+    import torch
+
+    wl = workload.synthetic(nbf=40, naux=4, nbeta=4, ncwo=3, seed=1)
     bt = d.eris_to_gpu(wl.b, "mixed", cuda_ctx)
-    with pytest.raises(_lib.DonofError) as e:
-        d.compute_Lagrange2(wl.C, wl.n, wl.H, bt, wl.cj12, wl.ck12, wl.p.nalpha, wl.p.nbeta)
-    assert e.value.status == _lib.ERR_ARG and "nbf <= 256" in str(e.value)
+    tC = d.to_device(wl.C)
+    out = torch.zeros(64 * 41 * 4, dtype=torch.float32, device="cuda")
+    for bad in (0, 41):
+        st = bt.ctx.lib.donof_mixed_tmp_dev(bt.handle, tC.data_ptr(), bad, out.data_ptr())
+        assert st == _lib.ERR_ARG
     bt.free()
