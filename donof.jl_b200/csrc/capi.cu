@@ -27,27 +27,41 @@ void set_error(donof_ctx* ctx, const char* fmt, ...) {
     g_tls_error = buf;
 }
 
+// Device memory comes from the stream-ordered allocator on the context's
+// stream: an allocation or free waits only for that stream's earlier work, never
+// for the whole device (cudaFree would), so jobs served side by side do not
+// stall each other when one of them starts, grows a buffer or ends.
+int dev_alloc(donof_ctx* ctx, void** p, size_t bytes) {
+    *p = nullptr;
+    cudaError_t e = cudaMallocAsync(p, bytes ? bytes : 256, ctx->stream);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        set_error(ctx, "device allocation of %zu bytes: %s", bytes, cudaGetErrorString(e));
+        return e == cudaErrorMemoryAllocation ? DONOF_ERR_OOM : DONOF_ERR_CUDA;
+    }
+    return DONOF_OK;
+}
+
+void dev_free(donof_ctx* ctx, const void* p) {
+    if (p) cudaFreeAsync(const_cast<void*>(p), ctx->stream);
+}
+
 int DevBuf::ensure(donof_ctx* ctx, size_t want) {
     if (want <= bytes && ptr != nullptr) return DONOF_OK;
     if (ptr) {
-        cudaFree(ptr);
+        dev_free(ctx, ptr);
         ptr = nullptr;
         bytes = 0;
     }
     ++gen;
     if (want == 0) want = 256;
-    cudaError_t e = cudaMalloc(&ptr, want);
-    if (e != cudaSuccess) {
-        ptr = nullptr;
-        set_error(ctx, "cudaMalloc(%zu bytes): %s", want, cudaGetErrorString(e));
-        return e == cudaErrorMemoryAllocation ? DONOF_ERR_OOM : DONOF_ERR_CUDA;
-    }
+    DONOF_CHECK(dev_alloc(ctx, &ptr, want));
     bytes = want;
     return DONOF_OK;
 }
 
-void DevBuf::release() {
-    if (ptr) cudaFree(ptr);
+void DevBuf::release(donof_ctx* ctx) {
+    dev_free(ctx, ptr);
     ptr = nullptr;
     bytes = 0;
 }
@@ -223,6 +237,15 @@ int donof_create(int device, donof_ctx** out) {
     }
     ctx->own_stream = true;
     cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device);
+    {
+        // keep freed blocks in the device's default pool (process-local) instead of
+        // returning them to the driver at every synchronisation
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+    }
     *out = ctx;
     return DONOF_OK;
 }
@@ -231,9 +254,9 @@ int donof_destroy(donof_ctx* ctx) {
     if (!ctx) return DONOF_OK;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-    ctx->stage_in.release();
-    ctx->stage_out.release();
-    ctx->rot.release();
+    ctx->stage_in.release(ctx);
+    ctx->stage_out.release(ctx);
+    ctx->rot.release(ctx);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     if (ctx->aux_stream) cudaStreamDestroy(ctx->aux_stream);
     if (ctx->prof_ev[0]) cudaEventDestroy(ctx->prof_ev[0]);
@@ -255,6 +278,13 @@ int donof_set_stream(donof_ctx* ctx, void* stream) {
 }
 
 void* donof_get_stream(donof_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int donof_set_cta_limit(donof_ctx* ctx, int max_ctas) {
+    if (!ctx) return DONOF_ERR_ARG;
+    REQUIRE(ctx, max_ctas >= 0, "max_ctas must be >= 0");
+    ctx->cta_limit = max_ctas;
+    return DONOF_OK;
+}
 
 int donof_synchronize(donof_ctx* ctx) {
     if (!ctx) return DONOF_ERR_ARG;
@@ -286,16 +316,15 @@ int donof_b_upload(donof_ctx* ctx, const double* b_host, int nbf, int naux, int 
     DONOF_CHECK(make_job(ctx, nbf, naux, precision, &j));
     const size_t bytes = sizeof(double) * (size_t)nbf * nbf * naux;
     void* d = nullptr;
-    cudaError_t e = cudaMalloc(&d, bytes);
-    if (e != cudaSuccess) {
+    int s0 = dev_alloc(ctx, &d, bytes);
+    if (s0 != DONOF_OK) {
         delete j;
-        set_error(ctx, "cudaMalloc(b, %zu bytes): %s", bytes, cudaGetErrorString(e));
-        return DONOF_ERR_OOM;
+        return s0;
     }
-    e = cudaMemcpyAsync(d, b_host, bytes, cudaMemcpyHostToDevice, ctx->stream);
+    cudaError_t e = cudaMemcpyAsync(d, b_host, bytes, cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) {
-        cudaFree(d);
+        dev_free(ctx, d);
         delete j;
         set_error(ctx, "upload of b: %s", cudaGetErrorString(e));
         return DONOF_ERR_CUDA;
@@ -322,16 +351,16 @@ int donof_iaux(donof_ctx* ctx, const double* G, const double* I3c, int nbf, int 
     DONOF_CHECK(make_job(ctx, nbf, naux, precision, &j));
     const size_t bytes = sizeof(double) * (size_t)nbf * nbf * naux;
     void* d = nullptr;
-    cudaError_t e = cudaMalloc(&d, bytes);
-    if (e != cudaSuccess) {
-        delete j;
-        set_error(ctx, "cudaMalloc(b, %zu bytes): %s", bytes, cudaGetErrorString(e));
-        return DONOF_ERR_OOM;
-    }
-    int s = iaux_f64(ctx, ctx->stream, G, I3c, nbf, naux, static_cast<double*>(d), &j->part);
+    int s = dev_alloc(ctx, &d, bytes);
     if (s != DONOF_OK) {
-        cudaFree(d);
-        j->part.release();
+        delete j;
+        return s;
+    }
+    s = iaux_f64(ctx, ctx->stream, G, I3c, nbf, naux, static_cast<double*>(d), &j->part);
+    if (s != DONOF_OK) {
+        cudaStreamSynchronize(ctx->stream);
+        dev_free(ctx, d);
+        j->part.release(ctx);
         delete j;
         return s;
     }
@@ -370,20 +399,22 @@ int donof_b_attach(donof_ctx* ctx, const double* b_dev, int nbf, int naux, int p
 
 int donof_job_free(donof_job* job) {
     if (!job) return DONOF_OK;
-    cudaSetDevice(job->ctx->device);
-    cudaStreamSynchronize(job->ctx->stream);
-    if (job->own_b && job->b) cudaFree((void*)job->b);
-    if (job->b16hi) cudaFree(job->b16hi);
-    if (job->b16lo) cudaFree(job->b16lo);
-    job->tmp.release();
-    job->bpq.release();
-    job->W.release();
-    job->part.release();
-    job->small.release();
-    job->orb.release();
+    donof_ctx* ctx = job->ctx;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);  // no work of the job is in flight (graphs are destroyed below)
+    if (job->own_b) dev_free(ctx, job->b);
+    dev_free(ctx, job->b16hi);
+    dev_free(ctx, job->b16lo);
+    job->tmp.release(ctx);
+    job->bpq.release(ctx);
+    job->W.release(ctx);
+    job->part.release(ctx);
+    job->small.release(ctx);
+    job->orb.release(ctx);
     if (job->orb_exec) cudaGraphExecDestroy(job->orb_exec);
     if (job->orb_graph) cudaGraphDestroy(job->orb_graph);
-    job->io.release();
+    job->io.release(ctx);
+    job->drv.release(ctx);
     delete job;
     return DONOF_OK;
 }

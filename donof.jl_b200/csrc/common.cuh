@@ -43,7 +43,7 @@ struct DevBuf {
     size_t bytes = 0;
     unsigned gen = 0;  // bumped on every reallocation (captured graphs check it)
     int ensure(donof_ctx* ctx, size_t want);
-    void release();
+    void release(donof_ctx* ctx);  // after the context's stream has no work using it
     template <class T>
     T* as() const { return static_cast<T*>(ptr); }
 };
@@ -67,9 +67,19 @@ struct donof_ctx {
     bool prof_recorded = false;
     // private stream for graph capture when the context uses the legacy default stream
     cudaStream_t aux_stream = nullptr;
+    // most CTAs a persistent or cooperative kernel of this context may use (0: one
+    // per SM); a server running several jobs at once gives each a share of the SMs
+    int cta_limit = 0;
 };
 
 namespace donof {
+// Stream-ordered device allocation on the context's stream (capi.cu).
+int dev_alloc(donof_ctx* ctx, void** p, size_t bytes);
+void dev_free(donof_ctx* ctx, const void* p);
+// CTAs for the persistent and cooperative kernels of a context.
+inline int ctx_ctas(const donof_ctx* c) {
+    return (c->cta_limit > 0 && c->cta_limit < c->sm_count) ? c->cta_limit : c->sm_count;
+}
 // Bracket the dominant kernel of a call with the context's profiling events.
 inline void prof_begin(donof_ctx* ctx, cudaStream_t st) {
     if (ctx->profile && ctx->prof_ev[0]) cudaEventRecord(ctx->prof_ev[0], st);
@@ -97,6 +107,8 @@ struct donof_job {
     donof::DevBuf orb;
     // host-API staging
     donof::DevBuf io;
+    // device arrays of the native energy loop (energy.cu)
+    donof::DevBuf drv;
     // captured optimiser loop (graph with a conditional WHILE node) and the
     // inputs it was captured for
     cudaGraph_t orb_graph = nullptr;

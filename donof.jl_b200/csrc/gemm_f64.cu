@@ -1,6 +1,11 @@
 // Host-side dispatch of the FP64 DMMA GEMM (tile shape, operand layout,
 // 16-byte vs 8-byte staging) and the split-K reduction.
 #include <atomic>
+#include <map>
+#include <mutex>
+#include <tuple>
+#include <vector>
+
 #include "gemm_f64.cuh"
 #include "kernels.cuh"
 
@@ -127,6 +132,95 @@ int gemm_f64_auto(donof_ctx* ctx, cudaStream_t st, bool a_kmajor, bool b_kmajor,
     return gemm_f64(ctx, st, a_kmajor, b_kmajor, p, tile);
 }
 
+// ---------------------------------------------------------------------------
+// Autotuner.  The first call of a GEMM shape (per device, outside stream
+// capture) times every candidate configuration on the call's own operands with
+// CUDA events and keeps the fastest; later calls of that shape, captured graphs
+// included, launch it directly.  Without split-K every tile shape sums each
+// output element over K in the same order, so the candidates write identical
+// results; with split-K the chosen partition is fixed once per process, so a
+// shape gives the same rounding in every later call.
+namespace {
+
+struct TuneKey {
+    int dev, M, N, K, batch, ak, bk, kind;
+    bool operator<(const TuneKey& o) const {
+        return std::tie(dev, M, N, K, batch, ak, bk, kind) < std::tie(o.dev, o.M, o.N, o.K, o.batch, o.ak, o.bk, o.kind);
+    }
+};
+struct TuneVal {
+    GemmTile tile;
+    int splits;
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, TuneVal> g_tune;
+
+bool capturing(cudaStream_t st) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    return cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone;
+}
+
+bool tune_lookup(const TuneKey& k, TuneVal* v) {
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    auto it = g_tune.find(k);
+    if (it == g_tune.end()) return false;
+    *v = it->second;
+    return true;
+}
+
+void tune_store(const TuneKey& k, const TuneVal& v) {
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    g_tune.emplace(k, v);
+}
+
+// Time run(candidate) for each candidate (one warm-up, two timed runs); returns
+// the index of the fastest, or -1 if a launch failed.
+template <class Run>
+int time_candidates(donof_ctx* ctx, cudaStream_t st, int count, Run run) {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        if (e0) cudaEventDestroy(e0);
+        return -1;
+    }
+    int best = -1;
+    float best_ms = 0.f;
+    for (int c = 0; c < count; ++c) {
+        if (run(c) != DONOF_OK) { best = -1; break; }
+        cudaEventRecord(e0, st);
+        int rc = run(c);
+        if (rc == DONOF_OK) rc = run(c);
+        cudaEventRecord(e1, st);
+        if (rc != DONOF_OK || cudaEventSynchronize(e1) != cudaSuccess) { best = -1; break; }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (best < 0 || ms < best_ms) { best = c; best_ms = ms; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (best < 0) set_error(ctx, "GEMM autotuning failed: %s", cudaGetErrorString(cudaGetLastError()));
+    return best;
+}
+
+const GemmTile kTiles[3] = {GemmTile::Large, GemmTile::Small, GemmTile::Tiny};
+const int kTileBM[3] = {128, 64, 32}, kTileBN[3] = {64, 64, 32};
+
+}  // namespace
+
+int gemm_f64_tuned(donof_ctx* ctx, cudaStream_t st, bool a_kmajor, bool b_kmajor, const GemmF64Args& p,
+                   GemmTile heuristic) {
+    const bool tunable = p.splits == 1 && p.beta == 0.0 && p.skip_le == nullptr && p.skip_nz == nullptr &&
+                         p.B_ptr == nullptr;
+    if (!tunable) return gemm_f64(ctx, st, a_kmajor, b_kmajor, p, heuristic);
+    const TuneKey key{ctx->device, p.M, p.N, p.K, p.batch, a_kmajor, b_kmajor, 0};
+    TuneVal v;
+    if (tune_lookup(key, &v)) return gemm_f64(ctx, st, a_kmajor, b_kmajor, p, v.tile);
+    if (capturing(st)) return gemm_f64(ctx, st, a_kmajor, b_kmajor, p, heuristic);
+    const int best = time_candidates(ctx, st, 3, [&](int c) { return gemm_f64(ctx, st, a_kmajor, b_kmajor, p, kTiles[c]); });
+    if (best < 0) return DONOF_ERR_CUDA;
+    tune_store(key, TuneVal{kTiles[best], 1});
+    return DONOF_OK;  // every candidate wrote the same C
+}
+
 int gemm_f64_partials(donof_ctx* ctx, cudaStream_t st, bool a_kmajor, bool b_kmajor, int M, int N, int K,
                       const double* A, long long lda, const double* B, long long ldb, DevBuf* part,
                       const double** out, int* nparts) {
@@ -134,21 +228,62 @@ int gemm_f64_partials(donof_ctx* ctx, cudaStream_t st, bool a_kmajor, bool b_kma
     p.M = M; p.N = N; p.K = K;
     p.A = A; p.lda = lda; p.B = B; p.ldb = ldb;
     p.alpha = 1.0; p.beta = 0.0; p.batch = 1; p.splits = 1; p.kchunk = K;
-    int splits = 1, kchunk = K;
-    const GemmTile tile = pick_tile(ctx, M, N, K, true, &splits);
-    if (splits > 1) {
-        kchunk = ((K + splits - 1) / splits + 15) / 16 * 16;
-        splits = (K + kchunk - 1) / kchunk;
+    // candidates: each tile shape with about one and about two CTAs per SM
+    std::vector<TuneVal> cands;
+    {
+        int sp = 1;
+        const GemmTile h = pick_tile(ctx, M, N, K, true, &sp);
+        cands.push_back(TuneVal{h, sp});
+        const int max_splits = K / 64 > 1 ? K / 64 : 1;
+        for (int t = 0; t < 3; ++t) {
+            const long long tiles = (long long)((M + kTileBM[t] - 1) / kTileBM[t]) * ((N + kTileBN[t] - 1) / kTileBN[t]);
+            for (int f = 1; f <= 2; ++f) {
+                long long s = (f * (long long)ctx->sm_count + tiles - 1) / tiles;
+                if (s > max_splits) s = max_splits;
+                if (s < 1) s = 1;
+                bool dup = false;
+                for (const TuneVal& c : cands) dup = dup || (c.tile == kTiles[t] && c.splits == (int)s);
+                if (!dup) cands.push_back(TuneVal{kTiles[t], (int)s});
+            }
+        }
     }
-    const long long per = (long long)M * N;
-    DONOF_CHECK(part->ensure(ctx, sizeof(double) * per * splits));
-    p.C = part->as<double>(); p.ldc = M;
-    if (splits > 1) {
-        p.splits = splits;
-        p.kchunk = kchunk;
-        p.strideSplit = per;
+    auto config = [&](const TuneVal& c, GemmF64Args* q, int* ns) {
+        *q = p;
+        int splits = c.splits, kchunk = K;
+        if (splits > 1) {
+            kchunk = ((K + splits - 1) / splits + 15) / 16 * 16;
+            splits = (K + kchunk - 1) / kchunk;
+        }
+        q->C = part->as<double>(); q->ldc = M;
+        if (splits > 1) {
+            q->splits = splits;
+            q->kchunk = kchunk;
+            q->strideSplit = (long long)M * N;
+        }
+        *ns = splits;
+    };
+    const TuneKey key{ctx->device, M, N, K, 1, a_kmajor, b_kmajor, 1};
+    TuneVal v = cands[0];
+    const bool known = tune_lookup(key, &v);
+    if (!known && !capturing(st)) {
+        int most = 1;
+        for (const TuneVal& c : cands) most = c.splits > most ? c.splits : most;
+        DONOF_CHECK(part->ensure(ctx, sizeof(double) * (size_t)M * N * most));
+        const int best = time_candidates(ctx, st, (int)cands.size(), [&](int c) {
+            GemmF64Args q;
+            int ns;
+            config(cands[c], &q, &ns);
+            return gemm_f64(ctx, st, a_kmajor, b_kmajor, q, cands[c].tile);
+        });
+        if (best < 0) return DONOF_ERR_CUDA;
+        v = cands[best];
+        tune_store(key, v);
     }
-    DONOF_CHECK(gemm_f64(ctx, st, a_kmajor, b_kmajor, p, tile));
+    GemmF64Args q;
+    int splits = 1;
+    DONOF_CHECK(part->ensure(ctx, sizeof(double) * (size_t)M * N * (v.splits > 1 ? v.splits : 1)));
+    config(v, &q, &splits);
+    DONOF_CHECK(gemm_f64(ctx, st, a_kmajor, b_kmajor, q, v.tile));
     *out = part->as<double>();
     *nparts = splits;
     return DONOF_OK;
@@ -176,3 +311,8 @@ int splitk_reduce(donof_ctx* ctx, cudaStream_t st, const double* part, long long
 }
 
 }  // namespace donof
+
+extern "C" int donof_autotune_entries(void) {
+    std::lock_guard<std::mutex> g(donof::g_tune_mu);
+    return (int)donof::g_tune.size();
+}

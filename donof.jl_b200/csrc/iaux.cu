@@ -40,17 +40,13 @@ struct DeviceScratch {
     template <class T>
     int alloc(T** out, size_t count) {
         void* d = nullptr;
-        const cudaError_t e = cudaMalloc(&d, sizeof(T) * count);
-        if (e != cudaSuccess) {
-            set_error(ctx, "cudaMalloc(%zu bytes): %s", sizeof(T) * count, cudaGetErrorString(e));
-            return DONOF_ERR_OOM;
-        }
+        DONOF_CHECK(dev_alloc(ctx, &d, sizeof(T) * count));
         p[n++] = d;
         *out = static_cast<T*>(d);
         return DONOF_OK;
     }
-    ~DeviceScratch() {
-        for (int i = 0; i < n; ++i) cudaFree(p[i]);
+    ~DeviceScratch() {  // stream-ordered after the work that used the scratch
+        for (int i = 0; i < n; ++i) dev_free(ctx, p[i]);
     }
 };
 

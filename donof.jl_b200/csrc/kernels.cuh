@@ -16,6 +16,13 @@ int gemm_f64(donof_ctx* ctx, cudaStream_t st, bool a_kmajor, bool b_kmajor, Gemm
 int splitk_reduce(donof_ctx* ctx, cudaStream_t st, const double* part, long long stride,
                   int splits, long long count, double* out, double beta);
 
+// gemm_f64 with the tile shape chosen by the autotuner (gemm_f64.cu): the first
+// call of a shape outside stream capture times the candidates and caches the
+// fastest; heuristic is used while capturing and for calls with beta != 0,
+// split-K or device-side gates.
+int gemm_f64_tuned(donof_ctx* ctx, cudaStream_t st, bool a_kmajor, bool b_kmajor, const GemmF64Args& p,
+                   GemmTile heuristic);
+
 // Tile shape (and split count, when can_split) that puts >= one CTA per SM.
 GemmTile pick_tile(donof_ctx* ctx, int M, int N, int K, bool can_split, int* splits_out);
 

@@ -23,56 +23,59 @@ namespace donof {
 
 namespace {
 
-// W builder: one CTA per aux index l, 32x32 tiles transposed through shared
-// memory so that the reads of b_pq^l / ck12 ([b + nbf5*q]) and the writes of
-// W ([q + nbf5*l + Kt*b]) are both coalesced.
-__global__ void build_w_kernel(const double* __restrict__ bpq, const double* __restrict__ n,
-                               const double* __restrict__ cj12, const double* __restrict__ ck12,
-                               int nbf5, int naux, int nalpha, int nbeta,
-                               double* __restrict__ W) {
-    extern __shared__ double sh[];
-    double* d = sh;             // nbf5
-    double* tv = sh + nbf5;     // nbf5
-    __shared__ double tb[32][33];
-    __shared__ double tk[32][33];
-    const int l = blockIdx.x;
-    const long long n55 = (long long)nbf5 * nbf5;
-    const double* B = bpq + n55 * l;
-    const long long Kt = (long long)nbf5 * naux;
-    for (int q = threadIdx.x; q < nbf5; q += blockDim.x) d[q] = B[(long long)q * (nbf5 + 1)];
-    __syncthreads();
-    for (int b = threadIdx.x; b < nbf5; b += blockDim.x) {
+// W of every aux index, W[q + nbf5 l + Kt b] (Kt = nbf5 naux):
+//   W_l[q, b] = delta_qb (n'_b d_b^l + t_b^l) - ck12[b, q] b_pq^l[b, q]
+// with d_b^l = b_pq^l[b, b], t_b^l = sum_q cj12[b, q] d_q^l and n'_b = n_b for
+// b < nbeta or b >= nalpha (0 when nbeta = 0).  Two fully parallel passes:
+// w_diag_kernel forms n'_b d_b^l + t_b^l (one thread per (b, l), cj12 read
+// along b); build_w_kernel the elementwise part over 32 x 32 tiles of (b, q),
+// one tile per CTA step, transposed through shared memory so that b_pq^l and
+// ck12 are read along b and W is written along q (b need not be symmetric).
+__global__ void w_diag_kernel(const double* __restrict__ bpq, const double* __restrict__ n,
+                              const double* __restrict__ cj12, int nbf5, int naux, int nalpha, int nbeta,
+                              double* __restrict__ tv) {
+    const long long n55 = (long long)nbf5 * nbf5, total = (long long)nbf5 * naux;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int b = (int)(i % nbf5);
+        const long long l = i / nbf5;
+        const double* B = bpq + n55 * l;
         double s = 0.0;
-        for (int q = 0; q < nbf5; ++q) s += cj12[b + (long long)nbf5 * q] * d[q];
+        for (int q = 0; q < nbf5; ++q) s += cj12[b + (long long)nbf5 * q] * B[(long long)q * (nbf5 + 1)];
         const bool dj = (nbeta > 0) && (b < nbeta || b >= nalpha);
-        tv[b] = (dj ? n[b] * d[b] : 0.0) + s;
+        tv[i] = (dj ? n[b] * B[(long long)b * (nbf5 + 1)] : 0.0) + s;
     }
-    __syncthreads();
-    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x (blockDim/32)
-    const int rows = blockDim.x >> 5;
+}
+
+// 256 threads: tx = threadIdx.x % 32, ty = threadIdx.x / 32 (8 rows per pass)
+__global__ void __launch_bounds__(256) build_w_kernel(const double* __restrict__ bpq, const double* __restrict__ ck12,
+                                                      const double* __restrict__ tv, int nbf5, int naux,
+                                                      double* __restrict__ W) {
+    __shared__ double tb[32][33];
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const long long n55 = (long long)nbf5 * nbf5, Kt = (long long)nbf5 * naux;
     const int nt = (nbf5 + 31) / 32;
-    for (int tile = 0; tile < nt * nt; ++tile) {
-        const int b0 = (tile % nt) * 32, q0 = (tile / nt) * 32;
-        for (int r = ty; r < 32; r += rows) {
+    const long long tiles = (long long)nt * nt * naux;
+    for (long long t = blockIdx.x; t < tiles; t += gridDim.x) {
+        const int b0 = (int)(t % nt) * 32, q0 = (int)((t / nt) % nt) * 32;
+        const long long l = t / ((long long)nt * nt);
+        const double* B = bpq + n55 * l;
+        __syncthreads();  // the previous tile's reads of tb are done
+        for (int r = ty; r < 32; r += 8) {
             const int b = b0 + tx, q = q0 + r;
-            double vb = 0.0, vk = 0.0;
+            double v = 0.0;
             if (b < nbf5 && q < nbf5) {
-                vb = B[b + (long long)nbf5 * q];
-                vk = ck12[b + (long long)nbf5 * q];
+                const long long e = b + (long long)nbf5 * q;
+                v = -ck12[e] * B[e];
+                if (q == b) v += tv[b + (long long)nbf5 * l];
             }
-            tb[r][tx] = vb;  // [q - q0][b - b0]
-            tk[r][tx] = vk;
+            tb[r][tx] = v;  // [q - q0][b - b0]
         }
         __syncthreads();
-        for (int r = ty; r < 32; r += rows) {
+        for (int r = ty; r < 32; r += 8) {
             const int q = q0 + tx, b = b0 + r;
-            if (b < nbf5 && q < nbf5) {
-                double v = -tk[tx][r] * tb[tx][r];
-                if (q == b) v += tv[b];
-                W[q + (long long)nbf5 * l + Kt * b] = v;
-            }
+            if (b < nbf5 && q < nbf5) W[q + (long long)nbf5 * l + Kt * b] = tb[tx][r];
         }
-        __syncthreads();
     }
 }
 
@@ -162,7 +165,7 @@ int transforms_f64(donof_job* job, cudaStream_t st, const double* C, int nbf5) {
         p.C = tmp; p.ldc = nbf; p.strideC = (long long)nbf * nbf5;
         p.alpha = 1.0; p.beta = 0.0; p.batch = naux; p.splits = 1;
         prof_begin(ctx, st);
-        DONOF_CHECK(gemm_f64(ctx, st, false, true, p, nbf >= 128 ? GemmTile::Large : GemmTile::Small));
+        DONOF_CHECK(gemm_f64_tuned(ctx, st, false, true, p, nbf >= 128 ? GemmTile::Large : GemmTile::Small));
         prof_end(ctx, st);
     }
     // T2: bpq_l(p,q) = sum_m C[m,p] tmp_l[m,q]
@@ -173,7 +176,7 @@ int transforms_f64(donof_job* job, cudaStream_t st, const double* C, int nbf5) {
         p.B = tmp; p.ldb = nbf; p.strideB = (long long)nbf * nbf5;
         p.C = bpq; p.ldc = nbf5; p.strideC = (long long)nbf5 * nbf5;
         p.alpha = 1.0; p.beta = 0.0; p.batch = naux; p.splits = 1;
-        DONOF_CHECK(gemm_f64(ctx, st, true, true, p, nbf5 > 64 ? GemmTile::Large : GemmTile::Small));
+        DONOF_CHECK(gemm_f64_tuned(ctx, st, true, true, p, nbf5 > 64 ? GemmTile::Large : GemmTile::Small));
     }
     return DONOF_OK;
 }
@@ -187,11 +190,20 @@ int lagrange2_f64(donof_job* job, cudaStream_t st, const double* C, const double
 
     DONOF_CHECK(transforms_f64(job, st, C, nbf5));
 
-    DONOF_CHECK(job->W.ensure(ctx, sizeof(double) * (size_t)Kt * nbf5));
+    DONOF_CHECK(job->W.ensure(ctx, sizeof(double) * (size_t)Kt * (nbf5 + 1)));
     double* W = job->W.as<double>();
-    build_w_kernel<<<naux, 256, sizeof(double) * 2 * nbf5, st>>>(job->bpq.as<double>(), n, cj12,
-                                                                 ck12, nbf5, naux, nalpha, nbeta, W); count_launch();
-    DONOF_CUDA(ctx, cudaGetLastError());
+    double* tv = W + (size_t)Kt * nbf5;  // n'_b d_b^l + t_b^l (Kt values)
+    {
+        const double* bpq = job->bpq.as<double>();
+        long long blocks = (Kt + 255) / 256;
+        if (blocks > 8LL * ctx->sm_count) blocks = 8LL * ctx->sm_count;
+        w_diag_kernel<<<(int)blocks, 256, 0, st>>>(bpq, n, cj12, nbf5, naux, nalpha, nbeta, tv); count_launch();
+        const long long nt = (nbf5 + 31) / 32;
+        blocks = nt * nt * naux;
+        if (blocks > 16LL * ctx->sm_count) blocks = 16LL * ctx->sm_count;
+        build_w_kernel<<<(int)blocks, 256, 0, st>>>(bpq, ck12, tv, nbf5, naux, W); count_launch();
+        DONOF_CUDA(ctx, cudaGetLastError());
+    }
 
     // Y = sum_{q,l} tmp[m, q + nbf5*l] W[q + nbf5*l, b], left as split-K partials
     const double* ypart = nullptr;
@@ -307,7 +319,7 @@ int lagrange2_f64_noalloc(donof_job* job, cudaStream_t st, const double* C, cons
     }
     const size_t s_tmp = round256((size_t)nbf * nbf5 * naux);
     const size_t s_bpq = round256((size_t)nbf5 * nbf5 * naux);
-    const size_t s_w = round256((size_t)Kt * nbf5);
+    const size_t s_w = round256((size_t)Kt * (nbf5 + 1));  // W and the diagonal terms
     const size_t s_small = round256((size_t)nbf * nbf5);
     const size_t s_part = round256((size_t)splits * nbf * nbf5);
     const size_t need = (s_tmp + s_bpq + s_w + 2 * s_small + s_part) * sizeof(double);
@@ -358,9 +370,15 @@ int lagrange2_f64_noalloc(donof_job* job, cudaStream_t st, const double* C, cons
         p.alpha = 1.0; p.beta = 0.0; p.batch = naux; p.splits = 1;
         DONOF_CHECK(gemm_f64(ctx, st, true, true, p, nbf5 > 64 ? GemmTile::Large : GemmTile::Small));
     }
-    build_w_kernel<<<naux, 256, sizeof(double) * 2 * nbf5, st>>>(bpq, n, cj12, ck12, nbf5, naux, nalpha,
-                                                                 nbeta, W); count_launch();
-    DONOF_CUDA(ctx, cudaGetLastError());
+    {
+        double* tv = W + (size_t)Kt * nbf5;
+        w_diag_kernel<<<grid_for(Kt, 256, ctx->sm_count), 256, 0, st>>>(bpq, n, cj12, nbf5, naux, nalpha, nbeta,
+                                                                        tv); count_launch();
+        const long long nt = (nbf5 + 31) / 32;
+        build_w_kernel<<<grid_for(nt * nt * naux * 256, 256, ctx->sm_count), 256, 0, st>>>(bpq, ck12, tv, nbf5,
+                                                                                           naux, W); count_launch();
+        DONOF_CUDA(ctx, cudaGetLastError());
+    }
     // Y = tmp W (split-K partials in the scratch, then reduced)
     {
         GemmF64Args p{};

@@ -720,7 +720,7 @@ int launch_mixed(donof_job* job, cudaStream_t st, int nbf5, int nalpha, int nbet
     return DONOF_OK;
 }
 
-int mixed_grid(donof_job* job) { return job->naux < job->ctx->sm_count ? job->naux : job->ctx->sm_count; }
+int mixed_grid(donof_job* job) { return job->naux < ctx_ctas(job->ctx) ? job->naux : ctx_ctas(job->ctx); }
 
 int check_mixed(donof_job* job, int nbf5) {
     if (job->b16hi == nullptr) {
@@ -743,21 +743,20 @@ int convert_b_f32(donof_job* job) {
     const size_t count = (size_t)64 * nb * nbf * job->naux;
     void* hi = nullptr;
     void* lo = nullptr;
-    DONOF_CUDA(ctx, cudaMalloc(&hi, sizeof(__nv_bfloat16) * count));
-    cudaError_t e = cudaMalloc(&lo, sizeof(__nv_bfloat16) * count);
-    if (e != cudaSuccess) {
-        cudaFree(hi);
-        set_error(ctx, "cudaMalloc(b split): %s", cudaGetErrorString(e));
-        return DONOF_ERR_OOM;
+    DONOF_CHECK(dev_alloc(ctx, &hi, sizeof(__nv_bfloat16) * count));
+    int s = dev_alloc(ctx, &lo, sizeof(__nv_bfloat16) * count);
+    if (s != DONOF_OK) {
+        dev_free(ctx, hi);
+        return s;
     }
     mx::split_b_kernel<<<8 * ctx->sm_count, 256, 0, ctx->stream>>>(job->b, nbf, nb, (long long)job->naux,
                                                                    static_cast<__nv_bfloat16*>(hi),
                                                                    static_cast<__nv_bfloat16*>(lo)); count_launch();
-    e = cudaGetLastError();
+    cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) {
-        cudaFree(hi);
-        cudaFree(lo);
+        dev_free(ctx, hi);
+        dev_free(ctx, lo);
         set_error(ctx, "bf16 split of b: %s", cudaGetErrorString(e));
         return DONOF_ERR_CUDA;
     }

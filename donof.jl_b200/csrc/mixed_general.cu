@@ -11,12 +11,15 @@
 //                                                      bf16 hi/lo split tmpQ[l][q][m]
 //   T2  b_pq^l[p, q] = sum_m C5[m, p] tmp_l[m, q]     D[p, q]; FP32 out
 //   W   W_l[q, b] = delta_qb (n'_b d_b + sum_q' cj12[b, q'] d_q') - ck12[b, q] b_bq^l
-//                                                      (mg_w_kernel, FP32, split out)
+//                                                      (mg_wdiag_kernel + mg_w_kernel, FP32, split out)
 //   Y   Y[m, b] = sum_l sum_q W_l[q, b] tmp_l[m, q]    D[b, m]; FP32 partial per aux chunk
 //
 // and the FP64 tail (tail.cu) forms H_mat, elag and E_elec from the Y
 // partials, as for the other forms (src/utils.jl:1-59 restructured:
 // elag[:, :nbf5] = C^T Y + n o H_mat).
+//
+// b is the RI tensor, symmetric in (m, n) like every tensor Iaux produces;
+// the W builder reads b_pq^l through the symmetry that follows from it.
 //
 // Every product is  A_hi B_hi + A_hi B_lo + A_lo B_hi  (the lo x lo term is
 // below FP32 rounding) with FP32 accumulation in TMEM.  Operands are staged by
@@ -347,43 +350,47 @@ __global__ void mg_prep_kernel(const double* __restrict__ C, int nbf, int nbf5, 
     }
 }
 
-// W of one aux index per CTA (FP32), written as the bf16 split
-// W_x[q + ldq b + ldq nbf5 l] (rows b, contiguous q: the K-major A operand of Y):
+// W (FP32), written as the bf16 split W_x[q + ldq b + ldq nbf5 l] (rows b,
+// contiguous q: the K-major A operand of Y):
 //   W[q, b] = delta_qb (n'_b d_b + sum_q' cj12[b, q'] d_q') - ck12[b, q] b_pq[q, b]
 // with d_q = b_pq[q, q] and n'_b = n_b for b < nbeta or b >= nalpha (0 when
-// nbeta = 0); b_pq is symmetric, so its row b is read as column b.
-__global__ void mg_w_kernel(const float* __restrict__ bpq, const float* __restrict__ n32,
-                            const float* __restrict__ cj32, const float* __restrict__ ckT, int nbf5, int ldq,
-                            int nalpha, int nbeta, __nv_bfloat16* __restrict__ w_hi, __nv_bfloat16* __restrict__ w_lo) {
-    extern __shared__ float shw[];
-    float* d = shw;          // nbf5
-    float* tv = shw + nbf5;  // nbf5
-    const int l = blockIdx.x;
-    const long long n55 = (long long)nbf5 * nbf5;
-    const float* B = bpq + n55 * l;
-    for (int q = threadIdx.x; q < nbf5; q += blockDim.x) d[q] = B[(long long)q * (nbf5 + 1)];
-    __syncthreads();
-    for (int b = threadIdx.x; b < nbf5; b += blockDim.x) {
+// nbeta = 0); b_pq is symmetric, so its row b is read as column b.  mg_wdiag
+// forms the diagonal terms (one thread per (b, l)), mg_w the elements (one
+// thread per element, reads and writes along q).
+__global__ void mg_wdiag_kernel(const float* __restrict__ bpq, const float* __restrict__ n32,
+                                const float* __restrict__ cj32, int nbf5, int naux, int nalpha, int nbeta,
+                                float* __restrict__ tv) {
+    const long long n55 = (long long)nbf5 * nbf5, total = (long long)nbf5 * naux;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int b = (int)(i % nbf5);
+        const float* B = bpq + n55 * (i / nbf5);
         float s = 0.f;
-        for (int q = 0; q < nbf5; ++q) s += cj32[b + (long long)nbf5 * q] * d[q];
+        for (int q = 0; q < nbf5; ++q) s += cj32[b + (long long)nbf5 * q] * B[(long long)q * (nbf5 + 1)];
         const bool dj = (nbeta > 0) && (b < nbeta || b >= nalpha);
-        tv[b] = (dj ? n32[b] * d[b] : 0.f) + s;
+        tv[i] = (dj ? n32[b] * B[(long long)b * (nbf5 + 1)] : 0.f) + s;
     }
-    __syncthreads();
-    const long long per = (long long)ldq * nbf5;
-    __nv_bfloat16* oh = w_hi + per * l;
-    __nv_bfloat16* ol = w_lo + per * l;
-    for (long long i = threadIdx.x; i < per; i += blockDim.x) {
-        const int q = (int)(i % ldq), b = (int)(i / ldq);
+}
+
+__global__ void mg_w_kernel(const float* __restrict__ bpq, const float* __restrict__ ckT,
+                            const float* __restrict__ tv, int nbf5, int ldq, int naux,
+                            __nv_bfloat16* __restrict__ w_hi, __nv_bfloat16* __restrict__ w_lo) {
+    const long long n55 = (long long)nbf5 * nbf5, total = (long long)ldq * nbf5 * naux;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int q = (int)(i % ldq);
+        const long long r = i / ldq;  // b + nbf5 l
+        const int b = (int)(r % nbf5);
+        const long long l = r / nbf5;
         float v = 0.f;
         if (q < nbf5) {
-            v = -ckT[q + (long long)nbf5 * b] * B[q + (long long)nbf5 * b];
-            if (q == b) v += tv[b];
+            v = -ckT[q + (long long)nbf5 * b] * bpq[q + (long long)nbf5 * b + n55 * l];
+            if (q == b) v += tv[r];
         }
         __nv_bfloat16 h, lo;
         split_bf16(v, h, lo);
-        oh[i] = h;
-        ol[i] = lo;
+        w_hi[i] = h;
+        w_lo[i] = lo;
     }
 }
 
@@ -438,13 +445,13 @@ int round8(int x) { return (x + 7) / 8 * 8; }
 struct GenScratch {
     int* status;
     __nv_bfloat16 *cs_hi, *cs_lo, *tq_hi, *tq_lo, *w_hi, *w_lo;
-    float *n32, *cj32, *ckT, *bpq, *ypart;
+    float *n32, *cj32, *ckT, *bpq, *ypart, *tv;
     int ldm, ldq, nchunks, lchunk;
 };
 
 void y_chunks(donof_job* job, int nbf5, int* nchunks, int* lchunk) {
     const int mtiles = (nbf5 + mg::BM - 1) / mg::BM, ntiles = (job->nbf + mg::BN - 1) / mg::BN;
-    int nc = job->ctx->sm_count / (mtiles * ntiles);
+    int nc = ctx_ctas(job->ctx) / (mtiles * ntiles);
     if (nc < 1) nc = 1;
     if (nc > job->naux) nc = job->naux;
     const int lc = (job->naux + nc - 1) / nc;
@@ -474,6 +481,7 @@ int gen_prepare(donof_job* job, cudaStream_t st, const double* C, const double* 
     const size_t wsz = with_w ? (size_t)S->ldq * nbf5 * naux : 0;
     const size_t o_w = take(2 * sizeof(__nv_bfloat16) * wsz);
     const size_t o_y = take(with_w ? sizeof(float) * (size_t)S->nchunks * nbf * nbf5 : 0);
+    const size_t o_tv = take(with_w ? sizeof(float) * (size_t)nbf5 * naux : 0);
     DONOF_CHECK(job->W.ensure(ctx, off));
     char* base = job->W.as<char>();
     S->status = reinterpret_cast<int*>(base + o_status);
@@ -486,6 +494,7 @@ int gen_prepare(donof_job* job, cudaStream_t st, const double* C, const double* 
     S->w_hi = reinterpret_cast<__nv_bfloat16*>(base + o_w);
     S->w_lo = S->w_hi + wsz;
     S->ypart = reinterpret_cast<float*>(base + o_y);
+    S->tv = reinterpret_cast<float*>(base + o_tv);
     DONOF_CUDA(ctx, cudaMemsetAsync(S->status, 0, sizeof(int) * 4, st));
     const long long work = (long long)S->ldm * nbf5 > (long long)nbf5 * nbf5 ? (long long)S->ldm * nbf5
                                                                              : (long long)nbf5 * nbf5;
@@ -508,7 +517,7 @@ int launch_gemm(donof_job* job, cudaStream_t st, const mg::Params& P, const CUte
         attr_mask.fetch_or(bit, std::memory_order_acq_rel);
     }
     const int nitems = P.nchunks * P.mtiles * P.ntiles;
-    const int grid = nitems < ctx->sm_count ? nitems : ctx->sm_count;
+    const int grid = nitems < ctx_ctas(ctx) ? nitems : ctx_ctas(ctx);
     mg::mg_gemm_kernel<<<grid, mg::NTHREADS, mg::SMEM_ALLOC, st>>>(a_hi, a_lo, b_hi, b_lo, P); count_launch();
     DONOF_CUDA(ctx, cudaGetLastError());
     return DONOF_OK;
@@ -584,9 +593,18 @@ int lagrange2_mixed_general(donof_job* job, cudaStream_t st, const double* C, co
     GenScratch S;
     DONOF_CHECK(gen_prepare(job, st, C, n, cj12, ck12, nbf5, true, &S));
     DONOF_CHECK(gen_transforms(job, st, nbf5, S));
-    mg::mg_w_kernel<<<naux, 256, sizeof(float) * 2 * nbf5, st>>>(S.bpq, S.n32, S.cj32, S.ckT, nbf5, S.ldq, nalpha,
-                                                                 nbeta, S.w_hi, S.w_lo); count_launch();
-    DONOF_CUDA(ctx, cudaGetLastError());
+    {
+        const long long nd = (long long)nbf5 * naux, nw = (long long)S.ldq * nbf5 * naux;
+        long long blocks = (nd + 255) / 256;
+        if (blocks > 8LL * ctx->sm_count) blocks = 8LL * ctx->sm_count;
+        mg::mg_wdiag_kernel<<<(int)blocks, 256, 0, st>>>(S.bpq, S.n32, S.cj32, nbf5, naux, nalpha, nbeta,
+                                                         S.tv); count_launch();
+        blocks = (nw + 255) / 256;
+        if (blocks > 16LL * ctx->sm_count) blocks = 16LL * ctx->sm_count;
+        mg::mg_w_kernel<<<(int)blocks, 256, 0, st>>>(S.bpq, S.ckT, S.tv, nbf5, S.ldq, naux, S.w_hi,
+                                                     S.w_lo); count_launch();
+        DONOF_CUDA(ctx, cudaGetLastError());
+    }
     CUtensorMap w_hi, w_lo, tm_hi, tm_lo;
     {   // W, rows b, contiguous q: (q, b, l)
         cuuint64_t dims[3] = {(cuuint64_t)nbf5, (cuuint64_t)nbf5, (cuuint64_t)naux};

@@ -1,0 +1,33 @@
+// Internal C++ interface of the native occupation layer (occupation.cu), for
+// host drivers inside the library (the energy loop of energy.cu).
+#pragma once
+
+#include <vector>
+
+#include "common.cuh"
+
+namespace donof {
+namespace occ {
+
+// Sizes and index tables of the GNOF occupation layer (names of src/param.jl).
+struct Occ {
+    int N, no1, ndoc, nsoc, nbeta, nalpha, ncwo, nv, ista, high_spin, method;
+    double h_cut;
+    std::vector<int> S, P, G;  // strong (ndoc); weak P[g*ncwo + w]; gamma index G[g*ncwo + w]
+};
+
+// false on inconsistent sizes or switches
+bool setup(const donof_occ_params* q, Occ& o);
+// n (N) and dn (N x nv, dn[i * nv + k]) of ocupacion_softmax / _trigonometric
+void occupations(const Occ& o, const double* gamma, double* n, double* dn);
+// GNOF cj12, ck12 (N x N, column-major) of CJCKD8
+void coupling(const Occ& o, const double* n, double* cj, double* ck);
+// occupation energy (calce) and, with grad != nullptr, its gamma-gradient (calcoccg)
+double energy_grad(const Occ& o, const double* gamma, const double* J, const double* K, const double* Hc,
+                   double* grad);
+// occoptr's minimisation over gamma (Hager-Zhang CG, strong-Wolfe line search)
+int cg(const Occ& o, const double* J_MO, const double* K_MO, const double* H_core, double* gamma,
+       double g_abstol, int max_iter, double* E, int* nit, int* converged);
+
+}  // namespace occ
+}  // namespace donof

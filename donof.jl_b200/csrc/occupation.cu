@@ -24,15 +24,10 @@
 #include <algorithm>
 #include <vector>
 
-#include "common.cuh"
+#include "occ.cuh"
 
-namespace {
-
-struct Occ {
-    int N, no1, ndoc, nsoc, nbeta, nalpha, ncwo, nv, ista, high_spin, method;
-    double h_cut;
-    std::vector<int> S, P, G;  // strong (ndoc); weak P[g*ncwo + w]; gamma index G[g*ncwo + w]
-};
+namespace donof {
+namespace occ {
 
 bool setup(const donof_occ_params* q, Occ& o) {
     if (!q) return false;
@@ -474,28 +469,8 @@ double dot(const std::vector<double>& a, const std::vector<double>& b) {
     return s;
 }
 
-}  // namespace
-
-extern "C" {
-
-int donof_occ_energy(const donof_occ_params* prm, const double* gamma, const double* J_MO, const double* K_MO,
-                     const double* H_core, double* E, double* grad) {
-    Occ o;
-    if (!setup(prm, o) || !gamma || !J_MO || !K_MO || !H_core || !E) {
-        donof::set_error(nullptr, "donof_occ_energy: invalid sizes or null pointer");
-        return DONOF_ERR_ARG;
-    }
-    *E = energy_grad(o, gamma, J_MO, K_MO, H_core, grad);
-    return DONOF_OK;
-}
-
-int donof_occ_cg(const donof_occ_params* prm, const double* J_MO, const double* K_MO, const double* H_core,
-                 double* gamma, double g_abstol, int max_iter, double* E, int* nit, int* converged) {
-    Occ o;
-    if (!setup(prm, o) || !gamma || !J_MO || !K_MO || !H_core || !E || !nit || !converged || max_iter < 0) {
-        donof::set_error(nullptr, "donof_occ_cg: invalid sizes, null pointer or max_iter < 0");
-        return DONOF_ERR_ARG;
-    }
+int cg(const Occ& o, const double* J_MO, const double* K_MO, const double* H_core, double* gamma,
+       double g_abstol, int max_iter, double* E, int* nit, int* converged) {
     const int nv = o.nv;
     const double eta = 0.4;
     std::vector<double> x(gamma, gamma + nv), gx(nv), d(nv), gn(nv), y(nv);
@@ -562,6 +537,36 @@ int donof_occ_cg(const donof_occ_params* prm, const double* J_MO, const double* 
     *E = fx;
     *nit = max_iter;
     return DONOF_OK;
+}
+
+}  // namespace occ
+}  // namespace donof
+
+extern "C" {
+
+using donof::occ::Occ;
+using donof::occ::setup;
+using donof::occ::energy_grad;
+
+int donof_occ_energy(const donof_occ_params* prm, const double* gamma, const double* J_MO, const double* K_MO,
+                     const double* H_core, double* E, double* grad) {
+    Occ o;
+    if (!setup(prm, o) || !gamma || !J_MO || !K_MO || !H_core || !E) {
+        donof::set_error(nullptr, "donof_occ_energy: invalid sizes or null pointer");
+        return DONOF_ERR_ARG;
+    }
+    *E = energy_grad(o, gamma, J_MO, K_MO, H_core, grad);
+    return DONOF_OK;
+}
+
+int donof_occ_cg(const donof_occ_params* prm, const double* J_MO, const double* K_MO, const double* H_core,
+                 double* gamma, double g_abstol, int max_iter, double* E, int* nit, int* converged) {
+    Occ o;
+    if (!setup(prm, o) || !gamma || !J_MO || !K_MO || !H_core || !E || !nit || !converged || max_iter < 0) {
+        donof::set_error(nullptr, "donof_occ_cg: invalid sizes, null pointer or max_iter < 0");
+        return DONOF_ERR_ARG;
+    }
+    return donof::occ::cg(o, J_MO, K_MO, H_core, gamma, g_abstol, max_iter, E, nit, converged);
 }
 
 }  // extern "C"

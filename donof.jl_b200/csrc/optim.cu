@@ -278,7 +278,8 @@ int orbopt_run(donof_job* job, int method, const double* n, const double* cj12, 
                                             (unsigned long long)(uintptr_t)ck12, (unsigned long long)(uintptr_t)H,
                                             (unsigned long long)nbf5 | ((unsigned long long)nalpha << 20) |
                                                 ((unsigned long long)nbeta << 40),
-                                            (unsigned long long)method, (unsigned long long)precision, gens,
+                                            (unsigned long long)method | ((unsigned long long)ctx_ctas(ctx) << 8),
+                                            (unsigned long long)precision, gens,
                                             (unsigned long long)(uintptr_t)base, (unsigned long long)(uintptr_t)st};
         bool valid = job->orb_exec != nullptr;
         for (int k = 0; k < 10 && valid; ++k) valid = (job->orb_key[k] == key[k]);

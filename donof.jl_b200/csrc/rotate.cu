@@ -361,7 +361,7 @@ int rotate_f64(donof_ctx* ctx, cudaStream_t st, const double* y, int nbf, int nb
         return DONOF_ERR_CUDA;
     }
     const int mt = (nbf + dtile::TM - 1) / dtile::TM, ntile = mt * ((nbf + RT_TN - 1) / RT_TN);
-    int grid = ctx->sm_count;                  // one CTA per SM (co-resident: the kernel has grid barriers)
+    int grid = ctx_ctas(ctx);                  // at most one CTA per SM (co-resident: the kernel has grid barriers)
     if (grid > 2 * ntile) grid = 2 * ntile;    // stage S2 has 2 * ntile tiles
     if (grid < 1) grid = 1;
     DONOF_CUDA(ctx, cudaMemsetAsync(a.cs, 0, sizeof(CoopState), st));

@@ -229,7 +229,7 @@ int elag_tail_f64(donof_job* job, cudaStream_t st, const double* C, const double
         set_error(ctx, "elag_tail_kernel does not fit on an SM");
         return DONOF_ERR_CUDA;
     }
-    const int grid = ctx->sm_count;  // one CTA per SM (co-resident: the kernel has grid barriers)
+    const int grid = ctx_ctas(ctx);  // at most one CTA per SM (co-resident: the kernel has grid barriers)
     DONOF_CUDA(ctx, cudaMemsetAsync(a.ts, 0, sizeof(TailState), st));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(grid);

@@ -42,6 +42,7 @@ SIGNATURES = {
     "donof_destroy": (_i, [_vp]),
     "donof_set_stream": (_i, [_vp, _vp]),
     "donof_get_stream": (_vp, [_vp]),
+    "donof_set_cta_limit": (_i, [_vp, _i]),
     "donof_synchronize": (_i, [_vp]),
     "donof_b_upload": (_i, [_vp, _vp, _i, _i, _i, ct.POINTER(_vp)]),
     "donof_b_attach": (_i, [_vp, _vp, _i, _i, _i, ct.POINTER(_vp)]),
@@ -51,6 +52,7 @@ SIGNATURES = {
     "donof_job_device_bytes": (ct.c_size_t, [_vp]),
     "donof_occ_energy": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "donof_occ_cg": (_i, [_vp, _vp, _vp, _vp, _vp, ct.c_double, _i, _vp, _vp, _vp]),
+    "donof_energy": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "donof_lagrange2": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp, _vp]),
     "donof_lagrange2_dev": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp, _vp]),
     "donof_lagrange2_prec_dev": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp, _vp]),
@@ -65,6 +67,7 @@ SIGNATURES = {
                               _ip, _ip]),
     "donof_transform_dev": (_i, [_vp, _i, _vp, _i, _vp]),
     "donof_launch_count": (ct.c_ulonglong, []),
+    "donof_autotune_entries": (_i, []),
     "donof_job_error_flag": (_i, [_vp, _ip]),
     "donof_profile_enable": (_i, [_vp, _i]),
     "donof_profile_last_ms": (_i, [_vp, ct.POINTER(ct.c_float)]),

@@ -70,6 +70,11 @@ class Context:
     def set_stream(self, stream_handle: int) -> None:
         self.check(self.lib.donof_set_stream(self.handle, ct.c_void_p(stream_handle)))
 
+    def set_cta_limit(self, max_ctas: int) -> None:
+        """Most CTAs this context's persistent and cooperative kernels may use
+        (0: one per SM)."""
+        self.check(self.lib.donof_set_cta_limit(self.handle, int(max_ctas)))
+
     def check(self, status: int) -> None:
         _lib.check(status, self.handle)
 
@@ -357,6 +362,43 @@ def occ_energy(gamma, J_MO, K_MO, H_core, p: Param, grad: bool = True):
     _lib.check(lib.donof_occ_energy(ct.byref(prm), _ptr(gamma), _ptr(J), _ptr(K), _ptr(Hc), ct.byref(E),
                                     _ptr(g) if grad else None))
     return E.value, g
+
+
+class _EnergyParams(ct.Structure):
+    _fields_ = [("occ", _OccParams), ("orb_method", ct.c_int), ("maxit", ct.c_int), ("maxloop", ct.c_int),
+                ("alpha", ct.c_double), ("threshgorb", ct.c_double), ("threshgocc", ct.c_double),
+                ("threshen", ct.c_double), ("order_subspaces", ct.c_int), ("freeze_occ", ct.c_int)]
+
+
+class _EnergyResult(ct.Structure):
+    _fields_ = [("E_elec", ct.c_double), ("iterations", ct.c_int), ("converged", ct.c_int),
+                ("tot_it_orb", ct.c_int), ("tot_it_occ", ct.c_int), ("max_grad_orb", ct.c_double),
+                ("norm_grad_occ", ct.c_double)]
+
+
+def energy_loop(H, b: BTensor, p: Param, C, gamma, maxit: Optional[int] = None, freeze_occ: bool = False,
+                order: bool = True):
+    """DoNOF.energy's orbital / occupation alternation in one native call
+    (donof_energy), in the precision b is set to.  Updates p.alpha and
+    p.maxloop like the reference.  Returns (C, gamma, n, elag, result fields,
+    history rows (E, E_diff, max|g_orb|, |g_occ|, nit_orb, nit_occ))."""
+    maxit = int(maxit or p.maxit)
+    prm = _EnergyParams(_occ_params(p), _lib.ORB_METHODS[p.orb_method], maxit, int(p.maxloop), float(p.alpha),
+                        float(p.threshgorb), float(p.threshgocc), float(p.threshen),
+                        int(bool(order) and p.ipnof > 4), int(bool(freeze_occ)))
+    Cio = np.array(_f64(C), copy=True, order="F")
+    g = np.array(gamma, dtype=np.float64, copy=True)
+    n = np.zeros(p.nbf5)
+    elag = np.zeros((p.nbf, p.nbf), order="F")
+    hist = np.zeros((maxit, 6))
+    res = _EnergyResult()
+    Hf = _f64(H)  # kept alive across the call
+    b.ctx.check(b.ctx.lib.donof_energy(b.handle, ct.byref(prm), _ptr(Hf), _ptr(Cio), _ptr(g), _ptr(n),
+                                       _ptr(elag), _ptr(hist), ct.byref(res)))
+    p.alpha = prm.alpha
+    p.maxloop = prm.maxloop
+    out = {f: getattr(res, f) for f, _ in _EnergyResult._fields_}
+    return Cio, g, n, elag, out, hist[:res.iterations]
 
 
 def occ_cg(gamma, J_MO, K_MO, H_core, p: Param, g_abstol: float, max_iter: int = 1000):

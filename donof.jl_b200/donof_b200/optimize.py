@@ -216,14 +216,28 @@ class EnergyResult:
 
 def energy(H, b: api.BTensor, p: Param, C, gamma=None, E_nuc: float = 0.0, freeze_occ: bool = False,
            maxit: Optional[int] = None, log: Optional[Callable[[dict], None]] = None,
-           order: bool = True) -> EnergyResult:
+           order: bool = True, native: bool = True) -> EnergyResult:
     """The orbital / occupation alternation of DoNOF.energy (src/energy.jl:140-224)
     for given core Hamiltonian H, device RI tensor b and starting orbitals C
     (the integral and guess set-up of energy.jl:29-105 is outside this path).
-    The orbital optimiser runs device resident in the precision of b."""
+    The orbital optimiser runs device resident in the precision of b.
+
+    native=True runs the whole alternation in the library (donof_energy), with
+    no interpreter work per iteration; native=False runs the same steps from
+    Python, one library call each (the two agree to rounding)."""
     H = np.asfortranarray(H, dtype=np.float64)
     C = np.array(C, dtype=np.float64, order="F")
     gamma = gnof.guess_gamma(p) if gamma is None else np.array(gamma, dtype=np.float64)
+    if native:
+        C, gamma, n, elag, r, hist = api.energy_loop(H, b, p, C, gamma, maxit=maxit, freeze_occ=freeze_occ,
+                                                     order=order)
+        rows = [dict(it=i + 1, nit_orb=int(h[4]), nit_occ=int(h[5]), E=h[0], E_tot=h[0] + E_nuc, E_diff=h[1],
+                     max_grad_orb=h[2], norm_grad_occ=h[3]) for i, h in enumerate(hist)]
+        if log:
+            for row in rows:
+                log(row)
+        return EnergyResult(r["E_elec"], r["E_elec"] + E_nuc, C, n, gamma, elag, r["iterations"],
+                            bool(r["converged"]), r["tot_it_orb"], r["tot_it_occ"], rows)
     n, _ = gnof.occupations(gamma, p)
     cj12, ck12 = gnof.coupling(n, p)
     E_old = 9999.0
@@ -264,7 +278,7 @@ def energy(H, b: api.BTensor, p: Param, C, gamma=None, E_nuc: float = 0.0, freez
 
 def energy_mixed_refined(H, b: api.BTensor, p: Param, C, gamma=None, E_nuc: float = 0.0,
                          maxit: Optional[int] = None, log: Optional[Callable[[dict], None]] = None,
-                         mixed_factor: float = 10.0):
+                         mixed_factor: float = 10.0, native: bool = True):
     """The mixed-precision form until its gradients are below mixed_factor times
     the thresholds (the bf16-split gradients carry ~1e-5 relative rounding, so
     driving them to the FP64 thresholds only adds iterations), then closing FP64
@@ -276,8 +290,8 @@ def energy_mixed_refined(H, b: api.BTensor, p: Param, C, gamma=None, E_nuc: floa
     pm.threshgorb = p.threshgorb * mixed_factor
     pm.threshgocc = p.threshgocc * mixed_factor
     b.set_precision("mixed")
-    r_mixed = energy(H, b, pm, C, gamma, E_nuc=E_nuc, maxit=maxit, log=log, order=False)
+    r_mixed = energy(H, b, pm, C, gamma, E_nuc=E_nuc, maxit=maxit, log=log, order=False, native=native)
     p.maxloop = pm.maxloop
     b.set_precision("fp64")
-    r = energy(H, b, p, r_mixed.C, r_mixed.gamma, E_nuc=E_nuc, maxit=maxit, log=log)
+    r = energy(H, b, p, r_mixed.C, r_mixed.gamma, E_nuc=E_nuc, maxit=maxit, log=log, native=native)
     return r, r_mixed

@@ -20,6 +20,7 @@ orbital state and the partial sums (see ``footprint``).
 """
 from __future__ import annotations
 
+import functools
 import itertools
 import threading
 import time
@@ -132,12 +133,15 @@ class Admission:
         self.inflight -= 1
 
 
-def run_energy(req: Request, device: int) -> Result:
-    """Executor: the energy loop of one request on its own context and stream."""
+def run_energy(req: Request, device: int, cta_limit: int = 0) -> Result:
+    """Executor: the energy loop of one request on its own context and stream;
+    cta_limit caps the CTAs of its persistent kernels (0: one per SM)."""
     from . import api
     from .optimize import energy, energy_mixed_refined
 
     ctx = api.Context(device, torch_stream=False)
+    if cta_limit:
+        ctx.set_cta_limit(cta_limit)
     b = None
     try:
         up = "fp64" if req.precision == "fp64" else "mixed"
@@ -154,19 +158,38 @@ def run_energy(req: Request, device: int) -> Result:
         ctx.close()
 
 
+def cta_share(max_inflight: int, sm_count: int = 148) -> int:
+    """CTAs per job for a server with max_inflight slots: all SMs for one job,
+    else about two jobs per SM, at least 16."""
+    if max_inflight <= 1:
+        return 0
+    return max(16, -(-2 * sm_count // max_inflight))
+
+
+def cta_share_for(max_inflight: int, device: int = 0) -> int:
+    import torch
+    return cta_share(max_inflight, torch.cuda.get_device_properties(device).multi_processor_count)
+
+
 class Server:
     """Accepts requests at any time; runs admitted jobs concurrently, each on
     its own stream.  ``executor(request, device) -> Result`` does the work
     (``run_energy`` by default)."""
 
     def __init__(self, device: int = 0, budget_bytes: Optional[int] = None, max_inflight: int = 8,
-                 max_bypass: int = 4, executor: Callable[[Request, int], Result] = run_energy):
+                 max_bypass: int = 4, executor: Callable[[Request, int], Result] = run_energy,
+                 cta_share: Optional[int] = None):
         if budget_bytes is None:
             import torch
             free, _ = torch.cuda.mem_get_info(device)
             budget_bytes = int(0.85 * free)
         self.device = device
         self.admission = Admission(budget_bytes, max_inflight, max_bypass)
+        if executor is run_energy:
+            # each in-flight job's persistent kernels get a share of the SMs (about
+            # two jobs' worth of overlap per SM), so that the jobs run side by side
+            share = cta_share if cta_share is not None else cta_share_for(max_inflight, device)
+            executor = functools.partial(run_energy, cta_limit=share)
         self.executor = executor
         self._lock = threading.Condition()
         self._tickets = itertools.count(1)

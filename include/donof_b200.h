@@ -43,7 +43,7 @@ extern "C" {
 
 /* precision of the b tensor held by a job and of the bulk contractions */
 #define DONOF_PREC_FP64 0   /* all contractions in FP64 (plain form) */
-#define DONOF_PREC_MIXED 1  /* tensor-core TF32x3 bulk contractions, FP32 accumulation */
+#define DONOF_PREC_MIXED 1  /* tensor-core 3 x bf16 split bulk contractions, FP32 accumulation */
 
 /* orbital optimisers (src/minimization.jl:242-630) */
 #define DONOF_ORB_ADAM 0
@@ -60,6 +60,10 @@ int donof_destroy(donof_ctx* ctx);
 /* use an existing cudaStream_t (passed as void*) instead of the own stream */
 int donof_set_stream(donof_ctx* ctx, void* stream);
 void* donof_get_stream(donof_ctx* ctx);
+/* Most CTAs the context's persistent and cooperative kernels may use (0, the
+ * default: one per SM).  A server running several jobs at once gives each
+ * context a share of the SMs so that their kernels run side by side.         */
+int donof_set_cta_limit(donof_ctx* ctx, int max_ctas);
 int donof_synchronize(donof_ctx* ctx);
 const char* donof_last_error(const donof_ctx* ctx);
 const char* donof_status_string(int status);
@@ -209,6 +213,39 @@ int donof_occ_cg(const donof_occ_params* p, const double* J_MO, const double* K_
                  const double* H_core, double* gamma, double g_abstol, int max_iter, double* E,
                  int* nit, int* converged);
 
+/* --- the energy loop ------------------------------------------------------------
+ * Switches and thresholds of DoNOF.energy's alternation (names of
+ * src/param.jl): the occupation layer, the orbital optimiser (DONOF_ORB_*),
+ * maxit outer iterations, maxloop and alpha (read and updated like p.maxloop and
+ * p.alpha), threshgorb / threshgocc (convergence) and threshen (g_abstol of
+ * occoptr); order_subspaces = 1 applies the final sort of src/guess.jl:58-106
+ * (ipnof > 4); freeze_occ = 1 keeps gamma fixed.                             */
+typedef struct {
+    donof_occ_params occ;
+    int orb_method;
+    int maxit;
+    int maxloop;
+    double alpha;
+    double threshgorb, threshgocc, threshen;
+    int order_subspaces;
+    int freeze_occ;
+} donof_energy_params;
+typedef struct {
+    double E_elec;                /* E of the last orbital optimisation */
+    int iterations, converged, tot_it_orb, tot_it_occ;
+    double max_grad_orb, norm_grad_occ;
+} donof_energy_result;
+/* The orbital / occupation alternation of DoNOF.energy (src/energy.jl:140-224)
+ * in one call, in the job's precision: orbopt on the device, occoptr (J_MO,
+ * K_MO, H_core on the device, conjugate gradient over gamma on the host),
+ * order_occupations_softmax, and the convergence test on max|g_orb| and
+ * |g_occ|.  Host arrays: H and C_inout (nbf x nbf), gamma_inout (nv); n_out
+ * (nbf5), elag_out (nbf x nbf) and history (6 per iteration: E, E_diff,
+ * max|g_orb|, |g_occ|, orbital and occupation iterations) may be NULL.     */
+int donof_energy(donof_job* job, donof_energy_params* params, const double* H, double* C_inout,
+                 double* gamma_inout, double* n_out, double* elag_out, double* history,
+                 donof_energy_result* result);
+
 /* --- diagnostics -------------------------------------------------------------
  * Number of CUDA kernels this library has launched in the process so far.    */
 unsigned long long donof_launch_count(void);
@@ -218,6 +255,9 @@ unsigned long long donof_launch_count(void);
  * waits for and returns the duration of the most recent one.                 */
 int donof_profile_enable(donof_ctx* ctx, int enable);
 int donof_profile_last_ms(donof_ctx* ctx, float* ms);
+/* Number of GEMM shapes whose configuration the autotuner has chosen in this
+ * process (each is timed once, at its first call outside stream capture).   */
+int donof_autotune_entries(void);
 /* Reads (synchronising the context stream) the job's device error flag: 1 if
  * a mixed-precision kernel gave up on a bounded wait since the last call that
  * reset it (each mixed-precision call resets it).                            */

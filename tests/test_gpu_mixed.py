@@ -134,3 +134,31 @@ def test_mixed_rejects_bad_nbf5(cuda_ctx):
         st = bt.ctx.lib.donof_mixed_tmp_dev(bt.handle, tC.data_ptr(), bad, out.data_ptr())
         assert st == _lib.ERR_ARG
     bt.free()
+
+
+@pytest.mark.parametrize("kw", [SIZES[1], SIZES[4]], ids=ids)
+def test_cta_limit_gives_the_same_lagrangian(cuda_ctx, kw):
+    """A context limited to a few CTAs (a served job's share of the SMs) runs
+    the same arithmetic; only the order of the partial sums changes."""
+    import torch
+
+    wl = workload.synthetic(**kw, seed=23)
+    p = wl.p
+    res = {}
+    for limit in (0, 8):
+        ctx = d.Context(0)
+        ctx.set_cta_limit(limit)
+        bt = d.eris_to_gpu(wl.b, "mixed", ctx)
+        tC, tH, tn, tcj, tck = (d.to_device(x) for x in (wl.C, wl.H, wl.n, wl.cj12, wl.ck12))
+        for prec in ("fp64", "mixed"):
+            el = torch.zeros(p.nbf, p.nbf, dtype=torch.float64, device="cuda")
+            hm = torch.zeros(p.nbf5, p.nbf, dtype=torch.float64, device="cuda")
+            E = torch.zeros(1, dtype=torch.float64, device="cuda")
+            d.compute_Lagrange2_dev(tC, tn, tH, bt, tcj, tck, p.nalpha, p.nbeta, el, hm, E, precision=prec)
+            torch.cuda.synchronize()
+            res[(limit, prec)] = d.from_device(el)
+        assert error_flag(bt) == 0
+        bt.free()
+        ctx.close()
+    assert rel(res[(8, "fp64")], res[(0, "fp64")]) <= 1e-12
+    assert rel(res[(8, "mixed")], res[(0, "mixed")]) <= 1e-5  # FP32 partial sums in another order

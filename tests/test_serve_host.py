@@ -88,3 +88,10 @@ def test_server_reports_a_failing_job_and_goes_on():
         r1, r2 = s.wait(t1, 5), s.wait(t2, 5)
     assert r1.error and "boom" in r1.error
     assert r2.error is None and r2.E_elec == 1.0
+
+
+def test_cta_share_splits_the_sms_between_inflight_jobs():
+    from donof_b200.serve import cta_share
+    assert cta_share(1, 148) == 0            # one job: all SMs
+    assert cta_share(8, 148) == 37           # about two jobs per SM
+    assert cta_share(32, 148) == 16          # never fewer than 16 CTAs
