@@ -20,6 +20,9 @@ FP64) exceeds the 126 MB L2, so no flush is needed between steps.
   energies  converged GNOF energies/s of the FP64 form and of the mixed form
           with closing FP64 iterations, from the same start, on a molecule-
           shaped surrogate (nbf = 96, naux = 384), with |dE| between them
+  serving  converged energies/s of a seeded Poisson stream of jobs of different
+          sizes, served with continuous batching, against the plain FP64 form
+          serving the same stream one job at a time; p50/p99 latency; |dE|
   --impl reference   the CPU restatement of the reference path (C/OpenMP FP64
           oracle, all host threads) on the same workload
 
@@ -62,6 +65,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-energies", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--profile-case", action="store_true",
                     help="run the mixed and FP64 Lagrangian and the rotation three times each on the "
                          "benchmark workload and exit (the case the committed ncu captures use)")
@@ -253,7 +257,7 @@ def energies_bench(d, torch, ctx):
         wl = workload.molecule_like(**ENERGY_CASE, seed=5, two_e_scale=0.2)
         p = wl.p
         p.threshgorb = p.threshgocc = 1e-6
-        p.threshen = 1e-10
+        p.threshen = 1e-10  # occupations solved tightly each iteration: both forms reach the same minimum
         b = d.eris_to_gpu(wl.b, "fp64" if form == "fp64" else "mixed", ctx)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -274,6 +278,83 @@ def energies_bench(d, torch, ctx):
     out["within_1uEh"] = out["abs_dE_Eh"] <= 1e-6
     out["speedup"] = out["mixed_refined"]["value"] / out["fp64"]["value"]
     return out
+
+
+# Served stream (shapes of the reference's serving workload: water clusters
+# (H2O)_k and linear alkanes CnH2n+2 in cc-pVDZ with a JK-fit set, as molecule-
+# shaped surrogates): (nbf, naux, nbeta, ncwo).
+SERVE_SHAPES = [(24 * k, 116 * k, 5 * k, 3) for k in (1, 2, 3, 4)] + \
+               [(24 * n + 10, int(4.8 * (24 * n + 10)), 4 * n + 1, 5) for n in (1, 2, 3)]
+SERVE_LARGE = (202, 974, 33, 5)   # n-octane shape
+SERVE = dict(jobs=24, large=2, rate_per_s=20.0, seed=7, thresh=1e-5, threshen=1e-6, inflight=8)  # threshen = thresh / 10
+
+
+def serving_bench(d, torch):
+    """Converged energies/s of a seeded Poisson stream of jobs of different
+    sizes: served with continuous batching (auto precision: the mixed form with
+    closing FP64 iterations where it pays off), and by the plain FP64 form
+    serving the same stream one job at a time; per-job |dE| between the two."""
+    import copy
+    from donof_b200 import workload
+    from donof_b200.serve import Request, Server, resolve_precision
+    rng = np.random.default_rng(SERVE["seed"])
+    shapes = [SERVE_SHAPES[i] for i in rng.integers(len(SERVE_SHAPES), size=SERVE["jobs"])]
+    for pos in rng.choice(len(shapes) + SERVE["large"], size=SERVE["large"], replace=False):
+        shapes.insert(int(pos), SERVE_LARGE)
+    gaps = rng.exponential(1.0 / SERVE["rate_per_s"], size=len(shapes))
+    arrivals = np.cumsum(gaps) - gaps[0]
+    jobs = []
+    for j, (nbf, naux, nbeta, ncwo) in enumerate(shapes):
+        wl = workload.molecule_like(nbf=nbf, naux=naux, nbeta=nbeta, ncwo=ncwo, seed=100 + j, two_e_scale=0.2)
+        wl.p.threshgorb = wl.p.threshgocc = SERVE["thresh"]
+        wl.p.threshen = SERVE["threshen"]
+        jobs.append(wl)
+
+    # tune every shape's GEMMs and load the kernels before either arm is timed
+    ctx = d.Context(0)
+    for shp in sorted(set(shapes)):
+        wl = jobs[shapes.index(shp)]
+        p = wl.p
+        prec = resolve_precision("auto", p.nbf, p.nbf5, p.nbfaux)
+        b = d.eris_to_gpu(wl.b, "fp64" if prec == "fp64" else "mixed", ctx)
+        for form in (("fp64",) if prec == "fp64" else ("fp64", "mixed")):
+            b.set_precision(form)
+            d.compute_Lagrange2(wl.C, wl.n, wl.H, b, wl.cj12, wl.ck12, p.nalpha, p.nbeta)
+            d.JKH_MO(wl.C, wl.H, b, p.nbf, p.nbf5, p.nbfaux)
+        b.free()
+    ctx.close()
+
+    def run(precision, inflight):
+        with Server(max_inflight=inflight) as srv:
+            t0 = time.perf_counter()
+            tickets = []
+            for wl, t_arr in zip(jobs, arrivals):
+                delay = t0 + t_arr - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+                tickets.append(srv.submit(Request(H=wl.H, b=wl.b, C=wl.C, p=copy.deepcopy(wl.p), gamma=wl.gamma,
+                                                  precision=precision, maxit=1000)))
+            res = [srv.wait(t) for t in tickets]
+            span = max(r.t_done for r in res) - t0
+        lat = np.array([r.latency for r in res])
+        return res, {"value": len(res) / span, "seconds": span, "converged": int(sum(r.converged for r in res)),
+                     "errors": [r.error for r in res if r.error][:2],
+                     "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))}}
+
+    ref, seq = run("fp64", 1)
+    res, served = run("auto", SERVE["inflight"])
+    dE = np.array([abs(a.E_elec - b.E_elec) for a, b in zip(res, ref)])
+    return {"unit": "energies/s",
+            "workload": f"{len(jobs)} jobs, Poisson arrivals at {SERVE['rate_per_s']:g}/s (seed {SERVE['seed']}): "
+                        "molecule-shaped surrogates of (H2O)_k k=1..4, CnH2n+2 n=1..3 and "
+                        f"{SERVE['large']} n-octane-sized jobs (nbf 24-202); max|g_orb|, |g_occ| < "
+                        f"{SERVE['thresh']:g}",
+            "served": {**served, "precision": "auto (mixed + closing FP64 for nbf*nbf5*naux >= 2e7, else FP64)",
+                       "max_inflight": SERVE["inflight"]},
+            "fp64_one_at_a_time": seq,
+            "speedup": served["value"] / seq["value"],
+            "abs_dE_Eh": {"max": float(dE.max()), "median": float(np.median(dE)),
+                          "within_1uEh": int(np.sum(dE <= 1e-6)), "of": len(dE)}}
 
 
 def profile_case(d, torch, wl, ctx):
@@ -331,7 +412,8 @@ def main():
     if args.profile_case:
         profile_case(d, torch, wl, ctx)
         return
-    bt = d.eris_to_gpu(wl.b, args.precision, ctx)
+    bt = d.eris_to_gpu(wl.b, "mixed", ctx)   # FP64 b and its bf16 split: both forms are timed
+    bt.set_precision(args.precision)
     tC0, tH, tn, tcj, tck = (d.to_device(x, dev) for x in (wl.C, wl.H, wl.n, wl.cj12, wl.ck12))
 
     def barrier():
@@ -363,6 +445,27 @@ def main():
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         t = float(tt.item())
     value = world * args.steps / t
+
+    # ---- the other form's device loop on the same workload (same step count)
+    other = "mixed" if args.precision == "fp64" else "fp64"
+    bt.set_precision(other)
+    tC.copy_(tC0)
+    d.orbopt_dev(args.method, tn, tcj, tck, tH, tC, bt, p, 0.01, args.warmup, 0.0)
+    tC.copy_(tC0)
+    torch.cuda.synchronize()
+    barrier()
+    ev0.record()
+    _, nit2, _, _, _ = d.orbopt_dev(args.method, tn, tcj, tck, tH, tC, bt, p, 0.01, args.steps, 0.0)
+    ev1.record()
+    torch.cuda.synchronize()
+    t2 = ev0.elapsed_time(ev1) / 1e3
+    if dist is not None:
+        tt = torch.tensor([t2], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t2 = float(tt.item())
+    other_form = {"precision": other, "value": world * nit2 / t2, "unit": UNIT, "ms_per_step": 1e3 * t2 / nit2}
+    bt.set_precision(args.precision)
+    tC.copy_(tC0)
 
     # ---- roofline of the dominant kernel, timed by the library's events on the launching stream
     nbf, naux, nbf5 = p.nbf, p.nbfaux, p.nbf5
@@ -443,6 +546,9 @@ def main():
     energies = None
     if rank == 0 and world == 1 and not args.no_energies:
         energies = energies_bench(d, torch, ctx)
+    serving = None
+    if rank == 0 and world == 1 and not args.no_serving:
+        serving = serving_bench(d, torch)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -456,9 +562,12 @@ def main():
                 "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64" if args.precision == "fp64" else "bf16x2-split+f64", "data": "synthetic",
                 "config": config(args, world), "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
-                "gpu_launches": int(launches), "clocks": clk.summary(), "final_E": E}
+                "gpu_launches": int(launches), "clocks": clk.summary(), "final_E": E,
+                "other_form": other_form}
         if energies is not None:
             line["energies"] = energies
+        if serving is not None:
+            line["serving"] = serving
         print(json.dumps(line), flush=True)
     bt.free()
     ctx.close()

@@ -274,6 +274,7 @@ extern "C" int donof_energy(donof_job* job, donof_energy_params* prm, const doub
             converged = 1;
             break;
         }
+        if (prm->stop_rel_de > 0.0 && it > 1 && fabs(E_diff) <= prm->stop_rel_de * fabs(E)) break;
     }
     if (it > prm->maxit) it = prm->maxit;
     // ---- ENERGY1r of the last iteration: elag at (C, occupations before the ordering)

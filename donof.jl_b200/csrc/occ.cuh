@@ -14,6 +14,8 @@ struct Occ {
     int N, no1, ndoc, nsoc, nbeta, nalpha, ncwo, nv, ista, high_spin, method;
     double h_cut;
     std::vector<int> S, P, G;  // strong (ndoc); weak P[g*ncwo + w]; gamma index G[g*ncwo + w]
+    std::vector<int> KG;       // the ncwo gamma entries of pair g: KG[g*ncwo + c] (dn is zero elsewhere)
+    std::vector<int> grp;      // pair of each orbital (-1 outside the pairs)
 };
 
 // false on inconsistent sizes or switches

@@ -51,12 +51,20 @@ bool setup(const donof_occ_params* q, Occ& o) {
     o.S.resize(o.ndoc);
     o.P.resize((size_t)o.ndoc * o.ncwo);
     o.G.resize((size_t)o.ndoc * o.ncwo);
+    o.KG.resize((size_t)o.ndoc * o.ncwo);
+    o.grp.assign(o.N, -1);
     for (int g = 0; g < o.ndoc; ++g) {
         o.S[g] = o.no1 + g;
+        o.grp[o.S[g]] = g;
         for (int w = 0; w < o.ncwo; ++w) {
             // Julia's ll:ndoc:ul for strong orbital g+1 (src/param.jl, pnof.jl)
             o.P[g * o.ncwo + w] = o.no1 + ndns + (o.ndoc - (g + 1)) + o.ndoc * w;
             o.G[g * o.ncwo + w] = (o.ndoc - (g + 1)) + o.ndoc * w;
+            o.grp[o.P[g * o.ncwo + w]] = g;
+            // columns of dn in the pair's rows: softmax, its gamma entries; trigonometric,
+            // the strong angle g and the ncwo - 1 weak angles of the pair
+            o.KG[g * o.ncwo + w] = (o.method == 0) ? o.G[g * o.ncwo + w]
+                                   : (w == 0 ? g : o.ndoc + (o.ndoc - (g + 1)) + o.ndoc * (w - 1));
         }
     }
     return true;
@@ -226,151 +234,265 @@ void coupling(const Occ& o, const double* n, double* cj, double* ck) {
     for (int i = 0; i < N; ++i) cj[i * N + i] = ck[i * N + i] = 0.0;
 }
 
-// Separable terms of der_CJCKD8: Dcj[i,j,:] = Mcj[i,j] dn[i,:],
-// Dck[i,j,:] = sum_t M[t][i,j] A[t][i,:], A = (dn, dfi, dnd12, dnd).
-void derivative_factors(const Occ& o, const double* n, const double* dn, std::vector<double>& dfi,
-                        std::vector<double>& dnd12, std::vector<double>& dnd, std::vector<double>& Mcj,
-                        std::vector<double> (&M)[4]) {
-    const int N = o.N, nv = o.nv;
-    std::vector<double> nd, F, coc;
-    dynamic(o, n, nd, F, coc);
-    dnd.assign((size_t)N * nv, 0.0);
-    for (int g = 0; g < o.ndoc; ++g) {
-        const int s = o.S[g];
-        const double k = 2.0 * coc[g] / o.h_cut;
-        for (int c = 0; c < nv; ++c) dnd[(size_t)s * nv + c] = F[g] * dn[(size_t)s * nv + c] * (1.0 + n[s] * k);
-        for (int a = 0; a < o.ncwo; ++a) {
-            const int w = o.P[g * o.ncwo + a];
-            for (int c = 0; c < nv; ++c)
-                dnd[(size_t)w * nv + c] = F[g] * dn[(size_t)w * nv + c] + F[g] * k * n[w] * dn[(size_t)s * nv + c];
-        }
-    }
-    std::vector<double> nd12(N), fi(N);
-    dnd12.assign((size_t)N * nv, 0.0);
+// ---------------------------------------------------------------- energy, gradient
+// The couplings of CJCKD8 (coupling() above) and the factors of their
+// derivatives (der_CJCKD8, src/pnof.jl:603-793) are, away from the pairs, a
+// function of the index classes of the two orbitals -- [0, no1), beta-occupied
+// [no1, nbeta), alpha-only [nbeta, nalpha), weak [nalpha, nbf5) -- and of four
+// per-orbital vectors (n, phi(n), n_d^{1/2}, n_d); inside a pair (a strong
+// orbital and its weak partners) they take special values.  Every double sum
+// over (i, j) therefore reduces to, per orbital i, a few dot products of
+// column i of J_MO / K_MO with those vectors over the class ranges (RowSums),
+// plus corrections for the 1 + ncwo members of i's pair.  The gradient
+// contracts the separable terms
+//   Dcj[i,j,:] = Mcj[i,j] dn[i,:],   Dck[i,j,:] = sum_t M_t[i,j] A_t[i,:],
+//   A = (dn, dphi, dn_d^{1/2}, dn_d),
+// whose rows A_t[i,:] are nonzero only on the ncwo gamma entries of i's pair.
+
+enum : int { V_N = 0, V_FI, V_ND12, V_ND, V_ONE, NVEC };
+
+inline int cls(const Occ& o, int i) { return i < o.no1 ? 0 : (i < o.nbeta ? 1 : (i < o.nalpha ? 2 : 3)); }
+
+struct OrbVecs {
+    std::vector<double> n, fi, nd12, nd, F, coc;  // per orbital; F, coc per pair (dynamic())
+};
+
+// S[R][k] = sum over j in class range R of vec_k[j] K(j, i); jn = sum_j n_j J(j, i)
+struct RowSums {
+    double S[4][NVEC];
+    double jn;
+};
+
+void row_sums(const Occ& o, const OrbVecs& v, const double* J, const double* K, std::vector<RowSums>& rs) {
+    const int N = o.N;
+    const int bnd[5] = {0, o.no1, o.nbeta, o.nalpha, N};
+    const double *vn = v.n.data(), *vf = v.fi.data(), *v12 = v.nd12.data(), *vd = v.nd.data();
+    rs.resize(N);
     for (int i = 0; i < N; ++i) {
-        nd12[i] = sqrt(nd[i]);
-        const double den = std::max(nd12[i], 1e-15);
-        for (int c = 0; c < nv; ++c) dnd12[(size_t)i * nv + c] = 0.5 * dnd[(size_t)i * nv + c] / den;
-    }
-    dfi.assign((size_t)N * nv, 0.0);
-    for (int i = 0; i < N; ++i) {
-        double f = n[i] * (1.0 - n[i]);
-        if (f < 0.0) f = 0.0;
-        fi[i] = phi_fn(n[i], o.ista);
-        if (i < o.no1) continue;
-        double fac;
-        if (o.ista == 3) {
-            const double al = 0.55, aa = pow(pow(2.0, 2.0 * al - 1.0), 1.0 / al);
-            const double a = std::max(aa * n[i] * (1.0 - n[i]), 1e-15);
-            fac = al * pow(a, al - 1.0) * aa * (1.0 - 2.0 * n[i]);
-        } else {
-            const double fi0 = sqrt(f) * (o.ista == 2 ? 0.9 : 1.0);
-            const double a = std::max(fi0, 1e-15);
-            const double scale = (o.ista == 2) ? 0.81 : 1.0;
-            fac = scale / (2.0 * a) * (1.0 - 2.0 * n[i]);
-            if (o.ista == 4) {
-                const double e = exp(-(n[i] - 0.5) * (n[i] - 0.5));
-                fac = fac * e - fi0 * 2.0 * (n[i] - 0.5) * e;
+        const double* Kc = K + (size_t)N * i;
+        const double* Jc = J + (size_t)N * i;
+        RowSums& r = rs[i];
+        for (int R = 0; R < 4; ++R) {
+            double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0, a4 = 0.0;
+            for (int j = bnd[R]; j < bnd[R + 1]; ++j) {
+                const double kj = Kc[j];
+                a0 += vn[j] * kj;
+                a1 += vf[j] * kj;
+                a2 += v12[j] * kj;
+                a3 += vd[j] * kj;
+                a4 += kj;
             }
+            r.S[R][V_N] = a0; r.S[R][V_FI] = a1; r.S[R][V_ND12] = a2; r.S[R][V_ND] = a3; r.S[R][V_ONE] = a4;
         }
-        for (int c = 0; c < nv; ++c) dfi[(size_t)i * nv + c] = fac * dn[(size_t)i * nv + c];
+        double jn = 0.0;
+        for (int j = 0; j < N; ++j) jn += vn[j] * Jc[j];
+        r.jn = jn;
     }
-    const int b0 = o.no1, b1 = o.nbeta, a1 = o.nalpha, c1 = N;
-    Mcj.assign((size_t)N * N, 0.0);
-    for (auto& m : M) m.assign((size_t)N * N, 0.0);
-    for (int i = 0; i < N; ++i)
-        for (int j = 0; j < N; ++j) {
-            const bool ibe = in(i, b0, b1), ial = in(i, b1, a1), icw = in(i, a1, c1);
-            const bool jbe = in(j, b0, b1), jal = in(j, b1, a1), jcw = in(j, a1, c1);
-            const size_t ij = (size_t)i * N + j;
-            Mcj[ij] = 2.0 * n[j];
-            M[0][ij] = n[j];
-            if (o.ista == 0) {
-                if ((ibe && jcw) || (icw && jbe) || (icw && jcw)) M[1][ij] += fi[j];
-                if (o.nsoc > 0) {
-                    if (ibe && jal) M[1][ij] += 0.25;
-                    if (icw && jal) M[1][ij] += 0.5;
-                }
-            } else {
-                M[1][ij] += fi[j];
-            }
-            if (o.nsoc > 1 && ial && jal)
-                for (auto& m : M) m[ij] = 0.0;
-            if ((ibe && jcw) || (icw && jbe)) {
-                M[2][ij] += nd12[j];
-                M[3][ij] -= nd[j];
-            }
-            if (icw && jcw) {
-                M[2][ij] -= nd12[j];
-                M[3][ij] -= nd[j];
-            }
+}
+
+// generic ck(i, j) of coupling(), before the pair overrides
+inline double gen_ck(const Occ& o, const OrbVecs& v, int i, int j) {
+    const int ci = cls(o, i), cj = cls(o, j);
+    const bool ibe = ci == 1, ial = ci == 2, icw = ci == 3, jbe = cj == 1, jal = cj == 2, jcw = cj == 3;
+    double k = v.n[i] * v.n[j];
+    if (o.ista == 0) {
+        if ((ibe && jcw) || (icw && jbe) || (icw && jcw)) k += v.fi[i] * v.fi[j];
+        if (o.nsoc > 0) {
+            if (ibe && jal) k += 0.25 * v.fi[i];
+            if (ial && jbe) k += 0.25 * v.fi[j];
+            if (ial && jcw) k += 0.5 * v.fi[j];
+            if (icw && jal) k += 0.5 * v.fi[i];
         }
-    for (int g = 0; g < o.ndoc; ++g) {
-        const int s = o.S[g];
-        const double sa = sqrt(std::max(n[s], 1e-15));
-        for (int a = 0; a < o.ncwo; ++a) {
-            const int w = o.P[g * o.ncwo + a];
-            const double sb = sqrt(std::max(n[w], 1e-15));
-            Mcj[(size_t)s * N + w] = Mcj[(size_t)w * N + s] = 0.0;
-            for (auto& m : M) m[(size_t)s * N + w] = m[(size_t)w * N + s] = 0.0;
-            M[0][(size_t)s * N + w] = 0.5 / sa * sqrt(n[w]);
-            M[0][(size_t)w * N + s] = 0.5 / sb * sqrt(n[s]);
-            for (int b = 0; b < o.ncwo; ++b) {
-                const int v = o.P[g * o.ncwo + b];
-                Mcj[(size_t)w * N + v] = 0.0;
-                for (auto& m : M) m[(size_t)w * N + v] = 0.0;
-                M[0][(size_t)w * N + v] = -0.5 * (1.0 / sb) * sqrt(n[v]);
-            }
+        if (o.nsoc > 1 && ial && jal) k = 0.5;
+    } else {
+        k += v.fi[i] * v.fi[j];
+    }
+    if ((ibe && jcw) || (icw && jbe)) k += v.nd12[i] * v.nd12[j] - v.nd[i] * v.nd[j];
+    if (icw && jcw) k -= v.nd12[i] * v.nd12[j] + v.nd[i] * v.nd[j];
+    return k;
+}
+
+// sum_j gen_ck(i, j) K(j, i) from the row sums
+inline double row_ck(const Occ& o, const OrbVecs& v, int i, const RowSums& r) {
+    const int ci = cls(o, i);
+    const double ni = v.n[i], fi = v.fi[i];
+    double s = ni * (r.S[0][V_N] + r.S[1][V_N] + r.S[2][V_N] + r.S[3][V_N]);
+    if (o.ista == 0) {
+        if (ci == 1) s += fi * r.S[3][V_FI];
+        if (ci == 3) s += fi * (r.S[1][V_FI] + r.S[3][V_FI]);
+        if (o.nsoc > 0) {
+            if (ci == 1) s += 0.25 * fi * r.S[2][V_ONE];
+            if (ci == 2) s += 0.25 * r.S[1][V_FI] + 0.5 * r.S[3][V_FI];
+            if (ci == 3) s += 0.5 * fi * r.S[2][V_ONE];
         }
+        if (o.nsoc > 1 && ci == 2) s += 0.5 * r.S[2][V_ONE] - ni * r.S[2][V_N];
+    } else {
+        s += fi * (r.S[0][V_FI] + r.S[1][V_FI] + r.S[2][V_FI] + r.S[3][V_FI]);
     }
-    for (int i = 0; i < N; ++i) {
-        Mcj[(size_t)i * N + i] = 0.0;
-        for (auto& m : M) m[(size_t)i * N + i] = 0.0;
+    if (ci == 1) s += v.nd12[i] * r.S[3][V_ND12] - v.nd[i] * r.S[3][V_ND];
+    if (ci == 3)
+        s += v.nd12[i] * (r.S[1][V_ND12] - r.S[3][V_ND12]) - v.nd[i] * (r.S[1][V_ND] + r.S[3][V_ND]);
+    return s;
+}
+
+// ck(i, j) inside a pair, i != j (coupling(): strong-weak sqrt(n_s n_w), weak-weak -sqrt(n_w) sqrt(n_v))
+inline double spec_ck(const Occ& o, const OrbVecs& v, int i, int j) {
+    const int g = o.grp[i];
+    if (i == o.S[g]) return sqrt(v.n[i] * v.n[j]);
+    if (j == o.S[g]) return sqrt(v.n[j] * v.n[i]);
+    return -(sqrt(v.n[i]) * sqrt(v.n[j]));
+}
+
+// generic derivative factors M_t(r, j) (t = 0..3) and Mcj(r, j) for a row r in a pair
+inline void gen_m(const Occ& o, const OrbVecs& v, int r, int j, double (&m)[4], double& mcj) {
+    const int cr = cls(o, r), cj = cls(o, j);
+    const bool rbe = cr == 1, rcw = cr == 3, jbe = cj == 1, jal = cj == 2, jcw = cj == 3;
+    mcj = 2.0 * v.n[j];
+    m[0] = v.n[j];
+    m[1] = m[2] = m[3] = 0.0;
+    if (o.ista == 0) {
+        if ((rbe && jcw) || (rcw && jbe) || (rcw && jcw)) m[1] += v.fi[j];
+        if (o.nsoc > 0) {
+            if (rbe && jal) m[1] += 0.25;
+            if (rcw && jal) m[1] += 0.5;
+        }
+    } else {
+        m[1] += v.fi[j];
     }
+    if ((rbe && jcw) || (rcw && jbe)) {
+        m[2] += v.nd12[j];
+        m[3] -= v.nd[j];
+    }
+    if (rcw && jcw) {
+        m[2] -= v.nd12[j];
+        m[3] -= v.nd[j];
+    }
+}
+
+// sum_j M_t(r, j) K(j, r) for the generic factors of a row r in a pair
+inline void row_m(const Occ& o, int r, const RowSums& s, double (&vk)[4]) {
+    const int cr = cls(o, r);
+    vk[0] = s.S[0][V_N] + s.S[1][V_N] + s.S[2][V_N] + s.S[3][V_N];
+    if (o.ista == 0) {
+        vk[1] = (cr == 1) ? s.S[3][V_FI] : s.S[1][V_FI] + s.S[3][V_FI];
+        if (o.nsoc > 0) vk[1] += (cr == 1 ? 0.25 : 0.5) * s.S[2][V_ONE];
+    } else {
+        vk[1] = s.S[0][V_FI] + s.S[1][V_FI] + s.S[2][V_FI] + s.S[3][V_FI];
+    }
+    if (cr == 1) {
+        vk[2] = s.S[3][V_ND12];
+        vk[3] = -s.S[3][V_ND];
+    } else {
+        vk[2] = s.S[1][V_ND12] - s.S[3][V_ND12];
+        vk[3] = -s.S[1][V_ND] - s.S[3][V_ND];
+    }
+}
+
+// d phi / d n_i (the factor of dfi = dphi * dn, der_CJCKD8)
+double dphi_factor(const Occ& o, double ni) {
+    double f = ni * (1.0 - ni);
+    if (f < 0.0) f = 0.0;
+    if (o.ista == 3) {
+        const double al = 0.55, aa = pow(pow(2.0, 2.0 * al - 1.0), 1.0 / al);
+        const double a = std::max(aa * ni * (1.0 - ni), 1e-15);
+        return al * pow(a, al - 1.0) * aa * (1.0 - 2.0 * ni);
+    }
+    const double fi0 = sqrt(f) * (o.ista == 2 ? 0.9 : 1.0);
+    const double a = std::max(fi0, 1e-15);
+    const double scale = (o.ista == 2) ? 0.81 : 1.0;
+    double fac = scale / (2.0 * a) * (1.0 - 2.0 * ni);
+    if (o.ista == 4) {
+        const double e = exp(-(ni - 0.5) * (ni - 0.5));
+        fac = fac * e - fi0 * 2.0 * (ni - 0.5) * e;
+    }
+    return fac;
 }
 
 // Occupation energy (calce, src/pnof.jl:1273-1300) and, when grad != nullptr,
 // its gamma-gradient (calcoccg, :1324-1377).
 double energy_grad(const Occ& o, const double* gamma, const double* J, const double* K, const double* Hc,
                    double* grad) {
-    const int N = o.N, nv = o.nv;
-    std::vector<double> n(N), dn((size_t)N * nv), cj((size_t)N * N), ck((size_t)N * N);
-    occupations(o, gamma, n.data(), dn.data());
-    coupling(o, n.data(), cj.data(), ck.data());
+    const int N = o.N, nv = o.nv, nc = o.ncwo;
+    thread_local OrbVecs v;
+    thread_local std::vector<double> dn, w;
+    thread_local std::vector<RowSums> rs;
+    v.n.resize(N);
+    dn.resize((size_t)N * (nv > 0 ? nv : 1));
+    occupations(o, gamma, v.n.data(), dn.data());
+    dynamic(o, v.n.data(), v.nd, v.F, v.coc);
+    v.fi.resize(N);
+    v.nd12.resize(N);
+    for (int i = 0; i < N; ++i) {
+        v.fi[i] = phi_fn(v.n[i], o.ista);
+        v.nd12[i] = sqrt(v.nd[i]);
+    }
     auto Jm = [&](int i, int j) { return J[i + (size_t)N * j]; };
     auto Km = [&](int i, int j) { return K[i + (size_t)N * j]; };
-    std::vector<double> w(N);
+    w.resize(N);
     for (int i = 0; i < N; ++i) w[i] = 2.0 * Hc[i] + Jm(i, i);
     double E = 0.0;
-    for (int i = 0; i < o.nbeta; ++i) E += n[i] * w[i];
+    for (int i = 0; i < o.nbeta; ++i) E += v.n[i] * w[i];
     if (o.nsoc > 0)
-        for (int i = o.nbeta; i < o.nalpha; ++i) E += 2.0 * n[i] * Hc[i];
-    for (int i = o.nalpha; i < N; ++i) E += n[i] * w[i];
+        for (int i = o.nbeta; i < o.nalpha; ++i) E += 2.0 * v.n[i] * Hc[i];
+    for (int i = o.nalpha; i < N; ++i) E += v.n[i] * w[i];
+    row_sums(o, v, J, K, rs);
+    // sum_ij cj12[i,j] J(j,i) - ck12[i,j] K(j,i): generic rows, minus the generic
+    // values on i's pair (or on the diagonal), plus the pair's special values
     double sj = 0.0, sk = 0.0;
-    for (int i = 0; i < N; ++i)
-        for (int j = 0; j < N; ++j) {
-            sj += cj[(size_t)i * N + j] * Jm(j, i);
-            sk += ck[(size_t)i * N + j] * Km(j, i);
+    for (int i = 0; i < N; ++i) {
+        double rj = 2.0 * v.n[i] * rs[i].jn, rk = row_ck(o, v, i, rs[i]);
+        const int g = o.grp[i];
+        auto corr = [&](int j) {
+            rj -= 2.0 * v.n[i] * v.n[j] * Jm(j, i);
+            rk -= gen_ck(o, v, i, j) * Km(j, i);
+            if (j != i) rk += spec_ck(o, v, i, j) * Km(j, i);
+        };
+        if (g < 0) {
+            corr(i);
+        } else {
+            corr(o.S[g]);
+            for (int a = 0; a < nc; ++a) corr(o.P[g * nc + a]);
         }
+        sj += rj;
+        sk += rk;
+    }
     E += sj - sk;
     if (grad) {
-        std::vector<double> dfi, dnd12, dnd, Mcj;
-        std::vector<double> M[4];
-        derivative_factors(o, n.data(), dn.data(), dfi, dnd12, dnd, Mcj, M);
-        const double* A[4] = {dn.data(), dfi.data(), dnd12.data(), dnd.data()};
         for (int k = 0; k < nv; ++k) grad[k] = 0.0;
-        auto row = [&](int r) { return (r >= o.no1 && r < o.nbeta) || (r >= o.nalpha && r < N); };
-        for (int r = 0; r < N; ++r) {
-            if (!row(r)) continue;
-            double vj = 0.0, vk[4] = {0.0, 0.0, 0.0, 0.0};
-            for (int j = 0; j < N; ++j) {
-                vj += Mcj[(size_t)r * N + j] * Jm(j, r);
-                for (int t = 0; t < 4; ++t) vk[t] += M[t][(size_t)r * N + j] * Km(j, r);
-            }
-            for (int k = 0; k < nv; ++k) {
-                double g = dn[(size_t)r * nv + k] * w[r] + 2.0 * dn[(size_t)r * nv + k] * vj;
-                for (int t = 0; t < 4; ++t) g -= 2.0 * A[t][(size_t)r * nv + k] * vk[t];
-                grad[k] += g;
+        for (int g = 0; g < o.ndoc; ++g) {
+            const int s = o.S[g];
+            const double kk = 2.0 * v.coc[g] / o.h_cut;
+            const double sa = sqrt(std::max(v.n[s], 1e-15));
+            for (int m = 0; m <= nc; ++m) {
+                const int r = (m == 0) ? s : o.P[g * nc + m - 1];
+                // vj = sum_j Mcj(r,j) J(j,r), vk_t = sum_j M_t(r,j) K(j,r)
+                double vj = 2.0 * rs[r].jn, vk[4];
+                row_m(o, r, rs[r], vk);
+                const double sb = sqrt(std::max(v.n[r], 1e-15));
+                for (int q = 0; q <= nc; ++q) {  // the pair's members: generic values out, special in
+                    const int j = (q == 0) ? s : o.P[g * nc + q - 1];
+                    double mg[4], mcj;
+                    gen_m(o, v, r, j, mg, mcj);
+                    vj -= mcj * Jm(j, r);
+                    for (int t = 0; t < 4; ++t) vk[t] -= mg[t] * Km(j, r);
+                    if (j == r) continue;
+                    double m0;
+                    if (r == s) m0 = 0.5 / sa * sqrt(v.n[j]);
+                    else if (j == s) m0 = 0.5 / sb * sqrt(v.n[s]);
+                    else m0 = -0.5 * (1.0 / sb) * sqrt(v.n[j]);
+                    vk[0] += m0 * Km(j, r);
+                }
+                const double cdn = w[r] + 2.0 * vj;
+                const double fac = dphi_factor(o, v.n[r]);
+                const double den = std::max(v.nd12[r], 1e-15);
+                for (int c = 0; c < nc; ++c) {
+                    const int k = o.KG[g * nc + c];
+                    const double a0 = dn[(size_t)r * nv + k];
+                    const double a3 = (r == s) ? v.F[g] * a0 * (1.0 + v.n[s] * kk)
+                                               : v.F[g] * a0 + v.F[g] * kk * v.n[r] * dn[(size_t)s * nv + k];
+                    const double a1 = fac * a0, a2 = 0.5 * a3 / den;
+                    grad[k] += a0 * cdn - 2.0 * (a0 * vk[0] + a1 * vk[1] + a2 * vk[2] + a3 * vk[3]);
+                }
             }
         }
     }

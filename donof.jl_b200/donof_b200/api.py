@@ -367,7 +367,8 @@ def occ_energy(gamma, J_MO, K_MO, H_core, p: Param, grad: bool = True):
 class _EnergyParams(ct.Structure):
     _fields_ = [("occ", _OccParams), ("orb_method", ct.c_int), ("maxit", ct.c_int), ("maxloop", ct.c_int),
                 ("alpha", ct.c_double), ("threshgorb", ct.c_double), ("threshgocc", ct.c_double),
-                ("threshen", ct.c_double), ("order_subspaces", ct.c_int), ("freeze_occ", ct.c_int)]
+                ("threshen", ct.c_double), ("order_subspaces", ct.c_int), ("freeze_occ", ct.c_int),
+                ("stop_rel_de", ct.c_double)]
 
 
 class _EnergyResult(ct.Structure):
@@ -377,7 +378,7 @@ class _EnergyResult(ct.Structure):
 
 
 def energy_loop(H, b: BTensor, p: Param, C, gamma, maxit: Optional[int] = None, freeze_occ: bool = False,
-                order: bool = True):
+                order: bool = True, stop_rel_de: float = 0.0):
     """DoNOF.energy's orbital / occupation alternation in one native call
     (donof_energy), in the precision b is set to.  Updates p.alpha and
     p.maxloop like the reference.  Returns (C, gamma, n, elag, result fields,
@@ -385,7 +386,7 @@ def energy_loop(H, b: BTensor, p: Param, C, gamma, maxit: Optional[int] = None, 
     maxit = int(maxit or p.maxit)
     prm = _EnergyParams(_occ_params(p), _lib.ORB_METHODS[p.orb_method], maxit, int(p.maxloop), float(p.alpha),
                         float(p.threshgorb), float(p.threshgocc), float(p.threshen),
-                        int(bool(order) and p.ipnof > 4), int(bool(freeze_occ)))
+                        int(bool(order) and p.ipnof > 4), int(bool(freeze_occ)), float(stop_rel_de))
     Cio = np.array(_f64(C), copy=True, order="F")
     g = np.array(gamma, dtype=np.float64, copy=True)
     n = np.zeros(p.nbf5)

@@ -216,7 +216,7 @@ class EnergyResult:
 
 def energy(H, b: api.BTensor, p: Param, C, gamma=None, E_nuc: float = 0.0, freeze_occ: bool = False,
            maxit: Optional[int] = None, log: Optional[Callable[[dict], None]] = None,
-           order: bool = True, native: bool = True) -> EnergyResult:
+           order: bool = True, native: bool = True, stop_rel_de: float = 0.0) -> EnergyResult:
     """The orbital / occupation alternation of DoNOF.energy (src/energy.jl:140-224)
     for given core Hamiltonian H, device RI tensor b and starting orbitals C
     (the integral and guess set-up of energy.jl:29-105 is outside this path).
@@ -230,7 +230,7 @@ def energy(H, b: api.BTensor, p: Param, C, gamma=None, E_nuc: float = 0.0, freez
     gamma = gnof.guess_gamma(p) if gamma is None else np.array(gamma, dtype=np.float64)
     if native:
         C, gamma, n, elag, r, hist = api.energy_loop(H, b, p, C, gamma, maxit=maxit, freeze_occ=freeze_occ,
-                                                     order=order)
+                                                     order=order, stop_rel_de=stop_rel_de)
         rows = [dict(it=i + 1, nit_orb=int(h[4]), nit_occ=int(h[5]), E=h[0], E_tot=h[0] + E_nuc, E_diff=h[1],
                      max_grad_orb=h[2], norm_grad_occ=h[3]) for i, h in enumerate(hist)]
         if log:
@@ -278,19 +278,22 @@ def energy(H, b: api.BTensor, p: Param, C, gamma=None, E_nuc: float = 0.0, freez
 
 def energy_mixed_refined(H, b: api.BTensor, p: Param, C, gamma=None, E_nuc: float = 0.0,
                          maxit: Optional[int] = None, log: Optional[Callable[[dict], None]] = None,
-                         mixed_factor: float = 10.0, native: bool = True):
+                         mixed_factor: float = 10.0, native: bool = True, mixed_noise: float = 1e-6):
     """The mixed-precision form until its gradients are below mixed_factor times
-    the thresholds (the bf16-split gradients carry ~1e-5 relative rounding, so
-    driving them to the FP64 thresholds only adds iterations), then closing FP64
-    iterations from its orbitals and occupations until the FP64 gradients meet
-    p's thresholds.  Returns (refined result, mixed-phase result); b must have
-    been uploaded with precision "mixed" and is left in FP64 mode."""
+    the thresholds, or until an outer iteration changes E by no more than
+    mixed_noise |E| (the bf16-split energies and gradients carry ~1e-5 relative
+    rounding; past that point they would steer the optimiser by their rounding),
+    then closing FP64 iterations from its orbitals and occupations until the
+    FP64 gradients meet p's thresholds.  Returns (refined result, mixed-phase
+    result); b must have been uploaded with precision "mixed" and is left in
+    FP64 mode.  The early stop needs the native loop (native=True)."""
     import copy
     pm = copy.copy(p)
     pm.threshgorb = p.threshgorb * mixed_factor
     pm.threshgocc = p.threshgocc * mixed_factor
     b.set_precision("mixed")
-    r_mixed = energy(H, b, pm, C, gamma, E_nuc=E_nuc, maxit=maxit, log=log, order=False, native=native)
+    r_mixed = energy(H, b, pm, C, gamma, E_nuc=E_nuc, maxit=maxit, log=log, order=False, native=native,
+                     stop_rel_de=mixed_noise if native else 0.0)
     p.maxloop = pm.maxloop
     b.set_precision("fp64")
     r = energy(H, b, p, r_mixed.C, r_mixed.gamma, E_nuc=E_nuc, maxit=maxit, log=log, native=native)

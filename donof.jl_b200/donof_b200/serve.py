@@ -32,7 +32,20 @@ import numpy as np
 
 from .param import Param
 
-PRECISIONS = ("fp64", "mixed", "mixed_refined")
+PRECISIONS = ("fp64", "mixed", "mixed_refined", "auto")
+
+# "auto": the mixed form with closing FP64 iterations where its bulk contractions
+# pay off, the FP64 form for small jobs, whose steps are bound by launch and
+# synchronisation latency rather than by the contractions (the mixed phase would
+# only add iterations there).  Threshold on nbf * nbf5 * naux, the size of the
+# three-index transform.
+AUTO_MIXED_MIN_WORK = 2.0e7
+
+
+def resolve_precision(precision: str, nbf: int, nbf5: int, naux: int) -> str:
+    if precision != "auto":
+        return precision
+    return "mixed_refined" if nbf * nbf5 * naux >= AUTO_MIXED_MIN_WORK else "fp64"
 
 
 @dataclass
@@ -144,9 +157,10 @@ def run_energy(req: Request, device: int, cta_limit: int = 0) -> Result:
         ctx.set_cta_limit(cta_limit)
     b = None
     try:
-        up = "fp64" if req.precision == "fp64" else "mixed"
+        prec = resolve_precision(req.precision, req.p.nbf, req.p.nbf5, req.p.nbfaux)
+        up = "fp64" if prec == "fp64" else "mixed"
         b = api.eris_to_gpu(req.b, up, ctx)
-        if req.precision == "mixed_refined":
+        if prec == "mixed_refined":
             r, _ = energy_mixed_refined(req.H, b, req.p, req.C, req.gamma, E_nuc=req.E_nuc, maxit=req.maxit)
         else:
             r = energy(req.H, b, req.p, req.C, req.gamma, E_nuc=req.E_nuc, maxit=req.maxit)
@@ -205,7 +219,7 @@ class Server:
         if req.precision not in PRECISIONS:
             raise ValueError(f"precision must be one of {PRECISIONS}")
         nbf, naux = req.p.nbf, req.p.nbfaux
-        nb = footprint(nbf, naux, req.p.nbf5, req.precision)
+        nb = footprint(nbf, naux, req.p.nbf5, resolve_precision(req.precision, nbf, req.p.nbf5, naux))
         with self._lock:
             if self._closed:
                 raise RuntimeError("server is shut down")

@@ -219,7 +219,10 @@ int donof_occ_cg(const donof_occ_params* p, const double* J_MO, const double* K_
  * maxit outer iterations, maxloop and alpha (read and updated like p.maxloop and
  * p.alpha), threshgorb / threshgocc (convergence) and threshen (g_abstol of
  * occoptr); order_subspaces = 1 applies the final sort of src/guess.jl:58-106
- * (ipnof > 4); freeze_occ = 1 keeps gamma fixed.                             */
+ * (ipnof > 4); freeze_occ = 1 keeps gamma fixed; stop_rel_de > 0 ends the
+ * loop once an outer iteration changes E by at most stop_rel_de |E| (the
+ * mixed-precision phase stops there, where its energies' rounding would
+ * steer the optimiser, and FP64 iterations take over).                      */
 typedef struct {
     donof_occ_params occ;
     int orb_method;
@@ -229,6 +232,7 @@ typedef struct {
     double threshgorb, threshgocc, threshen;
     int order_subspaces;
     int freeze_occ;
+    double stop_rel_de;  /* > 0: also stop (not converged) once |E - E_prev| <= stop_rel_de |E| */
 } donof_energy_params;
 typedef struct {
     double E_elec;                /* E of the last orbital optimisation */

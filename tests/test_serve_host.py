@@ -95,3 +95,13 @@ def test_cta_share_splits_the_sms_between_inflight_jobs():
     assert cta_share(1, 148) == 0            # one job: all SMs
     assert cta_share(8, 148) == 37           # about two jobs per SM
     assert cta_share(32, 148) == 16          # never fewer than 16 CTAs
+
+
+def test_auto_precision_picks_mixed_for_large_transforms_only():
+    from donof_b200.serve import resolve_precision, footprint
+    assert resolve_precision("auto", 48, 40, 232) == "fp64"
+    assert resolve_precision("auto", 202, 198, 974) == "mixed_refined"
+    assert resolve_precision("fp64", 202, 198, 974) == "fp64"
+    # the mixed footprint includes the bf16 split and, beyond the fused kernel's
+    # shapes, the general pipeline's scratch
+    assert footprint(202, 974, 198, "mixed_refined") > footprint(202, 974, 198, "fp64")
