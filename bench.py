@@ -66,9 +66,10 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-energies", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
-    ap.add_argument("--profile-case", action="store_true",
-                    help="run the mixed and FP64 Lagrangian and the rotation three times each on the "
-                         "benchmark workload and exit (the case the committed ncu captures use)")
+    ap.add_argument("--profile-case", nargs="?", const="synthetic256", choices=["synthetic256", "octane600"],
+                    help="run the mixed and FP64 Lagrangian and the rotation three times each and exit (the "
+                         "cases the committed ncu captures use): the benchmark workload, or an n-octane-shaped "
+                         "job (nbf 202, nbf5 198, naux 600) on the general-shape mixed pipeline")
     return ap.parse_args()
 
 
@@ -286,7 +287,7 @@ def energies_bench(d, torch, ctx):
 SERVE_SHAPES = [(24 * k, 116 * k, 5 * k, 3) for k in (1, 2, 3, 4)] + \
                [(24 * n + 10, int(4.8 * (24 * n + 10)), 4 * n + 1, 5) for n in (1, 2, 3)]
 SERVE_LARGE = (202, 974, 33, 5)   # n-octane shape
-SERVE = dict(jobs=24, large=2, rate_per_s=20.0, seed=7, thresh=1e-5, threshen=1e-6, inflight=8)  # threshen = thresh / 10
+SERVE = dict(jobs=64, large=4, rate_per_s=20.0, seed=7, thresh=1e-5, threshen=1e-6, inflight=8)  # threshen = thresh / 10
 
 
 def serving_bench(d, torch):
@@ -410,6 +411,8 @@ def main():
     p = wl.p
     ctx = d.Context(local)
     if args.profile_case:
+        if args.profile_case == "octane600":
+            wl = workload.synthetic(nbf=202, naux=600, nbeta=33, ncwo=5, seed=SEED)
         profile_case(d, torch, wl, ctx)
         return
     bt = d.eris_to_gpu(wl.b, "mixed", ctx)   # FP64 b and its bf16 split: both forms are timed

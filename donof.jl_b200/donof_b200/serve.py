@@ -148,12 +148,15 @@ class Admission:
 
 def run_energy(req: Request, device: int, cta_limit: int = 0) -> Result:
     """Executor: the energy loop of one request on its own context and stream;
-    cta_limit caps the CTAs of its persistent kernels (0: one per SM)."""
+    cta_limit caps the CTAs of a small job's persistent kernels (0: one per SM).
+    Large jobs (those auto runs in the mixed form) keep every SM: their
+    contractions fill the GPU, the small jobs' steps are latency-bound."""
     from . import api
     from .optimize import energy, energy_mixed_refined
 
     ctx = api.Context(device, torch_stream=False)
-    if cta_limit:
+    p = req.p
+    if cta_limit and p.nbf * p.nbf5 * p.nbfaux < AUTO_MIXED_MIN_WORK:
         ctx.set_cta_limit(cta_limit)
     b = None
     try:
