@@ -53,6 +53,11 @@ SIGNATURES = {
     "donof_occ_energy": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "donof_occ_cg": (_i, [_vp, _vp, _vp, _vp, _vp, ct.c_double, _i, _vp, _vp, _vp]),
     "donof_energy": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "donof_server_create": (_i, [_i, ct.c_size_t, _i, ct.POINTER(_vp)]),
+    "donof_server_submit": (_i, [_vp, _vp, _vp, _vp, ct.POINTER(ct.c_ulonglong)]),
+    "donof_server_poll": (_i, [_vp, ct.c_ulonglong, _vp, _ip]),
+    "donof_server_wait": (_i, [_vp, ct.c_ulonglong, _vp]),
+    "donof_server_destroy": (_i, [_vp]),
     "donof_lagrange2": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp, _vp]),
     "donof_lagrange2_dev": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp, _vp]),
     "donof_lagrange2_prec_dev": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp, _vp]),

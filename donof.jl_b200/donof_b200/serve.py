@@ -291,3 +291,81 @@ class Server:
 def percentiles(values, qs=(50, 99)) -> dict:
     v = np.asarray(values, dtype=np.float64)
     return {f"p{q}": float(np.percentile(v, q)) for q in qs} if v.size else {f"p{q}": None for q in qs}
+
+
+# ---------------------------------------------------------------- native server
+class NativeServer:
+    """The library's own server (donof_server_*): the same admission policy,
+    SM shares and energy loop in native code, behind a thread-safe queue.  The
+    request's arrays are kept alive here until the job is collected."""
+
+    def __init__(self, device: int = 0, budget_bytes: int = 0, max_inflight: int = 8):
+        import ctypes as ct
+        from . import _lib
+        self._ct = ct
+        self.lib = _lib.load()
+        h = ct.c_void_p()
+        _lib.check(self.lib.donof_server_create(int(device), int(budget_bytes), int(max_inflight), ct.byref(h)))
+        self.handle = h
+        self._keep: Dict[int, tuple] = {}
+
+    def submit(self, req: Request) -> int:
+        import ctypes as ct
+        from . import _lib, api, gnof
+        p = req.p
+        H, b, C = api._f64(req.H), api._f64(req.b), api._f64(req.C)
+        gamma = np.ascontiguousarray(gnof.guess_gamma(p) if req.gamma is None else req.gamma, dtype=np.float64)
+        prm = api._EnergyParams(api._occ_params(p), _lib.ORB_METHODS[p.orb_method], int(req.maxit or p.maxit),
+                                int(p.maxloop), float(p.alpha), float(p.threshgorb), float(p.threshgocc),
+                                float(p.threshen), int(p.ipnof > 4), 0, 0.0)
+        prec = {"fp64": 0, "mixed": 1, "mixed_refined": 1, "auto": 2}[req.precision]
+        r = _NativeRequest(H.ctypes.data, b.ctypes.data, C.ctypes.data, gamma.ctypes.data, p.nbf, p.nbfaux, prm,
+                           prec, float(req.E_nuc))
+        C_out = np.zeros((p.nbf, p.nbf), order="F")
+        n_out = np.zeros(p.nbf5)
+        t = ct.c_ulonglong()
+        _lib.check(self.lib.donof_server_submit(self.handle, ct.byref(r), C_out.ctypes.data, n_out.ctypes.data,
+                                                ct.byref(t)))
+        self._keep[t.value] = (H, b, C, gamma, r, C_out, n_out, req.tag)
+        return t.value
+
+    def wait(self, ticket: int) -> Result:
+        from . import _lib
+        res = _NativeResult()
+        _lib.check(self.lib.donof_server_wait(self.handle, self._ct.c_ulonglong(ticket), self._ct.byref(res)))
+        H, b, C, gamma, r, C_out, n_out, tag = self._keep.pop(ticket)
+        err = res.error.decode() if res.status != 0 else None
+        return Result(ticket=ticket, E_elec=res.E_elec, E_tot=res.E_tot, converged=bool(res.converged),
+                      iterations=res.iterations, C=C_out, n=n_out, error=err, t_submit=0.0,
+                      t_start=res.queue_s, t_done=res.latency_s, tag=tag)
+
+    def close(self) -> None:
+        if self.handle:
+            self.lib.donof_server_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def _native_types():
+    import ctypes as ct
+    from . import api
+
+    class Req(ct.Structure):
+        _fields_ = [("H", ct.c_void_p), ("b", ct.c_void_p), ("C", ct.c_void_p), ("gamma", ct.c_void_p),
+                    ("nbf", ct.c_int), ("naux", ct.c_int), ("params", api._EnergyParams), ("precision", ct.c_int),
+                    ("E_nuc", ct.c_double)]
+
+    class Res(ct.Structure):
+        _fields_ = [("status", ct.c_int), ("E_elec", ct.c_double), ("E_tot", ct.c_double),
+                    ("iterations", ct.c_int), ("converged", ct.c_int), ("precision", ct.c_int),
+                    ("queue_s", ct.c_double), ("latency_s", ct.c_double), ("error", ct.c_char * 256)]
+
+    return Req, Res
+
+
+_NativeRequest, _NativeResult = _native_types()

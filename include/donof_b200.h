@@ -250,6 +250,48 @@ int donof_energy(donof_job* job, donof_energy_params* params, const double* H, d
                  double* gamma_inout, double* n_out, double* elag_out, double* history,
                  donof_energy_result* result);
 
+/* --- serving ------------------------------------------------------------------
+ * Continuous batching of energy jobs on one GPU behind a thread-safe queue:
+ * jobs are admitted while their device footprint fits the budget (0: 85 % of
+ * the free memory) and one of max_inflight workers is free (first fit in
+ * arrival order, the head passed over at most 4 times); each worker runs its
+ * job on its own context and stream, so the jobs in flight overlap.
+ * precision: DONOF_PREC_FP64, DONOF_PREC_MIXED (the mixed form, then closing
+ * FP64 iterations to the thresholds) or DONOF_PREC_AUTO (mixed where
+ * nbf * nbf5 * naux >= DONOF_AUTO_MIXED_MIN_WORK, FP64 elsewhere).  A request's
+ * host arrays (H, b, C, gamma; gamma NULL: the reference's initial guess) and
+ * the output arrays (C_out nbf x nbf, n_out nbf5 or NULL) must stay valid until
+ * the job is collected by donof_server_poll / donof_server_wait.             */
+#define DONOF_PREC_AUTO 2
+#define DONOF_AUTO_MIXED_MIN_WORK 2.0e7
+typedef struct donof_server donof_server;
+typedef struct {
+    const double* H;
+    const double* b;
+    const double* C;
+    const double* gamma;
+    int nbf, naux;
+    donof_energy_params params;
+    int precision;
+    double E_nuc;
+} donof_request;
+typedef struct {
+    int status;                   /* DONOF_OK or the job's error (DONOF_ERR_STATE: cancelled) */
+    double E_elec, E_tot;
+    int iterations, converged;
+    int precision;                /* the form that ran */
+    double queue_s, latency_s;    /* submit -> start, submit -> done */
+    char error[256];
+} donof_result;
+int donof_server_create(int device, size_t budget_bytes, int max_inflight, donof_server** server);
+int donof_server_submit(donof_server* server, const donof_request* request, double* C_out, double* n_out,
+                        unsigned long long* ticket);
+/* done = 1 (and the result filled, the ticket released) once the job has ended */
+int donof_server_poll(donof_server* server, unsigned long long ticket, donof_result* result, int* done);
+int donof_server_wait(donof_server* server, unsigned long long ticket, donof_result* result);
+/* Cancels the jobs not started, waits for those in flight, frees the server. */
+int donof_server_destroy(donof_server* server);
+
 /* --- diagnostics -------------------------------------------------------------
  * Number of CUDA kernels this library has launched in the process so far.    */
 unsigned long long donof_launch_count(void);

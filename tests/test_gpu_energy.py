@@ -99,3 +99,39 @@ def test_native_energy_loop_matches_python_loop(cuda_ctx, prec):
         assert abs(h1["E"] - h0["E"]) <= 1e-4 * abs(h0["E"])
         assert abs(r1.E_elec - r0.E_elec) <= 1e-4 * abs(r0.E_elec)
     assert abs(np.sum(r1.n) - np.sum(r0.n)) <= 1e-9
+
+
+@pytest.mark.parametrize("variant", ["trigonometric", "ista3", "open_shell"])
+def test_native_energy_loop_variants(cuda_ctx, variant):
+    """The native loop against the Python loop for the other occupation map, a
+    non-default GNOF static term and an open shell (nalpha > nbeta)."""
+    from donof_b200 import gnof
+    from donof_b200.param import Param
+
+    nbf, naux = 32, 60
+    wl = workload.molecule_like(nbf=nbf, naux=naux, nbeta=4, ncwo=3, seed=8)
+
+    def params():
+        if variant == "trigonometric":
+            return workload.molecule_like(nbf=nbf, naux=naux, nbeta=4, ncwo=3, seed=8,
+                                          occ_method="Trigonometric").p
+        if variant == "ista3":
+            return workload.molecule_like(nbf=nbf, naux=naux, nbeta=4, ncwo=3, seed=8, ista=3).p
+        return Param(nbf=nbf, nbfaux=naux, nbeta=4, nalpha=6, ncwo=3)
+
+    out = {}
+    for native in (False, True):
+        p = params()
+        p.threshgorb, p.threshgocc, p.threshen = 1e-5, 1e-5, 1e-9
+        g0 = gnof.guess_gamma(p)
+        b = d.eris_to_gpu(wl.b, "fp64", cuda_ctx)
+        out[native] = energy(wl.H, b, p, wl.C, g0, maxit=300, native=native)
+        b.free()
+    r0, r1 = out[False], out[True]
+    h0, h1 = r0.history[0], r1.history[0]
+    assert h0["nit_orb"] == h1["nit_orb"] and abs(h1["nit_occ"] - h0["nit_occ"]) <= 1
+    assert abs(h1["E"] - h0["E"]) <= 1e-9 * abs(h0["E"])
+    assert r0.converged == r1.converged
+    if r0.converged:
+        assert abs(r1.E_elec - r0.E_elec) <= 1e-6
+    assert abs(np.sum(r1.n) - np.sum(r0.n)) <= 1e-9

@@ -43,3 +43,33 @@ def test_results_alone_equal_results_in_the_mix():
     # the jobs did share the device: some ran while others were in flight
     spans = sorted((m.t_start, m.t_done) for m in mix)
     assert any(spans[i + 1][0] < spans[i][1] for i in range(len(spans) - 1))
+
+
+def test_native_server_matches_sequential_fp64(cuda_ctx):
+    """donof_server_*: jobs of different sizes served natively (8 workers) give
+    the FP64 energies of running each job alone, and report every job done."""
+    import copy
+    import donof_b200 as d
+    from donof_b200.optimize import energy
+    from donof_b200.serve import NativeServer, Request
+
+    shapes = [(24, 58, 5, 3), (34, 80, 5, 5), (48, 116, 10, 3), (24, 58, 5, 3), (40, 90, 6, 3)]
+    wls = [workload.molecule_like(nbf=a, naux=b, nbeta=c, ncwo=e, seed=40 + i, two_e_scale=0.2)
+           for i, (a, b, c, e) in enumerate(shapes)]
+    for wl in wls:
+        wl.p.threshgorb = wl.p.threshgocc = 1e-5
+        wl.p.threshen = 1e-6
+    alone = []
+    for wl in wls:
+        bt = d.eris_to_gpu(wl.b, "fp64", cuda_ctx)
+        alone.append(energy(wl.H, bt, copy.deepcopy(wl.p), wl.C, wl.gamma, maxit=500))
+        bt.free()
+    with NativeServer(max_inflight=8) as srv:
+        tickets = [srv.submit(Request(H=wl.H, b=wl.b, C=wl.C, p=copy.deepcopy(wl.p), gamma=wl.gamma,
+                                      precision="fp64", maxit=500)) for wl in wls]
+        served = [srv.wait(t) for t in tickets]
+    for a, s in zip(alone, served):
+        assert s.error is None, s.error
+        assert s.converged == a.converged
+        assert abs(s.E_elec - a.E_elec) <= 1e-10 * max(1.0, abs(a.E_elec))
+        assert np.max(np.abs(s.n - a.n)) <= 1e-8
