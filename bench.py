@@ -66,10 +66,13 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-energies", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
-    ap.add_argument("--profile-case", nargs="?", const="synthetic256", choices=["synthetic256", "octane600"],
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--profile-case", nargs="?", const="synthetic256",
+                    choices=["synthetic256", "octane600", "batch64"],
                     help="run the mixed and FP64 Lagrangian and the rotation three times each and exit (the "
                          "cases the committed ncu captures use): the benchmark workload, or an n-octane-shaped "
-                         "job (nbf 202, nbf5 198, naux 600) on the general-shape mixed pipeline")
+                         "job (nbf 202, nbf5 198, naux 600) on the general-shape mixed pipeline; batch64: three "
+                         "grouped orbital steps of the 64-job water-cluster batch")
     return ap.parse_args()
 
 
@@ -358,6 +361,77 @@ def serving_bench(d, torch):
                           "within_1uEh": int(np.sum(dE <= 1e-6)), "of": len(dE)}}
 
 
+BATCH = dict(count=64, kmax=8, seed=11)
+
+
+def batched_bench(d, torch, ctx, steps, warmup, method, sequential_arm=True):
+    """Orbital-gradient steps/s of a batch of uneven jobs advanced together (one
+    grouped launch per stage of a step, the loop as one captured graph) against
+    the same jobs run one after the other through the single-job device loop:
+    64 water-cluster surrogates (H2O)_k, k uniform in 1..8 (nbf 24-192), FP64."""
+    from donof_b200 import workload
+    jobs = workload.water_clusters(**BATCH)
+    bts, ins = [], []
+    for j, (k, wl) in enumerate(jobs):
+        tb = workload.b_device(wl.p.nbf, wl.p.nbfaux, seed=BATCH["seed"] * 7919 + j)
+        bts.append(d.eris_to_gpu(tb, "fp64", ctx))
+        ins.append(dict(p=wl.p, C=d.to_device(wl.C), H=d.to_device(wl.H), n=d.to_device(wl.n),
+                        cj=d.to_device(wl.cj12), ck=d.to_device(wl.ck12)))
+    nj = len(jobs)
+    batch = d.Batch(bts, [x["p"] for x in ins], ctx)
+    cols = lambda key: [x[key] for x in ins]
+
+    def grouped(ml):
+        Cs = [x["C"].clone() for x in ins]
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = d.launch_count()
+        e0.record()
+        res = batch.orbopt(method, cols("n"), cols("cj"), cols("ck"), cols("H"), Cs, [0.01] * nj, [ml] * nj,
+                           [0.0] * nj)
+        e1.record()
+        torch.cuda.synchronize()
+        assert all(r[1] == ml for r in res), "every job takes exactly maxloop steps"
+        return e0.elapsed_time(e1) / 1e3, d.launch_count() - l0, res
+
+    grouped(warmup)  # autotune + capture
+    tg, lg, res_g = grouped(steps)
+
+    def sequential(ml):
+        Cs = [x["C"].clone() for x in ins]
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        res = [d.orbopt_dev(method, x["n"], x["cj"], x["ck"], x["H"], C, bt, x["p"], 0.01, ml, 0.0)
+               for x, C, bt in zip(ins, Cs, bts)]
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3, res
+
+    if not sequential_arm:
+        batch.free()
+        for b in bts:
+            b.free()
+        return {"grouped_ms_per_step": 1e3 * tg / steps, "launches_per_step": lg / steps}
+    sequential(warmup)
+    ts, res_s = sequential(steps)
+    dE = max(abs(a[0] - b[0]) / max(1.0, abs(b[0])) for a, b in zip(res_g, res_s))
+    out = {"workload": f"{nj} water-cluster surrogates (H2O)_k, k ~ U{{1..{BATCH['kmax']}}} (nbf 24-192, naux 116k, "
+                       f"nbf5 20k), FP64, {steps} orbital steps each",
+           "ks": [k for k, _ in jobs], "unit": "job orbital-gradient steps/s",
+           "grouped": {"value": nj * steps / tg, "ms_per_step": 1e3 * tg / steps, "launches_per_step": lg / steps,
+                       "path": "donof_batch_orbopt (grouped persistent GEMMs + grouped cooperative kernels, "
+                               "one graph)"},
+           "sequential": {"value": nj * steps / ts, "ms_per_round": 1e3 * ts / steps,
+                          "path": "donof_orbopt_dev per job, one after the other"},
+           "speedup": ts / tg, "max_rel_dE_grouped_vs_sequential": dE,
+           "device_bytes": batch.device_bytes()}
+    batch.free()
+    for b in bts:
+        b.free()
+    return out
+
+
 def profile_case(d, torch, wl, ctx):
     """Three calls each of the mixed and FP64 Lagrangian and of the rotation."""
     import numpy as np
@@ -410,6 +484,9 @@ def main():
     wl = workload.synthetic(**WORKLOAD, seed=SEED)
     p = wl.p
     ctx = d.Context(local)
+    if args.profile_case == "batch64":
+        print(json.dumps(batched_bench(d, torch, ctx, 3, 1, args.method, sequential_arm=False)), flush=True)
+        return
     if args.profile_case:
         if args.profile_case == "octane600":
             wl = workload.synthetic(nbf=202, naux=600, nbeta=33, ncwo=5, seed=SEED)
@@ -553,6 +630,10 @@ def main():
     if rank == 0 and world == 1 and not args.no_serving:
         serving = serving_bench(d, torch)
 
+    batched = None
+    if rank == 0 and world == 1 and not args.no_batched:
+        batched = batched_bench(d, torch, ctx, args.steps, args.warmup, args.method)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         done, dt, cores = run_cpu_steps(wl, 6, 20.0)
@@ -571,6 +652,8 @@ def main():
             line["energies"] = energies
         if serving is not None:
             line["serving"] = serving
+        if batched is not None:
+            line["batched"] = batched
         print(json.dumps(line), flush=True)
     bt.free()
     ctx.close()

@@ -294,13 +294,15 @@ __device__ __forceinline__ void red_release_add(unsigned* p, unsigned v) {
 }
 
 // epoch: barriers this CTA has passed (the same in every CTA); incremented here.
-__device__ __forceinline__ bool grid_barrier(GridSync* gs, unsigned& epoch) {
+// members: the CTAs that take part (gridDim.x for the whole grid; a grouped
+// launch gives each job its own GridSync and CTA range).
+__device__ __forceinline__ bool grid_barrier(GridSync* gs, unsigned& epoch, unsigned members) {
     __shared__ int fail;
     __syncthreads();
     if (threadIdx.x == 0) {
         fail = 0;
         red_release_add(&gs->count, 1u);
-        const unsigned target = (epoch + 1) * gridDim.x;
+        const unsigned target = (epoch + 1) * members;
         const long long t0 = clock64();
         while (ld_acquire(&gs->count) < target) {
             if (clock64() - t0 > BARRIER_CYCLES || *(volatile int*)&gs->err) {
@@ -313,6 +315,10 @@ __device__ __forceinline__ bool grid_barrier(GridSync* gs, unsigned& epoch) {
     __syncthreads();
     ++epoch;
     return fail == 0;
+}
+
+__device__ __forceinline__ bool grid_barrier(GridSync* gs, unsigned& epoch) {
+    return grid_barrier(gs, epoch, gridDim.x);
 }
 
 }  // namespace dtile

@@ -51,7 +51,87 @@ cudaError_t launch_layout(const GemmF64Args& p, bool ak, bool bk, bool vec, cuda
 
 bool aligned16(const void* ptr) { return (reinterpret_cast<uintptr_t>(ptr) & 15u) == 0; }
 
+template <int BM, int BN, int WM, int WN, bool AK, bool BKM, bool VEC>
+cudaError_t launch_grouped_cfg(const GemmF64Args* groups, const int* start, int ngroups, int total, int sm_count,
+                               int max_ctas, cudaStream_t st) {
+    constexpr int BK = 16, STAGES = 3;
+    using Cfg = GemmF64Cfg<BM, BN, BK, WM, WN, STAGES, AK, BKM, VEC>;
+    auto kern = gemm_f64_grouped_kernel<BM, BN, BK, WM, WN, STAGES, AK, BKM, VEC>;
+    static std::atomic<unsigned long long> attr_mask{0};
+    static std::atomic<int> per_sm_cached{0};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (!(attr_mask.load(std::memory_order_acquire) & bit)) {
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM_BYTES);
+        if (e != cudaSuccess) return e;
+        int per_sm = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, Cfg::THREADS, Cfg::SMEM_BYTES);
+        if (e != cudaSuccess) return e;
+        per_sm_cached.store(per_sm < 1 ? 1 : per_sm, std::memory_order_release);
+        attr_mask.fetch_or(bit, std::memory_order_acq_rel);
+    }
+    long long grid = (long long)per_sm_cached.load(std::memory_order_acquire) * sm_count;
+    if (max_ctas > 0 && grid > max_ctas) grid = max_ctas;
+    if (grid > total) grid = total;
+    if (grid < 1) grid = 1;
+    kern<<<(unsigned)grid, Cfg::THREADS, Cfg::SMEM_BYTES, st>>>(groups, start, ngroups); count_launch();
+    return cudaGetLastError();
+}
+
+template <int BM, int BN, int WM, int WN>
+cudaError_t launch_grouped_layout(const GemmF64Args* groups, const int* start, int ngroups, int total, int sm,
+                                  int max_ctas, bool ak, bool bk, bool vec, cudaStream_t st) {
+#define DONOF_GL(A_, B_)                                                                                       \
+    return vec ? launch_grouped_cfg<BM, BN, WM, WN, A_, B_, true>(groups, start, ngroups, total, sm, max_ctas, st) \
+               : launch_grouped_cfg<BM, BN, WM, WN, A_, B_, false>(groups, start, ngroups, total, sm, max_ctas, st)
+    if (ak && bk) DONOF_GL(true, true);
+    if (ak && !bk) DONOF_GL(true, false);
+    if (!ak && bk) DONOF_GL(false, true);
+    DONOF_GL(false, false);
+#undef DONOF_GL
+}
+
 }  // namespace
+
+bool gemm_f64_vec_ok(bool a_kmajor, bool b_kmajor, const GemmF64Args& p) {
+    int splits = p.splits < 1 ? 1 : p.splits;
+    const int kchunk = (splits == 1 || p.kchunk <= 0) ? p.K : p.kchunk;
+    const bool va = aligned16(p.A) && (p.lda % 2 == 0) && (p.strideA % 2 == 0) &&
+                    (a_kmajor ? (p.K % 2 == 0 && kchunk % 2 == 0) : (p.M % 2 == 0));
+    const bool vb = aligned16(p.B) && (p.ldb % 2 == 0) && (p.strideB % 2 == 0) &&
+                    (b_kmajor ? (p.K % 2 == 0 && kchunk % 2 == 0) : (p.N % 2 == 0));
+    return va && vb;
+}
+
+int gemm_f64_tiles(const GemmF64Args& p, GemmTile tile) {
+    const int bm = tile == GemmTile::Large ? 128 : (tile == GemmTile::Small ? 64 : 32);
+    const int bn = tile == GemmTile::Tiny ? 32 : 64;
+    if (p.M <= 0 || p.N <= 0 || p.batch <= 0) return 0;
+    return ((p.M + bm - 1) / bm) * ((p.N + bn - 1) / bn) * p.batch * (p.splits < 1 ? 1 : p.splits);
+}
+
+int gemm_f64_grouped(donof_ctx* ctx, cudaStream_t st, bool a_kmajor, bool b_kmajor, bool vec, GemmTile tile,
+                     const GemmF64Args* groups, const int* start, int ngroups, int total_tiles, int max_ctas) {
+    if (ngroups <= 0 || total_tiles <= 0) return DONOF_OK;
+    cudaError_t e;
+    if (tile == GemmTile::Large)
+        e = launch_grouped_layout<128, 64, 4, 2>(groups, start, ngroups, total_tiles, ctx->sm_count, max_ctas,
+                                                 a_kmajor, b_kmajor, vec, st);
+    else if (tile == GemmTile::Small)
+        e = launch_grouped_layout<64, 64, 2, 2>(groups, start, ngroups, total_tiles, ctx->sm_count, max_ctas,
+                                                a_kmajor, b_kmajor, vec, st);
+    else
+        e = launch_grouped_layout<32, 32, 2, 2>(groups, start, ngroups, total_tiles, ctx->sm_count, max_ctas,
+                                                a_kmajor, b_kmajor, vec, st);
+    if (e != cudaSuccess) {
+        set_error(ctx, "gemm_f64_grouped launch (%d groups, %d tiles): %s", ngroups, total_tiles,
+                  cudaGetErrorString(e));
+        return DONOF_ERR_CUDA;
+    }
+    return DONOF_OK;
+}
 
 int gemm_f64(donof_ctx* ctx, cudaStream_t st, bool a_kmajor, bool b_kmajor, GemmF64Args p,
              GemmTile tile) {

@@ -137,13 +137,14 @@ struct GemmF64Cfg {
     static_assert(BK % 4 == 0, "BK must be a multiple of 4");
 };
 
+// One output tile (bx, by) of batch/split index bz = z * splits + split: the
+// whole body of gemm_f64_kernel, shared with the grouped persistent kernel
+// below (same staging, same MMA order, so both write identical results).
 template <int BM, int BN, int BK, int WARPS_M, int WARPS_N, int STAGES, bool AK, bool BKM, bool VEC>
-__global__ void __launch_bounds__(32 * WARPS_M * WARPS_N)
-gemm_f64_kernel(const GemmF64Args p) {
+__device__ __forceinline__ void gemm_f64_tile(const GemmF64Args& p, int bx, int by, int bz, double* smem) {
     using Cfg = GemmF64Cfg<BM, BN, BK, WARPS_M, WARPS_N, STAGES, AK, BKM, VEC>;
     constexpr int KS = gemm_detail::kMmaK;
     static_assert(BK % KS == 0, "BK must be a multiple of the MMA depth");
-    extern __shared__ __align__(16) double smem[];
 
     const int tid = threadIdx.x;
     const int lane = tid & 31;
@@ -153,10 +154,10 @@ gemm_f64_kernel(const GemmF64Args p) {
     const int g = lane >> 2;  // groupID
     const int t = lane & 3;   // threadID_in_group
 
-    const int z = blockIdx.z / p.splits;
-    const int split = blockIdx.z % p.splits;
-    const int m0 = blockIdx.x * BM;
-    const int n0 = blockIdx.y * BN;
+    const int z = bz / p.splits;
+    const int split = bz % p.splits;
+    const int m0 = bx * BM;
+    const int n0 = by * BN;
     const int kbeg = split * p.kchunk;
     const int kend = min(p.K, kbeg + p.kchunk);
     const double* __restrict__ A = p.A + (long long)z * p.strideA;
@@ -292,6 +293,36 @@ gemm_f64_kernel(const GemmF64Args p) {
                 }
             }
         }
+    }
+}
+
+template <int BM, int BN, int BK, int WARPS_M, int WARPS_N, int STAGES, bool AK, bool BKM, bool VEC>
+__global__ void __launch_bounds__(32 * WARPS_M * WARPS_N)
+gemm_f64_kernel(const GemmF64Args p) {
+    extern __shared__ __align__(16) double smem[];
+    gemm_f64_tile<BM, BN, BK, WARPS_M, WARPS_N, STAGES, AK, BKM, VEC>(p, blockIdx.x, blockIdx.y, blockIdx.z, smem);
+}
+
+// Grouped persistent form: `ngroups` independent GEMMs (one per job of a
+// batch; every group with its own sizes, operands, batch count, split-K and
+// device-side gates) share one launch.  Group g owns the tiles
+// [start[g], start[g + 1]) of a flat work list (tile t of a group is
+// (bx, by, bz) = (t % gx, (t / gx) % gy, t / (gx gy)) as in the 3-D grid of
+// gemm_f64_kernel); each CTA walks the list with stride gridDim.x.
+template <int BM, int BN, int BK, int WARPS_M, int WARPS_N, int STAGES, bool AK, bool BKM, bool VEC>
+__global__ void __launch_bounds__(32 * WARPS_M * WARPS_N)
+gemm_f64_grouped_kernel(const GemmF64Args* __restrict__ groups, const int* __restrict__ start, int ngroups) {
+    extern __shared__ __align__(16) double smem[];
+    const int total = start[ngroups];
+    int g = 0;
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        while (g + 1 < ngroups && start[g + 1] <= t) ++g;  // t only grows: advance the group
+        const GemmF64Args p = groups[g];
+        const int lt = t - start[g];
+        const int gx = (p.M + BM - 1) / BM, gy = (p.N + BN - 1) / BN;
+        __syncthreads();  // the previous tile's last shared-memory reads are done
+        gemm_f64_tile<BM, BN, BK, WARPS_M, WARPS_N, STAGES, AK, BKM, VEC>(p, lt % gx, (lt / gx) % gy, lt / (gx * gy),
+                                                                           smem);
     }
 }
 

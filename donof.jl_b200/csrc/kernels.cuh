@@ -23,6 +23,16 @@ int splitk_reduce(donof_ctx* ctx, cudaStream_t st, const double* part, long long
 int gemm_f64_tuned(donof_ctx* ctx, cudaStream_t st, bool a_kmajor, bool b_kmajor, const GemmF64Args& p,
                    GemmTile heuristic);
 
+// Grouped persistent GEMM (gemm_f64.cuh, gemm_f64_grouped_kernel): ngroups
+// GEMMs of one operand layout in one launch.  groups and start live in device
+// memory: group g owns tiles [start[g], start[g+1]) of the flat work list
+// (start[ngroups] == total_tiles, each group's count from gemm_f64_tiles with
+// the same tile shape).  vec: every group passes gemm_f64_vec_ok.
+int gemm_f64_grouped(donof_ctx* ctx, cudaStream_t st, bool a_kmajor, bool b_kmajor, bool vec, GemmTile tile,
+                     const GemmF64Args* groups, const int* start, int ngroups, int total_tiles, int max_ctas);
+int gemm_f64_tiles(const GemmF64Args& p, GemmTile tile);
+bool gemm_f64_vec_ok(bool a_kmajor, bool b_kmajor, const GemmF64Args& p);
+
 // Tile shape (and split count, when can_split) that puts >= one CTA per SM.
 GemmTile pick_tile(donof_ctx* ctx, int M, int N, int K, bool can_split, int* splits_out);
 
@@ -88,6 +98,36 @@ int rotate_f64(donof_ctx* ctx, cudaStream_t st, const double* y, int nbf, int nb
 int rotate_f64_gated(donof_ctx* ctx, cudaStream_t st, const double* y, int nbf, int nbf5,
                      const double* C, double* Cnew, const int* done, DevBuf* part);
 size_t rotate_scratch_bytes(int nbf);
+
+// Grouped cooperative kernels for a batch of jobs (batch.cu): one launch runs
+// the rotation (or the Lagrangian tail) of every job, job j on the CTAs
+// [cta0, cta0 + ctas) with its own barrier state in a GROUP_STATE_BYTES slot of
+// `states` (zeroed by the launcher).  Ranges are disjoint except that jobs with
+// ctas == 1 may share a CTA; grid <= sm_count (co-resident).  A job whose
+// *skip is nonzero is left out.
+constexpr int GROUP_STATE_BYTES = 64;
+struct RotJob {
+    const double* y;
+    const double* C;
+    double* Cnew;
+    double* work;  // rotate_work_doubles(nbf)
+    void* state;
+    const int* skip;
+    int nbf, nbf5, cta0, ctas;
+};
+size_t rotate_work_doubles(int nbf);
+int rotate_grouped(donof_ctx* ctx, cudaStream_t st, const RotJob* jobs, int njobs, void* states, int grid);
+struct TailJob {
+    const double *C, *H, *n;
+    const void* part;  // Y partials: part[g * pstride + m + nbf * b], g < nparts
+    long long pstride;
+    double *Hmat, *elag, *E;
+    double* work;  // 3 * nbf * nbf5 doubles
+    void* state;
+    const int* skip;
+    int nbf, nbf5, part_f32, nparts, cta0, ctas;
+};
+int tail_grouped(donof_ctx* ctx, cudaStream_t st, const TailJob* jobs, int njobs, void* states, int grid);
 
 // Orbital-gradient helpers (optim.cu): g = pack(4 elag - 4 elag^T); when
 // maxabs != nullptr also atomically max-reduces |g| into it (must be zeroed).

@@ -18,65 +18,32 @@
 #include <mutex>
 
 #include "kernels.cuh"
+#include "wbuild.cuh"
 
 namespace donof {
 
 namespace {
 
-// W of every aux index, W[q + nbf5 l + Kt b] (Kt = nbf5 naux):
-//   W_l[q, b] = delta_qb (n'_b d_b^l + t_b^l) - ck12[b, q] b_pq^l[b, q]
-// with d_b^l = b_pq^l[b, b], t_b^l = sum_q cj12[b, q] d_q^l and n'_b = n_b for
-// b < nbeta or b >= nalpha (0 when nbeta = 0).  Two fully parallel passes:
-// w_diag_kernel forms n'_b d_b^l + t_b^l (one thread per (b, l), cj12 read
-// along b); build_w_kernel the elementwise part over 32 x 32 tiles of (b, q),
-// one tile per CTA step, transposed through shared memory so that b_pq^l and
-// ck12 are read along b and W is written along q (b need not be symmetric).
+// W of every aux index (wbuild.cuh) in two fully parallel passes: w_diag_kernel
+// forms n'_b d_b^l + t_b^l (one thread per (b, l), cj12 read along b);
+// build_w_kernel the elementwise part over 32 x 32 tiles of (b, q), one tile per
+// CTA step (b need not be symmetric).
 __global__ void w_diag_kernel(const double* __restrict__ bpq, const double* __restrict__ n,
                               const double* __restrict__ cj12, int nbf5, int naux, int nalpha, int nbeta,
                               double* __restrict__ tv) {
-    const long long n55 = (long long)nbf5 * nbf5, total = (long long)nbf5 * naux;
+    const long long total = (long long)nbf5 * naux;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
-         i += (long long)gridDim.x * blockDim.x) {
-        const int b = (int)(i % nbf5);
-        const long long l = i / nbf5;
-        const double* B = bpq + n55 * l;
-        double s = 0.0;
-        for (int q = 0; q < nbf5; ++q) s += cj12[b + (long long)nbf5 * q] * B[(long long)q * (nbf5 + 1)];
-        const bool dj = (nbeta > 0) && (b < nbeta || b >= nalpha);
-        tv[i] = (dj ? n[b] * B[(long long)b * (nbf5 + 1)] : 0.0) + s;
-    }
+         i += (long long)gridDim.x * blockDim.x)
+        tv[i] = wbuild::diag_value(bpq, n, cj12, nbf5, nalpha, nbeta, i);
 }
 
-// 256 threads: tx = threadIdx.x % 32, ty = threadIdx.x / 32 (8 rows per pass)
 __global__ void __launch_bounds__(256) build_w_kernel(const double* __restrict__ bpq, const double* __restrict__ ck12,
                                                       const double* __restrict__ tv, int nbf5, int naux,
                                                       double* __restrict__ W) {
     __shared__ double tb[32][33];
-    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-    const long long n55 = (long long)nbf5 * nbf5, Kt = (long long)nbf5 * naux;
     const int nt = (nbf5 + 31) / 32;
     const long long tiles = (long long)nt * nt * naux;
-    for (long long t = blockIdx.x; t < tiles; t += gridDim.x) {
-        const int b0 = (int)(t % nt) * 32, q0 = (int)((t / nt) % nt) * 32;
-        const long long l = t / ((long long)nt * nt);
-        const double* B = bpq + n55 * l;
-        __syncthreads();  // the previous tile's reads of tb are done
-        for (int r = ty; r < 32; r += 8) {
-            const int b = b0 + tx, q = q0 + r;
-            double v = 0.0;
-            if (b < nbf5 && q < nbf5) {
-                const long long e = b + (long long)nbf5 * q;
-                v = -ck12[e] * B[e];
-                if (q == b) v += tv[b + (long long)nbf5 * l];
-            }
-            tb[r][tx] = v;  // [q - q0][b - b0]
-        }
-        __syncthreads();
-        for (int r = ty; r < 32; r += 8) {
-            const int q = q0 + tx, b = b0 + r;
-            if (b < nbf5 && q < nbf5) W[q + (long long)nbf5 * l + Kt * b] = tb[tx][r];
-        }
-    }
+    for (long long t = blockIdx.x; t < tiles; t += gridDim.x) wbuild::tile(bpq, ck12, tv, nbf5, naux, W, t, tb);
 }
 
 // elag[a, b] = n_b H_mat[a, b] for b < nbf5 (the 2ndH/dy_ab term,

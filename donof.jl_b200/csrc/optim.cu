@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "kernels.cuh"
+#include "orbupd.cuh"
 
 namespace donof {
 
@@ -119,39 +120,10 @@ struct OrbState {
 __global__ void orb_update_kernel(const OrbState* __restrict__ s, long long nvar, const double* __restrict__ g,
                                   double* __restrict__ m, double* __restrict__ v, double* __restrict__ vmax,
                                   double* __restrict__ y) {
-    const int i = s->it + 1;
-    const int method = s->method;
-    double beta1 = (method == DONOF_ORB_DEMON) ? 0.6 : 0.5;
-    const double beta2 = (method == DONOF_ORB_DEMON) ? 0.999 : 0.9;
-    if (method == DONOF_ORB_DEMON) {
-        const double binit = beta1;
-        const double rate = (i - 1.0) / (s->maxloop - 1.0);
-        beta1 = binit * (1.0 - rate) / ((1.0 - binit) + binit * (1.0 - rate));
-    }
-    const double bc1 = 1.0 - pow(beta1, (double)i), bc2 = 1.0 - pow(beta2, (double)i);
-    const double alpha = s->alpha;
+    const orbupd::Coef c = orbupd::coef(s->method, s->it + 1, s->maxloop, s->alpha);
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nvar;
-         k += (long long)gridDim.x * blockDim.x) {
-        const double gk = g[k];
-        const double mk = beta1 * m[k] + (1.0 - beta1) * gk;
-        double vk;
-        if (method == DONOF_ORB_ADABELIEF) {
-            const double dd = gk - mk;
-            vk = beta2 * v[k] + (1.0 - beta2) * (dd * dd);
-        } else if (method == DONOF_ORB_YOGI) {
-            const double g2 = gk * gk;
-            const double dv = v[k] - g2;
-            const double sg = (dv > 0.0) ? 1.0 : ((dv < 0.0) ? -1.0 : 0.0);
-            vk = v[k] - (1.0 - beta2) * sg * g2;
-        } else {
-            vk = beta2 * v[k] + (1.0 - beta2) * (gk * gk);
-        }
-        const double vm = fmax(vmax[k], vk / bc2);
-        m[k] = mk;
-        v[k] = vk;
-        vmax[k] = vm;
-        y[k] = -alpha * (mk / bc1) / sqrt(vm + 1e-16);
-    }
+         k += (long long)gridDim.x * blockDim.x)
+        orbupd::step(c, k, g, m, v, vmax, y);
 }
 
 // End of iteration it+1: best-E tracking and the stopping rule evaluated at the

@@ -229,15 +229,15 @@ __device__ __forceinline__ dtile::Gemm sq_gemm(int n, const double* A, const dou
     return g;
 }
 
-__device__ __forceinline__ void run_tiles(const dtile::Gemm& g, double* sm) {
+__device__ __forceinline__ void run_tiles(const dtile::Gemm& g, double* sm, int cta, int G) {
     const int nt = dtile::tiles<RT_TN>(g);
-    for (int w = blockIdx.x; w < nt; w += gridDim.x) dtile::tile<RT_TN>(g, w, sm);
+    for (int w = cta; w < nt; w += G) dtile::tile<RT_TN>(g, w, sm);
 }
 
-__global__ void __launch_bounds__(dtile::THREADS) rotate_coop_kernel(const CoopArgs a) {
-    extern __shared__ __align__(16) double sm[];
+// The whole rotation of one job on CTAs cta = 0..G-1 (of a cooperative launch).
+__device__ __forceinline__ void rotate_body(const CoopArgs& a, int cta, int G, double* sm) {
     __shared__ double red[dtile::WARPS];
-    const int n = a.nbf, G = gridDim.x, cta = blockIdx.x, tid = threadIdx.x;
+    const int n = a.nbf, tid = threadIdx.x;
     const long long nn = (long long)n * n;
     CoopState* cs = a.cs;
     dtile::GridSync* gs = &cs->gs;
@@ -262,15 +262,15 @@ __global__ void __launch_bounds__(dtile::THREADS) rotate_coop_kernel(const CoopA
         }
         __syncthreads();
     }
-    if (!dtile::grid_barrier(gs, epoch)) return;
+    if (!dtile::grid_barrier(gs, epoch, G)) return;
     const double norm = __longlong_as_double((long long)cs->norm_bits);
     int s = 0;
     if (norm > 0.25) s = (int)ceil(log2(norm / 0.25));
     if (s > SMAX) s = SMAX;
     const double sc = ldexp(1.0, -s);  // X = sc * Y (a power of two: exact)
     // S1: X2 = X X
-    run_tiles(sq_gemm(n, a.Y, a.Y, a.X2, sc * sc, false), sm);
-    if (!dtile::grid_barrier(gs, epoch)) return;
+    run_tiles(sq_gemm(n, a.Y, a.Y, a.X2, sc * sc, false), sm, cta, G);
+    if (!dtile::grid_barrier(gs, epoch, G)) return;
     // S2: X3 = X2 X, X4 = X2 X2
     {
         const dtile::Gemm g3 = sq_gemm(n, a.X2, a.Y, a.X3, sc, false);
@@ -281,7 +281,7 @@ __global__ void __launch_bounds__(dtile::THREADS) rotate_coop_kernel(const CoopA
             else dtile::tile<RT_TN>(g4, w - nt, sm);
         }
     }
-    if (!dtile::grid_barrier(gs, epoch)) return;
+    if (!dtile::grid_barrier(gs, epoch, G)) return;
     // S3: the three polynomial blocks of the degree-12 Taylor sum (1/k! coefficients)
     {
         double c[13];
@@ -312,22 +312,83 @@ __global__ void __launch_bounds__(dtile::THREADS) rotate_coop_kernel(const CoopA
             }
         }
     }
-    if (!dtile::grid_barrier(gs, epoch)) return;
+    if (!dtile::grid_barrier(gs, epoch, G)) return;
     // S4: E1 += P X4;  S5: E0 = bufs[0] += E1 X4
-    run_tiles(sq_gemm(n, a.P, a.X4, a.E1, 1.0, true), sm);
-    if (!dtile::grid_barrier(gs, epoch)) return;
-    run_tiles(sq_gemm(n, a.E1, a.X4, a.bufs, 1.0, true), sm);
-    if (!dtile::grid_barrier(gs, epoch)) return;
+    run_tiles(sq_gemm(n, a.P, a.X4, a.E1, 1.0, true), sm, cta, G);
+    if (!dtile::grid_barrier(gs, epoch, G)) return;
+    run_tiles(sq_gemm(n, a.E1, a.X4, a.bufs, 1.0, true), sm, cta, G);
+    if (!dtile::grid_barrier(gs, epoch, G)) return;
     // squarings: bufs[k+1] = bufs[k]^2
     for (int k = 0; k < s; ++k) {
-        run_tiles(sq_gemm(n, a.bufs + k * nn, a.bufs + k * nn, a.bufs + (k + 1) * nn, 1.0, false), sm);
-        if (!dtile::grid_barrier(gs, epoch)) return;
+        run_tiles(sq_gemm(n, a.bufs + k * nn, a.bufs + k * nn, a.bufs + (k + 1) * nn, 1.0, false), sm, cta, G);
+        if (!dtile::grid_barrier(gs, epoch, G)) return;
     }
     // C_new = C E^(2^s)
-    run_tiles(sq_gemm(n, a.C, a.bufs + s * nn, a.Cnew, 1.0, false), sm);
+    run_tiles(sq_gemm(n, a.C, a.bufs + s * nn, a.Cnew, 1.0, false), sm, cta, G);
+}
+
+__global__ void __launch_bounds__(dtile::THREADS) rotate_coop_kernel(const CoopArgs a) {
+    extern __shared__ __align__(16) double sm[];
+    rotate_body(a, blockIdx.x, gridDim.x, sm);
+}
+
+static_assert(sizeof(CoopState) <= GROUP_STATE_BYTES, "rotation state slot too small");
+
+// Grouped form: the rotations of several jobs in one cooperative launch, job j
+// on CTAs [cta0, cta0 + ctas) with its own barrier state.  A CTA that lies in
+// several jobs' ranges (only jobs with ctas == 1 share CTAs) runs them in order.
+__global__ void __launch_bounds__(dtile::THREADS) rotate_grouped_kernel(const RotJob* __restrict__ jobs, int njobs) {
+    extern __shared__ __align__(16) double sm[];
+    const int cta = blockIdx.x;
+    for (int j = 0; j < njobs; ++j) {
+        const int c0 = jobs[j].cta0, cn = jobs[j].ctas;
+        if (cta < c0 || cta >= c0 + cn) continue;
+        const RotJob r = jobs[j];
+        if (r.skip != nullptr && *r.skip != 0) continue;
+        const long long nn = (long long)r.nbf * r.nbf;
+        CoopArgs a{};
+        a.y = r.y; a.nbf = r.nbf; a.nbf5 = r.nbf5; a.C = r.C; a.Cnew = r.Cnew;
+        a.cs = static_cast<CoopState*>(r.state);
+        a.Y = r.work;
+        a.X2 = a.Y + nn; a.X3 = a.Y + 2 * nn; a.X4 = a.Y + 3 * nn; a.P = a.Y + 4 * nn;
+        a.bufs = a.Y + 5 * nn;
+        a.E1 = a.bufs + (SMAX + 1) * nn;
+        rotate_body(a, cta - c0, cn, sm);
+        __syncthreads();
+    }
 }
 
 }  // namespace
+
+size_t rotate_work_doubles(int nbf) { return (size_t)nbf * nbf * (5 + SMAX + 2); }
+
+int rotate_grouped(donof_ctx* ctx, cudaStream_t st, const RotJob* jobs, int njobs, void* states, int grid) {
+    const int smem = (int)sizeof(double) * dtile::smem_doubles<RT_TN>();
+    static std::atomic<unsigned long long> attr_mask{0};
+    const unsigned long long bit = 1ull << (ctx->device & 63);
+    if (!(attr_mask.load(std::memory_order_acquire) & bit)) {
+        DONOF_CUDA(ctx, cudaFuncSetAttribute(rotate_grouped_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        attr_mask.fetch_or(bit, std::memory_order_acq_rel);
+    }
+    if (grid < 1 || grid > ctx->sm_count) {
+        set_error(ctx, "rotate_grouped: %d CTAs (1..%d allowed)", grid, ctx->sm_count);
+        return DONOF_ERR_ARG;
+    }
+    DONOF_CUDA(ctx, cudaMemsetAsync(states, 0, (size_t)GROUP_STATE_BYTES * njobs, st));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(dtile::THREADS);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    DONOF_CUDA(ctx, cudaLaunchKernelEx(&cfg, rotate_grouped_kernel, jobs, njobs));
+    count_launch();
+    return DONOF_OK;
+}
 
 int rotate_f64(donof_ctx* ctx, cudaStream_t st, const double* y, int nbf, int nbf5,
                const double* C, double* Cnew) {

@@ -43,9 +43,9 @@ struct TailArgs {
     TailState* ts;
 };
 
-__global__ void __launch_bounds__(dtile::THREADS) elag_tail_kernel(const TailArgs a) {
-    extern __shared__ __align__(16) double sm[];
-    const int nbf = a.nbf, nbf5 = a.nbf5, G = gridDim.x, cta = blockIdx.x, tid = threadIdx.x;
+// The whole tail of one job on CTAs cta = 0..G-1 (of a cooperative launch).
+__device__ __forceinline__ void tail_body(const TailArgs& a, int cta, int G, double* sm) {
+    const int nbf = a.nbf, nbf5 = a.nbf5, tid = threadIdx.x;
     const long long ny = (long long)nbf * nbf5;
     dtile::GridSync* gs = &a.ts->gs;
     unsigned epoch = 0;
@@ -147,12 +147,12 @@ __global__ void __launch_bounds__(dtile::THREADS) elag_tail_kernel(const TailArg
         for (long long i = z0 + (long long)cta * dtile::THREADS + tid; i < zn; i += (long long)G * dtile::THREADS)
             a.elag[i] = 0.0;
     }
-    if (!dtile::grid_barrier(gs, epoch)) return;
+    if (!dtile::grid_barrier(gs, epoch, G)) return;
 
     // ---- stage 2: Bp = HC diag(n) + Y
     for (long long i = (long long)cta * dtile::THREADS + tid; i < ny; i += (long long)G * dtile::THREADS)
         a.Bp[i] = a.HC[i] * a.n[i / nbf] + a.Y[i];
-    if (!dtile::grid_barrier(gs, epoch)) return;
+    if (!dtile::grid_barrier(gs, epoch, G)) return;
 
     // ---- stage 3: H_mat = C^T HC, elag[:, :nbf5] = C^T Bp
     dtile::Gemm gh;
@@ -197,7 +197,65 @@ __global__ void __launch_bounds__(dtile::THREADS) elag_tail_kernel(const TailArg
     }
 }
 
+__global__ void __launch_bounds__(dtile::THREADS) elag_tail_kernel(const TailArgs a) {
+    extern __shared__ __align__(16) double sm[];
+    tail_body(a, blockIdx.x, gridDim.x, sm);
+}
+
+static_assert(sizeof(TailState) <= GROUP_STATE_BYTES, "tail state slot too small");
+
+// Grouped form: the tails of several jobs in one cooperative launch, job j on
+// CTAs [cta0, cta0 + ctas) with its own barrier state (as rotate_grouped_kernel).
+__global__ void __launch_bounds__(dtile::THREADS) tail_grouped_kernel(const TailJob* __restrict__ jobs, int njobs) {
+    extern __shared__ __align__(16) double sm[];
+    const int cta = blockIdx.x;
+    for (int j = 0; j < njobs; ++j) {
+        const int c0 = jobs[j].cta0, cn = jobs[j].ctas;
+        if (cta < c0 || cta >= c0 + cn) continue;
+        const TailJob t = jobs[j];
+        if (t.skip != nullptr && *t.skip != 0) continue;
+        const long long ny = (long long)t.nbf * t.nbf5;
+        TailArgs a{};
+        a.C = t.C; a.H = t.H; a.n = t.n;
+        a.nbf = t.nbf; a.nbf5 = t.nbf5;
+        a.part = t.part; a.part_f32 = t.part_f32; a.nparts = t.nparts; a.pstride = t.pstride;
+        a.ts = static_cast<TailState*>(t.state);
+        a.Y = t.work; a.HC = a.Y + ny; a.Bp = a.HC + ny;
+        a.Hmat = t.Hmat; a.elag = t.elag; a.E = t.E;
+        tail_body(a, cta - c0, cn, sm);
+        __syncthreads();
+    }
+}
+
 }  // namespace
+
+int tail_grouped(donof_ctx* ctx, cudaStream_t st, const TailJob* jobs, int njobs, void* states, int grid) {
+    const int smem = (int)sizeof(double) * dtile::smem_doubles<TL_TN>();
+    static std::atomic<unsigned long long> attr_mask{0};
+    const unsigned long long bit = 1ull << (ctx->device & 63);
+    if (!(attr_mask.load(std::memory_order_acquire) & bit)) {
+        DONOF_CUDA(ctx, cudaFuncSetAttribute(tail_grouped_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        attr_mask.fetch_or(bit, std::memory_order_acq_rel);
+    }
+    if (grid < 1 || grid > ctx->sm_count) {
+        set_error(ctx, "tail_grouped: %d CTAs (1..%d allowed)", grid, ctx->sm_count);
+        return DONOF_ERR_ARG;
+    }
+    DONOF_CUDA(ctx, cudaMemsetAsync(states, 0, (size_t)GROUP_STATE_BYTES * njobs, st));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(dtile::THREADS);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    DONOF_CUDA(ctx, cudaLaunchKernelEx(&cfg, tail_grouped_kernel, jobs, njobs));
+    count_launch();
+    return DONOF_OK;
+}
 
 int elag_tail_f64(donof_job* job, cudaStream_t st, const double* C, const double* H, const double* n, int nbf5,
                   const void* part, bool part_f32, int nparts, long long pstride, double* Hmat, double* elag,

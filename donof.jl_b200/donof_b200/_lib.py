@@ -79,6 +79,11 @@ SIGNATURES = {
     "donof_mixed_tmp_dev": (_i, [_vp, _vp, _i, _vp]),
     "donof_orbopt": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _i, _i, _i, _dp, _ip, ct.c_double, _vp, _dp,
                           _ip, _ip]),
+    "donof_batch_create": (_i, [_vp, _i, _vp, ct.POINTER(_vp)]),
+    "donof_batch_destroy": (_i, [_vp]),
+    "donof_batch_device_bytes": (ct.c_size_t, [_vp]),
+    "donof_batch_orbopt": (_i, [_vp, _i, _vp]),
+    "donof_batch_lagrange2": (_i, [_vp, _vp, _vp, _vp, _vp]),
 }
 
 

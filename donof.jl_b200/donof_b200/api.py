@@ -309,6 +309,81 @@ def orbopt_dev(method: str, n, cj12, ck12, H, C, b: BTensor, p: Param, alpha: fl
     return E.value, nit.value, bool(ok.value), a.value, ml.value
 
 
+class _BatchShape(ct.Structure):
+    _fields_ = [("job", ct.c_void_p), ("nbf5", ct.c_int), ("nalpha", ct.c_int), ("nbeta", ct.c_int)]
+
+
+class _BatchItem(ct.Structure):
+    _fields_ = [("n", ct.c_void_p), ("cj12", ct.c_void_p), ("ck12", ct.c_void_p), ("H", ct.c_void_p),
+                ("C", ct.c_void_p), ("alpha", ct.c_double), ("maxloop", ct.c_int), ("threshgorb", ct.c_double),
+                ("E", ct.c_double), ("nit", ct.c_int), ("success", ct.c_int)]
+
+
+class Batch:
+    """Several jobs optimised together (donof_batch_*): every gradient step of
+    all jobs runs as one grouped launch per stage, the loop as one captured
+    graph.  ``jobs`` are FP64 BTensors of one context, ``params`` the matching
+    Param objects (nbf5, nalpha, nbeta are read).  DoNOF.jl optimises one
+    molecule per call; each job here gives what ``orbopt_dev`` gives alone."""
+
+    def __init__(self, jobs, params, ctx: Optional[Context] = None):
+        if len(jobs) != len(params) or not jobs:
+            raise ValueError("one Param per job, at least one job")
+        self.ctx = ctx or jobs[0].ctx
+        self.jobs, self.params = list(jobs), list(params)
+        shapes = (_BatchShape * len(jobs))()
+        for s, b, p in zip(shapes, jobs, params):
+            s.job, s.nbf5, s.nalpha, s.nbeta = b.handle.value if hasattr(b.handle, "value") else b.handle, \
+                p.nbf5, p.nalpha, p.nbeta
+        h = ct.c_void_p()
+        self.ctx.check(self.ctx.lib.donof_batch_create(self.ctx.handle, len(jobs), shapes, ct.byref(h)))
+        self.handle = h
+
+    def __len__(self):
+        return len(self.jobs)
+
+    def device_bytes(self) -> int:
+        return int(self.ctx.lib.donof_batch_device_bytes(self.handle))
+
+    def _items(self, n, cj12, ck12, H, C, alpha=None, maxloop=None, threshgorb=None):
+        items = (_BatchItem * len(self.jobs))()
+        for j, it in enumerate(items):
+            it.n, it.cj12, it.ck12, it.H, it.C = (_ptr(x[j]) for x in (n, cj12, ck12, H, C))
+            if alpha is not None:
+                it.alpha, it.maxloop, it.threshgorb = float(alpha[j]), int(maxloop[j]), float(threshgorb[j])
+        return items
+
+    def orbopt(self, method: str, n, cj12, ck12, H, C, alpha, maxloop, threshgorb):
+        """Optimiser loop of every job; per-job lists of CUDA tensors (Julia
+        layout; C updated in place) and scalars.  Returns one
+        (E, nit, success, alpha, maxloop) tuple per job."""
+        items = self._items(n, cj12, ck12, H, C, alpha, maxloop, threshgorb)
+        self.ctx.check(self.ctx.lib.donof_batch_orbopt(self.handle, _lib.ORB_METHODS[method], items))
+        return [(it.E, it.nit, bool(it.success), it.alpha, it.maxloop) for it in items]
+
+    def lagrange2(self, n, cj12, ck12, H, C, elag, Hmat):
+        """compute_Lagrange2 of every job at C[j] into elag[j], Hmat[j] (CUDA
+        tensors); returns the E_elec of each job."""
+        items = self._items(n, cj12, ck12, H, C)
+        k = len(self.jobs)
+        pe = (ct.c_void_p * k)(*[_ptr(x) for x in elag])
+        ph = (ct.c_void_p * k)(*[_ptr(x) for x in Hmat])
+        E = (ct.c_double * k)()
+        self.ctx.check(self.ctx.lib.donof_batch_lagrange2(self.handle, items, pe, ph, E))
+        return list(E)
+
+    def free(self) -> None:
+        if getattr(self, "handle", None) and getattr(self.ctx, "handle", None):
+            self.ctx.lib.donof_batch_destroy(self.handle)
+        self.handle = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
 def transform_dev(C, b: BTensor, nbf5: int, out=None, precision=None):
     """b_pq^l = C5^T b_l C5 on the device (out: CUDA tensor or None)."""
     prec = b.precision if precision is None else _prec(precision)

@@ -83,6 +83,31 @@ def molecule_like(nbf: int = 256, naux: int = 1024, nbeta: int = 16, ncwo: int =
     return Workload(p, b, C, H, gamma, n, np.asfortranarray(cj12), np.asfortranarray(ck12))
 
 
+def b_device(nbf: int, naux: int, seed: int, device="cuda"):
+    """The RI tensor of ``make_b``'s distribution generated on the GPU (seeded
+    torch generator): a CUDA tensor of shape (naux, nbf, nbf) holding b[m, n, l]
+    in Julia's column-major order, for workloads too large to build on the host."""
+    import torch
+
+    g = torch.Generator(device=device)
+    g.manual_seed(int(seed))
+    raw = torch.randn((naux, nbf, nbf), generator=g, device=device, dtype=torch.float64) * (1.0 / np.sqrt(naux))
+    raw += raw.transpose(1, 2).clone()
+    raw *= 0.5
+    return raw.contiguous()
+
+
+def water_clusters(count: int = 64, kmax: int = 8, seed: int = 11) -> list:
+    """Shapes of a batch of (H2O)_k clusters, k uniform in 1..kmax (seeded), as
+    molecule-shaped surrogates of cc-pVDZ with its JK-fit set: nbf = 24k,
+    naux = 116k, nbeta = 5k, ncwo = 3 (nbf5 = 20k).  b is not built here
+    (``b_device``); each entry is (k, Workload without b)."""
+    rng = np.random.default_rng(seed)
+    ks = rng.integers(1, kmax + 1, size=count)
+    return [(int(k), synthetic(nbf=24 * int(k), naux=116 * int(k), nbeta=5 * int(k), ncwo=3,
+                               seed=seed * 1000 + j, with_b=False)) for j, k in enumerate(ks)]
+
+
 # Named workloads (sizes of the molecule-shaped surrogates: nbf, naux, nbeta, ncwo)
 CONFIGS = {
     "water-ccpvdz-surrogate": dict(nbf=24, naux=116, nbeta=5, ncwo=3),

@@ -188,6 +188,52 @@ int donof_orbopt_dev(donof_job* job, int method, const double* n, const double* 
                      double* alpha, int* maxloop, double threshgorb, double* C_inout, double* E,
                      int* nit, int* success);
 
+/* --- grouped orbital optimiser over a batch of jobs --------------------------
+ * The orbital optimiser above (orbopt_adam / _adabelief / _yogi / _demon,
+ * src/minimization.jl:242-630, plain FP64 form) run for several molecules at
+ * once: each gradient step of all jobs is one grouped launch per stage (the
+ * three-index transforms and the Lagrangian GEMM as grouped persistent tensor-
+ * core kernels over a work list spanning every job, the rotation and the
+ * Lagrangian tail as grouped cooperative kernels), and the whole loop is one
+ * captured CUDA graph that repeats the step until every job has met its own
+ * stopping rule.  DoNOF.jl optimises one molecule per call; each job here
+ * gives what donof_orbopt_dev gives for it alone (same iterations, same
+ * stopping decisions, results within 1e-10).
+ * donof_batch_create fixes the jobs (each with its FP64 RI tensor uploaded by
+ * donof_b_upload / donof_b_attach on the same device) and their sizes, and
+ * allocates the batch's device scratch (donof_batch_device_bytes).  The first
+ * call times the tile shapes of the grouped GEMMs on the batch's operands (the
+ * batch's autotuner) and captures the loop graph; make it outside any stream
+ * capture.  Calls of one batch must not overlap.                             */
+typedef struct donof_batch donof_batch;
+typedef struct {
+    donof_job* job;   /* RI tensor b of this instance (nbf, naux from the job) */
+    int nbf5, nalpha, nbeta;
+} donof_batch_shape;
+/* Per-job inputs and outputs, all arrays in DEVICE memory (layouts as above). */
+typedef struct {
+    const double* n;      /* nbf5 occupations */
+    const double* cj12;   /* nbf5 x nbf5 */
+    const double* ck12;   /* nbf5 x nbf5 */
+    const double* H;      /* nbf x nbf core Hamiltonian */
+    double* C;            /* nbf x nbf: start orbitals in, optimised orbitals out (orbopt) */
+    double alpha;         /* in/out, as *alpha of donof_orbopt */
+    int maxloop;          /* in/out, as *maxloop of donof_orbopt */
+    double threshgorb;    /* in */
+    double E;             /* out: E_elec */
+    int nit, success;     /* out */
+} donof_batch_item;
+int donof_batch_create(donof_ctx* ctx, int count, const donof_batch_shape* shapes, donof_batch** batch);
+int donof_batch_destroy(donof_batch* batch);
+size_t donof_batch_device_bytes(const donof_batch* batch);
+/* Optimiser loop of every job (items[j] for shapes[j]); returns when all ended. */
+int donof_batch_orbopt(donof_batch* batch, int method, donof_batch_item* items);
+/* compute_Lagrange2 (src/utils.jl:1-59) of every job at items[j].C in one
+ * grouped evaluation: elag[j] (nbf x nbf) and H_mat[j] (nbf x nbf5) device
+ * arrays (or NULL), E[j] = E_elec on the host (E may be NULL).               */
+int donof_batch_lagrange2(donof_batch* batch, const donof_batch_item* items, double* const* elag,
+                          double* const* H_mat, double* E);
+
 /* --- occupation layer and occupation optimiser (host, FP64) ------------------
  * Native host code, no GPU: DoNOF.jl runs this part on the host too.
  * Sizes and switches of the GNOF occupation layer (names of src/param.jl):

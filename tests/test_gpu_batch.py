@@ -1,0 +1,160 @@
+"""Grouped multi-job path (donof_batch_*): several molecules of different sizes
+advance together, one grouped launch per stage of a gradient step.
+
+Checks, through the C ABI:
+  * the grouped Lagrangian of every job against the CPU oracle (<= 1e-10) and
+    against the single-job FP64 path;
+  * the grouped optimiser loop against each job optimised alone with
+    donof_orbopt_dev (same iteration counts, stopping decisions and step
+    back-off; energies and orbitals within 1e-10 / 1e-8) and against the
+    oracle's loop;
+  * a job's result is bit-for-bit the same alone (a batch of one) and in the
+    mix, whatever else the batch holds.
+"""
+import numpy as np
+import pytest
+
+from oracle import gnof as ognof
+from oracle import native, orbital
+
+import donof_b200 as d
+
+from test_gpu_parity import case, rel
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-10
+
+# water-cluster and alkane surrogates of different sizes, an open shell, odd sizes
+SHAPES = [
+    dict(nbf=24, naux=116, nbeta=5, ncwo=3, seed=1),
+    dict(nbf=48, naux=232, nbeta=10, ncwo=1, seed=2),
+    dict(nbf=13, naux=29, nbeta=3, ncwo=3, seed=3),
+    dict(nbf=20, naux=17, nbeta=3, ncwo=3, nalpha=5, seed=4),
+    dict(nbf=96, naux=120, nbeta=6, ncwo=3, seed=5),
+    dict(nbf=72, naux=348, nbeta=15, ncwo=3, seed=6),
+]
+
+
+def device_inputs(cases):
+    import torch  # noqa: F401
+
+    out = []
+    for p, b, C, H, n, cj, ck in cases:
+        out.append(dict(p=p, b=b, C=C, H=H, n=n, cj=cj, ck=ck, tC=d.to_device(C), tH=d.to_device(H),
+                        tn=d.to_device(n), tcj=d.to_device(cj), tck=d.to_device(ck)))
+    return out
+
+
+def make_batch(ctx, inputs):
+    bts = [d.eris_to_gpu(x["b"], "fp64", ctx) for x in inputs]
+    return d.Batch(bts, [x["p"] for x in inputs], ctx), bts
+
+
+def test_batch_lagrange2_matches_oracle_and_single_job(cuda_ctx):
+    import torch
+
+    inputs = device_inputs([case(**kw) for kw in SHAPES])
+    batch, bts = make_batch(cuda_ctx, inputs)
+    elag = [torch.zeros(x["p"].nbf, x["p"].nbf, dtype=torch.float64, device="cuda") for x in inputs]
+    hmat = [torch.zeros(x["p"].nbf5, x["p"].nbf, dtype=torch.float64, device="cuda") for x in inputs]
+    E = batch.lagrange2([x["tn"] for x in inputs], [x["tcj"] for x in inputs], [x["tck"] for x in inputs],
+                        [x["tH"] for x in inputs], [x["tC"] for x in inputs], elag, hmat)
+    torch.cuda.synchronize()
+    for j, x in enumerate(inputs):
+        p = x["p"]
+        e_ref, h_ref = native.lagrange2(x["C"], x["n"], x["H"], x["b"], x["cj"], x["ck"], p.nalpha, p.nbeta)
+        e, h = d.from_device(elag[j]), d.from_device(hmat[j])
+        assert rel(h, h_ref) <= TOL, j
+        assert rel(e, e_ref) <= TOL, j
+        assert np.all(e[:, p.nbf5:] == 0.0)
+        E_ref = orbital.e_elec(h_ref, x["n"], e_ref, p.nbf5)
+        assert abs(E[j] - E_ref) <= TOL * max(1.0, abs(E_ref)), j
+        # the single-job FP64 path at the same C
+        e1, h1, E1 = d.compute_Lagrange2(x["C"], x["n"], x["H"], bts[j], x["cj"], x["ck"], p.nalpha, p.nbeta,
+                                         return_energy=True)
+        assert np.array_equal(h, h1), j  # H_mat has no split-K sum: identical
+        assert rel(e, e1) <= 1e-12, j
+        assert abs(E[j] - E1) <= 1e-12 * max(1.0, abs(E1)), j
+    batch.free()
+    for b in bts:
+        b.free()
+
+
+def run_alone(ctx, x, method, alpha, maxloop, thresh):
+    bt = d.eris_to_gpu(x["b"], "fp64", ctx)
+    C = x["tC"].clone()
+    E, nit, ok, a, ml = d.orbopt_dev(method, x["tn"], x["tcj"], x["tck"], x["tH"], C, bt, x["p"], alpha, maxloop,
+                                     thresh)
+    bt.free()
+    return E, nit, ok, a, ml, d.from_device(C)
+
+
+@pytest.mark.parametrize("method", ["ADAM", "Demon"])
+def test_batch_orbopt_matches_each_job_alone(cuda_ctx, method):
+    inputs = device_inputs([case(**kw) for kw in SHAPES])
+    batch, bts = make_batch(cuda_ctx, inputs)
+    k = len(inputs)
+    # different step sizes, loop lengths and thresholds per job: the jobs stop at
+    # different iterations, some on the gradient rule, some on maxloop
+    alpha = [0.01, 0.02, 0.01, 0.005, 0.01, 0.02]
+    maxloop = [6, 9, 3, 12, 5, 8]
+    thresh = [1e-4, 1e-1, 1e-4, 1.0, 1e-4, 1e-4]
+    Cs = [x["tC"].clone() for x in inputs]
+    res = batch.orbopt(method, [x["tn"] for x in inputs], [x["tcj"] for x in inputs], [x["tck"] for x in inputs],
+                       [x["tH"] for x in inputs], Cs, alpha, maxloop, thresh)
+    for j, x in enumerate(inputs):
+        E0, nit0, ok0, a0, ml0, C0 = run_alone(cuda_ctx, x, method, alpha[j], maxloop[j], thresh[j])
+        E, nit, ok, a, ml = res[j]
+        assert (nit, ok, a, ml) == (nit0, ok0, a0, ml0), (j, res[j], (E0, nit0, ok0, a0, ml0))
+        assert abs(E - E0) <= TOL * max(1.0, abs(E0)), j
+        # the two paths split the Lagrangian GEMM's K range differently; the AMSGrad
+        # step divides by sqrt(v), so the last-bit differences of the gradients grow
+        # over the iterations (up to 12 here): orbitals within 1e-8
+        assert rel(d.from_device(Cs[j]), C0) <= 1e-8, j
+    batch.free()
+    for b in bts:
+        b.free()
+
+
+def test_batch_orbopt_matches_oracle_loop(cuda_ctx):
+    kws = [SHAPES[0], SHAPES[2], dict(nbf=48, naux=60, nbeta=4, ncwo=3, seed=4)]
+    inputs = device_inputs([case(**kw) for kw in kws])
+    batch, bts = make_batch(cuda_ctx, inputs)
+    Cs = [x["tC"].clone() for x in inputs]
+    res = batch.orbopt("YOGI", [x["tn"] for x in inputs], [x["tcj"] for x in inputs], [x["tck"] for x in inputs],
+                       [x["tH"] for x in inputs], Cs, [0.01] * 3, [6] * 3, [1e-4] * 3)
+    for j, x in enumerate(inputs):
+        p = x["p"]
+        s = ognof.Sizes(nbf=p.nbf, nbeta=p.nbeta, nalpha=p.nalpha, ncwo=p.ncwo, naux=p.nbfaux)
+        E0, C0, nit0, ok0, a0, ml0 = orbital.orbopt("YOGI", x["n"], x["cj"], x["ck"], x["C"], x["H"], x["b"], s,
+                                                    0.01, 6, 1e-4)
+        E, nit, ok, a, ml = res[j]
+        assert (nit, ok, a, ml) == (nit0, ok0, a0, ml0), j
+        assert abs(E - E0) <= TOL * max(1.0, abs(E0)), j
+        assert rel(d.from_device(Cs[j]), C0) <= 1e-9, j
+    batch.free()
+    for b in bts:
+        b.free()
+
+
+def test_batch_result_same_alone_and_in_the_mix(cuda_ctx):
+    inputs = device_inputs([case(**kw) for kw in SHAPES])
+    target = 4  # nbf 96
+    args = lambda xs: ([x["tn"] for x in xs], [x["tcj"] for x in xs], [x["tck"] for x in xs], [x["tH"] for x in xs])
+    one, bt1 = make_batch(cuda_ctx, [inputs[target]])
+    C1 = [inputs[target]["tC"].clone()]
+    r1 = one.orbopt("ADAM", *args([inputs[target]]), C1, [0.01], [7], [1e-4])
+    mix, btm = make_batch(cuda_ctx, inputs)
+    Cm = [x["tC"].clone() for x in inputs]
+    rm = mix.orbopt("ADAM", *args(inputs), Cm, [0.01] * len(inputs), [7] * len(inputs), [1e-4] * len(inputs))
+    assert r1[0] == rm[target]
+    assert np.array_equal(d.from_device(C1[0]), d.from_device(Cm[target]))
+    # a second call of the same batch (graph replayed) gives the same again
+    Cm2 = [x["tC"].clone() for x in inputs]
+    rm2 = mix.orbopt("ADAM", *args(inputs), Cm2, [0.01] * len(inputs), [7] * len(inputs), [1e-4] * len(inputs))
+    assert rm2 == rm
+    assert all(np.array_equal(d.from_device(a), d.from_device(b)) for a, b in zip(Cm, Cm2))
+    for o in (one, mix):
+        o.free()
+    for b in bt1 + btm:
+        b.free()
