@@ -137,51 +137,64 @@ struct GemmF64Cfg {
     static_assert(BK % 4 == 0, "BK must be a multiple of 4");
 };
 
-// One output tile (bx, by) of batch/split index bz = z * splits + split: the
-// whole body of gemm_f64_kernel, shared with the grouped persistent kernel
-// below (same staging, same MMA order, so both write identical results).
+// One output tile (bx, by) of batch/split index bz = z * splits + split, in
+// four steps that a kernel can interleave across tiles: init (operands,
+// extents, gates), prologue (the first STAGES - 1 cp.async stages, one commit
+// group each), mainloop (acc += A B over the tile's K range) and epilogue
+// (alpha, beta, column-major store).  gemm_f64_kernel runs them in order for
+// its one tile; the grouped persistent kernel issues the next tile's prologue
+// before the current tile's epilogue.  Both use the same staging and MMA order,
+// so they write identical results.
 template <int BM, int BN, int BK, int WARPS_M, int WARPS_N, int STAGES, bool AK, bool BKM, bool VEC>
-__device__ __forceinline__ void gemm_f64_tile(const GemmF64Args& p, int bx, int by, int bz, double* smem) {
+struct GemmTileF64 {
     using Cfg = GemmF64Cfg<BM, BN, BK, WARPS_M, WARPS_N, STAGES, AK, BKM, VEC>;
-    constexpr int KS = gemm_detail::kMmaK;
+    static constexpr int KS = gemm_detail::kMmaK;
     static_assert(BK % KS == 0, "BK must be a multiple of the MMA depth");
+    using Acc = double[Cfg::MI][Cfg::NI][4];
 
-    const int tid = threadIdx.x;
-    const int lane = tid & 31;
-    const int warp = tid >> 5;
-    const int wm = warp % WARPS_M;
-    const int wn = warp / WARPS_M;
-    const int g = lane >> 2;  // groupID
-    const int t = lane & 3;   // threadID_in_group
+    const double* A;
+    const double* B;
+    double* Cout;
+    long long lda, ldb, ldc;
+    double alpha, beta;
+    int M, N, m0, n0, kbeg, kend, nk;
+    bool use_beta, skip;
 
-    const int z = bz / p.splits;
-    const int split = bz % p.splits;
-    const int m0 = bx * BM;
-    const int n0 = by * BN;
-    const int kbeg = split * p.kchunk;
-    const int kend = min(p.K, kbeg + p.kchunk);
-    const double* __restrict__ A = p.A + (long long)z * p.strideA;
-    const double* __restrict__ B = (p.B_ptr != nullptr ? *p.B_ptr : p.B) + (long long)z * p.strideB;
-    double* __restrict__ Cout = p.C + (long long)z * p.strideC +
-                                (p.splits > 1 ? (long long)split * p.strideSplit : 0LL);
+    __device__ __forceinline__ void init(const GemmF64Args& p, int bx, int by, int bz) {
+        const int z = bz / p.splits;
+        const int split = bz % p.splits;
+        m0 = bx * BM;
+        n0 = by * BN;
+        kbeg = split * p.kchunk;
+        kend = min(p.K, kbeg + p.kchunk);
+        nk = (kend > kbeg) ? (kend - kbeg + BK - 1) / BK : 0;
+        A = p.A + (long long)z * p.strideA;
+        B = (p.B_ptr != nullptr ? *p.B_ptr : p.B) + (long long)z * p.strideB;
+        Cout = p.C + (long long)z * p.strideC + (p.splits > 1 ? (long long)split * p.strideSplit : 0LL);
+        lda = p.lda; ldb = p.ldb; ldc = p.ldc;
+        M = p.M; N = p.N;
+        alpha = p.alpha; beta = p.beta;
+        use_beta = (p.splits == 1) && (p.beta != 0.0);
+        skip = (p.skip_le != nullptr && *p.skip_le <= p.skip_level) || (p.skip_nz != nullptr && *p.skip_nz != 0);
+    }
 
-    if (p.skip_le != nullptr && *p.skip_le <= p.skip_level) return;
-    if (p.skip_nz != nullptr && *p.skip_nz != 0) return;
+    static __device__ __forceinline__ double* As(double* smem, int s) { return smem + (size_t)s * Cfg::STAGE_ELEMS; }
+    static __device__ __forceinline__ double* Bs(double* smem, int s) {
+        return smem + (size_t)s * Cfg::STAGE_ELEMS + Cfg::A_ELEMS;
+    }
 
-    auto As = [&](int s) { return smem + (size_t)s * Cfg::STAGE_ELEMS; };
-    auto Bs = [&](int s) { return smem + (size_t)s * Cfg::STAGE_ELEMS + Cfg::A_ELEMS; };
-
-    auto load_tile = [&](int stage, int k0) {
-        double* as = As(stage);
-        double* bs = Bs(stage);
+    __device__ __forceinline__ void load(double* smem, int stage, int k0) const {
+        const int tid = threadIdx.x;
+        double* as = As(smem, stage);
+        double* bs = Bs(smem, stage);
         // ---- A tile: BM x BK
         if constexpr (AK) {
             constexpr int CPR = BK / Cfg::VW;  // copies per row
             for (int c = tid; c < BM * CPR; c += Cfg::THREADS) {
                 const int i = c / CPR, kk = (c % CPR) * Cfg::VW;
                 const int gi = m0 + i, gk = k0 + kk;
-                const bool ok = (gi < p.M) && (gk < kend);
-                const double* src = ok ? (A + (long long)gi * p.lda + gk) : A;
+                const bool ok = (gi < M) && (gk < kend);
+                const double* src = ok ? (A + (long long)gi * lda + gk) : A;
                 gemm_detail::cp_async<8 * Cfg::VW>(as + i * Cfg::SA + kk, src, ok);
             }
         } else {
@@ -189,8 +202,8 @@ __device__ __forceinline__ void gemm_f64_tile(const GemmF64Args& p, int bx, int 
             for (int c = tid; c < BK * CPR; c += Cfg::THREADS) {
                 const int kk = c / CPR, i = (c % CPR) * Cfg::VW;
                 const int gi = m0 + i, gk = k0 + kk;
-                const bool ok = (gi < p.M) && (gk < kend);
-                const double* src = ok ? (A + gi + (long long)gk * p.lda) : A;
+                const bool ok = (gi < M) && (gk < kend);
+                const double* src = ok ? (A + gi + (long long)gk * lda) : A;
                 gemm_detail::cp_async<8 * Cfg::VW>(as + kk * Cfg::SA + i, src, ok);
             }
         }
@@ -200,8 +213,8 @@ __device__ __forceinline__ void gemm_f64_tile(const GemmF64Args& p, int bx, int 
             for (int c = tid; c < BN * CPR; c += Cfg::THREADS) {
                 const int j = c / CPR, kk = (c % CPR) * Cfg::VW;
                 const int gj = n0 + j, gk = k0 + kk;
-                const bool ok = (gj < p.N) && (gk < kend);
-                const double* src = ok ? (B + gk + (long long)gj * p.ldb) : B;
+                const bool ok = (gj < N) && (gk < kend);
+                const double* src = ok ? (B + gk + (long long)gj * ldb) : B;
                 gemm_detail::cp_async<8 * Cfg::VW>(bs + j * Cfg::SB + kk, src, ok);
             }
         } else {
@@ -209,98 +222,114 @@ __device__ __forceinline__ void gemm_f64_tile(const GemmF64Args& p, int bx, int 
             for (int c = tid; c < BK * CPR; c += Cfg::THREADS) {
                 const int kk = c / CPR, j = (c % CPR) * Cfg::VW;
                 const int gj = n0 + j, gk = k0 + kk;
-                const bool ok = (gj < p.N) && (gk < kend);
-                const double* src = ok ? (B + (long long)gk * p.ldb + gj) : B;
+                const bool ok = (gj < N) && (gk < kend);
+                const double* src = ok ? (B + (long long)gk * ldb + gj) : B;
                 gemm_detail::cp_async<8 * Cfg::VW>(bs + kk * Cfg::SB + j, src, ok);
             }
         }
-    };
-
-    double acc[Cfg::MI][Cfg::NI][4];
-#pragma unroll
-    for (int a = 0; a < Cfg::MI; ++a)
-#pragma unroll
-        for (int b = 0; b < Cfg::NI; ++b)
-#pragma unroll
-            for (int e = 0; e < 4; ++e) acc[a][b][e] = 0.0;
-
-    const int nk = (kend > kbeg) ? (kend - kbeg + BK - 1) / BK : 0;
-
-#pragma unroll
-    for (int s = 0; s < STAGES - 1; ++s) {
-        if (s < nk) load_tile(s, kbeg + s * BK);
-        gemm_detail::cp_async_commit();
     }
 
-    const int wrow = wm * Cfg::WTM;
-    const int wcol = wn * Cfg::WTN;
-
-    for (int kt = 0; kt < nk; ++kt) {
-        gemm_detail::cp_async_wait<STAGES - 2>();
-        __syncthreads();
-        {
-            const int nt = kt + STAGES - 1;
-            if (nt < nk) load_tile(nt % STAGES, kbeg + nt * BK);
+    __device__ __forceinline__ void prologue(double* smem) const {
+#pragma unroll
+        for (int s = 0; s < STAGES - 1; ++s) {
+            if (s < nk) load(smem, s, kbeg + s * BK);
             gemm_detail::cp_async_commit();
         }
-        const double* as = As(kt % STAGES);
-        const double* bs = Bs(kt % STAGES);
+    }
+
+    __device__ __forceinline__ void mainloop(double* smem, Acc& acc) const {
+        const int lane = threadIdx.x & 31;
+        const int warp = threadIdx.x >> 5;
+        const int g = lane >> 2;  // groupID
+        const int t = lane & 3;   // threadID_in_group
+        const int wrow = (warp % WARPS_M) * Cfg::WTM;
+        const int wcol = (warp / WARPS_M) * Cfg::WTN;
 #pragma unroll
-        for (int kk = 0; kk < BK; kk += KS) {
-            double af[Cfg::MI][KS / 2];
-            double bf[Cfg::NI][KS / 4];
+        for (int a = 0; a < Cfg::MI; ++a)
 #pragma unroll
-            for (int a = 0; a < Cfg::MI; ++a) {
+            for (int b = 0; b < Cfg::NI; ++b)
 #pragma unroll
-                for (int e = 0; e < KS / 2; ++e) {
-                    const int r = wrow + a * 16 + g + 8 * (e & 1);
-                    const int k = kk + t + 4 * (e >> 1);
-                    af[a][e] = AK ? as[r * Cfg::SA + k] : as[k * Cfg::SA + r];
-                }
+                for (int e = 0; e < 4; ++e) acc[a][b][e] = 0.0;
+        for (int kt = 0; kt < nk; ++kt) {
+            gemm_detail::cp_async_wait<STAGES - 2>();
+            __syncthreads();
+            {
+                const int nt = kt + STAGES - 1;
+                if (nt < nk) load(smem, nt % STAGES, kbeg + nt * BK);
+                gemm_detail::cp_async_commit();
             }
+            const double* as = As(smem, kt % STAGES);
+            const double* bs = Bs(smem, kt % STAGES);
+#pragma unroll
+            for (int kk = 0; kk < BK; kk += KS) {
+                double af[Cfg::MI][KS / 2];
+                double bf[Cfg::NI][KS / 4];
+#pragma unroll
+                for (int a = 0; a < Cfg::MI; ++a) {
+#pragma unroll
+                    for (int e = 0; e < KS / 2; ++e) {
+                        const int r = wrow + a * 16 + g + 8 * (e & 1);
+                        const int k = kk + t + 4 * (e >> 1);
+                        af[a][e] = AK ? as[r * Cfg::SA + k] : as[k * Cfg::SA + r];
+                    }
+                }
+#pragma unroll
+                for (int b = 0; b < Cfg::NI; ++b) {
+                    const int cidx = wcol + b * 8 + g;
+#pragma unroll
+                    for (int e = 0; e < KS / 4; ++e) {
+                        const int k = kk + t + 4 * e;
+                        bf[b][e] = BKM ? bs[cidx * Cfg::SB + k] : bs[k * Cfg::SB + cidx];
+                    }
+                }
+#pragma unroll
+                for (int a = 0; a < Cfg::MI; ++a)
+#pragma unroll
+                    for (int b = 0; b < Cfg::NI; ++b) gemm_detail::mma_f64<KS>(acc[a][b], af[a], bf[b]);
+            }
+        }
+    }
+
+    __device__ __forceinline__ void epilogue(const Acc& acc) const {
+        const int lane = threadIdx.x & 31;
+        const int warp = threadIdx.x >> 5;
+        const int g = lane >> 2;
+        const int t = lane & 3;
+        const int wrow = (warp % WARPS_M) * Cfg::WTM;
+        const int wcol = (warp / WARPS_M) * Cfg::WTN;
+#pragma unroll
+        for (int a = 0; a < Cfg::MI; ++a) {
 #pragma unroll
             for (int b = 0; b < Cfg::NI; ++b) {
-                const int cidx = wcol + b * 8 + g;
 #pragma unroll
-                for (int e = 0; e < KS / 4; ++e) {
-                    const int k = kk + t + 4 * e;
-                    bf[b][e] = BKM ? bs[cidx * Cfg::SB + k] : bs[k * Cfg::SB + cidx];
-                }
-            }
-#pragma unroll
-            for (int a = 0; a < Cfg::MI; ++a)
-#pragma unroll
-                for (int b = 0; b < Cfg::NI; ++b) gemm_detail::mma_f64<KS>(acc[a][b], af[a], bf[b]);
-        }
-    }
-    gemm_detail::cp_async_wait<0>();
-
-    // ---- epilogue
-    const bool use_beta = (p.splits == 1) && (p.beta != 0.0);
-#pragma unroll
-    for (int a = 0; a < Cfg::MI; ++a) {
-#pragma unroll
-        for (int b = 0; b < Cfg::NI; ++b) {
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const int i = m0 + wrow + a * 16 + g + ((e >= 2) ? 8 : 0);
-                const int j = n0 + wcol + b * 8 + 2 * t + (e & 1);
-                if (i < p.M && j < p.N) {
-                    double* dst = Cout + i + (long long)j * p.ldc;
-                    double v = p.alpha * acc[a][b][e];
-                    if (use_beta) v += p.beta * (*dst);
-                    *dst = v;
+                for (int e = 0; e < 4; ++e) {
+                    const int i = m0 + wrow + a * 16 + g + ((e >= 2) ? 8 : 0);
+                    const int j = n0 + wcol + b * 8 + 2 * t + (e & 1);
+                    if (i < M && j < N) {
+                        double* dst = Cout + i + (long long)j * ldc;
+                        double v = alpha * acc[a][b][e];
+                        if (use_beta) v += beta * (*dst);
+                        *dst = v;
+                    }
                 }
             }
         }
     }
-}
+};
 
 template <int BM, int BN, int BK, int WARPS_M, int WARPS_N, int STAGES, bool AK, bool BKM, bool VEC>
 __global__ void __launch_bounds__(32 * WARPS_M * WARPS_N)
 gemm_f64_kernel(const GemmF64Args p) {
     extern __shared__ __align__(16) double smem[];
-    gemm_f64_tile<BM, BN, BK, WARPS_M, WARPS_N, STAGES, AK, BKM, VEC>(p, blockIdx.x, blockIdx.y, blockIdx.z, smem);
+    using Tile = GemmTileF64<BM, BN, BK, WARPS_M, WARPS_N, STAGES, AK, BKM, VEC>;
+    Tile T;
+    T.init(p, blockIdx.x, blockIdx.y, blockIdx.z);
+    if (T.skip) return;
+    typename Tile::Acc acc;
+    T.prologue(smem);
+    T.mainloop(smem, acc);
+    gemm_detail::cp_async_wait<0>();
+    T.epilogue(acc);
 }
 
 // Grouped persistent form: `ngroups` independent GEMMs (one per job of a
@@ -308,22 +337,54 @@ gemm_f64_kernel(const GemmF64Args p) {
 // device-side gates) share one launch.  Group g owns the tiles
 // [start[g], start[g + 1]) of a flat work list (tile t of a group is
 // (bx, by, bz) = (t % gx, (t / gx) % gy, t / (gx gy)) as in the 3-D grid of
-// gemm_f64_kernel); each CTA walks the list with stride gridDim.x.
+// gemm_f64_kernel); each CTA walks the list with stride gridDim.x and starts
+// the cp.async prologue of its next tile before it stores the current one, so
+// the loads of the next tile are in flight during the epilogue (the tiles of
+// the batch's jobs have short K ranges, where the prologue is a large share).
+// CTAs per SM the grouped kernel is compiled for (a register cap): as many as
+// fit without spills: 6 (32 x 32), 3 (64 x 64), 2 (128 x 64).
+template <int BM, int BN, int WARPS_M, int WARPS_N>
+constexpr int grouped_min_ctas() { return BM * BN <= 32 * 32 ? 6 : (WARPS_M * WARPS_N <= 4 ? 3 : 2); }
+
 template <int BM, int BN, int BK, int WARPS_M, int WARPS_N, int STAGES, bool AK, bool BKM, bool VEC>
-__global__ void __launch_bounds__(32 * WARPS_M * WARPS_N)
+__global__ void __launch_bounds__(32 * WARPS_M * WARPS_N, (grouped_min_ctas<BM, BN, WARPS_M, WARPS_N>()))
 gemm_f64_grouped_kernel(const GemmF64Args* __restrict__ groups, const int* __restrict__ start, int ngroups) {
     extern __shared__ __align__(16) double smem[];
+    using Tile = GemmTileF64<BM, BN, BK, WARPS_M, WARPS_N, STAGES, AK, BKM, VEC>;
     const int total = start[ngroups];
     int g = 0;
-    for (int t = blockIdx.x; t < total; t += gridDim.x) {
-        while (g + 1 < ngroups && start[g + 1] <= t) ++g;  // t only grows: advance the group
-        const GemmF64Args p = groups[g];
-        const int lt = t - start[g];
-        const int gx = (p.M + BM - 1) / BM, gy = (p.N + BN - 1) / BN;
-        __syncthreads();  // the previous tile's last shared-memory reads are done
-        gemm_f64_tile<BM, BN, BK, WARPS_M, WARPS_N, STAGES, AK, BKM, VEC>(p, lt % gx, (lt / gx) % gy, lt / (gx * gy),
-                                                                           smem);
+    // next tile at or after t that is not gated off; returns its index (total if none)
+    auto next = [&](int t, Tile& T) {
+        for (; t < total; t += gridDim.x) {
+            while (g + 1 < ngroups && start[g + 1] <= t) ++g;  // t only grows: advance the group
+            const GemmF64Args& p = groups[g];
+            const int lt = t - start[g];
+            const int gx = (p.M + BM - 1) / BM, gy = (p.N + BN - 1) / BN;
+            T.init(p, lt % gx, (lt / gx) % gy, lt / (gx * gy));
+            if (!T.skip) break;
+        }
+        return t;
+    };
+    Tile cur;
+    int t = next(blockIdx.x, cur);
+    if (t >= total) return;
+    cur.prologue(smem);
+    typename Tile::Acc acc;
+    while (true) {
+        cur.mainloop(smem, acc);
+        Tile nxt;
+        const int tn = next(t + gridDim.x, nxt);
+        const bool more = tn < total;
+        if (more) {
+            __syncthreads();  // every warp is done with the stages the prologue overwrites
+            nxt.prologue(smem);
+        }
+        cur.epilogue(acc);
+        if (!more) break;
+        cur = nxt;
+        t = tn;
     }
+    gemm_detail::cp_async_wait<0>();
 }
 
 }  // namespace donof
