@@ -68,11 +68,11 @@ def parse():
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--profile-case", nargs="?", const="synthetic256",
-                    choices=["synthetic256", "octane600", "batch64"],
+                    choices=["synthetic256", "octane600", "batch64", "batch8"],
                     help="run the mixed and FP64 Lagrangian and the rotation three times each and exit (the "
                          "cases the committed ncu captures use): the benchmark workload, or an n-octane-shaped "
                          "job (nbf 202, nbf5 198, naux 600) on the general-shape mixed pipeline; batch64: three "
-                         "grouped orbital steps of the 64-job water-cluster batch")
+                         "grouped orbital steps of the 64-job water-cluster batch; batch8: the same for its first 8 jobs")
     return ap.parse_args()
 
 
@@ -364,16 +364,17 @@ def serving_bench(d, torch):
 BATCH = dict(count=64, kmax=8, seed=11)
 
 
-def batched_bench(d, torch, ctx, steps, warmup, method, sequential_arm=True):
+def batched_bench(d, torch, ctx, steps, warmup, method, sequential_arm=True, spec=None):
     """Orbital-gradient steps/s of a batch of uneven jobs advanced together (one
     grouped launch per stage of a step, the loop as one captured graph) against
     the same jobs run one after the other through the single-job device loop:
     64 water-cluster surrogates (H2O)_k, k uniform in 1..8 (nbf 24-192), FP64."""
     from donof_b200 import workload
-    jobs = workload.water_clusters(**BATCH)
+    spec = spec or BATCH
+    jobs = workload.water_clusters(**spec)
     bts, ins = [], []
     for j, (k, wl) in enumerate(jobs):
-        tb = workload.b_device(wl.p.nbf, wl.p.nbfaux, seed=BATCH["seed"] * 7919 + j)
+        tb = workload.b_device(wl.p.nbf, wl.p.nbfaux, seed=spec["seed"] * 7919 + j)
         bts.append(d.eris_to_gpu(tb, "fp64", ctx))
         ins.append(dict(p=wl.p, C=d.to_device(wl.C), H=d.to_device(wl.H), n=d.to_device(wl.n),
                         cj=d.to_device(wl.cj12), ck=d.to_device(wl.ck12)))
@@ -416,7 +417,7 @@ def batched_bench(d, torch, ctx, steps, warmup, method, sequential_arm=True):
     sequential(warmup)
     ts, res_s = sequential(steps)
     dE = max(abs(a[0] - b[0]) / max(1.0, abs(b[0])) for a, b in zip(res_g, res_s))
-    out = {"workload": f"{nj} water-cluster surrogates (H2O)_k, k ~ U{{1..{BATCH['kmax']}}} (nbf 24-192, naux 116k, "
+    out = {"workload": f"{nj} water-cluster surrogates (H2O)_k, k ~ U{{1..{spec['kmax']}}} (nbf 24-192, naux 116k, "
                        f"nbf5 20k), FP64, {steps} orbital steps each",
            "ks": [k for k, _ in jobs], "unit": "job orbital-gradient steps/s",
            "grouped": {"value": nj * steps / tg, "ms_per_step": 1e3 * tg / steps, "launches_per_step": lg / steps,
@@ -426,6 +427,62 @@ def batched_bench(d, torch, ctx, steps, warmup, method, sequential_arm=True):
                           "path": "donof_orbopt_dev per job, one after the other"},
            "speedup": ts / tg, "max_rel_dE_grouped_vs_sequential": dE,
            "device_bytes": batch.device_bytes()}
+    batch.free()
+    for b in bts:
+        b.free()
+    return out
+
+
+BATCH_E = dict(count=16, kmax=4, seed=13, thresh=1e-6)
+
+
+def batched_energies_bench(d, torch, ctx):
+    """Converged GNOF energies/s of a batch of water-cluster-shaped molecules
+    (k uniform in 1..4: nbf 24-96), FP64: every job's energy loop with the
+    orbital optimisations of all running jobs grouped per outer iteration
+    (donof_batch_energy), against the same jobs through donof_energy one after
+    the other; both from the same start to the same thresholds."""
+    from donof_b200 import workload
+    from donof_b200.gnof import guess_gamma
+    rng = np.random.default_rng(BATCH_E["seed"])
+    ks = [int(k) for k in rng.integers(1, BATCH_E["kmax"] + 1, size=BATCH_E["count"])]
+    th = BATCH_E["thresh"]
+
+    def make(j, k):
+        wl = workload.molecule_like(nbf=24 * k, naux=116 * k, nbeta=5 * k, ncwo=3, seed=BATCH_E["seed"] * 100 + j,
+                                    two_e_scale=0.2)
+        wl.p.threshgorb = wl.p.threshgocc = th
+        wl.p.threshen = th / 1e4
+        return wl
+
+    wls = [make(j, k) for j, k in enumerate(ks)]
+    g0 = [guess_gamma(wl.p) for wl in wls]
+    bts = [d.eris_to_gpu(wl.b, "fp64", ctx) for wl in wls]
+    fresh = lambda: [make(j, k).p for j, k in enumerate(ks)]
+    # warm-up (autotuning, graph capture, scratch) of both arms
+    batch = d.Batch(bts, fresh(), ctx)
+    batch.energy([wl.H for wl in wls], [wl.C for wl in wls], g0, maxit=1)
+    for wl, bt, p, g in zip(wls, bts, fresh(), g0):
+        d.api.energy_loop(wl.H, bt, p, wl.C, g, maxit=1)
+    torch.cuda.synchronize()
+    batch.params = fresh()
+    t0 = time.perf_counter()
+    rb = batch.energy([wl.H for wl in wls], [wl.C for wl in wls], g0, maxit=1000)
+    tb = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    rs = [d.api.energy_loop(wl.H, bt, p, wl.C, g, maxit=1000)[4] for wl, bt, p, g in zip(wls, bts, fresh(), g0)]
+    ts = time.perf_counter() - t0
+    dEs = sorted(abs(a[3]["E_elec"] - b["E_elec"]) for a, b in zip(rb, rs))
+    out = {"workload": f"{len(ks)} water-cluster-shaped molecule surrogates (H2O)_k, k ~ U{{1..{BATCH_E['kmax']}}} "
+                       f"(nbf 24-96, naux 116k), FP64, max|g_orb|, |g_occ| < {th}",
+           "ks": ks, "unit": "energies/s",
+           "grouped": {"value": len(ks) / tb, "seconds": tb, "converged": sum(r[3]["converged"] for r in rb),
+                       "outer_iterations": [r[3]["iterations"] for r in rb],
+                       "path": "donof_batch_energy (orbital loops of all running jobs grouped per outer iteration)"},
+           "sequential": {"value": len(ks) / ts, "seconds": ts, "converged": sum(r["converged"] for r in rs),
+                          "path": "donof_energy per job, one after the other"},
+           "speedup": ts / tb, "abs_dE_Eh": {"median": dEs[len(dEs) // 2], "max": dEs[-1],
+                                              "within_1uEh": sum(x <= 1e-6 for x in dEs)}}
     batch.free()
     for b in bts:
         b.free()
@@ -484,8 +541,9 @@ def main():
     wl = workload.synthetic(**WORKLOAD, seed=SEED)
     p = wl.p
     ctx = d.Context(local)
-    if args.profile_case == "batch64":
-        print(json.dumps(batched_bench(d, torch, ctx, 3, 1, args.method, sequential_arm=False)), flush=True)
+    if args.profile_case in ("batch64", "batch8"):
+        spec = dict(BATCH, count=8) if args.profile_case == "batch8" else BATCH
+        print(json.dumps(batched_bench(d, torch, ctx, 3, 1, args.method, sequential_arm=False, spec=spec)), flush=True)
         return
     if args.profile_case:
         if args.profile_case == "octane600":
@@ -630,9 +688,10 @@ def main():
     if rank == 0 and world == 1 and not args.no_serving:
         serving = serving_bench(d, torch)
 
-    batched = None
+    batched = batched_e = None
     if rank == 0 and world == 1 and not args.no_batched:
         batched = batched_bench(d, torch, ctx, args.steps, args.warmup, args.method)
+        batched_e = batched_energies_bench(d, torch, ctx)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -654,6 +713,7 @@ def main():
             line["serving"] = serving
         if batched is not None:
             line["batched"] = batched
+            line["batched_energies"] = batched_e
         print(json.dumps(line), flush=True)
     bt.free()
     ctx.close()

@@ -134,6 +134,7 @@ __global__ void __launch_bounds__(256) b_copy_kernel(const BJob* __restrict__ jo
         const int j = job_of(pre, njobs, u);
         const BJob& J = jobs[j];
         const long long k0 = (long long)(u - pre[j]) * CH, k1 = min(J.nn, k0 + CH);
+        if (J.S->stopped) continue;  // jobs left out of the call, and jobs that have stopped
         if (mode == COPY_IN_TO_NEW) {
             for (long long k = k0 + threadIdx.x; k < k1; k += blockDim.x) J.Cnew[k] = J.Cin[k];
         } else if (mode == COPY_NEW_TO_CUR_BEST) {
@@ -143,7 +144,6 @@ __global__ void __launch_bounds__(256) b_copy_kernel(const BJob* __restrict__ jo
                 J.Cbest[k] = c;
             }
         } else {
-            if (J.S->stopped) continue;
             const bool best = J.S->improved_now != 0;
             for (long long k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
                 const double c = J.Cnew[k];
@@ -570,8 +570,8 @@ int check_items(donof_batch* B, const donof_batch_item* items, bool orbopt) {
             set_error(ctx, "batch item %d: null device pointer", j);
             return DONOF_ERR_ARG;
         }
-        if (orbopt && it.maxloop < 1) {
-            set_error(ctx, "batch item %d: maxloop must be >= 1", j);
+        if (orbopt && it.maxloop < 0) {
+            set_error(ctx, "batch item %d: maxloop must be >= 0", j);
             return DONOF_ERR_ARG;
         }
     }
@@ -877,6 +877,7 @@ int donof_batch_orbopt(donof_batch* B, int method, donof_batch_item* items) {
         hs[j].alpha = items[j].alpha;
         hs[j].thresh = items[j].threshgorb;
         hs[j].maxloop = items[j].maxloop;
+        hs[j].stopped = (items[j].maxloop == 0) ? 1 : 0;  // left out of this call
     }
     DONOF_CHECK(start_call(B, st, items, hs));
     DONOF_CHECK(gradient(B, st));
@@ -948,6 +949,7 @@ int donof_batch_orbopt(donof_batch* B, int method, donof_batch_item* items) {
     // back-off and result of each job, as the single-job loop (src/minimization.jl:425-437)
     for (int j = 0; j < nj; ++j) {
         donof_batch_item& it = items[j];
+        if (it.maxloop == 0) continue;
         if (!hs[j].improved) {
             it.alpha = 0.3 * it.alpha;
             it.maxloop = it.maxloop + 10;
@@ -960,6 +962,70 @@ int donof_batch_orbopt(donof_batch* B, int method, donof_batch_item* items) {
         it.success = hs[j].success;
     }
     DONOF_CUDA(ctx, cudaStreamSynchronize(st));
+    return DONOF_OK;
+}
+
+int donof_batch_energy(donof_batch* B, donof_energy_params* params, const double* const* H, double* const* C_inout,
+                       double* const* gamma_inout, double* const* n_out, donof_energy_result* results) {
+    if (!B) return DONOF_ERR_ARG;
+    donof_ctx* ctx = B->ctx;
+    if (!params || !H || !C_inout || !gamma_inout || !results) {
+        set_error(ctx, "donof_batch_energy: null argument");
+        return DONOF_ERR_ARG;
+    }
+    const int nj = B->nj;
+    const int method = params[0].orb_method;
+    for (int j = 0; j < nj; ++j) {
+        const donof_batch::Shape& h = B->sh[j];
+        const donof_energy_params& q = params[j];
+        if (!H[j] || !C_inout[j] || !gamma_inout[j]) {
+            set_error(ctx, "donof_batch_energy: job %d: null array", j);
+            return DONOF_ERR_ARG;
+        }
+        if (q.occ.nbf5 != h.nbf5 || q.occ.nalpha != h.nalpha || q.occ.nbeta != h.nbeta) {
+            set_error(ctx, "donof_batch_energy: job %d: nbf5/nalpha/nbeta differ from the batch's shape", j);
+            return DONOF_ERR_ARG;
+        }
+        if (q.orb_method != method) {
+            set_error(ctx, "donof_batch_energy: every job of a call uses the same orbital optimiser");
+            return DONOF_ERR_ARG;
+        }
+        if (h.job->precision != DONOF_PREC_FP64) {
+            set_error(ctx, "donof_batch_energy: job %d is not in the FP64 form", j);
+            return DONOF_ERR_ARG;
+        }
+    }
+    std::vector<EnergyJob> E(nj);
+    for (int j = 0; j < nj; ++j)
+        DONOF_CHECK(E[j].setup(B->sh[j].job, &params[j], H[j], C_inout[j], gamma_inout[j], nullptr));
+    std::vector<donof_batch_item> items(nj);
+    for (;;) {
+        bool any = false;
+        for (int j = 0; j < nj; ++j) {
+            donof_batch_item& it = items[j];
+            it.n = E[j].dev_n(); it.cj12 = E[j].dev_cj(); it.ck12 = E[j].dev_ck(); it.H = E[j].dev_H();
+            it.C = E[j].dev_C();
+            it.alpha = params[j].alpha;
+            it.threshgorb = params[j].threshgorb;
+            it.maxloop = 0;  // left out unless running
+            if (E[j].done()) continue;
+            DONOF_CHECK(E[j].begin());
+            // the job's coefficient upload is on its own context's stream
+            DONOF_CUDA(ctx, cudaStreamSynchronize(B->sh[j].job->ctx->stream));
+            it.maxloop = params[j].maxloop;
+            any = true;
+        }
+        if (!any) break;
+        DONOF_CHECK(donof_batch_orbopt(B, method, items.data()));
+        for (int j = 0; j < nj; ++j) {
+            if (items[j].maxloop == 0) continue;
+            params[j].alpha = items[j].alpha;
+            params[j].maxloop = items[j].maxloop;
+            DONOF_CHECK(E[j].after_orbopt(items[j].E, items[j].nit));
+        }
+    }
+    for (int j = 0; j < nj; ++j)
+        DONOF_CHECK(E[j].finish(C_inout[j], gamma_inout[j], n_out ? n_out[j] : nullptr, nullptr, &results[j]));
     return DONOF_OK;
 }
 

@@ -61,7 +61,6 @@ struct Loop {
     donof_job* job;
     donof_ctx* ctx;
     cudaStream_t st;
-    const donof::occ::Occ& o;
     int nbf, N, nalpha, nbeta, prec;
     Dev D;
 
@@ -168,22 +167,49 @@ void order_subspaces(const donof::occ::Occ& o, const std::vector<double>& ed, st
 
 }  // namespace
 
-}  // namespace donof
-
-using namespace donof;
-
-extern "C" int donof_energy(donof_job* job, donof_energy_params* prm, const double* H, double* C_inout,
-                            double* gamma_inout, double* n_out, double* elag_out, double* history,
-                            donof_energy_result* res) {
-    if (!job || !prm || !H || !C_inout || !gamma_inout || !res) return DONOF_ERR_ARG;
-    donof_ctx* ctx = job->ctx;
+// One job's pass through DoNOF.energy's alternation (see the file header):
+// setup, then per outer iteration begin() (the occupations of gamma on the
+// device), the orbital optimisation of D.C at them, after_orbopt() (occoptr,
+// ordering, convergence; sets done), and finish() once done.  donof_energy
+// drives one with the single-job optimiser; donof_batch_energy (batch.cu)
+// drives several, with the orbital optimisation of all of them as one grouped
+// call.
+struct EnergyJob::Impl {
+    donof_job* job = nullptr;
+    donof_energy_params* prm = nullptr;
     donof::occ::Occ o;
-    if (!donof::occ::setup(&prm->occ, o) || prm->occ.nbf5 > job->nbf || prm->maxit < 1 || prm->maxloop < 1 ||
+    Loop L{};
+    double* history = nullptr;
+    std::vector<double> gamma, dn, n, cj, ck, n_occ, cj_occ, ck_occ, J, K, Hc, gocc;
+    std::vector<int> perm;
+    double E = 9999.0, E_old = 9999.0, gorb = 0.0, gocc_norm = 0.0;
+    int it = 1, tot_orb = 0, tot_occ = 0, converged = 0;
+    bool done = false;
+};
+
+EnergyJob::EnergyJob() : p(new Impl) {}
+EnergyJob::~EnergyJob() { delete p; }
+bool EnergyJob::done() const { return p->done; }
+const double* EnergyJob::dev_n() const { return p->L.D.n; }
+const double* EnergyJob::dev_cj() const { return p->L.D.cj; }
+const double* EnergyJob::dev_ck() const { return p->L.D.ck; }
+const double* EnergyJob::dev_H() const { return p->L.D.H; }
+double* EnergyJob::dev_C() const { return p->L.D.C; }
+
+int EnergyJob::setup(donof_job* job, donof_energy_params* prm, const double* H, const double* C,
+                     const double* gamma_in, double* history) {
+    Impl& S = *p;
+    donof_ctx* ctx = job->ctx;
+    if (!donof::occ::setup(&prm->occ, S.o) || prm->occ.nbf5 > job->nbf || prm->maxit < 1 || prm->maxloop < 1 ||
         prm->orb_method < DONOF_ORB_ADAM || prm->orb_method > DONOF_ORB_DEMON) {
         set_error(ctx, "donof_energy: invalid sizes, switches, maxit or maxloop");
         return DONOF_ERR_ARG;
     }
     DONOF_CUDA(ctx, cudaSetDevice(ctx->device));
+    S.job = job;
+    S.prm = prm;
+    S.history = history;
+    const donof::occ::Occ& o = S.o;
     const int nbf = job->nbf, N = o.N, nv = o.nv;
     const size_t nn = (size_t)nbf * nbf, n55 = (size_t)N * N;
     const long long nvar = nvar_of(nbf, N);
@@ -195,113 +221,152 @@ extern "C" int donof_energy(donof_job* job, donof_energy_params* prm, const doub
                  og = take(8 * (size_t)nvar), ogm = take(8), op = take(sizeof(int) * (size_t)nbf);
     DONOF_CHECK(job->drv.ensure(ctx, off));
     char* base = job->drv.as<char>();
-    Loop L{job, ctx, ctx->stream, o, nbf, N, prm->occ.nalpha, prm->occ.nbeta, job->precision, {}};
-    L.D.H = (double*)(base + oH);
-    L.D.C = (double*)(base + oC);
-    L.D.C2 = (double*)(base + oC2);
-    L.D.n = (double*)(base + on);
-    L.D.cj = (double*)(base + ocj);
-    L.D.ck = (double*)(base + ock);
-    L.D.elag = (double*)(base + oel);
-    L.D.Hmat = (double*)(base + oHm);
-    L.D.E = (double*)(base + oE);
-    L.D.J = (double*)(base + oJ);
-    L.D.K = (double*)(base + oK);
-    L.D.Hc = (double*)(base + oHc);
-    L.D.g = (double*)(base + og);
-    L.D.gmax = (unsigned long long*)(base + ogm);
-    L.D.perm = (int*)(base + op);
+    S.L = Loop{job, ctx, ctx->stream, nbf, N, prm->occ.nalpha, prm->occ.nbeta, job->precision, {}};
+    Dev& D = S.L.D;
+    D.H = (double*)(base + oH);
+    D.C = (double*)(base + oC);
+    D.C2 = (double*)(base + oC2);
+    D.n = (double*)(base + on);
+    D.cj = (double*)(base + ocj);
+    D.ck = (double*)(base + ock);
+    D.elag = (double*)(base + oel);
+    D.Hmat = (double*)(base + oHm);
+    D.E = (double*)(base + oE);
+    D.J = (double*)(base + oJ);
+    D.K = (double*)(base + oK);
+    D.Hc = (double*)(base + oHc);
+    D.g = (double*)(base + og);
+    D.gmax = (unsigned long long*)(base + ogm);
+    D.perm = (int*)(base + op);
+    DONOF_CUDA(ctx, cudaMemcpyAsync(D.H, H, 8 * nn, cudaMemcpyHostToDevice, S.L.st));
+    DONOF_CUDA(ctx, cudaMemcpyAsync(D.C, C, 8 * nn, cudaMemcpyHostToDevice, S.L.st));
+    S.gamma.assign(gamma_in, gamma_in + nv);
+    S.dn.assign((size_t)N * (nv > 0 ? nv : 1), 0.0);
+    S.n.assign(N, 0.0); S.n_occ.assign(N, 0.0);
+    S.cj.assign(n55, 0.0); S.ck.assign(n55, 0.0); S.cj_occ.assign(n55, 0.0); S.ck_occ.assign(n55, 0.0);
+    S.J.assign(n55, 0.0); S.K.assign(n55, 0.0); S.Hc.assign(N, 0.0);
+    S.gocc.assign(nv > 0 ? nv : 1, 0.0);
+    S.perm.assign(nbf, 0);
+    donof::occ::occupations(o, S.gamma.data(), S.n.data(), S.dn.data());
+    donof::occ::coupling(o, S.n.data(), S.cj.data(), S.ck.data());
+    return DONOF_OK;
+}
+
+int EnergyJob::begin() { return p->L.put_coef(p->n, p->cj, p->ck); }
+
+int EnergyJob::after_orbopt(double E_orb, int nit_orb) {
+    Impl& S = *p;
+    Loop& L = S.L;
+    const donof::occ::Occ& o = S.o;
+    donof_energy_params* prm = S.prm;
+    donof_ctx* ctx = L.ctx;
     cudaStream_t st = L.st;
-    DONOF_CUDA(ctx, cudaMemcpyAsync(L.D.H, H, 8 * nn, cudaMemcpyHostToDevice, st));
-    DONOF_CUDA(ctx, cudaMemcpyAsync(L.D.C, C_inout, 8 * nn, cudaMemcpyHostToDevice, st));
-
-    std::vector<double> gamma(gamma_inout, gamma_inout + nv), dn((size_t)N * (nv > 0 ? nv : 1));
-    std::vector<double> n(N), cj(n55), ck(n55), n_occ(N), cj_occ(n55), ck_occ(n55);
-    std::vector<double> J(n55), K(n55), Hc(N), gocc(nv > 0 ? nv : 1);
-    std::vector<int> perm(nbf);
-    donof::occ::occupations(o, gamma.data(), n.data(), dn.data());
-    donof::occ::coupling(o, n.data(), cj.data(), ck.data());
-
-    double E = 9999.0, E_old = 9999.0, gorb = 0.0, gocc_norm = 0.0;
-    int it = 0, tot_orb = 0, tot_occ = 0, converged = 0;
-    for (it = 1; it <= prm->maxit; ++it) {
-        // ---- orbopt at the occupations of gamma
-        DONOF_CHECK(L.put_coef(n, cj, ck));
-        double E_orb = 0.0;
-        int nit_orb = 0, ok_orb = 0;
-        DONOF_CHECK(orbopt_run(job, prm->orb_method, L.D.n, L.D.cj, L.D.ck, L.D.H, N, L.nalpha, L.nbeta,
-                               &prm->alpha, &prm->maxloop, prm->threshgorb, L.D.C, &E_orb, &nit_orb, &ok_orb,
-                               L.prec));
-        // ---- occoptr
-        int nit_occ = 0;
-        if (o.ndoc > 0 && !prm->freeze_occ) {
-            DONOF_CHECK(L.jkh(J, K, Hc));
-            double E_occ = 0.0;
-            int conv = 0;
-            DONOF_CHECK(donof::occ::cg(o, J.data(), K.data(), Hc.data(), gamma.data(), prm->threshen, 1000, &E_occ,
-                                       &nit_occ, &conv));
-            if (nit_occ < 1) prm->maxloop += 10;
-        }
-        donof::occ::occupations(o, gamma.data(), n_occ.data(), dn.data());
-        donof::occ::coupling(o, n_occ.data(), cj_occ.data(), ck_occ.data());
-        // ---- order_occupations_softmax
-        if (o.method == 0 && order_softmax(o, gamma, perm)) DONOF_CHECK(L.permute(perm));
-        tot_orb += nit_orb;
-        tot_occ += nit_occ;
-        E = E_orb;
-        const double E_diff = E - E_old;
-        E_old = E;
-        // ---- convergence: orbital gradient at the new occupations, occupation gradient
-        donof::occ::occupations(o, gamma.data(), n.data(), dn.data());
-        donof::occ::coupling(o, n.data(), cj.data(), ck.data());
-        DONOF_CHECK(L.put_coef(n, cj, ck));
-        DONOF_CHECK(L.lagrangian());
-        DONOF_CUDA(ctx, cudaMemsetAsync(L.D.gmax, 0, sizeof(unsigned long long), st));
-        DONOF_CHECK(pack_grad(ctx, st, L.D.elag, nbf, N, L.D.g, L.D.gmax));
-        unsigned long long gbits = 0;
-        DONOF_CUDA(ctx, cudaMemcpyAsync(&gbits, L.D.gmax, sizeof(gbits), cudaMemcpyDeviceToHost, st));
-        DONOF_CHECK(L.jkh(J, K, Hc));  // synchronises the stream
-        memcpy(&gorb, &gbits, sizeof(double));
-        donof::occ::energy_grad(o, gamma.data(), J.data(), K.data(), Hc.data(), gocc.data());
-        double s2 = 0.0;
-        for (int k = 0; k < nv; ++k) s2 += gocc[k] * gocc[k];
-        gocc_norm = sqrt(s2);
-        if (history) {
-            double* h = history + 6 * (size_t)(it - 1);
-            h[0] = E; h[1] = E_diff; h[2] = gorb; h[3] = gocc_norm; h[4] = nit_orb; h[5] = nit_occ;
-        }
-        if (gorb < prm->threshgorb && gocc_norm < prm->threshgocc) {
-            converged = 1;
-            break;
-        }
-        if (prm->stop_rel_de > 0.0 && it > 1 && fabs(E_diff) <= prm->stop_rel_de * fabs(E)) break;
+    const int nv = o.nv;
+    // ---- occoptr
+    int nit_occ = 0;
+    if (o.ndoc > 0 && !prm->freeze_occ) {
+        DONOF_CHECK(L.jkh(S.J, S.K, S.Hc));
+        double E_occ = 0.0;
+        int conv = 0;
+        DONOF_CHECK(donof::occ::cg(o, S.J.data(), S.K.data(), S.Hc.data(), S.gamma.data(), prm->threshen, 1000,
+                                   &E_occ, &nit_occ, &conv));
+        if (nit_occ < 1) prm->maxloop += 10;
     }
-    if (it > prm->maxit) it = prm->maxit;
-    // ---- ENERGY1r of the last iteration: elag at (C, occupations before the ordering)
-    DONOF_CHECK(L.put_coef(n_occ, cj_occ, ck_occ));
+    donof::occ::occupations(o, S.gamma.data(), S.n_occ.data(), S.dn.data());
+    donof::occ::coupling(o, S.n_occ.data(), S.cj_occ.data(), S.ck_occ.data());
+    // ---- order_occupations_softmax
+    if (o.method == 0 && order_softmax(o, S.gamma, S.perm)) DONOF_CHECK(L.permute(S.perm));
+    S.tot_orb += nit_orb;
+    S.tot_occ += nit_occ;
+    S.E = E_orb;
+    const double E_diff = S.E - S.E_old;
+    S.E_old = S.E;
+    // ---- convergence: orbital gradient at the new occupations, occupation gradient
+    donof::occ::occupations(o, S.gamma.data(), S.n.data(), S.dn.data());
+    donof::occ::coupling(o, S.n.data(), S.cj.data(), S.ck.data());
+    DONOF_CHECK(L.put_coef(S.n, S.cj, S.ck));
     DONOF_CHECK(L.lagrangian());
-    if (prm->order_subspaces) {
+    DONOF_CUDA(ctx, cudaMemsetAsync(L.D.gmax, 0, sizeof(unsigned long long), st));
+    DONOF_CHECK(pack_grad(ctx, st, L.D.elag, L.nbf, L.N, L.D.g, L.D.gmax));
+    unsigned long long gbits = 0;
+    DONOF_CUDA(ctx, cudaMemcpyAsync(&gbits, L.D.gmax, sizeof(gbits), cudaMemcpyDeviceToHost, st));
+    DONOF_CHECK(L.jkh(S.J, S.K, S.Hc));  // synchronises the stream
+    memcpy(&S.gorb, &gbits, sizeof(double));
+    donof::occ::energy_grad(o, S.gamma.data(), S.J.data(), S.K.data(), S.Hc.data(), S.gocc.data());
+    double s2 = 0.0;
+    for (int k = 0; k < nv; ++k) s2 += S.gocc[k] * S.gocc[k];
+    S.gocc_norm = sqrt(s2);
+    if (S.history) {
+        double* h = S.history + 6 * (size_t)(S.it - 1);
+        h[0] = S.E; h[1] = E_diff; h[2] = S.gorb; h[3] = S.gocc_norm; h[4] = nit_orb; h[5] = nit_occ;
+    }
+    if (S.gorb < prm->threshgorb && S.gocc_norm < prm->threshgocc) {
+        S.converged = 1;
+        S.done = true;
+    } else if (prm->stop_rel_de > 0.0 && S.it > 1 && fabs(E_diff) <= prm->stop_rel_de * fabs(S.E)) {
+        S.done = true;
+    } else if (S.it >= prm->maxit) {
+        S.done = true;
+    } else {
+        ++S.it;
+    }
+    return DONOF_OK;
+}
+
+int EnergyJob::finish(double* C_out, double* gamma_out, double* n_out, double* elag_out, donof_energy_result* res) {
+    Impl& S = *p;
+    Loop& L = S.L;
+    donof_ctx* ctx = L.ctx;
+    cudaStream_t st = L.st;
+    const int nbf = L.nbf, N = L.N;
+    const size_t nn = (size_t)nbf * nbf;
+    // ---- ENERGY1r of the last iteration: elag at (C, occupations before the ordering)
+    DONOF_CHECK(L.put_coef(S.n_occ, S.cj_occ, S.ck_occ));
+    DONOF_CHECK(L.lagrangian());
+    if (S.prm->order_subspaces) {
         std::vector<double> el(nn), ed(N);
         DONOF_CUDA(ctx, cudaMemcpyAsync(el.data(), L.D.elag, 8 * nn, cudaMemcpyDeviceToHost, st));
         DONOF_CUDA(ctx, cudaStreamSynchronize(st));
         for (int i = 0; i < N; ++i) ed[i] = el[i + (size_t)nbf * i];
-        order_subspaces(o, ed, n, perm);
-        DONOF_CHECK(L.permute(perm));
-        donof::occ::coupling(o, n.data(), cj.data(), ck.data());
-        DONOF_CHECK(L.put_coef(n, cj, ck));
+        order_subspaces(S.o, ed, S.n, S.perm);
+        DONOF_CHECK(L.permute(S.perm));
+        donof::occ::coupling(S.o, S.n.data(), S.cj.data(), S.ck.data());
+        DONOF_CHECK(L.put_coef(S.n, S.cj, S.ck));
         DONOF_CHECK(L.lagrangian());
     }
-    DONOF_CUDA(ctx, cudaMemcpyAsync(C_inout, L.D.C, 8 * nn, cudaMemcpyDeviceToHost, st));
+    DONOF_CUDA(ctx, cudaMemcpyAsync(C_out, L.D.C, 8 * nn, cudaMemcpyDeviceToHost, st));
     if (elag_out) DONOF_CUDA(ctx, cudaMemcpyAsync(elag_out, L.D.elag, 8 * nn, cudaMemcpyDeviceToHost, st));
     DONOF_CUDA(ctx, cudaStreamSynchronize(st));
-    std::copy(gamma.begin(), gamma.end(), gamma_inout);
-    if (n_out) std::copy(n.begin(), n.end(), n_out);
-    res->E_elec = E;
-    res->iterations = it;
-    res->converged = converged;
-    res->tot_it_orb = tot_orb;
-    res->tot_it_occ = tot_occ;
-    res->max_grad_orb = gorb;
-    res->norm_grad_occ = gocc_norm;
+    std::copy(S.gamma.begin(), S.gamma.end(), gamma_out);
+    if (n_out) std::copy(S.n.begin(), S.n.end(), n_out);
+    res->E_elec = S.E;
+    res->iterations = S.it;
+    res->converged = S.converged;
+    res->tot_it_orb = S.tot_orb;
+    res->tot_it_occ = S.tot_occ;
+    res->max_grad_orb = S.gorb;
+    res->norm_grad_occ = S.gocc_norm;
     return DONOF_OK;
+}
+
+}  // namespace donof
+
+using namespace donof;
+
+extern "C" int donof_energy(donof_job* job, donof_energy_params* prm, const double* H, double* C_inout,
+                            double* gamma_inout, double* n_out, double* elag_out, double* history,
+                            donof_energy_result* res) {
+    if (!job || !prm || !H || !C_inout || !gamma_inout || !res) return DONOF_ERR_ARG;
+    EnergyJob E;
+    DONOF_CHECK(E.setup(job, prm, H, C_inout, gamma_inout, history));
+    while (!E.done()) {
+        DONOF_CHECK(E.begin());
+        double E_orb = 0.0;
+        int nit_orb = 0, ok_orb = 0;
+        DONOF_CHECK(orbopt_run(job, prm->orb_method, E.dev_n(), E.dev_cj(), E.dev_ck(), E.dev_H(), prm->occ.nbf5,
+                               prm->occ.nalpha, prm->occ.nbeta, &prm->alpha, &prm->maxloop, prm->threshgorb,
+                               E.dev_C(), &E_orb, &nit_orb, &ok_orb, job->precision));
+        DONOF_CHECK(E.after_orbopt(E_orb, nit_orb));
+    }
+    return E.finish(C_inout, gamma_inout, n_out, elag_out, res);
 }

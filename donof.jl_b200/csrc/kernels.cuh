@@ -129,6 +129,34 @@ struct TailJob {
 };
 int tail_grouped(donof_ctx* ctx, cudaStream_t st, const TailJob* jobs, int njobs, void* states, int grid);
 
+// One job through DoNOF.energy's orbital / occupation alternation (energy.cu),
+// driven step by step: setup; while !done(): begin() (the occupations of the
+// current gamma to dev_n/dev_cj/dev_ck), the orbital optimisation of dev_C at
+// them, after_orbopt(E, iterations); then finish().  donof_energy runs it with
+// the single-job optimiser, donof_batch_energy with the grouped one.
+class EnergyJob {
+public:
+    EnergyJob();
+    ~EnergyJob();
+    EnergyJob(const EnergyJob&) = delete;
+    EnergyJob& operator=(const EnergyJob&) = delete;
+    int setup(donof_job* job, donof_energy_params* prm, const double* H, const double* C, const double* gamma,
+              double* history);
+    int begin();
+    int after_orbopt(double E_orb, int nit_orb);
+    int finish(double* C_out, double* gamma_out, double* n_out, double* elag_out, donof_energy_result* res);
+    bool done() const;
+    const double* dev_n() const;
+    const double* dev_cj() const;
+    const double* dev_ck() const;
+    const double* dev_H() const;
+    double* dev_C() const;
+
+private:
+    struct Impl;
+    Impl* p;
+};
+
 // Orbital-gradient helpers (optim.cu): g = pack(4 elag - 4 elag^T); when
 // maxabs != nullptr also atomically max-reduces |g| into it (must be zeroed).
 int pack_grad(donof_ctx* ctx, cudaStream_t st, const double* elag, int nbf, int nbf5, double* g,

@@ -84,6 +84,7 @@ SIGNATURES = {
     "donof_batch_device_bytes": (ct.c_size_t, [_vp]),
     "donof_batch_orbopt": (_i, [_vp, _i, _vp]),
     "donof_batch_lagrange2": (_i, [_vp, _vp, _vp, _vp, _vp]),
+    "donof_batch_energy": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
 }
 
 

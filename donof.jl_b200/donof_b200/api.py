@@ -372,6 +372,32 @@ class Batch:
         self.ctx.check(self.ctx.lib.donof_batch_lagrange2(self.handle, items, pe, ph, E))
         return list(E)
 
+    def energy(self, Hs, Cs, gammas, maxit: Optional[int] = None, order: bool = True):
+        """DoNOF.energy's alternation for every job (donof_batch_energy): each
+        outer iteration runs the orbital optimisation of all jobs still going as
+        one grouped call.  Host (numpy) H, C, gamma per job; updates each job's
+        Param alpha / maxloop.  Returns one (C, gamma, n, result fields) per job."""
+        k = len(self.jobs)
+        prms = (_EnergyParams * k)()
+        for prm, p in zip(prms, self.params):
+            prm.occ = _occ_params(p)
+            prm.orb_method = _lib.ORB_METHODS[p.orb_method]
+            prm.maxit, prm.maxloop, prm.alpha = int(maxit or p.maxit), int(p.maxloop), float(p.alpha)
+            prm.threshgorb, prm.threshgocc, prm.threshen = float(p.threshgorb), float(p.threshgocc), float(p.threshen)
+            prm.order_subspaces = int(bool(order) and p.ipnof > 4)
+        Hf = [_f64(H) for H in Hs]
+        Cio = [np.array(_f64(C), copy=True, order="F") for C in Cs]
+        gio = [np.array(g, dtype=np.float64, copy=True) for g in gammas]
+        ns = [np.zeros(p.nbf5) for p in self.params]
+        arr = lambda xs: (ct.c_void_p * k)(*[_ptr(x) for x in xs])
+        res = (_EnergyResult * k)()
+        self.ctx.check(self.ctx.lib.donof_batch_energy(self.handle, prms, arr(Hf), arr(Cio), arr(gio), arr(ns), res))
+        out = []
+        for j, p in enumerate(self.params):
+            p.alpha, p.maxloop = prms[j].alpha, prms[j].maxloop
+            out.append((Cio[j], gio[j], ns[j], {f: getattr(res[j], f) for f, _ in _EnergyResult._fields_}))
+        return out
+
     def free(self) -> None:
         if getattr(self, "handle", None) and getattr(self.ctx, "handle", None):
             self.ctx.lib.donof_batch_destroy(self.handle)

@@ -226,13 +226,15 @@ typedef struct {
 int donof_batch_create(donof_ctx* ctx, int count, const donof_batch_shape* shapes, donof_batch** batch);
 int donof_batch_destroy(donof_batch* batch);
 size_t donof_batch_device_bytes(const donof_batch* batch);
-/* Optimiser loop of every job (items[j] for shapes[j]); returns when all ended. */
+/* Optimiser loop of every job (items[j] for shapes[j]); returns when all ended.
+ * An item with maxloop = 0 leaves its job out of the call (untouched).       */
 int donof_batch_orbopt(donof_batch* batch, int method, donof_batch_item* items);
 /* compute_Lagrange2 (src/utils.jl:1-59) of every job at items[j].C in one
  * grouped evaluation: elag[j] (nbf x nbf) and H_mat[j] (nbf x nbf5) device
  * arrays (or NULL), E[j] = E_elec on the host (E may be NULL).               */
 int donof_batch_lagrange2(donof_batch* batch, const donof_batch_item* items, double* const* elag,
                           double* const* H_mat, double* E);
+
 
 /* --- occupation layer and occupation optimiser (host, FP64) ------------------
  * Native host code, no GPU: DoNOF.jl runs this part on the host too.
@@ -295,6 +297,16 @@ typedef struct {
 int donof_energy(donof_job* job, donof_energy_params* params, const double* H, double* C_inout,
                  double* gamma_inout, double* n_out, double* elag_out, double* history,
                  donof_energy_result* result);
+/* donof_energy (above) for every job of a batch (donof_batch_create): per outer iteration one
+ * grouped orbital optimisation of the jobs still running, then each job's
+ * occoptr, ordering and convergence test.  params[j], H[j], C_inout[j],
+ * gamma_inout[j] and n_out[j] (or n_out NULL) as for donof_energy, host
+ * arrays; every job uses the same orb_method and the FP64 form.  Each job
+ * takes the steps donof_energy takes for it alone (results agree to
+ * rounding: the Lagrangian GEMM splits its K range differently).            */
+int donof_batch_energy(donof_batch* batch, donof_energy_params* params, const double* const* H,
+                       double* const* C_inout, double* const* gamma_inout, double* const* n_out,
+                       donof_energy_result* results);
 
 /* --- serving ------------------------------------------------------------------
  * Continuous batching of energy jobs on one GPU behind a thread-safe queue:

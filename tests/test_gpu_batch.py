@@ -158,3 +158,60 @@ def test_batch_result_same_alone_and_in_the_mix(cuda_ctx):
         o.free()
     for b in bt1 + btm:
         b.free()
+
+
+def test_batch_energy_matches_each_job_alone(cuda_ctx):
+    """donof_batch_energy: DoNOF.energy's alternation for several molecules, the
+    orbital optimisation of all of them grouped per outer iteration.  Each job
+    converges to the energy donof_energy gives it alone (to what the 1e-5
+    gradient thresholds leave; the two paths round the Lagrangian differently),
+    and a job that converges early leaves the later grouped calls."""
+    from donof_b200 import workload
+    from oracle import driver
+
+    shapes = [dict(nbf=24, naux=96, nbeta=5, ncwo=3, seed=3), dict(nbf=40, naux=80, nbeta=4, ncwo=3, seed=4),
+              dict(nbf=20, naux=30, nbeta=3, ncwo=3, seed=2), dict(nbf=48, naux=96, nbeta=4, ncwo=3, seed=5)]
+    wls = [workload.molecule_like(**kw) for kw in shapes]
+    for wl in wls:
+        wl.p.threshgorb, wl.p.threshgocc, wl.p.threshen = 1e-5, 1e-5, 1e-9
+    g0 = [ognof.guess_gamma_softmax(wl.p.nbeta, wl.p.ncwo) for wl in wls]
+    bts = [d.eris_to_gpu(wl.b, "fp64", cuda_ctx) for wl in wls]
+    batch = d.Batch(bts, [wl.p for wl in wls], cuda_ctx)
+    res = batch.energy([wl.H for wl in wls], [wl.C for wl in wls], g0, maxit=1000)
+    its = []
+    for j, (kw, wl) in enumerate(zip(shapes, wls)):
+        C, gamma, n, r = res[j]
+        assert r["converged"], j
+        p = workload.molecule_like(**kw).p
+        p.threshgorb, p.threshgocc, p.threshen = 1e-5, 1e-5, 1e-9
+        C1, g1, n1, _, r1, _ = d.api.energy_loop(wl.H, bts[j], p, wl.C, g0[j], maxit=1000)
+        assert r1["converged"], j
+        assert abs(r["E_elec"] - r1["E_elec"]) <= 1e-7, (j, r["E_elec"], r1["E_elec"])
+        assert np.max(np.abs(n - n1)) <= 1e-4, j
+        its.append(r["iterations"])
+    assert len(set(its)) > 1, "the jobs should need different numbers of outer iterations"
+    # the smallest case against the oracle's energy loop
+    s = ognof.Sizes(nbf=20, nbeta=3, nalpha=3, ncwo=3, naux=30)
+    E0, _, _, _, conv0 = driver.energy(wls[2].H, wls[2].b, s, wls[2].C, g0[2], threshgorb=1e-5, threshgocc=1e-5,
+                                       threshen=1e-9, maxit=1000)
+    assert conv0 and abs(res[2][3]["E_elec"] - E0) <= 1e-7
+    batch.free()
+    for b in bts:
+        b.free()
+
+
+def test_batch_orbopt_leaves_out_jobs_with_maxloop_zero(cuda_ctx):
+    inputs = device_inputs([case(**kw) for kw in SHAPES[:3]])
+    batch, bts = make_batch(cuda_ctx, inputs)
+    Cs = [x["tC"].clone() for x in inputs]
+    res = batch.orbopt("ADAM", [x["tn"] for x in inputs], [x["tcj"] for x in inputs], [x["tck"] for x in inputs],
+                       [x["tH"] for x in inputs], Cs, [0.01, 0.01, 0.02], [5, 0, 4], [1e-4] * 3)
+    assert res[1][1] == 0 and res[1][3:] == (0.01, 0)  # untouched
+    assert np.array_equal(d.from_device(Cs[1]), inputs[1]["C"])
+    for j in (0, 2):
+        E0, nit0, ok0, a0, ml0, C0 = run_alone(cuda_ctx, inputs[j], "ADAM", [0.01, 0.01, 0.02][j], [5, 0, 4][j], 1e-4)
+        assert res[j][1:] == (nit0, ok0, a0, ml0)
+        assert abs(res[j][0] - E0) <= TOL * max(1.0, abs(E0))
+    batch.free()
+    for b in bts:
+        b.free()
