@@ -18,9 +18,10 @@
 // step until every job has stopped.  A job that has stopped is skipped by every
 // launch (device-side gates), so each job takes exactly the iterations it
 // takes alone.  Every product sums in the same order as the single-job FP64
-// path (same tile routine; the tile shape does not change the summation order)
-// except the split of the Lagrangian GEMM's K range, which is fixed per job by
-// its own shape: a job's result does not depend on the other jobs in the batch.
+// path: the same tile routine (the tile shape does not change the summation
+// order), and for the Lagrangian GEMM the same split of its K range (the
+// autotuner's entry for the job's shape).  A job's result is bit-for-bit what
+// the single-job path gives it, whatever else the batch holds.
 #include <math.h>
 #include <string.h>
 
@@ -265,7 +266,7 @@ struct donof_batch {
         double *m, *v, *vm, *y, *g, *Ccur, *Cnew, *Cbest, *elag, *Hmat;
     };
     std::vector<Ptrs> pt;
-    DevBuf arena, tab;
+    DevBuf arena, tab, ypbuf;  // ypbuf: the split-K partials of the Lagrangian GEMM
     double* mvv = nullptr;  // m, v, vmax of every job (one contiguous span)
     size_t mvv_doubles = 0;
     // device table addresses
@@ -655,15 +656,8 @@ int donof_batch_create(donof_ctx* ctx, int count, const donof_batch_shape* shape
         h.nalpha = shapes[j].nalpha; h.nbeta = shapes[j].nbeta;
         h.nvar = nvar_of(h.nbf, h.nbf5);
         h.nn = (long long)h.nbf * h.nbf;
-        // split of the Lagrangian GEMM's K = nbf5 naux range: about 8192 per split,
-        // a function of the job's own shape only
-        const long long Kt = (long long)h.nbf5 * h.naux;
-        long long sp = (Kt + 8191) / 8192;
-        if (sp > 64) sp = 64;
-        if (sp < 1) sp = 1;
-        long long kc = ((Kt + sp - 1) / sp + 15) / 16 * 16;
-        h.kchunk = (int)kc;
-        h.splits = (int)((Kt + kc - 1) / kc);
+        h.splits = 1;  // set below, once the operands exist
+        h.kchunk = h.nbf5 * h.naux;
     }
     // arena: per-field spans, so that m, v and vmax of every job form one block
     std::vector<size_t> off_tmp(count), off_bpq(count), off_W(count), off_tv(count), off_yp(count), off_tw(count),
@@ -692,7 +686,6 @@ int donof_batch_create(donof_ctx* ctx, int count, const donof_batch_shape* shape
     field(off_bpq, [](const S& h) { return (size_t)h.nbf5 * h.nbf5 * h.naux; });
     field(off_W, [](const S& h) { return (size_t)h.nbf5 * h.nbf5 * h.naux; });
     field(off_tv, [](const S& h) { return (size_t)h.nbf5 * h.naux; });
-    field(off_yp, [](const S& h) { return (size_t)h.splits * h.nbf * h.nbf5; });
     field(off_tw, [](const S& h) { return (size_t)3 * h.nbf * h.nbf5; });
     field(off_rw, [](const S& h) { return rotate_work_doubles(h.nbf); });
     int rc = B->arena.ensure(ctx, sizeof(double) * acc);
@@ -710,7 +703,33 @@ int donof_batch_create(donof_ctx* ctx, int count, const donof_batch_shape* shape
         p.Ccur = base + off_Cc[j]; p.Cnew = base + off_Cn[j]; p.Cbest = base + off_Cb[j]; p.elag = base + off_el[j];
         p.Hmat = base + off_Hm[j];
         p.tmp = base + off_tmp[j]; p.bpq = base + off_bpq[j]; p.W = base + off_W[j]; p.tv = base + off_tv[j];
-        p.ypart = base + off_yp[j]; p.twork = base + off_tw[j]; p.rwork = base + off_rw[j];
+        p.twork = base + off_tw[j]; p.rwork = base + off_rw[j];
+    }
+    // Split of each job's Lagrangian GEMM (K = nbf5 naux): the one the single-job
+    // FP64 path uses for that shape (the process's autotuner entry, timed now on
+    // the batch's operands if there is none yet), so that a job sums in the same
+    // order in a batch and alone.  Then the partials' storage.
+    {
+        DevBuf scratch;
+        size_t yp = 0;
+        std::vector<size_t> off_yp(count);
+        for (int j = 0; j < count && rc == DONOF_OK; ++j) {
+            S& h = B->sh[j];
+            const long long Kt = (long long)h.nbf5 * h.naux;
+            rc = gemm_f64_partials_splits(ctx, ctx->stream, false, true, h.nbf, h.nbf5, (int)Kt, B->pt[j].tmp, h.nbf,
+                                          B->pt[j].W, Kt, &scratch, &h.splits, &h.kchunk);
+            off_yp[j] = yp;
+            yp += al32((size_t)h.splits * h.nbf * h.nbf5);
+        }
+        scratch.release(ctx);
+        if (rc == DONOF_OK) rc = B->ypbuf.ensure(ctx, sizeof(double) * yp);
+        if (rc != DONOF_OK) {
+            B->ypbuf.release(ctx);
+            B->arena.release(ctx);
+            delete B;
+            return rc;
+        }
+        for (int j = 0; j < count; ++j) B->pt[j].ypart = B->ypbuf.as<double>() + off_yp[j];
     }
     // device tables
     size_t tb = 0;
@@ -726,6 +745,7 @@ int donof_batch_create(donof_ctx* ctx, int count, const donof_batch_shape* shape
     for (int k = 0; k < 4; ++k) o_pre[k] = take(sizeof(int) * (count + 1));
     rc = B->tab.ensure(ctx, tb);
     if (rc != DONOF_OK) {
+        B->ypbuf.release(ctx);
         B->arena.release(ctx);
         delete B;
         return rc;
@@ -755,6 +775,7 @@ int donof_batch_create(donof_ctx* ctx, int count, const donof_batch_shape* shape
             if (v > 0x7fffffffLL) {
                 set_error(ctx, "donof_batch_create: too much work for one batch");
                 B->tab.release(ctx);
+                B->ypbuf.release(ctx);
                 B->arena.release(ctx);
                 delete B;
                 return DONOF_ERR_ARG;
@@ -768,6 +789,7 @@ int donof_batch_create(donof_ctx* ctx, int count, const donof_batch_shape* shape
                             ctx->stream) != cudaSuccess) {
             set_error(ctx, "donof_batch_create: upload of the work tables failed");
             B->tab.release(ctx);
+            B->ypbuf.release(ctx);
             B->arena.release(ctx);
             delete B;
             return DONOF_ERR_CUDA;
@@ -787,6 +809,7 @@ int donof_batch_create(donof_ctx* ctx, int count, const donof_batch_shape* shape
     }
     if (rc != DONOF_OK) {
         B->tab.release(ctx);
+        B->ypbuf.release(ctx);
         B->arena.release(ctx);
         delete B;
         return rc;
@@ -804,13 +827,16 @@ int donof_batch_destroy(donof_batch* B) {
     if (B->exec) cudaGraphExecDestroy(B->exec);
     if (B->graph) cudaGraphDestroy(B->graph);
     B->tab.release(ctx);
+    B->ypbuf.release(ctx);
     B->arena.release(ctx);
     cudaStreamSynchronize(ctx->stream);
     delete B;
     return DONOF_OK;
 }
 
-size_t donof_batch_device_bytes(const donof_batch* B) { return B ? B->arena.bytes + B->tab.bytes : 0; }
+size_t donof_batch_device_bytes(const donof_batch* B) {
+    return B ? B->arena.bytes + B->tab.bytes + B->ypbuf.bytes : 0;
+}
 
 int donof_batch_lagrange2(donof_batch* B, const donof_batch_item* items, double* const* elag, double* const* H_mat,
                           double* E) {

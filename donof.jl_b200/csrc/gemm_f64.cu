@@ -301,9 +301,15 @@ int gemm_f64_tuned(donof_ctx* ctx, cudaStream_t st, bool a_kmajor, bool b_kmajor
     return DONOF_OK;  // every candidate wrote the same C
 }
 
-int gemm_f64_partials(donof_ctx* ctx, cudaStream_t st, bool a_kmajor, bool b_kmajor, int M, int N, int K,
-                      const double* A, long long lda, const double* B, long long ldb, DevBuf* part,
-                      const double** out, int* nparts) {
+namespace {
+
+// The (tile, split) configuration gemm_f64_partials uses for a shape: the
+// cached autotuner choice, else (outside stream capture) timed now on the
+// given operands, else (while capturing) the heuristic.  *splits_out: the
+// number of partial products that configuration writes.
+int partials_choice(donof_ctx* ctx, cudaStream_t st, bool a_kmajor, bool b_kmajor, int M, int N, int K,
+                    const double* A, long long lda, const double* B, long long ldb, DevBuf* part, TuneVal* out,
+                    GemmF64Args* q_out, int* splits_out) {
     GemmF64Args p{};
     p.M = M; p.N = N; p.K = K;
     p.A = A; p.lda = lda; p.B = B; p.ldb = ldb;
@@ -359,13 +365,34 @@ int gemm_f64_partials(donof_ctx* ctx, cudaStream_t st, bool a_kmajor, bool b_kma
         v = cands[best];
         tune_store(key, v);
     }
+    DONOF_CHECK(part->ensure(ctx, sizeof(double) * (size_t)M * N * (v.splits > 1 ? v.splits : 1)));
+    *out = v;
+    config(v, q_out, splits_out);
+    return DONOF_OK;
+}
+
+}  // namespace
+
+int gemm_f64_partials(donof_ctx* ctx, cudaStream_t st, bool a_kmajor, bool b_kmajor, int M, int N, int K,
+                      const double* A, long long lda, const double* B, long long ldb, DevBuf* part,
+                      const double** out, int* nparts) {
+    TuneVal v;
     GemmF64Args q;
     int splits = 1;
-    DONOF_CHECK(part->ensure(ctx, sizeof(double) * (size_t)M * N * (v.splits > 1 ? v.splits : 1)));
-    config(v, &q, &splits);
+    DONOF_CHECK(partials_choice(ctx, st, a_kmajor, b_kmajor, M, N, K, A, lda, B, ldb, part, &v, &q, &splits));
     DONOF_CHECK(gemm_f64(ctx, st, a_kmajor, b_kmajor, q, v.tile));
     *out = part->as<double>();
     *nparts = splits;
+    return DONOF_OK;
+}
+
+int gemm_f64_partials_splits(donof_ctx* ctx, cudaStream_t st, bool a_kmajor, bool b_kmajor, int M, int N, int K,
+                             const double* A, long long lda, const double* B, long long ldb, DevBuf* part,
+                             int* splits, int* kchunk) {
+    TuneVal v;
+    GemmF64Args q;
+    DONOF_CHECK(partials_choice(ctx, st, a_kmajor, b_kmajor, M, N, K, A, lda, B, ldb, part, &v, &q, splits));
+    *kchunk = (*splits > 1) ? q.kchunk : K;
     return DONOF_OK;
 }
 

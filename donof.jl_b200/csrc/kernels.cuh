@@ -49,6 +49,14 @@ int gemm_f64_partials(donof_ctx* ctx, cudaStream_t st, bool a_kmajor, bool b_kma
                       const double* A, long long lda, const double* B, long long ldb, DevBuf* part,
                       const double** out, int* nparts);
 
+// The split of gemm_f64_partials for this shape (the autotuner's choice, timed
+// now on these operands if the process has none yet): *splits partial products
+// of *kchunk K-elements each.  A caller that splits the same way sums in the
+// same order.
+int gemm_f64_partials_splits(donof_ctx* ctx, cudaStream_t st, bool a_kmajor, bool b_kmajor, int M, int N, int K,
+                             const double* A, long long lda, const double* B, long long ldb, DevBuf* part,
+                             int* splits, int* kchunk);
+
 // Fused FP64 tail of the Lagrangian (tail.cu): Y = sum of nparts partials
 // (FP32 or FP64, part[g * pstride + m + nbf * b]), HC = H C5, H_mat = C^T HC,
 // elag = [n o H_mat + C^T Y | 0] and E_elec (when E != nullptr).

@@ -197,8 +197,9 @@ int donof_orbopt_dev(donof_job* job, int method, const double* n, const double* 
  * Lagrangian tail as grouped cooperative kernels), and the whole loop is one
  * captured CUDA graph that repeats the step until every job has met its own
  * stopping rule.  DoNOF.jl optimises one molecule per call; each job here
- * gives what donof_orbopt_dev gives for it alone (same iterations, same
- * stopping decisions, results within 1e-10).
+ * gives bit-for-bit what donof_orbopt_dev gives it alone (every product sums
+ * in the same order; the Lagrangian GEMM takes the autotuner's split for the
+ * job's shape, as the single-job path does).
  * donof_batch_create fixes the jobs (each with its FP64 RI tensor uploaded by
  * donof_b_upload / donof_b_attach on the same device) and their sizes, and
  * allocates the batch's device scratch (donof_batch_device_bytes).  The first
@@ -302,8 +303,7 @@ int donof_energy(donof_job* job, donof_energy_params* params, const double* H, d
  * occoptr, ordering and convergence test.  params[j], H[j], C_inout[j],
  * gamma_inout[j] and n_out[j] (or n_out NULL) as for donof_energy, host
  * arrays; every job uses the same orb_method and the FP64 form.  Each job
- * takes the steps donof_energy takes for it alone (results agree to
- * rounding: the Lagrangian GEMM splits its K range differently).            */
+ * gives bit-for-bit what donof_energy gives it alone.                       */
 int donof_batch_energy(donof_batch* batch, donof_energy_params* params, const double* const* H,
                        double* const* C_inout, double* const* gamma_inout, double* const* n_out,
                        donof_energy_result* results);
