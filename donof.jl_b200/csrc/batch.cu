@@ -26,6 +26,8 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
+#include <thread>
 #include <vector>
 
 #include "kernels.cuh"
@@ -234,8 +236,6 @@ __global__ void b_commit_kernel(const BJob* __restrict__ jobs, int njobs, cudaGr
 
 size_t al32(size_t doubles) { return (doubles + 31) / 32 * 32; }  // 256-byte segments
 
-int tile_bm(GemmTile t) { return t == GemmTile::Large ? 128 : (t == GemmTile::Small ? 64 : 32); }
-
 // Heuristic tile shape of an M x N output: the largest tile that the output fills.
 GemmTile heuristic_tile(int M, int N) {
     if (M >= 128 && N >= 48) return GemmTile::Large;
@@ -349,7 +349,7 @@ int upload_gemm_tables(donof_batch* B, cudaStream_t st) {
         std::vector<GemmF64Args> args;
         std::vector<int> starts;
         B->launches[s].clear();
-        const GemmTile order[3] = {GemmTile::Large, GemmTile::Small, GemmTile::Tiny};
+        const GemmTile order[4] = {GemmTile::Large, GemmTile::SmallW8, GemmTile::Small, GemmTile::Tiny};
         for (GemmTile t : order) {
             std::vector<int> js;
             for (int j = 0; j < B->nj; ++j)
@@ -506,9 +506,9 @@ int upload_call_tables(donof_batch* B, cudaStream_t st, const donof_batch_item* 
 }
 
 // The batch's own tile autotuner: for each grouped GEMM stage, times the launch
-// list of four candidate assignments (the per-job heuristic, all 128 x 64, all
-// 64 x 64, all 32 x 32 tiles) on the batch's operands with CUDA events (one
-// warm-up and two timed runs each) and keeps the fastest.  Every candidate
+// list of five candidate assignments (the per-job heuristic, all 128 x 64, all
+// 64 x 64, all 32 x 32, all 64 x 64 over 8 warps) on the batch's operands with
+// CUDA events (one warm-up and two timed runs each) and keeps the fastest.  Every candidate
 // writes the same result (the tile shape does not change any summation order).
 int autotune(donof_batch* B, cudaStream_t st) {
     donof_ctx* ctx = B->ctx;
@@ -523,11 +523,12 @@ int autotune(donof_batch* B, cudaStream_t st) {
     std::vector<GemmTile> best[NSTAGE];
     for (int s = 0; s < NSTAGE && rc == DONOF_OK; ++s) {
         float best_ms = -1.f;
-        for (int c = 0; c < 4 && rc == DONOF_OK; ++c) {
+        for (int c = 0; c < 5 && rc == DONOF_OK; ++c) {
             for (int j = 0; j < B->nj; ++j) {
                 const donof_batch::Shape& h = B->sh[j];
                 const int M = (s == ST_T2) ? h.nbf5 : h.nbf;
-                const GemmTile cand[4] = {heuristic_tile(M, h.nbf5), GemmTile::Large, GemmTile::Small, GemmTile::Tiny};
+                const GemmTile cand[5] = {heuristic_tile(M, h.nbf5), GemmTile::Large, GemmTile::Small, GemmTile::Tiny,
+                                          GemmTile::SmallW8};
                 B->tile[s][j] = cand[c];
             }
             if ((rc = upload_gemm_tables(B, st)) != DONOF_OK) break;
@@ -1043,11 +1044,31 @@ int donof_batch_energy(donof_batch* B, donof_energy_params* params, const double
         }
         if (!any) break;
         DONOF_CHECK(donof_batch_orbopt(B, method, items.data()));
+        std::vector<int> run;
         for (int j = 0; j < nj; ++j) {
             if (items[j].maxloop == 0) continue;
             params[j].alpha = items[j].alpha;
             params[j].maxloop = items[j].maxloop;
-            DONOF_CHECK(E[j].after_orbopt(items[j].E, items[j].nit));
+            DONOF_CHECK(E[j].occ_fetch());
+            run.push_back(j);
+        }
+        // the occupation optimisations of the running jobs, on host threads
+        std::vector<int> st(run.size(), DONOF_OK);
+        {
+            std::atomic<size_t> next{0};
+            auto work = [&]() {
+                for (size_t i = next.fetch_add(1); i < run.size(); i = next.fetch_add(1)) st[i] = E[run[i]].occ_solve();
+            };
+            const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+            const size_t nt = std::min<size_t>(run.size(), hw);
+            std::vector<std::thread> pool;
+            for (size_t t = 1; t < nt; ++t) pool.emplace_back(work);
+            work();
+            for (std::thread& t : pool) t.join();
+        }
+        for (size_t i = 0; i < run.size(); ++i) {
+            DONOF_CHECK(st[i]);
+            DONOF_CHECK(E[run[i]].end_iteration(items[run[i]].E, items[run[i]].nit));
         }
     }
     for (int j = 0; j < nj; ++j)

@@ -105,19 +105,81 @@ int check_sizes(donof_ctx* ctx, int nbf, int nbf5, int nalpha, int nbeta) {
         }                                       \
     } while (0)
 
-// Copies `count` doubles host -> device staging slot.
+// Moves caller host arrays to and from device staging slots.  Host data goes
+// through the context's page-locked buffer: an input is copied into it on the
+// host and then sent by an asynchronous DMA; an output is DMA'd into it and
+// copied to the caller's array once finish() has synchronised the stream.
+// Page-locked transfers run at full PCIe speed whatever memory the caller
+// passes.  Without pin() the copies use the caller's memory directly.
 struct Stager {
     donof_ctx* ctx;
     cudaStream_t st;
     char* base;
     size_t off = 0;
+    char* pinned = nullptr;
+    size_t pinned_bytes = 0, hoff = 0;
+    struct Out {
+        void* dst;
+        const char* src;
+        size_t bytes;
+    };
+    Out outs[8];
+    int nout = 0;
+
+    static size_t bytes(size_t count) { return ((count * sizeof(double) + 255) / 256) * 256; }
+
+    // page-locked room for `total` bytes of inputs and outputs
+    int pin(size_t total) {
+        if (ctx->hstage_busy) {  // an earlier call that failed may still be copying through it
+            DONOF_CUDA(ctx, cudaStreamSynchronize(st));
+            ctx->hstage_busy = false;
+        }
+        if (ctx->hstage_bytes < total) {
+            if (ctx->hstage) cudaFreeHost(ctx->hstage);
+            ctx->hstage = nullptr;
+            ctx->hstage_bytes = 0;
+            DONOF_CUDA(ctx, cudaMallocHost(&ctx->hstage, total));
+            ctx->hstage_bytes = total;
+        }
+        pinned = static_cast<char*>(ctx->hstage);
+        pinned_bytes = ctx->hstage_bytes;
+        return DONOF_OK;
+    }
+    // device slot for `count` doubles, filled from h (if not null)
     double* put(const double* h, size_t count) {
         double* d = reinterpret_cast<double*>(base + off);
-        off += ((count * sizeof(double) + 255) / 256) * 256;
-        if (h != nullptr) cudaMemcpyAsync(d, h, count * sizeof(double), cudaMemcpyHostToDevice, st);
+        const size_t b = bytes(count);
+        off += b;
+        if (h == nullptr) return d;
+        if (pinned && hoff + b <= pinned_bytes) {
+            memcpy(pinned + hoff, h, count * sizeof(double));
+            cudaMemcpyAsync(d, pinned + hoff, count * sizeof(double), cudaMemcpyHostToDevice, st);
+            hoff += b;
+            ctx->hstage_busy = true;
+        } else {
+            cudaMemcpyAsync(d, h, count * sizeof(double), cudaMemcpyHostToDevice, st);
+        }
         return d;
     }
-    static size_t bytes(size_t count) { return ((count * sizeof(double) + 255) / 256) * 256; }
+    // device -> caller array h, complete after finish()
+    int get(double* h, const double* d, size_t count) {
+        const size_t b = bytes(count);
+        if (pinned && hoff + b <= pinned_bytes && nout < 8) {
+            DONOF_CUDA(ctx, cudaMemcpyAsync(pinned + hoff, d, count * sizeof(double), cudaMemcpyDeviceToHost, st));
+            outs[nout++] = Out{h, pinned + hoff, count * sizeof(double)};
+            hoff += b;
+            ctx->hstage_busy = true;
+        } else {
+            DONOF_CUDA(ctx, cudaMemcpyAsync(h, d, count * sizeof(double), cudaMemcpyDeviceToHost, st));
+        }
+        return DONOF_OK;
+    }
+    int finish() {
+        DONOF_CUDA(ctx, cudaStreamSynchronize(st));
+        for (int i = 0; i < nout; ++i) memcpy(outs[i].dst, outs[i].src, outs[i].bytes);
+        ctx->hstage_busy = false;
+        return DONOF_OK;
+    }
 };
 
 int effective_precision(donof_job* job, int precision) {
@@ -257,6 +319,7 @@ int donof_destroy(donof_ctx* ctx) {
     ctx->stage_in.release(ctx);
     ctx->stage_out.release(ctx);
     ctx->rot.release(ctx);
+    if (ctx->hstage) cudaFreeHost(ctx->hstage);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     if (ctx->aux_stream) cudaStreamDestroy(ctx->aux_stream);
     if (ctx->prof_ev[0]) cudaEventDestroy(ctx->prof_ev[0]);
@@ -474,6 +537,7 @@ int donof_lagrange2(donof_job* job, const double* C, const double* n, const doub
                         Stager::bytes(nbf * nbf5) + Stager::bytes(1);
     DONOF_CHECK(job->io.ensure(ctx, need));
     Stager sg{ctx, ctx->stream, job->io.as<char>()};
+    DONOF_CHECK(sg.pin(job->io.bytes));
     const double* dC = sg.put(C, nn);
     const double* dH = sg.put(H, nn);
     const double* dn = sg.put(n, nbf5);
@@ -484,12 +548,11 @@ int donof_lagrange2(donof_job* job, const double* C, const double* n, const doub
     double* dE = sg.put(nullptr, 1);
     DONOF_CUDA(ctx, cudaGetLastError());
     DONOF_CHECK(donof_lagrange2_dev(job, dC, dn, dH, dcj, dck, nbf5, nalpha, nbeta, del, dHm, dE));
-    DONOF_CUDA(ctx, cudaMemcpyAsync(elag, del, nn * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    DONOF_CUDA(ctx, cudaMemcpyAsync(H_mat, dHm, nbf * nbf5 * sizeof(double), cudaMemcpyDeviceToHost,
-                                    ctx->stream));
+    DONOF_CHECK(sg.get(elag, del, nn));
+    DONOF_CHECK(sg.get(H_mat, dHm, nbf * nbf5));
     if (E_elec)
-        DONOF_CUDA(ctx, cudaMemcpyAsync(E_elec, dE, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    DONOF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        DONOF_CHECK(sg.get(E_elec, dE, 1));
+    DONOF_CHECK(sg.finish());
     return DONOF_OK;
 }
 
@@ -522,6 +585,7 @@ int donof_jkh_mo(donof_job* job, const double* C, const double* H, int nbf5, dou
     const size_t nbf = job->nbf, nn = nbf * nbf, n55 = (size_t)nbf5 * nbf5;
     DONOF_CHECK(job->io.ensure(ctx, Stager::bytes(nn) * 2 + Stager::bytes(n55) * 2 + Stager::bytes(nbf5)));
     Stager sg{ctx, ctx->stream, job->io.as<char>()};
+    DONOF_CHECK(sg.pin(job->io.bytes));
     const double* dC = sg.put(C, nn);
     const double* dH = sg.put(H, nn);
     double* dJ = sg.put(nullptr, n55);
@@ -529,10 +593,10 @@ int donof_jkh_mo(donof_job* job, const double* C, const double* H, int nbf5, dou
     double* dh = sg.put(nullptr, nbf5);
     DONOF_CUDA(ctx, cudaGetLastError());
     DONOF_CHECK(donof_jkh_mo_dev(job, dC, dH, nbf5, dJ, dK, dh));
-    DONOF_CUDA(ctx, cudaMemcpyAsync(J_MO, dJ, n55 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    DONOF_CUDA(ctx, cudaMemcpyAsync(K_MO, dK, n55 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    DONOF_CUDA(ctx, cudaMemcpyAsync(H_core, dh, nbf5 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    DONOF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    DONOF_CHECK(sg.get(J_MO, dJ, n55));
+    DONOF_CHECK(sg.get(K_MO, dK, n55));
+    DONOF_CHECK(sg.get(H_core, dh, nbf5));
+    DONOF_CHECK(sg.finish());
     return DONOF_OK;
 }
 
@@ -554,13 +618,14 @@ int donof_rotate(donof_ctx* ctx, const double* y, int nbf, int nbf5, const doubl
     const size_t nn = (size_t)nbf * nbf, nvar = (size_t)nvar_of(nbf, nbf5);
     DONOF_CHECK(ctx->stage_in.ensure(ctx, Stager::bytes(nvar) + Stager::bytes(nn) * 2));
     Stager sg{ctx, ctx->stream, ctx->stage_in.as<char>()};
+    DONOF_CHECK(sg.pin(ctx->stage_in.bytes));
     const double* dy = sg.put(y, nvar);
     const double* dC = sg.put(C, nn);
     double* dCn = sg.put(nullptr, nn);
     DONOF_CUDA(ctx, cudaGetLastError());
     DONOF_CHECK(rotate_f64(ctx, ctx->stream, dy, nbf, nbf5, dC, dCn));
-    DONOF_CUDA(ctx, cudaMemcpyAsync(C_new, dCn, nn * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    DONOF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    DONOF_CHECK(sg.get(C_new, dCn, nn));
+    DONOF_CHECK(sg.finish());
     return DONOF_OK;
 }
 
@@ -578,6 +643,7 @@ int donof_orbgrad(donof_job* job, const double* y, const double* C, const double
                         Stager::bytes(n55) * 2 + Stager::bytes(nbf * nbf5);
     DONOF_CHECK(job->io.ensure(ctx, need));
     Stager sg{ctx, ctx->stream, job->io.as<char>()};
+    DONOF_CHECK(sg.pin(job->io.bytes));
     const double* dy = sg.put(y, nvar);
     const double* dC = sg.put(C, nn);
     const double* dH = sg.put(H, nn);
@@ -596,8 +662,8 @@ int donof_orbgrad(donof_job* job, const double* y, const double* C, const double
     }
     DONOF_CHECK(donof_lagrange2_dev(job, Cuse, dn, dH, dcj, dck, nbf5, nalpha, nbeta, del, dHm, nullptr));
     DONOF_CHECK(pack_grad(ctx, ctx->stream, del, (int)nbf, nbf5, dg, nullptr));
-    DONOF_CUDA(ctx, cudaMemcpyAsync(grad, dg, nvar * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    DONOF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    DONOF_CHECK(sg.get(grad, dg, nvar));
+    DONOF_CHECK(sg.finish());
     return DONOF_OK;
 }
 
@@ -615,6 +681,7 @@ int donof_orbopt(donof_job* job, int method, const double* n, const double* cj12
     const size_t nbf = job->nbf, nn = nbf * nbf, n55 = (size_t)nbf5 * nbf5;
     DONOF_CHECK(job->io.ensure(ctx, Stager::bytes(nn) * 2 + Stager::bytes(nbf5) + Stager::bytes(n55) * 2));
     Stager sg{ctx, ctx->stream, job->io.as<char>()};
+    DONOF_CHECK(sg.pin(job->io.bytes));
     double* dC = sg.put(C_inout, nn);
     const double* dH = sg.put(H, nn);
     const double* dn = sg.put(n, nbf5);
@@ -623,8 +690,8 @@ int donof_orbopt(donof_job* job, int method, const double* n, const double* cj12
     DONOF_CUDA(ctx, cudaGetLastError());
     DONOF_CHECK(orbopt_run(job, method, dn, dcj, dck, dH, nbf5, nalpha, nbeta, alpha, maxloop, threshgorb,
                            dC, E, nit, success, job->precision));
-    DONOF_CUDA(ctx, cudaMemcpyAsync(C_inout, dC, nn * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    DONOF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    DONOF_CHECK(sg.get(C_inout, dC, nn));
+    DONOF_CHECK(sg.finish());
     return DONOF_OK;
 }
 

@@ -58,6 +58,11 @@ struct donof_ctx {
     int sm_count = 148;
     // host-pointer staging (device side) shared by the host-buffer entry points
     donof::DevBuf stage_in, stage_out;
+    // page-locked host buffer the host-buffer entry points copy through
+    // (grown on demand; hstage_busy while a call's copies may be in flight)
+    void* hstage = nullptr;
+    size_t hstage_bytes = 0;
+    bool hstage_busy = false;
     // scratch for the rotation (exp of the generator)
     donof::DevBuf rot;
     // optional timing of the dominant kernel of each call (donof_profile_*):

@@ -183,8 +183,8 @@ struct EnergyJob::Impl {
     std::vector<double> gamma, dn, n, cj, ck, n_occ, cj_occ, ck_occ, J, K, Hc, gocc;
     std::vector<int> perm;
     double E = 9999.0, E_old = 9999.0, gorb = 0.0, gocc_norm = 0.0;
-    int it = 1, tot_orb = 0, tot_occ = 0, converged = 0;
-    bool done = false;
+    int it = 1, tot_orb = 0, tot_occ = 0, converged = 0, nit_occ = 0;
+    bool done = false, moved = false;
 };
 
 EnergyJob::EnergyJob() : p(new Impl) {}
@@ -255,6 +255,41 @@ int EnergyJob::setup(donof_job* job, donof_energy_params* prm, const double* H, 
 int EnergyJob::begin() { return p->L.put_coef(p->n, p->cj, p->ck); }
 
 int EnergyJob::after_orbopt(double E_orb, int nit_orb) {
+    DONOF_CHECK(occ_fetch());
+    DONOF_CHECK(occ_solve());
+    return end_iteration(E_orb, nit_orb);
+}
+
+// occoptr, device part: J_MO, K_MO, H_core at the optimised orbitals, to the host.
+int EnergyJob::occ_fetch() {
+    Impl& S = *p;
+    if (S.o.ndoc > 0 && !S.prm->freeze_occ) DONOF_CHECK(S.L.jkh(S.J, S.K, S.Hc));
+    return DONOF_OK;
+}
+
+// occoptr, host part (no CUDA call: jobs may run it on several threads at once):
+// the conjugate gradient over gamma, the occupations and couplings it gives, and
+// the column order of order_occupations_softmax.
+int EnergyJob::occ_solve() {
+    Impl& S = *p;
+    const donof::occ::Occ& o = S.o;
+    donof_energy_params* prm = S.prm;
+    S.nit_occ = 0;
+    if (o.ndoc > 0 && !prm->freeze_occ) {
+        double E_occ = 0.0;
+        int conv = 0;
+        const int rc = donof::occ::cg(o, S.J.data(), S.K.data(), S.Hc.data(), S.gamma.data(), prm->threshen, 1000,
+                                      &E_occ, &S.nit_occ, &conv);
+        if (rc != DONOF_OK) return rc;
+        if (S.nit_occ < 1) prm->maxloop += 10;
+    }
+    donof::occ::occupations(o, S.gamma.data(), S.n_occ.data(), S.dn.data());
+    donof::occ::coupling(o, S.n_occ.data(), S.cj_occ.data(), S.ck_occ.data());
+    S.moved = (o.method == 0) && order_softmax(o, S.gamma, S.perm);
+    return DONOF_OK;
+}
+
+int EnergyJob::end_iteration(double E_orb, int nit_orb) {
     Impl& S = *p;
     Loop& L = S.L;
     const donof::occ::Occ& o = S.o;
@@ -262,20 +297,9 @@ int EnergyJob::after_orbopt(double E_orb, int nit_orb) {
     donof_ctx* ctx = L.ctx;
     cudaStream_t st = L.st;
     const int nv = o.nv;
-    // ---- occoptr
-    int nit_occ = 0;
-    if (o.ndoc > 0 && !prm->freeze_occ) {
-        DONOF_CHECK(L.jkh(S.J, S.K, S.Hc));
-        double E_occ = 0.0;
-        int conv = 0;
-        DONOF_CHECK(donof::occ::cg(o, S.J.data(), S.K.data(), S.Hc.data(), S.gamma.data(), prm->threshen, 1000,
-                                   &E_occ, &nit_occ, &conv));
-        if (nit_occ < 1) prm->maxloop += 10;
-    }
-    donof::occ::occupations(o, S.gamma.data(), S.n_occ.data(), S.dn.data());
-    donof::occ::coupling(o, S.n_occ.data(), S.cj_occ.data(), S.ck_occ.data());
-    // ---- order_occupations_softmax
-    if (o.method == 0 && order_softmax(o, S.gamma, S.perm)) DONOF_CHECK(L.permute(S.perm));
+    const int nit_occ = S.nit_occ;
+    // ---- order_occupations_softmax on the device
+    if (S.moved) DONOF_CHECK(L.permute(S.perm));
     S.tot_orb += nit_orb;
     S.tot_occ += nit_occ;
     S.E = E_orb;

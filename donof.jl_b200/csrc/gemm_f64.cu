@@ -106,7 +106,7 @@ bool gemm_f64_vec_ok(bool a_kmajor, bool b_kmajor, const GemmF64Args& p) {
 }
 
 int gemm_f64_tiles(const GemmF64Args& p, GemmTile tile) {
-    const int bm = tile == GemmTile::Large ? 128 : (tile == GemmTile::Small ? 64 : 32);
+    const int bm = tile == GemmTile::Large ? 128 : (tile == GemmTile::Tiny ? 32 : 64);
     const int bn = tile == GemmTile::Tiny ? 32 : 64;
     if (p.M <= 0 || p.N <= 0 || p.batch <= 0) return 0;
     return ((p.M + bm - 1) / bm) * ((p.N + bn - 1) / bn) * p.batch * (p.splits < 1 ? 1 : p.splits);
@@ -121,6 +121,9 @@ int gemm_f64_grouped(donof_ctx* ctx, cudaStream_t st, bool a_kmajor, bool b_kmaj
                                                  a_kmajor, b_kmajor, vec, st);
     else if (tile == GemmTile::Small)
         e = launch_grouped_layout<64, 64, 2, 2>(groups, start, ngroups, total_tiles, ctx->sm_count, max_ctas,
+                                                a_kmajor, b_kmajor, vec, st);
+    else if (tile == GemmTile::SmallW8)
+        e = launch_grouped_layout<64, 64, 2, 4>(groups, start, ngroups, total_tiles, ctx->sm_count, max_ctas,
                                                 a_kmajor, b_kmajor, vec, st);
     else
         e = launch_grouped_layout<32, 32, 2, 2>(groups, start, ngroups, total_tiles, ctx->sm_count, max_ctas,
@@ -148,7 +151,7 @@ int gemm_f64(donof_ctx* ctx, cudaStream_t st, bool a_kmajor, bool b_kmajor, Gemm
     cudaError_t e;
     if (tile == GemmTile::Large)
         e = launch_layout<128, 64, 4, 2>(p, a_kmajor, b_kmajor, vec, st);
-    else if (tile == GemmTile::Small)
+    else if (tile == GemmTile::Small || tile == GemmTile::SmallW8)
         e = launch_layout<64, 64, 2, 2>(p, a_kmajor, b_kmajor, vec, st);
     else
         e = launch_layout<32, 32, 2, 2>(p, a_kmajor, b_kmajor, vec, st);

@@ -342,9 +342,12 @@ gemm_f64_kernel(const GemmF64Args p) {
 // the loads of the next tile are in flight during the epilogue (the tiles of
 // the batch's jobs have short K ranges, where the prologue is a large share).
 // CTAs per SM the grouped kernel is compiled for (a register cap): as many as
-// fit without spills: 6 (32 x 32), 3 (64 x 64), 2 (128 x 64).
+// fit without spills: 6 (32 x 32), 3 (64 x 64 over 4 warps), 2 (64 x 64 over 8
+// warps, 128 x 64).
 template <int BM, int BN, int WARPS_M, int WARPS_N>
-constexpr int grouped_min_ctas() { return BM * BN <= 32 * 32 ? 6 : (WARPS_M * WARPS_N <= 4 ? 3 : 2); }
+constexpr int grouped_min_ctas() {
+    return BM * BN <= 32 * 32 ? 6 : ((BM * BN <= 64 * 64 && WARPS_M * WARPS_N <= 4) ? 3 : 2);
+}
 
 template <int BM, int BN, int BK, int WARPS_M, int WARPS_N, int STAGES, bool AK, bool BKM, bool VEC>
 __global__ void __launch_bounds__(32 * WARPS_M * WARPS_N, (grouped_min_ctas<BM, BN, WARPS_M, WARPS_N>()))

@@ -6,7 +6,9 @@
 
 namespace donof {
 
-enum class GemmTile { Large /*128x64*/, Small /*64x64*/, Tiny /*32x32*/ };
+// Tile shapes of the FP64 GEMM.  SmallW8 (64 x 64 over 8 warps of 32 x 16) is
+// a grouped-kernel-only shape: more warps per SM for short-K products.
+enum class GemmTile { Large /*128x64*/, Small /*64x64*/, Tiny /*32x32*/, SmallW8 /*64x64, 8 warps*/ };
 
 // C = alpha*op(A)op(B) + beta*C on stream st (see gemm_f64.cuh for addressing).
 int gemm_f64(donof_ctx* ctx, cudaStream_t st, bool a_kmajor, bool b_kmajor, GemmF64Args p,
@@ -151,7 +153,12 @@ public:
     int setup(donof_job* job, donof_energy_params* prm, const double* H, const double* C, const double* gamma,
               double* history);
     int begin();
+    // after the orbital optimisation: occ_fetch (device), occ_solve (host only,
+    // safe to run for several jobs on several threads), end_iteration (device)
     int after_orbopt(double E_orb, int nit_orb);
+    int occ_fetch();
+    int occ_solve();
+    int end_iteration(double E_orb, int nit_orb);
     int finish(double* C_out, double* gamma_out, double* n_out, double* elag_out, donof_energy_result* res);
     bool done() const;
     const double* dev_n() const;
