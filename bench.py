@@ -185,6 +185,17 @@ def traffic_from_profiles(kernel_key):
     return None
 
 
+def max_over_ranks(t, dist, device=None):
+    """The largest of the ranks' values (a multi-GPU run takes as long as its
+    slowest rank); t itself with a single process."""
+    if dist is None:
+        return t
+    import torch
+    tt = torch.tensor([float(t)], dtype=torch.float64, device=device)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return float(tt.item())
+
+
 def host_adam(state, g, i, alpha, beta1=0.5, beta2=0.9):
     m, v, vmax = state
     m[:] = beta1 * m + (1 - beta1) * g
@@ -578,10 +589,7 @@ def main():
     barrier()
     t = ev0.elapsed_time(ev1) / 1e3
     assert nit == args.steps, (nit, args.steps)
-    if dist is not None:
-        tt = torch.tensor([t], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t = float(tt.item())
+    t = max_over_ranks(t, dist, dev)
     value = world * args.steps / t
 
     # ---- the other form's device loop on the same workload (same step count)
@@ -597,10 +605,7 @@ def main():
     ev1.record()
     torch.cuda.synchronize()
     t2 = ev0.elapsed_time(ev1) / 1e3
-    if dist is not None:
-        tt = torch.tensor([t2], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t2 = float(tt.item())
+    t2 = max_over_ranks(t2, dist, dev)
     other_form = {"precision": other, "value": world * nit2 / t2, "unit": UNIT, "ms_per_step": 1e3 * t2 / nit2}
     bt.set_precision(args.precision)
     tC.copy_(tC0)
@@ -669,10 +674,7 @@ def main():
         torch.cuda.synchronize()
         te = evs[0].elapsed_time(evs[-1]) / 1e3
         per_step = [evs[i - 1].elapsed_time(evs[i]) for i in range(1, args.steps + 1)]
-        if dist is not None:
-            tt = torch.tensor([te], device=dev)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            te = float(tt.item())
+        te = max_over_ranks(te, dist, dev)
         nn, n55 = nbf * nbf, nbf5 * nbf5
         h2d = 8 * (p.nvar + nn) + 8 * (nn + nn + nbf5 + 2 * n55)
         d2h = 8 * nn + 8 * (nn + nbf * nbf5 + 1)
