@@ -145,6 +145,36 @@ class Admission:
         self.used -= nbytes
         self.inflight -= 1
 
+    def take_group(self, eligible: Callable[[int], bool], max_group: int, min_group: int = 2,
+                   scale: float = 2.0) -> List[tuple]:
+        """Queued tickets to run together as one group on one slot: when the head
+        of the queue is eligible, the eligible tickets in arrival order (at most
+        max_group) whose bytes, times ``scale`` (a group holds each job's scratch
+        twice: the grouped loop's and the per-job steps'), fit the free budget.
+        Fewer than min_group: nothing (the single-job path takes them)."""
+        if self.inflight >= self.max_inflight or not self.queue or not eligible(self.queue[0][0]):
+            return []
+        room = self.budget - self.used
+        group = []
+        for t, nb in self.queue:
+            if len(group) >= max_group:
+                break
+            need = int(scale * nb)
+            if eligible(t) and need <= room:
+                group.append((t, need))
+                room -= need
+        if len(group) < min_group:
+            return []
+        picked = {t for t, _ in group}
+        self.queue = deque(q for q in self.queue if q[0] not in picked)
+        self._head_bypassed = 0
+        self.used += sum(nb for _, nb in group)
+        self.inflight += 1
+        return group
+
+    def release_group(self, nbytes_total: int) -> None:
+        self.release(nbytes_total)
+
 
 def run_energy(req: Request, device: int, cta_limit: int = 0) -> Result:
     """Executor: the energy loop of one request on its own context and stream;
@@ -175,6 +205,44 @@ def run_energy(req: Request, device: int, cta_limit: int = 0) -> Result:
         ctx.close()
 
 
+def run_energy_group(reqs: List[Request], device: int) -> List[Result]:
+    """Executor of a group: the energy loops of several FP64 jobs on one context
+    as one batch (``api.Batch.energy``, donof_batch_energy): each outer
+    iteration optimises the orbitals of every job still running with grouped
+    launches, one per stage of a gradient step.  Every job's result is
+    bit-for-bit what ``run_energy`` gives it alone."""
+    import copy
+
+    from . import api, gnof
+
+    ctx = api.Context(device, torch_stream=False)
+    bts = []
+    batch = None
+    try:
+        ps = []
+        for r in reqs:
+            p = copy.copy(r.p)
+            if r.maxit is not None:
+                p.maxit = int(r.maxit)
+            ps.append(p)
+            bts.append(api.eris_to_gpu(r.b, "fp64", ctx))
+        batch = api.Batch(bts, ps, ctx)
+        gammas = [gnof.guess_gamma(p) if r.gamma is None else r.gamma for r, p in zip(reqs, ps)]
+        out = batch.energy([r.H for r in reqs], [r.C for r in reqs], gammas)
+        res = []
+        for r, p, (C, gamma, n, f) in zip(reqs, ps, out):
+            r.p.alpha, r.p.maxloop = p.alpha, p.maxloop
+            res.append(Result(ticket=-1, E_elec=f["E_elec"], E_tot=f["E_elec"] + r.E_nuc,
+                              converged=bool(f["converged"]), iterations=f["iterations"], C=C, n=n))
+        return res
+    finally:
+        if batch is not None:
+            batch.free()
+        for b in bts:
+            b.free()
+        ctx.close()
+
+
 def cta_share(max_inflight: int, sm_count: int = 148) -> int:
     """CTAs per job for a server with max_inflight slots: all SMs for one job,
     else about two jobs per SM, at least 16."""
@@ -191,11 +259,19 @@ def cta_share_for(max_inflight: int, device: int = 0) -> int:
 class Server:
     """Accepts requests at any time; runs admitted jobs concurrently, each on
     its own stream.  ``executor(request, device) -> Result`` does the work
-    (``run_energy`` by default)."""
+    (``run_energy`` by default).
+
+    With ``group_max > 1``, the FP64 jobs waiting in the queue when a slot frees
+    (those ``auto`` runs in FP64: the small ones) start together as one group
+    on that slot, through ``group_executor(requests, device) -> [Result]``
+    (``run_energy_group``: one batch whose gradient steps advance every job of
+    the group with grouped launches); the other jobs start one per slot as
+    before."""
 
     def __init__(self, device: int = 0, budget_bytes: Optional[int] = None, max_inflight: int = 8,
                  max_bypass: int = 4, executor: Callable[[Request, int], Result] = run_energy,
-                 cta_share: Optional[int] = None):
+                 cta_share: Optional[int] = None, group_max: int = 0,
+                 group_executor: Callable[[List[Request], int], List[Result]] = run_energy_group):
         if budget_bytes is None:
             import torch
             free, _ = torch.cuda.mem_get_info(device)
@@ -208,6 +284,8 @@ class Server:
             share = cta_share if cta_share is not None else cta_share_for(max_inflight, device)
             executor = functools.partial(run_energy, cta_limit=share)
         self.executor = executor
+        self.group_max = int(group_max)
+        self.group_executor = group_executor
         self._lock = threading.Condition()
         self._tickets = itertools.count(1)
         self._pending: Dict[int, Request] = {}
@@ -262,12 +340,41 @@ class Server:
         self.shutdown()
 
     # ---- scheduling
+    def _groupable(self, t: int) -> bool:
+        p = self._pending[t].p
+        return resolve_precision(self._pending[t].precision, p.nbf, p.nbf5, p.nbfaux) == "fp64"
+
     def _admit_locked(self) -> None:
+        while self.group_max > 1:
+            group = self.admission.take_group(self._groupable, self.group_max)
+            if not group:
+                break
+            reqs = [self._pending.pop(t) for t, _ in group]
+            th = threading.Thread(target=self._run_group, args=(group, reqs), daemon=True)
+            self._threads.append(th)
+            th.start()
         for t, nb in self.admission.take():
             req = self._pending.pop(t)
             th = threading.Thread(target=self._run, args=(t, req, nb), daemon=True)
             self._threads.append(th)
             th.start()
+
+    def _run_group(self, group: List[tuple], reqs: List[Request]) -> None:
+        t0 = time.perf_counter()
+        try:
+            out = self.group_executor(reqs, self.device)
+        except Exception as e:  # every job of the group fails, the server goes on
+            out = [Result(ticket=-1, error=f"{type(e).__name__}: {e}") for _ in reqs]
+        t1 = time.perf_counter()
+        with self._lock:
+            for (t, nb), req, r in zip(group, reqs, out):
+                r.ticket, r.t_start, r.t_done, r.footprint, r.tag = t, t0, t1, nb, req.tag
+                r.t_submit = self._submit_t.pop(t)
+                self._bytes.pop(t)
+                self._results[t] = r
+            self.admission.release_group(sum(nb for _, nb in group))
+            self._admit_locked()
+            self._lock.notify_all()
 
     def _run(self, t: int, req: Request, nb: int) -> None:
         t0 = time.perf_counter()

@@ -73,3 +73,32 @@ def test_native_server_matches_sequential_fp64(cuda_ctx):
         assert s.converged == a.converged
         assert abs(s.E_elec - a.E_elec) <= 1e-10 * max(1.0, abs(a.E_elec))
         assert np.max(np.abs(s.n - a.n)) <= 1e-8
+
+
+def test_grouped_server_gives_each_job_its_alone_result():
+    """Small FP64 jobs that wait together start as one group (donof_batch_energy:
+    their gradient steps advance with grouped launches); each job's energy,
+    occupations and orbitals are bit-for-bit those of the job served alone."""
+    import copy
+
+    shapes = [(24, 58, 5, 3), (34, 80, 5, 5), (48, 116, 10, 3), (24, 58, 5, 3), (40, 90, 6, 3)]
+    wls = [workload.molecule_like(nbf=a, naux=b, nbeta=c, ncwo=e, seed=60 + i, two_e_scale=0.2)
+           for i, (a, b, c, e) in enumerate(shapes)]
+    for wl in wls:
+        wl.p.threshgorb = wl.p.threshgocc = 1e-5
+        wl.p.threshen = 1e-6
+    req = lambda wl, i: Request(H=wl.H, b=wl.b, C=wl.C, p=copy.deepcopy(wl.p), gamma=wl.gamma, precision="auto",
+                                maxit=500, tag=i)
+    with Server(max_inflight=1) as s:
+        alone = [s.wait(s.submit(req(wl, i)), timeout=600) for i, wl in enumerate(wls)]
+    with Server(max_inflight=1, group_max=8) as s:
+        tickets = [s.submit(req(wl, i)) for i, wl in enumerate(wls)]
+        grouped = [s.wait(t, timeout=600) for t in tickets]
+    # the first job took the slot alone; the others waited and ran as one group
+    starts = [g.t_start for g in grouped]
+    assert len(set(starts[1:])) == 1 and starts[1] > starts[0]
+    for a, g in zip(alone, grouped):
+        assert a.error is None and g.error is None, (a.error, g.error)
+        assert a.converged and g.converged
+        assert g.E_elec == a.E_elec and g.iterations == a.iterations
+        assert np.array_equal(g.n, a.n) and np.array_equal(g.C, a.C)

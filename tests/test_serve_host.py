@@ -105,3 +105,45 @@ def test_auto_precision_picks_mixed_for_large_transforms_only():
     # the mixed footprint includes the bf16 split and, beyond the fused kernel's
     # shapes, the general pipeline's scratch
     assert footprint(202, 974, 198, "mixed_refined") > footprint(202, 974, 198, "fp64")
+
+
+def test_take_group_collects_eligible_jobs_behind_an_eligible_head():
+    a = Admission(budget_bytes=100, max_inflight=2)
+    for t, nb in [(1, 10), (2, 30), (3, 10), (4, 10), (5, 10)]:
+        a.push(t, nb)
+    small = lambda t: t != 2                           # ticket 2 is not groupable
+    g = a.take_group(small, max_group=3, scale=2.0)
+    assert [t for t, _ in g] == [1, 3, 4]              # in arrival order, 2 left in the queue
+    assert [nb for _, nb in g] == [20, 20, 20]         # each job's bytes times the scale
+    assert a.inflight == 1 and a.used == 60
+    assert [t for t, _ in a.queue] == [2, 5]
+    assert a.take_group(small, max_group=3) == []      # head (2) not eligible: no group passes it
+    assert [t for t, _ in a.take()] == [2]             # the single-job path takes the head
+    a.release_group(60)
+    assert a.inflight == 1 and a.used == 30
+    assert a.take_group(small, max_group=3) == []      # one eligible job left: below min_group
+
+
+def test_server_runs_small_fp64_jobs_as_groups_and_the_rest_alone():
+    groups, singles = [], []
+
+    def fake_group(reqs, device):
+        groups.append([r.tag for r in reqs])
+        time.sleep(0.05)
+        return [Result(ticket=-1, E_elec=float(r.p.nbf), converged=True) for r in reqs]
+
+    def fake(req, device):
+        singles.append(req.tag)
+        time.sleep(0.1)  # the other jobs queue up meanwhile
+        return Result(ticket=-1, E_elec=float(req.p.nbf), converged=True)
+
+    with Server(budget_bytes=10**12, max_inflight=1, executor=fake, group_max=4,
+                group_executor=fake_group) as s:
+        # the first job takes the only slot; the next five wait and then start as groups
+        tickets = [s.submit(_req(8 + i, tag=i)) for i in range(6)]
+        res = [s.wait(t, timeout=10) for t in tickets]
+    assert [r.E_elec for r in res] == [8.0 + i for i in range(6)]
+    assert [r.tag for r in res] == list(range(6))
+    assert sum(len(g) for g in groups) + len(singles) == 6
+    assert any(len(g) >= 2 for g in groups)
+    assert all(len(g) <= 4 for g in groups)
