@@ -385,6 +385,31 @@ def guess_gamma(p: Param) -> np.ndarray:
     return g
 
 
+def n_to_gammas(n, p: Param) -> np.ndarray:
+    """gamma whose occupations are n: the restart path of DoNOF.energy
+    (src/energy.jl:95-99), n_to_gammas_softmax (src/utils.jl:539-561) and
+    n_to_gammas_trigonometric (src/utils.jl:563-584)."""
+    n = np.asarray(n, dtype=np.float64)
+    g = np.zeros(p.nv)
+    nd, nc = p.ndoc, p.ncwo
+    P = p.pair_table()
+    if p.occ_method == "Softmax":
+        # the reference divides by n[i] with i the pair index (1-based), kept as is
+        g[p.gamma_table()] = np.log(np.maximum(n[P], 1e-16)) - np.log(n[:nd])[:, None]
+    elif p.occ_method == "Trigonometric":
+        strong = p.no1 + np.arange(nd)
+        g[:nd] = np.arccos(np.sqrt(2.0 * n[strong] - 1.0))
+        for i in range(nd):
+            pref = max(1.0 - n[strong[i]], 1e-14)
+            cols = nd + (nd - (i + 1)) + nd * np.arange(nc - 1)
+            for j in range(nc - 1):
+                g[cols[j]] = math.asin(math.sqrt(n[P[i, j]] / pref))
+                pref *= math.cos(g[cols[j]]) ** 2
+    else:
+        raise ValueError(f"occupation method {p.occ_method!r} is not supported")
+    return g
+
+
 def order_occupations_softmax(C, gamma, p: Param):
     """Sort each pair's orbitals by gamma, descending (src/utils.jl:586-616)."""
     C = np.array(C, copy=True, order="F")

@@ -423,6 +423,32 @@ def guess_gamma_trigonometric(ndoc: int, ncwo: int) -> np.ndarray:
     return g
 
 
+def n_to_gammas_softmax(n, p: Sizes) -> np.ndarray:
+    """src/utils.jl:539-561 (line by line, 0-based)."""
+    gamma = np.zeros(p.nv)
+    for i in range(1, p.ndoc + 1):
+        n_pi = _cwo(p.no1, p.ndns, p.ndoc, p.ncwo, i)            # ll:ndoc:ul
+        gamma_pi = (p.ndoc - i) + p.ndoc * np.arange(p.ncwo)    # llg:ndoc:ulg
+        for j in range(p.ncwo):
+            gamma[gamma_pi[j]] = math.log(max(n[n_pi[j]], 1e-16)) - math.log(n[i - 1])
+    return gamma
+
+
+def n_to_gammas_trigonometric(n, p: Sizes) -> np.ndarray:
+    """src/utils.jl:563-584 (line by line, 0-based)."""
+    gamma = np.zeros(p.nv)
+    for i in range(1, p.ndoc + 1):
+        idx = p.no1 + i - 1
+        gamma[i - 1] = math.acos(math.sqrt(2.0 * n[idx] - 1.0))
+        prefactor = max(1 - n[idx], 1e-14)
+        n_pi = _cwo(p.no1, p.ndns, p.ndoc, p.ncwo, i)
+        gamma_pi = p.ndoc + (p.ndoc - i) + p.ndoc * np.arange(p.ncwo - 1)
+        for j in range(p.ncwo - 1):
+            gamma[gamma_pi[j]] = math.asin(math.sqrt(n[n_pi[j]] / prefactor))
+            prefactor = prefactor * math.cos(gamma[gamma_pi[j]]) ** 2
+    return gamma
+
+
 def order_occupations_softmax(old_C, old_gamma, p: Sizes):
     """src/utils.jl:586-616."""
     C = old_C.copy()

@@ -110,3 +110,24 @@ def test_create_without_gpu_reports_an_error():
     st = lib.donof_create(0, ct.byref(h))
     assert st != _lib.OK and not h.value
     assert b"device" in lib.donof_last_error(None)
+
+
+@pytest.mark.parametrize("occ", ["Softmax", "Trigonometric"])
+@pytest.mark.parametrize("case", [dict(nbf=40, nbeta=5, nalpha=5, ncwo=3), dict(nbf=30, nbeta=4, nalpha=6, ncwo=2),
+                                  dict(nbf=24, nbeta=3, nalpha=3, ncwo=1)])
+def test_n_to_gammas_restart(case, occ):
+    """Restart from occupations (src/energy.jl:95-99): n_to_gammas matches the
+    oracle's line-by-line restatement of src/utils.jl:539-584, and the gamma it
+    gives reproduces the occupations."""
+    p = Param(nbfaux=8, occ_method=occ, **case)
+    s = ognof.Sizes(nbf=case["nbf"], nbeta=case["nbeta"], nalpha=case["nalpha"], ncwo=case["ncwo"], occ_method=occ)
+    rng = np.random.default_rng(3)
+    gamma = rng.standard_normal(p.nv)
+    if occ == "Trigonometric":
+        gamma = np.abs(gamma) % (np.pi / 2)           # the principal branch acos / asin return
+    n, _ = gnof.occupations(gamma, p)
+    g1 = gnof.n_to_gammas(n, p)
+    g0 = (ognof.n_to_gammas_softmax if occ == "Softmax" else ognof.n_to_gammas_trigonometric)(n, s)
+    assert np.allclose(g1, g0, rtol=0, atol=1e-13)
+    n1, _ = gnof.occupations(g1, p)
+    assert np.allclose(n1, n, rtol=0, atol=1e-12)
