@@ -170,9 +170,9 @@ __global__ void __launch_bounds__(256) b_wdiag_kernel(const BJob* __restrict__ j
     }
 }
 
-__global__ void __launch_bounds__(256) b_buildw_kernel(const BJob* __restrict__ jobs, const int* __restrict__ pre,
+__global__ void __launch_bounds__(256, 4) b_buildw_kernel(const BJob* __restrict__ jobs, const int* __restrict__ pre,
                                                        int njobs) {
-    __shared__ double tb[32][33];
+    __shared__ double tb[wbuild::LT][32][33];
     const int total = pre[njobs];
     for (int u = blockIdx.x; u < total; u += gridDim.x) {
         const int j = job_of(pre, njobs, u);
@@ -768,9 +768,8 @@ int donof_batch_create(donof_ctx* ctx, int count, const donof_batch_shape* shape
     for (int k = 0; k < 4; ++k) pre[k].assign(count + 1, 0);
     for (int j = 0; j < count; ++j) {
         const S& h = B->sh[j];
-        const long long nt = (h.nbf5 + 31) / 32;
         const long long u[4] = {(h.nvar + CH - 1) / CH, (h.nn + CH - 1) / CH,
-                                ((long long)h.nbf5 * h.naux + CH - 1) / CH, nt * nt * h.naux};
+                                ((long long)h.nbf5 * h.naux + CH - 1) / CH, wbuild::tiles(h.nbf5, h.naux)};
         for (int k = 0; k < 4; ++k) {
             const long long v = pre[k][j] + u[k];
             if (v > 0x7fffffffLL) {

@@ -26,8 +26,8 @@ namespace {
 
 // W of every aux index (wbuild.cuh) in two fully parallel passes: w_diag_kernel
 // forms n'_b d_b^l + t_b^l (one thread per (b, l), cj12 read along b);
-// build_w_kernel the elementwise part over 32 x 32 tiles of (b, q), one tile per
-// CTA step (b need not be symmetric).
+// build_w_kernel the elementwise part over tiles of 32 x 32 (b, q) and
+// wbuild::LT aux indices, one tile per CTA step (b need not be symmetric).
 __global__ void w_diag_kernel(const double* __restrict__ bpq, const double* __restrict__ n,
                               const double* __restrict__ cj12, int nbf5, int naux, int nalpha, int nbeta,
                               double* __restrict__ tv) {
@@ -37,12 +37,11 @@ __global__ void w_diag_kernel(const double* __restrict__ bpq, const double* __re
         tv[i] = wbuild::diag_value(bpq, n, cj12, nbf5, nalpha, nbeta, i);
 }
 
-__global__ void __launch_bounds__(256) build_w_kernel(const double* __restrict__ bpq, const double* __restrict__ ck12,
+__global__ void __launch_bounds__(256, 4) build_w_kernel(const double* __restrict__ bpq, const double* __restrict__ ck12,
                                                       const double* __restrict__ tv, int nbf5, int naux,
                                                       double* __restrict__ W) {
-    __shared__ double tb[32][33];
-    const int nt = (nbf5 + 31) / 32;
-    const long long tiles = (long long)nt * nt * naux;
+    __shared__ double tb[wbuild::LT][32][33];
+    const long long tiles = wbuild::tiles(nbf5, naux);
     for (long long t = blockIdx.x; t < tiles; t += gridDim.x) wbuild::tile(bpq, ck12, tv, nbf5, naux, W, t, tb);
 }
 
@@ -165,8 +164,7 @@ int lagrange2_f64(donof_job* job, cudaStream_t st, const double* C, const double
         long long blocks = (Kt + 255) / 256;
         if (blocks > 8LL * ctx->sm_count) blocks = 8LL * ctx->sm_count;
         w_diag_kernel<<<(int)blocks, 256, 0, st>>>(bpq, n, cj12, nbf5, naux, nalpha, nbeta, tv); count_launch();
-        const long long nt = (nbf5 + 31) / 32;
-        blocks = nt * nt * naux;
+        blocks = wbuild::tiles(nbf5, naux);
         if (blocks > 16LL * ctx->sm_count) blocks = 16LL * ctx->sm_count;
         build_w_kernel<<<(int)blocks, 256, 0, st>>>(bpq, ck12, tv, nbf5, naux, W); count_launch();
         DONOF_CUDA(ctx, cudaGetLastError());
@@ -341,9 +339,8 @@ int lagrange2_f64_noalloc(donof_job* job, cudaStream_t st, const double* C, cons
         double* tv = W + (size_t)Kt * nbf5;
         w_diag_kernel<<<grid_for(Kt, 256, ctx->sm_count), 256, 0, st>>>(bpq, n, cj12, nbf5, naux, nalpha, nbeta,
                                                                         tv); count_launch();
-        const long long nt = (nbf5 + 31) / 32;
-        build_w_kernel<<<grid_for(nt * nt * naux * 256, 256, ctx->sm_count), 256, 0, st>>>(bpq, ck12, tv, nbf5,
-                                                                                           naux, W); count_launch();
+        build_w_kernel<<<grid_for(wbuild::tiles(nbf5, naux) * 256, 256, ctx->sm_count), 256, 0, st>>>(
+            bpq, ck12, tv, nbf5, naux, W); count_launch();
         DONOF_CUDA(ctx, cudaGetLastError());
     }
     // Y = tmp W (split-K partials in the scratch, then reduced)

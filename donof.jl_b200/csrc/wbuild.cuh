@@ -23,35 +23,68 @@ __device__ __forceinline__ double diag_value(const double* __restrict__ bpq, con
     return (dj ? n[b] * B[(long long)b * (nbf5 + 1)] : 0.0) + s;
 }
 
-// Tile t of the (b, q, l) tile list, 32 x 32 (b, q) per tile and nt = ceil(nbf5 / 32)
-// tiles per side; 256 threads (tx = threadIdx.x % 32, ty = threadIdx.x / 32),
-// transposed through shared memory so that b_pq^l and ck12 are read along b and
-// W is written along q.  Starts with a block barrier (the previous tile's reads
-// of tb are done).
+// Aux indices per tile: a tile covers 32 x 32 (b, q) for LT consecutive l.
+constexpr int LT = 4;
+
+// Number of tiles for nbf5, naux.
+__host__ __device__ __forceinline__ long long tiles(int nbf5, int naux) {
+    const long long nt = (nbf5 + 31) / 32;
+    return nt * nt * ((naux + LT - 1) / LT);
+}
+
+// Tile t of the (b, q, l-group) tile list: 32 x 32 (b, q) for the aux indices
+// l0 .. l0 + LT - 1; 256 threads (tx = threadIdx.x % 32, ty = threadIdx.x / 32).
+// Every load of the tile (ck12 once, b_pq^l for each l) is issued before the
+// first barrier; the transpose through shared memory makes b_pq^l and ck12 read
+// along b and W written along q.  Starts with a block barrier (the previous
+// tile's reads of tb are done).
 __device__ __forceinline__ void tile(const double* __restrict__ bpq, const double* __restrict__ ck12,
                                      const double* __restrict__ tv, int nbf5, int naux, double* __restrict__ W,
-                                     long long t, double (*tb)[33]) {
+                                     long long t, double (*tb)[32][33]) {
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     const long long n55 = (long long)nbf5 * nbf5, Kt = (long long)nbf5 * naux;
     const int nt = (nbf5 + 31) / 32;
     const int b0 = (int)(t % nt) * 32, q0 = (int)((t / nt) % nt) * 32;
-    const long long l = t / ((long long)nt * nt);
-    const double* B = bpq + n55 * l;
-    __syncthreads();
-    for (int r = ty; r < 32; r += 8) {
-        const int b = b0 + tx, q = q0 + r;
-        double v = 0.0;
-        if (b < nbf5 && q < nbf5) {
-            const long long e = b + (long long)nbf5 * q;
-            v = -ck12[e] * B[e];
-            if (q == b) v += tv[b + (long long)nbf5 * l];
+    const long long l0 = (t / ((long long)nt * nt)) * LT;
+    const int b = b0 + tx;
+    double ck[4], v[LT][4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const int q = q0 + ty + 8 * r;
+        ck[r] = (b < nbf5 && q < nbf5) ? ck12[b + (long long)nbf5 * q] : 0.0;
+    }
+#pragma unroll
+    for (int k = 0; k < LT; ++k) {
+        const long long l = l0 + k;
+        const double* B = bpq + n55 * l;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const int q = q0 + ty + 8 * r;
+            v[k][r] = (l < naux && b < nbf5 && q < nbf5) ? B[b + (long long)nbf5 * q] : 0.0;
         }
-        tb[r][tx] = v;  // [q - q0][b - b0]
     }
     __syncthreads();
-    for (int r = ty; r < 32; r += 8) {
-        const int q = q0 + tx, b = b0 + r;
-        if (b < nbf5 && q < nbf5) W[q + (long long)nbf5 * l + Kt * b] = tb[tx][r];
+#pragma unroll
+    for (int k = 0; k < LT; ++k) {
+        const long long l = l0 + k;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const int q = q0 + ty + 8 * r;
+            double w = -ck[r] * v[k][r];
+            if (q == b && l < naux && b < nbf5) w += tv[b + (long long)nbf5 * l];
+            tb[k][ty + 8 * r][tx] = w;  // [l - l0][q - q0][b - b0]
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < LT; ++k) {
+        const long long l = l0 + k;
+        if (l >= naux) break;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const int q = q0 + tx, bb = b0 + ty + 8 * r;
+            if (bb < nbf5 && q < nbf5) W[q + (long long)nbf5 * l + Kt * bb] = tb[k][tx][ty + 8 * r];
+        }
     }
 }
 
