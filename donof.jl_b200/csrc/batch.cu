@@ -244,6 +244,7 @@ GemmTile heuristic_tile(int M, int N) {
 }
 
 enum Stage { ST_T1 = 0, ST_T2 = 1, ST_Y = 2, NSTAGE = 3 };
+constexpr int NTILE = 4;  // tile shapes a stage's launch list can hold (GemmTile values)
 
 }  // namespace
 }  // namespace donof
@@ -299,12 +300,11 @@ struct donof_batch {
 
 namespace {
 
-bool stage_layout(int s, bool* ak, bool* bk) {
+void stage_layout(int s, bool* ak, bool* bk) {
     // T1: A = b (M-contiguous), B = C K-major; T2: A = C^T (K-major), B = tmp K-major;
     // Y: A = tmp (M-contiguous), B = W K-major.
     *ak = (s == ST_T2);
     *bk = true;
-    return true;
 }
 
 GemmF64Args stage_args(const donof_batch* B, int s, int j) {
@@ -349,7 +349,7 @@ int upload_gemm_tables(donof_batch* B, cudaStream_t st) {
         std::vector<GemmF64Args> args;
         std::vector<int> starts;
         B->launches[s].clear();
-        const GemmTile order[4] = {GemmTile::Large, GemmTile::SmallW8, GemmTile::Small, GemmTile::Tiny};
+        const GemmTile order[NTILE] = {GemmTile::Large, GemmTile::SmallW8, GemmTile::Small, GemmTile::Tiny};
         for (GemmTile t : order) {
             std::vector<int> js;
             for (int j = 0; j < B->nj; ++j)
@@ -741,7 +741,7 @@ int donof_batch_create(donof_ctx* ctx, int count, const donof_batch_shape* shape
     size_t o_gemm[NSTAGE], o_start[NSTAGE], o_pre[4];
     for (int s = 0; s < NSTAGE; ++s) {
         o_gemm[s] = take(sizeof(GemmF64Args) * count);
-        o_start[s] = take(sizeof(int) * (count + 3));
+        o_start[s] = take(sizeof(int) * (count + NTILE));  // one start array of n_k + 1 entries per tile shape
     }
     for (int k = 0; k < 4; ++k) o_pre[k] = take(sizeof(int) * (count + 1));
     rc = B->tab.ensure(ctx, tb);
