@@ -47,19 +47,17 @@ constexpr int KB = 64;                // n rows per b stage (8 KB TMA boxes)
 constexpr int BOX_M = 64;             // m per TMA box (128 B of bf16) = one T1 quarter
 constexpr int BOX_BYTES = KB * BOX_M * 2;           // 8 KB
 constexpr int STAGE_BYTES = 2 * BOX_BYTES;          // hi + lo, 16 KB
-constexpr int RING = 4;                             // b stages in shared memory (64 KB)
+constexpr int RING = 5;                             // b stages in shared memory (80 KB)
 constexpr int CS_BOX_BYTES = 128 * 64 * 2;          // 16 KB: 128 rows x 64 k
 constexpr int CS_BYTES = 4 * CS_BOX_BYTES;          // K up to 256 -> 64 KB
 constexpr int A2_BYTES = 4 * CS_BOX_BYTES;          // tmp split, 64 KB
 constexpr int A3_BYTES = CS_BOX_BYTES;              // W split, 16 KB
-constexpr int CK_BYTES = 64 * 64 * 4;                // ck12 (transposed, FP32), 16 KB
 // shared-memory map (offsets from a 1024-aligned base)
 constexpr int OFF_CS = 0;
 constexpr int OFF_RING = OFF_CS + CS_BYTES;
 constexpr int OFF_A2 = OFF_RING + RING * STAGE_BYTES;
 constexpr int OFF_A3 = OFF_A2 + A2_BYTES;
-constexpr int OFF_CK = OFF_A3 + A3_BYTES;
-constexpr int OFF_DS = OFF_CK + CK_BYTES;            // 64 floats d
+constexpr int OFF_DS = OFF_A3 + A3_BYTES;            // 64 floats d
 constexpr int OFF_BAR = OFF_DS + 256;
 constexpr int NBAR = 32;
 constexpr int OFF_MISC = OFF_BAR + NBAR * 8;         // tmem base, abort flag
@@ -339,12 +337,8 @@ lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_const
             epi_sync();
             return r;
         };
-        // ck12 (transposed) staged once per CTA: cks[b * 64 + q] = ck12[b, q]
-        float* cks = reinterpret_cast<float*>(sm + OFF_CK);
-#pragma unroll
-        for (int i = 0; i < 8; ++i)
-            reinterpret_cast<float4*>(cks)[threadIdx.x + 128 * i] =
-                __ldg(reinterpret_cast<const float4*>(P.ck32t) + threadIdx.x + 128 * i);
+        // ck12 (transposed, 16 KB) is read through L1 where W is built: the shared
+        // memory it would take holds a fifth stage of the b ring instead.
         // row q of cj12 restricted to this thread's half of the columns, kept in registers
         float cjr[32];
 #pragma unroll
@@ -464,11 +458,11 @@ lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_const
                 // This thread builds part of A3 row b = q (hi: prow(q, 0), lo: prow(q, 1)) over
                 // K = k in [off, off + 32), using the symmetry of b_pq (bq[i] = b_pq[off + i, q]):
                 // W[k, q] = delta_kq (n'_q d_q + t_q) - ck12[q, k] b_pq[q, k]
-                const float4* ckrow = reinterpret_cast<const float4*>(cks + q * 64 + off);  // ck12[q, off + i]
+                const float4* ckrow = reinterpret_cast<const float4*>(P.ck32t + q * 64 + off);  // ck12[q, off + i]
                 const int rh = prow(q, 0), rl = prow(q, 1);
 #pragma unroll
                 for (int c = 0; c < 4; ++c) {
-                    const float4 k0 = ckrow[2 * c], k1 = ckrow[2 * c + 1];
+                    const float4 k0 = __ldg(ckrow + 2 * c), k1 = __ldg(ckrow + 2 * c + 1);
                     const float ck8[8] = {k0.x, k0.y, k0.z, k0.w, k1.x, k1.y, k1.z, k1.w};
                     __align__(16) __nv_bfloat16 h[8], lo[8];
 #pragma unroll
