@@ -641,7 +641,7 @@ def main():
         peak = measured_dgemm_tflops(torch, dev)
         roof = {"bound": "tensor", "achieved": flops / tr / 1e12, "peak": peak, "unit": "TFLOP/s",
                 "frac": flops / tr / 1e12 / peak, "traffic": traffic_from_profiles("t1_f64"),
-                "kernel": "gemm_f64_kernel<128,64> T1: tmp_l = b_l C5, batched over naux (DMMA)",
+                "kernel": "gemm_f64 T1 (DMMA; tile shape and grid form chosen by the autotuner): tmp_l = b_l C5, batched over naux",
                 "algorithmic": f"2*nbf^2*nbf5*naux = {flops:.4e} FLOP per launch", "ms": tr * 1e3,
                 "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor pipe); of measured"}
     else:

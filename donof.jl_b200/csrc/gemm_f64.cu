@@ -14,7 +14,40 @@ namespace donof {
 namespace {
 
 template <int BM, int BN, int WM, int WN, bool AK, bool BKM, bool VEC>
-cudaError_t launch_cfg(const GemmF64Args& p, cudaStream_t st) {
+cudaError_t launch_persistent(const GemmF64Args& p, cudaStream_t st) {
+    constexpr int BK = 16, STAGES = 3;
+    using Cfg = GemmF64Cfg<BM, BN, BK, WM, WN, STAGES, AK, BKM, VEC>;
+    auto kern = gemm_f64_persistent_kernel<BM, BN, BK, WM, WN, STAGES, AK, BKM, VEC>;
+    static std::atomic<unsigned long long> attr_mask{0};
+    static std::atomic<int> per_sm_cached{0};
+    static std::atomic<int> sm_cached{0};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (!(attr_mask.load(std::memory_order_acquire) & bit)) {
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM_BYTES);
+        if (e != cudaSuccess) return e;
+        int per_sm = 0, sms = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, Cfg::THREADS, Cfg::SMEM_BYTES);
+        if (e != cudaSuccess) return e;
+        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) return e;
+        per_sm_cached.store(per_sm < 1 ? 1 : per_sm, std::memory_order_release);
+        sm_cached.store(sms, std::memory_order_release);
+        attr_mask.fetch_or(bit, std::memory_order_acq_rel);
+    }
+    const long long total = (long long)((p.M + BM - 1) / BM) * ((p.N + BN - 1) / BN) * p.batch * p.splits;
+    long long grid = (long long)per_sm_cached.load(std::memory_order_acquire) * sm_cached.load(std::memory_order_acquire);
+    if (grid > total) grid = total;
+    if (grid < 1) grid = 1;
+    kern<<<(unsigned)grid, Cfg::THREADS, Cfg::SMEM_BYTES, st>>>(p); count_launch();
+    return cudaGetLastError();
+}
+
+template <int BM, int BN, int WM, int WN, bool AK, bool BKM, bool VEC>
+cudaError_t launch_cfg(const GemmF64Args& p, cudaStream_t st, bool persistent) {
+    if (persistent) return launch_persistent<BM, BN, WM, WN, AK, BKM, VEC>(p, st);
     constexpr int BK = 16, STAGES = 3;
     using Cfg = GemmF64Cfg<BM, BN, BK, WM, WN, STAGES, AK, BKM, VEC>;
     auto kern = gemm_f64_kernel<BM, BN, BK, WM, WN, STAGES, AK, BKM, VEC>;
@@ -36,17 +69,17 @@ cudaError_t launch_cfg(const GemmF64Args& p, cudaStream_t st) {
 }
 
 template <int BM, int BN, int WM, int WN, bool AK, bool BKM>
-cudaError_t launch_vec(const GemmF64Args& p, bool vec, cudaStream_t st) {
-    return vec ? launch_cfg<BM, BN, WM, WN, AK, BKM, true>(p, st)
-               : launch_cfg<BM, BN, WM, WN, AK, BKM, false>(p, st);
+cudaError_t launch_vec(const GemmF64Args& p, bool vec, cudaStream_t st, bool persistent) {
+    return vec ? launch_cfg<BM, BN, WM, WN, AK, BKM, true>(p, st, persistent)
+               : launch_cfg<BM, BN, WM, WN, AK, BKM, false>(p, st, persistent);
 }
 
 template <int BM, int BN, int WM, int WN>
-cudaError_t launch_layout(const GemmF64Args& p, bool ak, bool bk, bool vec, cudaStream_t st) {
-    if (ak && bk) return launch_vec<BM, BN, WM, WN, true, true>(p, vec, st);
-    if (ak && !bk) return launch_vec<BM, BN, WM, WN, true, false>(p, vec, st);
-    if (!ak && bk) return launch_vec<BM, BN, WM, WN, false, true>(p, vec, st);
-    return launch_vec<BM, BN, WM, WN, false, false>(p, vec, st);
+cudaError_t launch_layout(const GemmF64Args& p, bool ak, bool bk, bool vec, cudaStream_t st, bool persistent) {
+    if (ak && bk) return launch_vec<BM, BN, WM, WN, true, true>(p, vec, st, persistent);
+    if (ak && !bk) return launch_vec<BM, BN, WM, WN, true, false>(p, vec, st, persistent);
+    if (!ak && bk) return launch_vec<BM, BN, WM, WN, false, true>(p, vec, st, persistent);
+    return launch_vec<BM, BN, WM, WN, false, false>(p, vec, st, persistent);
 }
 
 bool aligned16(const void* ptr) { return (reinterpret_cast<uintptr_t>(ptr) & 15u) == 0; }
@@ -138,6 +171,11 @@ int gemm_f64_grouped(donof_ctx* ctx, cudaStream_t st, bool a_kmajor, bool b_kmaj
 
 int gemm_f64(donof_ctx* ctx, cudaStream_t st, bool a_kmajor, bool b_kmajor, GemmF64Args p,
              GemmTile tile) {
+    return gemm_f64_run(ctx, st, a_kmajor, b_kmajor, p, tile, false);
+}
+
+int gemm_f64_run(donof_ctx* ctx, cudaStream_t st, bool a_kmajor, bool b_kmajor, GemmF64Args p,
+                 GemmTile tile, bool persistent) {
     if (p.M <= 0 || p.N <= 0 || p.batch <= 0) return DONOF_OK;
     if (p.splits < 1) p.splits = 1;
     if (p.splits == 1 || p.kchunk <= 0) p.kchunk = p.K;
@@ -150,11 +188,11 @@ int gemm_f64(donof_ctx* ctx, cudaStream_t st, bool a_kmajor, bool b_kmajor, Gemm
     const bool vec = va && vb;
     cudaError_t e;
     if (tile == GemmTile::Large)
-        e = launch_layout<128, 64, 4, 2>(p, a_kmajor, b_kmajor, vec, st);
+        e = launch_layout<128, 64, 4, 2>(p, a_kmajor, b_kmajor, vec, st, persistent);
     else if (tile == GemmTile::Small || tile == GemmTile::SmallW8)
-        e = launch_layout<64, 64, 2, 2>(p, a_kmajor, b_kmajor, vec, st);
+        e = launch_layout<64, 64, 2, 2>(p, a_kmajor, b_kmajor, vec, st, persistent);
     else
-        e = launch_layout<32, 32, 2, 2>(p, a_kmajor, b_kmajor, vec, st);
+        e = launch_layout<32, 32, 2, 2>(p, a_kmajor, b_kmajor, vec, st, persistent);
     if (e != cudaSuccess) {
         set_error(ctx, "gemm_f64 launch (M=%d N=%d K=%d batch=%d splits=%d): %s", p.M, p.N, p.K,
                   p.batch, p.splits, cudaGetErrorString(e));
@@ -234,6 +272,7 @@ struct TuneKey {
 struct TuneVal {
     GemmTile tile;
     int splits;
+    bool persistent = false;  // gemm_f64_persistent_kernel instead of one CTA per tile
 };
 std::mutex g_tune_mu;
 std::map<TuneKey, TuneVal> g_tune;
@@ -296,11 +335,14 @@ int gemm_f64_tuned(donof_ctx* ctx, cudaStream_t st, bool a_kmajor, bool b_kmajor
     if (!tunable) return gemm_f64(ctx, st, a_kmajor, b_kmajor, p, heuristic);
     const TuneKey key{ctx->device, p.M, p.N, p.K, p.batch, a_kmajor, b_kmajor, 0};
     TuneVal v;
-    if (tune_lookup(key, &v)) return gemm_f64(ctx, st, a_kmajor, b_kmajor, p, v.tile);
+    if (tune_lookup(key, &v)) return gemm_f64_run(ctx, st, a_kmajor, b_kmajor, p, v.tile, v.persistent);
     if (capturing(st)) return gemm_f64(ctx, st, a_kmajor, b_kmajor, p, heuristic);
-    const int best = time_candidates(ctx, st, 3, [&](int c) { return gemm_f64(ctx, st, a_kmajor, b_kmajor, p, kTiles[c]); });
+    // every tile shape, one CTA per tile and persistent
+    const int best = time_candidates(ctx, st, 6, [&](int c) {
+        return gemm_f64_run(ctx, st, a_kmajor, b_kmajor, p, kTiles[c % 3], c >= 3);
+    });
     if (best < 0) return DONOF_ERR_CUDA;
-    tune_store(key, TuneVal{kTiles[best], 1});
+    tune_store(key, TuneVal{kTiles[best % 3], 1, best >= 3});
     return DONOF_OK;  // every candidate wrote the same C
 }
 
@@ -335,6 +377,8 @@ int partials_choice(donof_ctx* ctx, cudaStream_t st, bool a_kmajor, bool b_kmajo
                 if (!dup) cands.push_back(TuneVal{kTiles[t], (int)s});
             }
         }
+        const size_t nplain = cands.size();
+        for (size_t c = 0; c < nplain; ++c) cands.push_back(TuneVal{cands[c].tile, cands[c].splits, true});
     }
     auto config = [&](const TuneVal& c, GemmF64Args* q, int* ns) {
         *q = p;
@@ -362,7 +406,7 @@ int partials_choice(donof_ctx* ctx, cudaStream_t st, bool a_kmajor, bool b_kmajo
             GemmF64Args q;
             int ns;
             config(cands[c], &q, &ns);
-            return gemm_f64(ctx, st, a_kmajor, b_kmajor, q, cands[c].tile);
+            return gemm_f64_run(ctx, st, a_kmajor, b_kmajor, q, cands[c].tile, cands[c].persistent);
         });
         if (best < 0) return DONOF_ERR_CUDA;
         v = cands[best];
@@ -383,7 +427,7 @@ int gemm_f64_partials(donof_ctx* ctx, cudaStream_t st, bool a_kmajor, bool b_kma
     GemmF64Args q;
     int splits = 1;
     DONOF_CHECK(partials_choice(ctx, st, a_kmajor, b_kmajor, M, N, K, A, lda, B, ldb, part, &v, &q, &splits));
-    DONOF_CHECK(gemm_f64(ctx, st, a_kmajor, b_kmajor, q, v.tile));
+    DONOF_CHECK(gemm_f64_run(ctx, st, a_kmajor, b_kmajor, q, v.tile, v.persistent));
     *out = part->as<double>();
     *nparts = splits;
     return DONOF_OK;

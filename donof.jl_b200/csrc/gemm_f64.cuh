@@ -349,6 +349,44 @@ constexpr int grouped_min_ctas() {
     return BM * BN <= 32 * 32 ? 6 : ((BM * BN <= 64 * 64 && WARPS_M * WARPS_N <= 4) ? 3 : 2);
 }
 
+// Persistent form of one GEMM: a grid of about one wave of CTAs walks the
+// tiles of gemm_f64_kernel's 3-D grid (in its order, x fastest) and starts the
+// cp.async prologue of its next tile before it stores the current one.  Same
+// tile routine, so it writes what gemm_f64_kernel writes; the autotuner picks
+// between the two.  The device-side gates hold for the whole launch.
+template <int BM, int BN, int BK, int WARPS_M, int WARPS_N, int STAGES, bool AK, bool BKM, bool VEC>
+__global__ void __launch_bounds__(32 * WARPS_M * WARPS_N, (grouped_min_ctas<BM, BN, WARPS_M, WARPS_N>()))
+gemm_f64_persistent_kernel(const GemmF64Args p) {
+    extern __shared__ __align__(16) double smem[];
+    using Tile = GemmTileF64<BM, BN, BK, WARPS_M, WARPS_N, STAGES, AK, BKM, VEC>;
+    const int gx = (p.M + BM - 1) / BM, gy = (p.N + BN - 1) / BN;
+    const int total = gx * gy * p.batch * p.splits;
+    int t = blockIdx.x;
+    if (t >= total) return;
+    Tile cur;
+    cur.init(p, t % gx, (t / gx) % gy, t / (gx * gy));
+    if (cur.skip) return;
+    cur.prologue(smem);
+    typename Tile::Acc acc;
+    while (true) {
+        cur.mainloop(smem, acc);
+        const int tn = t + gridDim.x;
+        const bool more = tn < total;
+        Tile nxt;
+        if (more) {
+            nxt.init(p, tn % gx, (tn / gx) % gy, tn / (gx * gy));
+            __syncthreads();  // every warp is done with the stages the prologue overwrites
+            nxt.prologue(smem);
+        }
+        cur.epilogue(acc);
+        if (!more) break;
+        cur = nxt;
+        t = tn;
+    }
+    gemm_detail::cp_async_wait<0>();
+}
+
+
 template <int BM, int BN, int BK, int WARPS_M, int WARPS_N, int STAGES, bool AK, bool BKM, bool VEC>
 __global__ void __launch_bounds__(32 * WARPS_M * WARPS_N, (grouped_min_ctas<BM, BN, WARPS_M, WARPS_N>()))
 gemm_f64_grouped_kernel(const GemmF64Args* __restrict__ groups, const int* __restrict__ start, int ngroups) {

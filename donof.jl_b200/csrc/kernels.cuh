@@ -13,6 +13,10 @@ enum class GemmTile { Large /*128x64*/, Small /*64x64*/, Tiny /*32x32*/, SmallW8
 // C = alpha*op(A)op(B) + beta*C on stream st (see gemm_f64.cuh for addressing).
 int gemm_f64(donof_ctx* ctx, cudaStream_t st, bool a_kmajor, bool b_kmajor, GemmF64Args p,
              GemmTile tile);
+// Same; persistent: one wave of CTAs walks the tiles (gemm_f64_persistent_kernel),
+// which writes the same result.
+int gemm_f64_run(donof_ctx* ctx, cudaStream_t st, bool a_kmajor, bool b_kmajor, GemmF64Args p,
+                 GemmTile tile, bool persistent);
 
 // out[i] = sum_s part[i + s*stride] (+ beta*out[i]), i < count
 int splitk_reduce(donof_ctx* ctx, cudaStream_t st, const double* part, long long stride,
