@@ -159,14 +159,13 @@ __global__ void __launch_bounds__(256) b_copy_kernel(const BJob* __restrict__ jo
 
 __global__ void __launch_bounds__(256) b_wdiag_kernel(const BJob* __restrict__ jobs, const int* __restrict__ pre,
                                                       int njobs) {
+    __shared__ double sd[wbuild::DIAG_SM];
     const int total = pre[njobs];
     for (int u = blockIdx.x; u < total; u += gridDim.x) {
         const int j = job_of(pre, njobs, u);
         const BJob& J = jobs[j];
         if (J.S->stopped) continue;
-        const long long k0 = (long long)(u - pre[j]) * CH, k1 = min((long long)J.nbf5 * J.naux, k0 + CH);
-        for (long long k = k0 + threadIdx.x; k < k1; k += blockDim.x)
-            J.tv[k] = wbuild::diag_value(J.bpq, J.n, J.cj12, J.nbf5, J.nalpha, J.nbeta, k);
+        wbuild::diag_unit(J.bpq, J.n, J.cj12, J.nbf5, J.naux, J.nalpha, J.nbeta, J.tv, u - pre[j], sd);
     }
 }
 
@@ -276,7 +275,7 @@ struct donof_batch {
     TailJob* d_tail = nullptr;
     GemmF64Args* d_gemm[NSTAGE] = {};
     int* d_start[NSTAGE] = {};
-    int* d_pre[4] = {};  // units of: nvar chunks, nn chunks, wdiag chunks, build_w tiles
+    int* d_pre[4] = {};  // units of: nvar chunks, nn chunks, W diagonal groups, build_w tiles
     void* d_rstate = nullptr;
     void* d_tstate = nullptr;
     BOrbState* d_state = nullptr;
@@ -769,7 +768,7 @@ int donof_batch_create(donof_ctx* ctx, int count, const donof_batch_shape* shape
     for (int j = 0; j < count; ++j) {
         const S& h = B->sh[j];
         const long long u[4] = {(h.nvar + CH - 1) / CH, (h.nn + CH - 1) / CH,
-                                ((long long)h.nbf5 * h.naux + CH - 1) / CH, wbuild::tiles(h.nbf5, h.naux)};
+                                wbuild::diag_units(h.nbf5, h.naux), wbuild::tiles(h.nbf5, h.naux)};
         for (int k = 0; k < 4; ++k) {
             const long long v = pre[k][j] + u[k];
             if (v > 0x7fffffffLL) {

@@ -25,16 +25,17 @@ namespace donof {
 namespace {
 
 // W of every aux index (wbuild.cuh) in two fully parallel passes: w_diag_kernel
-// forms n'_b d_b^l + t_b^l (one thread per (b, l), cj12 read along b);
+// forms n'_b d_b^l + t_b^l (one thread per (b, l), cj12 read along b, the
+// diagonals d^l staged in shared memory per group of aux indices);
 // build_w_kernel the elementwise part over tiles of 32 x 32 (b, q) and
 // wbuild::LT aux indices, one tile per CTA step (b need not be symmetric).
-__global__ void w_diag_kernel(const double* __restrict__ bpq, const double* __restrict__ n,
-                              const double* __restrict__ cj12, int nbf5, int naux, int nalpha, int nbeta,
-                              double* __restrict__ tv) {
-    const long long total = (long long)nbf5 * naux;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
-         i += (long long)gridDim.x * blockDim.x)
-        tv[i] = wbuild::diag_value(bpq, n, cj12, nbf5, nalpha, nbeta, i);
+__global__ void __launch_bounds__(256) w_diag_kernel(const double* __restrict__ bpq, const double* __restrict__ n,
+                                                     const double* __restrict__ cj12, int nbf5, int naux, int nalpha,
+                                                     int nbeta, double* __restrict__ tv) {
+    __shared__ double sd[wbuild::DIAG_SM];
+    const long long units = wbuild::diag_units(nbf5, naux);
+    for (long long u = blockIdx.x; u < units; u += gridDim.x)
+        wbuild::diag_unit(bpq, n, cj12, nbf5, naux, nalpha, nbeta, tv, u, sd);
 }
 
 __global__ void __launch_bounds__(256, 4) build_w_kernel(const double* __restrict__ bpq, const double* __restrict__ ck12,
@@ -161,7 +162,7 @@ int lagrange2_f64(donof_job* job, cudaStream_t st, const double* C, const double
     double* tv = W + (size_t)Kt * nbf5;  // n'_b d_b^l + t_b^l (Kt values)
     {
         const double* bpq = job->bpq.as<double>();
-        long long blocks = (Kt + 255) / 256;
+        long long blocks = wbuild::diag_units(nbf5, naux);
         if (blocks > 8LL * ctx->sm_count) blocks = 8LL * ctx->sm_count;
         w_diag_kernel<<<(int)blocks, 256, 0, st>>>(bpq, n, cj12, nbf5, naux, nalpha, nbeta, tv); count_launch();
         blocks = wbuild::tiles(nbf5, naux);
@@ -337,8 +338,8 @@ int lagrange2_f64_noalloc(donof_job* job, cudaStream_t st, const double* C, cons
     }
     {
         double* tv = W + (size_t)Kt * nbf5;
-        w_diag_kernel<<<grid_for(Kt, 256, ctx->sm_count), 256, 0, st>>>(bpq, n, cj12, nbf5, naux, nalpha, nbeta,
-                                                                        tv); count_launch();
+        w_diag_kernel<<<grid_for(wbuild::diag_units(nbf5, naux) * 256, 256, ctx->sm_count), 256, 0, st>>>(
+            bpq, n, cj12, nbf5, naux, nalpha, nbeta, tv); count_launch();
         build_w_kernel<<<grid_for(wbuild::tiles(nbf5, naux) * 256, 256, ctx->sm_count), 256, 0, st>>>(
             bpq, ck12, tv, nbf5, naux, W); count_launch();
         DONOF_CUDA(ctx, cudaGetLastError());

@@ -23,6 +23,61 @@ __device__ __forceinline__ double diag_value(const double* __restrict__ bpq, con
     return (dj ? n[b] * B[(long long)b * (nbf5 + 1)] : 0.0) + s;
 }
 
+// The diagonal terms for a group of aux indices at a time: their diagonals
+// d^l staged in shared memory once per block (DIAG_SM doubles), then one
+// thread per (b, l) sums over q in the order of diag_value (same result).
+constexpr int DIAG_SM = 2048;
+
+// aux indices per group for nbf5 (about one (b, l) per thread of a 256-thread
+// block); 0 when nbf5 is too large to stage (diag_value per element instead)
+__host__ __device__ __forceinline__ int diag_group(int nbf5) {
+    if (nbf5 > DIAG_SM) return 0;
+    int g = 256 / nbf5;
+    if (g < 1) g = 1;
+    if (g * nbf5 > DIAG_SM) g = DIAG_SM / nbf5;
+    return g;
+}
+
+// Work units for nbf5, naux: groups of diag_group(nbf5) aux indices, or
+// 1024-element chunks of the (b, l) list when nbf5 cannot be staged.
+__host__ __device__ __forceinline__ long long diag_units(int nbf5, int naux) {
+    const int g = diag_group(nbf5);
+    return g > 0 ? (naux + g - 1) / g : ((long long)nbf5 * naux + 1023) / 1024;
+}
+
+// Unit u of diag_units; sd: DIAG_SM doubles of shared memory.  Starts with a
+// block barrier (the previous unit's reads of sd are done).
+__device__ __forceinline__ void diag_unit(const double* __restrict__ bpq, const double* __restrict__ n,
+                                          const double* __restrict__ cj12, int nbf5, int naux, int nalpha, int nbeta,
+                                          double* __restrict__ tv, long long u, double* sd) {
+    const int g = diag_group(nbf5);
+    if (g == 0) {
+        const long long k0 = u * 1024, k1 = min((long long)nbf5 * naux, k0 + 1024);
+        for (long long k = k0 + threadIdx.x; k < k1; k += blockDim.x)
+            tv[k] = diag_value(bpq, n, cj12, nbf5, nalpha, nbeta, k);
+        return;
+    }
+    const long long n55 = (long long)nbf5 * nbf5, l0 = u * g;
+    const int items = g * nbf5;
+    __syncthreads();
+    for (int i = threadIdx.x; i < items; i += blockDim.x) {
+        const int li = i / nbf5, q = i - li * nbf5;
+        const long long l = l0 + li;
+        sd[i] = (l < naux) ? bpq[n55 * l + (long long)q * (nbf5 + 1)] : 0.0;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < items; i += blockDim.x) {
+        const int li = i / nbf5, b = i - li * nbf5;
+        const long long l = l0 + li;
+        if (l >= naux) continue;
+        const double* d = sd + li * nbf5;
+        double s = 0.0;
+        for (int q = 0; q < nbf5; ++q) s += cj12[b + (long long)nbf5 * q] * d[q];
+        const bool dj = (nbeta > 0) && (b < nbeta || b >= nalpha);
+        tv[b + (long long)nbf5 * l] = (dj ? n[b] * d[b] : 0.0) + s;
+    }
+}
+
 // Aux indices per tile: a tile covers 32 x 32 (b, q) for LT consecutive l.
 constexpr int LT = 4;
 

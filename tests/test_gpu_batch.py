@@ -211,3 +211,37 @@ def test_batch_orbopt_leaves_out_jobs_with_maxloop_zero(cuda_ctx):
     batch.free()
     for b in bts:
         b.free()
+
+
+def test_batch_energy_variants_match_each_job_alone(cuda_ctx):
+    """The batched energy loop for trigonometric occupations, an open shell and
+    another GNOF variant (ista 1), with the ADABelief orbital optimiser: every
+    job bit-for-bit what donof_energy gives it alone."""
+    import copy
+
+    from donof_b200 import Param, workload
+    from donof_b200.gnof import guess_gamma
+
+    def job(kw, seed, **over):
+        wl = workload.molecule_like(**kw, seed=seed, two_e_scale=0.2)
+        p = Param(nbf=kw["nbf"], nbfaux=kw["naux"], nbeta=kw["nbeta"], nalpha=over.pop("nalpha", kw["nbeta"]),
+                  ncwo=kw["ncwo"], **over)
+        p.orb_method = "ADABelief"
+        p.threshgorb = p.threshgocc = 1e-5
+        p.threshen = 1e-9
+        return wl, p, guess_gamma(p)
+
+    jobs = [job(dict(nbf=28, naux=60, nbeta=4, ncwo=3), 11, occ_method="Trigonometric"),
+            job(dict(nbf=30, naux=64, nbeta=4, ncwo=3), 12, nalpha=6),
+            job(dict(nbf=24, naux=50, nbeta=3, ncwo=3), 13, ista=1)]
+    bts = [d.eris_to_gpu(wl.b, "fp64", cuda_ctx) for wl, _, _ in jobs]
+    batch = d.Batch(bts, [copy.deepcopy(p) for _, p, _ in jobs], cuda_ctx)
+    res = batch.energy([wl.H for wl, _, _ in jobs], [wl.C for wl, _, _ in jobs], [g for _, _, g in jobs], maxit=500)
+    for j, ((wl, p, g), bt) in enumerate(zip(jobs, bts)):
+        C, gamma, n, r = res[j]
+        C1, g1, n1, _, r1, _ = d.api.energy_loop(wl.H, bt, copy.deepcopy(p), wl.C, g, maxit=500)
+        assert r == r1, (j, r, r1)
+        assert np.array_equal(C, C1) and np.array_equal(gamma, g1) and np.array_equal(n, n1), j
+    batch.free()
+    for b in bts:
+        b.free()
