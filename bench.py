@@ -204,11 +204,19 @@ def host_adam(state, g, i, alpha, beta1=0.5, beta2=0.9):
     return -alpha * (m / (1 - beta1 ** i)) / np.sqrt(vmax + 1e-16)
 
 
+_PACK_INDEX = {}
+
+
 def pack(elag, nbf5):
-    g = 4.0 * (elag - elag.T)
-    iu = np.triu_indices(elag.shape[0], 1)
-    sel = iu[0] < nbf5
-    return g[iu[0][sel], iu[1][sel]]
+    """calcorbg's packing of 4 (elag - elag^T), row-wise over i < nbf5, j > i
+    (src/pnof.jl:1395-1403); the index arrays are built once per size."""
+    key = (elag.shape[0], nbf5)
+    if key not in _PACK_INDEX:
+        iu = np.triu_indices(elag.shape[0], 1)
+        sel = iu[0] < nbf5
+        _PACK_INDEX[key] = (iu[0][sel], iu[1][sel])
+    i, j = _PACK_INDEX[key]
+    return 4.0 * (elag[i, j] - elag[j, i])
 
 
 def run_cpu_steps(wl, steps, budget_s, threads=None):
