@@ -21,8 +21,15 @@ FP64) exceeds the 126 MB L2, so no flush is needed between steps.
           with closing FP64 iterations, from the same start, on a molecule-
           shaped surrogate (nbf = 96, naux = 384), with |dE| between them
   serving  converged energies/s of a seeded Poisson stream of jobs of different
-          sizes, served with continuous batching, against the plain FP64 form
-          serving the same stream one job at a time; p50/p99 latency; |dE|
+          sizes, served with continuous batching (and with small FP64 jobs
+          started as grouped batches), against the plain FP64 form serving the
+          same stream one job at a time; p50/p99 latency; |dE|
+  batched  job orbital-gradient steps/s of 64 uneven water-cluster surrogates
+          advanced together (one grouped launch per stage of a step, the loop as
+          one captured graph) against the same jobs one after the other
+  batched_energies  converged energies/s of 16 molecule surrogates through the
+          batched energy loop against donof_energy per job (|dE| = 0: the
+          grouped path is bit-for-bit the single-job one)
   --impl reference   the CPU restatement of the reference path (C/OpenMP FP64
           oracle, all host threads) on the same workload
 

@@ -110,7 +110,8 @@ int check_sizes(donof_ctx* ctx, int nbf, int nbf5, int nalpha, int nbeta) {
 // host and then sent by an asynchronous DMA; an output is DMA'd into it and
 // copied to the caller's array once finish() has synchronised the stream.
 // Page-locked transfers run at full PCIe speed whatever memory the caller
-// passes.  Without pin() the copies use the caller's memory directly.
+// passes.  Without pin(), or when no page-locked memory can be allocated, the
+// copies use the caller's memory directly.
 struct Stager {
     donof_ctx* ctx;
     cudaStream_t st;
@@ -138,7 +139,12 @@ struct Stager {
             if (ctx->hstage) cudaFreeHost(ctx->hstage);
             ctx->hstage = nullptr;
             ctx->hstage_bytes = 0;
-            DONOF_CUDA(ctx, cudaMallocHost(&ctx->hstage, total));
+            if (cudaMallocHost(&ctx->hstage, total) != cudaSuccess) {
+                // no page-locked memory to be had: copy from the caller's arrays directly
+                cudaGetLastError();
+                ctx->hstage = nullptr;
+                return DONOF_OK;
+            }
             ctx->hstage_bytes = total;
         }
         pinned = static_cast<char*>(ctx->hstage);
