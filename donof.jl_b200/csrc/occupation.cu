@@ -263,12 +263,50 @@ struct RowSums {
     double jn;
 };
 
+// Rows are taken four at a time (the last ones one at a time): every row keeps
+// its own accumulators summed in order of j, so the result is the same as row by
+// row, with four independent chains per sum in flight instead of one.
 void row_sums(const Occ& o, const OrbVecs& v, const double* J, const double* K, std::vector<RowSums>& rs) {
     const int N = o.N;
     const int bnd[5] = {0, o.no1, o.nbeta, o.nalpha, N};
     const double *vn = v.n.data(), *vf = v.fi.data(), *v12 = v.nd12.data(), *vd = v.nd.data();
     rs.resize(N);
-    for (int i = 0; i < N; ++i) {
+    constexpr int RB = 4;
+    int i0 = 0;
+    for (; i0 + RB <= N; i0 += RB) {
+        const double* Kc[RB];
+        const double* Jc[RB];
+        for (int u = 0; u < RB; ++u) {
+            Kc[u] = K + (size_t)N * (i0 + u);
+            Jc[u] = J + (size_t)N * (i0 + u);
+        }
+        for (int R = 0; R < 4; ++R) {
+            double a0[RB] = {}, a1[RB] = {}, a2[RB] = {}, a3[RB] = {}, a4[RB] = {};
+            for (int j = bnd[R]; j < bnd[R + 1]; ++j) {
+                const double n_ = vn[j], f_ = vf[j], h_ = v12[j], d_ = vd[j];
+                for (int u = 0; u < RB; ++u) {
+                    const double kj = Kc[u][j];
+                    a0[u] += n_ * kj;
+                    a1[u] += f_ * kj;
+                    a2[u] += h_ * kj;
+                    a3[u] += d_ * kj;
+                    a4[u] += kj;
+                }
+            }
+            for (int u = 0; u < RB; ++u) {
+                RowSums& r = rs[i0 + u];
+                r.S[R][V_N] = a0[u]; r.S[R][V_FI] = a1[u]; r.S[R][V_ND12] = a2[u]; r.S[R][V_ND] = a3[u];
+                r.S[R][V_ONE] = a4[u];
+            }
+        }
+        double jn[RB] = {};
+        for (int j = 0; j < N; ++j) {
+            const double n_ = vn[j];
+            for (int u = 0; u < RB; ++u) jn[u] += n_ * Jc[u][j];
+        }
+        for (int u = 0; u < RB; ++u) rs[i0 + u].jn = jn[u];
+    }
+    for (int i = i0; i < N; ++i) {
         const double* Kc = K + (size_t)N * i;
         const double* Jc = J + (size_t)N * i;
         RowSums& r = rs[i];
