@@ -70,13 +70,25 @@ bool setup(const donof_occ_params* q, Occ& o) {
     return true;
 }
 
-// n (N) and dn (N x nv, dn[i * nv + k]) for the configured occupation map
-void occupations(const Occ& o, const double* gamma, double* n, double* dn) {
+namespace {
+
+// n and dn; with full, every entry of dn is written, else only the pair blocks
+// (the rows of a pair's members at the pair's gamma columns, KG), the only
+// entries energy_grad reads.
+void occupations_impl(const Occ& o, const double* gamma, double* n, double* dn, bool full) {
     const int N = o.N, nv = o.nv, nd = o.ndoc, nc = o.ncwo;
     for (int i = 0; i < N; ++i) n[i] = 0.0;
     for (int i = 0; i < o.no1; ++i) n[i] = 1.0;
     for (int i = o.no1 + nd; i < o.no1 + nd + o.nsoc; ++i) n[i] = o.high_spin ? 1.0 : 0.5;
-    std::fill(dn, dn + (size_t)N * nv, 0.0);
+    if (full) {
+        std::fill(dn, dn + (size_t)N * nv, 0.0);
+    } else {
+        for (int g = 0; g < nd; ++g)
+            for (int m = 0; m <= nc; ++m) {
+                const int r = (m == 0) ? o.S[g] : o.P[g * nc + m - 1];
+                for (int c = 0; c < nc; ++c) dn[(size_t)r * nv + o.KG[g * nc + c]] = 0.0;
+            }
+    }
     if (o.method == 0) {  // softmax (src/pnof.jl:1122-1163)
         std::vector<double> w((size_t)nd * nc);
         for (int g = 0; g < nd; ++g) {
@@ -151,6 +163,13 @@ void occupations(const Occ& o, const double* gamma, double* n, double* dn) {
         for (int r = 0; r < nc; ++r)
             for (int j = 0; j < nb; ++j) dn[(size_t)o.P[g * nc + r] * nv + cols[j]] = B(r, j);
     }
+}
+
+}  // namespace
+
+// n (N) and dn (N x nv, dn[i * nv + k]) for the configured occupation map
+void occupations(const Occ& o, const double* gamma, double* n, double* dn) {
+    occupations_impl(o, gamma, n, dn, true);
 }
 
 double phi_fn(double ni, int ista) {
@@ -456,7 +475,7 @@ double energy_grad(const Occ& o, const double* gamma, const double* J, const dou
     thread_local std::vector<RowSums> rs;
     v.n.resize(N);
     dn.resize((size_t)N * (nv > 0 ? nv : 1));
-    occupations(o, gamma, v.n.data(), dn.data());
+    occupations_impl(o, gamma, v.n.data(), dn.data(), false);  // only the pair blocks are read below
     dynamic(o, v.n.data(), v.nd, v.F, v.coc);
     v.fi.resize(N);
     v.nd12.resize(N);
