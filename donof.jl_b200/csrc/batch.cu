@@ -865,6 +865,7 @@ int donof_batch_lagrange2(donof_batch* B, const donof_batch_item* items, double*
     }
     DONOF_CUDA(ctx, cudaMemcpyAsync(hs.data(), B->d_state, sizeof(BOrbState) * B->nj, cudaMemcpyDeviceToHost, st));
     DONOF_CUDA(ctx, cudaStreamSynchronize(st));
+    DONOF_CHECK(failure_status(ctx));
     if (E)
         for (int j = 0; j < B->nj; ++j) E[j] = hs[j].E;
     return DONOF_OK;
@@ -968,6 +969,7 @@ int donof_batch_orbopt(donof_batch* B, int method, donof_batch_item* items) {
     DONOF_CUDA(ctx, cudaGraphLaunch(B->exec, st));
     DONOF_CUDA(ctx, cudaMemcpyAsync(hs.data(), B->d_state, sizeof(BOrbState) * nj, cudaMemcpyDeviceToHost, st));
     DONOF_CUDA(ctx, cudaStreamSynchronize(st));
+    DONOF_CHECK(failure_status(ctx));
     int iters = 0;
     for (int j = 0; j < nj; ++j) iters = std::max(iters, hs[j].it);
     g_launch_adjust((long long)B->per_iter * iters);

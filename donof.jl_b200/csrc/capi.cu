@@ -46,6 +46,73 @@ void dev_free(donof_ctx* ctx, const void* p) {
     if (p) cudaFreeAsync(const_cast<void*>(p), ctx->stream);
 }
 
+int take_failures(donof_ctx* ctx) {
+    if (!ctx->fail_host) return 0;
+    int mask = 0;
+    for (int k = 0; k < FAIL_WORDS; ++k)
+        if (ctx->fail_host[k]) {
+            mask |= 1 << k;
+            ctx->fail_host[k] = 0;
+        }
+    return mask;
+}
+
+int sync_and_check(donof_ctx* ctx) {
+    DONOF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return failure_status(ctx);
+}
+
+int failure_status(donof_ctx* ctx) {
+    const int f = take_failures(ctx) & ((1 << FAIL_MBAR) | (1 << FAIL_BARRIER));
+    if (f) {
+        set_error(ctx, "a kernel gave up on a bounded %s wait; the call's outputs are not valid",
+                  (f & (1 << FAIL_MBAR)) ? "mbarrier" : "grid-barrier");
+        return DONOF_ERR_TIMEOUT;
+    }
+    return DONOF_OK;
+}
+
+namespace {
+// Sets the context's FAIL_NONFINITE word if any of the count values is a NaN or
+// an infinity (the word may be host memory: plain stores of 1).
+__global__ void scan_nonfinite_kernel(const double* __restrict__ v, long long count, int* __restrict__ word) {
+    bool bad = false;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if ((reinterpret_cast<uintptr_t>(v) & 15) == 0) {
+        const long long n2 = count / 2;
+        const double2* v2 = reinterpret_cast<const double2*>(v);
+        for (long long k = i; k < n2; k += stride) {
+            const double2 x = __ldg(v2 + k);
+            bad |= !isfinite(x.x) || !isfinite(x.y);
+        }
+        for (long long k = 2 * n2 + i; k < count; k += stride) bad |= !isfinite(__ldg(v + k));
+    } else {
+        for (long long k = i; k < count; k += stride) bad |= !isfinite(__ldg(v + k));
+    }
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) *reinterpret_cast<volatile int*>(word) = 1;
+}
+}  // namespace
+
+// DONOF_ERR_ARG if the device array holds a NaN or an infinity (one pass,
+// synchronises the context stream).
+int check_finite(donof_ctx* ctx, const double* v, long long count, const char* what) {
+    if (!ctx->fail_dev) return DONOF_OK;
+    long long blocks = (count / 2 + 255) / 256;
+    if (blocks > 8LL * ctx->sm_count) blocks = 8LL * ctx->sm_count;
+    if (blocks < 1) blocks = 1;
+    scan_nonfinite_kernel<<<(int)blocks, 256, 0, ctx->stream>>>(v, count, ctx->fail_dev + FAIL_NONFINITE);
+    count_launch();
+    DONOF_CUDA(ctx, cudaGetLastError());
+    DONOF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (ctx->fail_host[FAIL_NONFINITE]) {
+        ctx->fail_host[FAIL_NONFINITE] = 0;
+        set_error(ctx, "%s holds a NaN or an infinity", what);
+        return DONOF_ERR_ARG;
+    }
+    return DONOF_OK;
+}
+
 int DevBuf::ensure(donof_ctx* ctx, size_t want) {
     if (want <= bytes && ptr != nullptr) return DONOF_OK;
     if (ptr) {
@@ -71,7 +138,6 @@ int orbopt_run(donof_job* job, int method, const double* n, const double* cj12, 
                double threshgorb, double* C, double* E_out, int* nit_out, int* success_out,
                int precision);
 int convert_b_f32(donof_job* job);
-int mixed_status(donof_job* job, int* out);
 int mixed_t1_debug(donof_job* job, cudaStream_t st, const double* C, int nbf5, float* tmp_out);
 
 }  // namespace donof
@@ -181,10 +247,11 @@ struct Stager {
         return DONOF_OK;
     }
     int finish() {
-        DONOF_CUDA(ctx, cudaStreamSynchronize(st));
+        const int s = sync_and_check(ctx);
+        if (s == DONOF_ERR_CUDA) return s;
         for (int i = 0; i < nout; ++i) memcpy(outs[i].dst, outs[i].src, outs[i].bytes);
         ctx->hstage_busy = false;
-        return DONOF_OK;
+        return s;
     }
 };
 
@@ -232,11 +299,27 @@ int donof_profile_last_ms(donof_ctx* ctx, float* ms) {
     return DONOF_OK;
 }
 
+int donof_error_flags(donof_ctx* ctx, int* flags) {
+    if (!ctx || !flags) return DONOF_ERR_ARG;
+    DONOF_CHECK(use_device(ctx));
+    DONOF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    *flags = take_failures(ctx);
+    return DONOF_OK;
+}
+
 int donof_job_error_flag(donof_job* job, int* flag) {
     if (!job || !flag) return DONOF_ERR_ARG;
-    DONOF_CHECK(use_device(job->ctx));
-    DONOF_CUDA(job->ctx, cudaStreamSynchronize(job->ctx->stream));
-    return mixed_status(job, flag);
+    int f = 0;
+    DONOF_CHECK(donof_error_flags(job->ctx, &f));
+    *flag = f ? 1 : 0;
+    return DONOF_OK;
+}
+
+int donof_set_wait_limit(donof_ctx* ctx, long long cycles) {
+    if (!ctx) return DONOF_ERR_ARG;
+    REQUIRE(ctx, cycles >= 0, "the wait budget must be >= 0");
+    ctx->wait_limit = cycles;
+    return DONOF_OK;
 }
 
 int donof_mixed_tmp_dev(donof_job* job, const double* C, int nbf5, float* tmp) {
@@ -272,6 +355,7 @@ const char* donof_status_string(int s) {
         case DONOF_ERR_OOM: return "out of device memory";
         case DONOF_ERR_STATE: return "invalid state";
         case DONOF_ERR_NOT_CONVERGED: return "not converged";
+        case DONOF_ERR_TIMEOUT: return "a bounded wait ran out";
         default: return "unknown status";
     }
 }
@@ -304,6 +388,22 @@ int donof_create(int device, donof_ctx** out) {
         return DONOF_ERR_CUDA;
     }
     ctx->own_stream = true;
+    {
+        // failure words: page-locked host memory the kernels write through its device alias
+        void* h = nullptr;
+        void* d = nullptr;
+        if (cudaHostAlloc(&h, 256, cudaHostAllocMapped | cudaHostAllocPortable) != cudaSuccess ||
+            cudaHostGetDevicePointer(&d, h, 0) != cudaSuccess) {
+            set_error(nullptr, "donof_create: cannot map the failure words on device %d", device);
+            if (h) cudaFreeHost(h);
+            cudaStreamDestroy(ctx->stream);
+            delete ctx;
+            return DONOF_ERR_CUDA;
+        }
+        memset(h, 0, 256);
+        ctx->fail_host = static_cast<volatile int*>(h);
+        ctx->fail_dev = static_cast<int*>(d);
+    }
     cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device);
     {
         // keep freed blocks in the device's default pool (process-local) instead of
@@ -326,6 +426,7 @@ int donof_destroy(donof_ctx* ctx) {
     ctx->stage_out.release(ctx);
     ctx->rot.release(ctx);
     if (ctx->hstage) cudaFreeHost(ctx->hstage);
+    if (ctx->fail_host) cudaFreeHost(const_cast<int*>(ctx->fail_host));
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     if (ctx->aux_stream) cudaStreamDestroy(ctx->aux_stream);
     if (ctx->prof_ev[0]) cudaEventDestroy(ctx->prof_ev[0]);
@@ -400,6 +501,13 @@ int donof_b_upload(donof_ctx* ctx, const double* b_host, int nbf, int naux, int 
     }
     j->b = static_cast<const double*>(d);
     j->own_b = true;
+    {
+        const int sf = check_finite(ctx, j->b, (long long)nbf * nbf * naux, "b");
+        if (sf != DONOF_OK) {
+            donof_job_free(j);
+            return sf;
+        }
+    }
     if (precision == DONOF_PREC_MIXED) {
         int s = convert_b_f32(j);
         if (s != DONOF_OK) {
@@ -435,6 +543,11 @@ int donof_iaux(donof_ctx* ctx, const double* G, const double* I3c, int nbf, int 
     }
     j->b = static_cast<const double*>(d);
     j->own_b = true;
+    s = check_finite(ctx, j->b, (long long)nbf * nbf * naux, "b = I G^-1/2");
+    if (s != DONOF_OK) {
+        donof_job_free(j);
+        return s;
+    }
     if (precision == DONOF_PREC_MIXED) {
         s = convert_b_f32(j);
         if (s != DONOF_OK) {
@@ -455,6 +568,13 @@ int donof_b_attach(donof_ctx* ctx, const double* b_dev, int nbf, int naux, int p
     DONOF_CHECK(make_job(ctx, nbf, naux, precision, &j));
     j->b = b_dev;
     j->own_b = false;
+    {
+        const int sf = check_finite(ctx, j->b, (long long)nbf * nbf * naux, "b");
+        if (sf != DONOF_OK) {
+            donof_job_free(j);
+            return sf;
+        }
+    }
     if (precision == DONOF_PREC_MIXED) {
         int s = convert_b_f32(j);
         if (s != DONOF_OK) {

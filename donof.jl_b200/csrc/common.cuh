@@ -75,9 +75,33 @@ struct donof_ctx {
     // most CTAs a persistent or cooperative kernel of this context may use (0: one
     // per SM); a server running several jobs at once gives each a share of the SMs
     int cta_limit = 0;
+    // Failure words written by the context's kernels, in page-locked host memory
+    // mapped into the device (kernels store 1 into a word; the host reads it after
+    // synchronising the stream, no copy needed).  Sticky until read and cleared.
+    //   [FAIL_MBAR]     a mixed-form kernel gave up on a bounded mbarrier wait
+    //   [FAIL_BARRIER]  a cooperative kernel gave up on its bounded grid barrier
+    //   [FAIL_NONFINITE] a finiteness scan found a NaN or an infinity
+    volatile int* fail_host = nullptr;
+    int* fail_dev = nullptr;
+    // cycle budget of every bounded wait in this context's kernels (0: the
+    // built-in ~1-2 s); a small value makes waits run out, for testing the
+    // failure path without a fault or a hang
+    long long wait_limit = 0;
 };
 
 namespace donof {
+enum { FAIL_MBAR = 0, FAIL_BARRIER = 1, FAIL_NONFINITE = 2, FAIL_WORDS = 4 };
+// Reads and clears the context's failure words (the stream must have been
+// synchronised): returns a bit mask, bit k set when word k was set.
+int take_failures(donof_ctx* ctx);
+// After the caller has synchronised the stream the kernels ran on: turns a
+// recorded wait failure into DONOF_ERR_TIMEOUT (with the error text), else
+// DONOF_OK.  sync_and_check synchronises the context stream first.
+int failure_status(donof_ctx* ctx);
+int sync_and_check(donof_ctx* ctx);
+// DONOF_ERR_ARG (with the error text) if the device array holds a NaN or an
+// infinity; one pass, synchronises the context stream, allocates nothing.
+int check_finite(donof_ctx* ctx, const double* v, long long count, const char* what);
 // Stream-ordered device allocation on the context's stream (capi.cu).
 int dev_alloc(donof_ctx* ctx, void** p, size_t bytes);
 void dev_free(donof_ctx* ctx, const void* p);

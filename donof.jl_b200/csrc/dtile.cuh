@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "common.cuh"
 #include "gemm_f64.cuh"
 
 namespace donof {
@@ -273,8 +274,9 @@ __device__ __forceinline__ void tile(const Gemm& g, int t, double* sm) {
 // ---------------------------------------------------------------------------
 // Bounded grid barrier for a cooperatively launched grid: a monotonic arrival
 // counter (zeroed before the launch); barrier number e completes when the
-// counter reaches (e + 1) * gridDim.x.  On a timeout (or when another CTA gave
-// up) it records the error and returns false; callers then return without
+// counter reaches (e + 1) * members.  On a timeout (or when another CTA gave
+// up) it records the error -- in the GridSync and, once per launch, in the
+// context's failure word -- and returns false; callers then return without
 // touching their outputs further.
 struct GridSync {
     unsigned count;
@@ -283,6 +285,17 @@ struct GridSync {
 };
 
 constexpr long long BARRIER_CYCLES = 2000000000LL;  // ~1 s
+
+// How a launch's grid barriers wait: the cycle budget (<= 0: BARRIER_CYCLES)
+// and the failure word to set on a timeout (may be null).
+struct WaitCtl {
+    long long cycles;
+    int* fail;
+};
+// The WaitCtl of a context's launches.
+inline WaitCtl wait_ctl(const donof_ctx* ctx) {
+    return WaitCtl{ctx->wait_limit, ctx->fail_dev ? ctx->fail_dev + FAIL_BARRIER : nullptr};
+}
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
     unsigned v;
@@ -296,17 +309,19 @@ __device__ __forceinline__ void red_release_add(unsigned* p, unsigned v) {
 // epoch: barriers this CTA has passed (the same in every CTA); incremented here.
 // members: the CTAs that take part (gridDim.x for the whole grid; a grouped
 // launch gives each job its own GridSync and CTA range).
-__device__ __forceinline__ bool grid_barrier(GridSync* gs, unsigned& epoch, unsigned members) {
+__device__ __forceinline__ bool grid_barrier(GridSync* gs, unsigned& epoch, unsigned members, const WaitCtl& w) {
     __shared__ int fail;
     __syncthreads();
     if (threadIdx.x == 0) {
         fail = 0;
         red_release_add(&gs->count, 1u);
         const unsigned target = (epoch + 1) * members;
+        const long long budget = w.cycles > 0 ? w.cycles : BARRIER_CYCLES;
         const long long t0 = clock64();
         while (ld_acquire(&gs->count) < target) {
-            if (clock64() - t0 > BARRIER_CYCLES || *(volatile int*)&gs->err) {
-                atomicExch(&gs->err, 1);
+            if (clock64() - t0 > budget || *(volatile int*)&gs->err) {
+                // the CTA that gives up first reports it (plain store: the word may be host memory)
+                if (atomicExch(&gs->err, 1) == 0 && w.fail) *reinterpret_cast<volatile int*>(w.fail) = 1;
                 fail = 1;
                 break;
             }
@@ -315,10 +330,6 @@ __device__ __forceinline__ bool grid_barrier(GridSync* gs, unsigned& epoch, unsi
     __syncthreads();
     ++epoch;
     return fail == 0;
-}
-
-__device__ __forceinline__ bool grid_barrier(GridSync* gs, unsigned& epoch) {
-    return grid_barrier(gs, epoch, gridDim.x);
 }
 
 }  // namespace dtile

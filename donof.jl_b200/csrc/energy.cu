@@ -25,6 +25,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 #include <numeric>
 #include <vector>
 
@@ -86,7 +87,7 @@ struct Loop {
         DONOF_CUDA(ctx, cudaMemcpyAsync(K.data(), D.K, sizeof(double) * K.size(), cudaMemcpyDeviceToHost, st));
         DONOF_CUDA(ctx, cudaMemcpyAsync(Hc.data(), D.Hc, sizeof(double) * Hc.size(), cudaMemcpyDeviceToHost, st));
         DONOF_CUDA(ctx, cudaStreamSynchronize(st));
-        return DONOF_OK;
+        return failure_status(ctx);
     }
     // C <- C[:, perm]
     int permute(const std::vector<int>& perm) {
@@ -361,6 +362,7 @@ int EnergyJob::finish(double* C_out, double* gamma_out, double* n_out, double* e
     DONOF_CUDA(ctx, cudaMemcpyAsync(C_out, L.D.C, 8 * nn, cudaMemcpyDeviceToHost, st));
     if (elag_out) DONOF_CUDA(ctx, cudaMemcpyAsync(elag_out, L.D.elag, 8 * nn, cudaMemcpyDeviceToHost, st));
     DONOF_CUDA(ctx, cudaStreamSynchronize(st));
+    DONOF_CHECK(failure_status(ctx));
     std::copy(S.gamma.begin(), S.gamma.end(), gamma_out);
     if (n_out) std::copy(S.n.begin(), S.n.end(), n_out);
     res->E_elec = S.E;
@@ -377,13 +379,18 @@ int EnergyJob::finish(double* C_out, double* gamma_out, double* n_out, double* e
 
 using namespace donof;
 
-extern "C" int donof_energy(donof_job* job, donof_energy_params* prm, const double* H, double* C_inout,
-                            double* gamma_inout, double* n_out, double* elag_out, double* history,
-                            donof_energy_result* res) {
-    if (!job || !prm || !H || !C_inout || !gamma_inout || !res) return DONOF_ERR_ARG;
+namespace donof {
+
+int energy_run(donof_job* job, donof_energy_params* prm, const double* H, double* C_inout, double* gamma_inout,
+               double* n_out, double* elag_out, double* history, donof_energy_result* res,
+               const std::atomic<int>* cancel) {
     EnergyJob E;
     DONOF_CHECK(E.setup(job, prm, H, C_inout, gamma_inout, history));
     while (!E.done()) {
+        if (cancel && cancel->load(std::memory_order_relaxed)) {
+            set_error(job->ctx, "cancelled");
+            return DONOF_ERR_STATE;
+        }
         DONOF_CHECK(E.begin());
         double E_orb = 0.0;
         int nit_orb = 0, ok_orb = 0;
@@ -393,4 +400,13 @@ extern "C" int donof_energy(donof_job* job, donof_energy_params* prm, const doub
         DONOF_CHECK(E.after_orbopt(E_orb, nit_orb));
     }
     return E.finish(C_inout, gamma_inout, n_out, elag_out, res);
+}
+
+}  // namespace donof
+
+extern "C" int donof_energy(donof_job* job, donof_energy_params* prm, const double* H, double* C_inout,
+                            double* gamma_inout, double* n_out, double* elag_out, double* history,
+                            donof_energy_result* res) {
+    if (!job || !prm || !H || !C_inout || !gamma_inout || !res) return DONOF_ERR_ARG;
+    return energy_run(job, prm, H, C_inout, gamma_inout, n_out, elag_out, history, res, nullptr);
 }

@@ -1,6 +1,8 @@
 // Internal (non-exported) entry points shared between the translation units.
 #pragma once
 
+#include <atomic>
+
 #include "common.cuh"
 #include "gemm_f64.cuh"
 
@@ -175,6 +177,13 @@ private:
     struct Impl;
     Impl* p;
 };
+
+// donof_energy with a cancellation flag, read before every outer iteration
+// (cancel may be null): a set flag ends the loop with DONOF_ERR_STATE and the
+// error text "cancelled" (energy.cu).
+int energy_run(donof_job* job, donof_energy_params* prm, const double* H, double* C_inout, double* gamma_inout,
+               double* n_out, double* elag_out, double* history, donof_energy_result* res,
+               const std::atomic<int>* cancel);
 
 // Orbital-gradient helpers (optim.cu): g = pack(4 elag - 4 elag^T); when
 // maxabs != nullptr also atomically max-reduces |g| into it (must be zeroed).

@@ -25,7 +25,8 @@
 // TMA producer, warp 5 TMEM allocator + MMA issuer.  Operands are staged by
 // TMA (cp.async.bulk.tensor, no multicast) with 128-byte swizzle; every wait
 // on an mbarrier is bounded by a clock budget after which the CTA records an
-// error in the status word, drains its in-flight copies, frees TMEM and exits.
+// error in its context's failure word, drains its in-flight copies, frees TMEM
+// and exits.
 //
 // Shapes: nbf <= 256, nbf5 <= 64 (one MMA tile per aux index); larger jobs
 // run the general-shape pipeline of mixed_general.cu.
@@ -98,7 +99,8 @@ struct Params {
     float* d_out;            // d[q + nbf5*l]
     float* y_part;           // per CTA: Y[m + nbf*b]
     float* k_part;           // per CTA: K[p + nbf5*q]
-    int* status;             // nonzero on timeout
+    int* fail;               // the context's failure word for mbarrier waits (set to 1 on a timeout)
+    long long wait;          // cycle budget of every bounded wait (drains excepted)
 };
 
 using namespace sm100;
@@ -181,7 +183,7 @@ lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_const
                     for (int kb = 0; kb < P.nkb; ++kb, ++it) {
                         const int s = it % RING;
                         const uint32_t ph = (uint32_t)((it / RING) & 1);
-                        if (!mbar_wait(bar(B_EMPTY + s), ph ^ 1u, abort_flag)) { ok = false; break; }
+                        if (!mbar_wait(bar(B_EMPTY + s), ph ^ 1u, abort_flag, P.wait)) { ok = false; break; }
                         mbar_expect_tx(bar(B_FULL + s), (uint32_t)STAGE_BYTES);
                         const uint32_t st = sbase + OFF_RING + s * STAGE_BYTES;
                         tma_load_4d(st, &map_bhi, bar(B_FULL + s), 0, kb * KB, qb, l);
@@ -206,7 +208,7 @@ lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_const
             const uint32_t id_t1 = idesc(128, BOX_M, 0, 1);
             const uint32_t id_t2 = idesc(128, 128, 0, 0);
             const uint32_t id_y = idesc(128, ncol, 0, 1);
-            bool ok = mbar_wait(bar(B_CS), 0, abort_flag);
+            bool ok = mbar_wait(bar(B_CS), 0, abort_flag, P.wait);
             fence_after();
             int it = 0;          // ring stages consumed
             int tq = 0;          // T1 quarters issued (slot = tq & 1)
@@ -234,7 +236,7 @@ lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_const
                         issue_y();
                     }
                     if (*abort_flag) return false;
-                    if (clock64() - t0 > WAIT_CYCLES) { *abort_flag = 1; return false; }
+                    if (clock64() - t0 > P.wait) { *abort_flag = 1; return false; }
                 }
                 return true;
             };
@@ -292,7 +294,7 @@ lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_const
                     for (; ahead < ahead_max && ok; ++ahead) ok = t1_quarter();
                 if (!ok) break;
                 // W(l) ready (and the T2 region drained)
-                if (!mbar_wait(bar(B_A3), lph, abort_flag)) { ok = false; break; }
+                if (!mbar_wait(bar(B_A3), lph, abort_flag, P.wait)) { ok = false; break; }
                 fence_after();
                 if (y_li >= 0) issue_y();
             }
@@ -311,7 +313,7 @@ lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_const
         volatile int* epi_ok = reinterpret_cast<volatile int*>(sm + OFF_MISC + 32);
         // one thread waits, the 128 epilogue threads agree on the outcome
         auto epi_wait = [&](int b, uint32_t parity) -> bool {
-            if (threadIdx.x == 0) *epi_ok = mbar_wait(bar(b), parity, abort_flag) ? 1 : 0;
+            if (threadIdx.x == 0) *epi_ok = mbar_wait(bar(b), parity, abort_flag, P.wait) ? 1 : 0;
             epi_sync();
             const bool r = *epi_ok != 0;
             epi_sync();
@@ -321,7 +323,7 @@ lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_const
         // one warp waits on its own (lane 0 polls, the warp agrees)
         auto warp_wait = [&](int b, uint32_t parity) -> bool {
             int r = 1;
-            if (lane == 0) r = mbar_wait(bar(b), parity, abort_flag) ? 1 : 0;
+            if (lane == 0) r = mbar_wait(bar(b), parity, abort_flag, P.wait) ? 1 : 0;
             r = __shfl_sync(0xffffffffu, r, 0);
             if (r) fence_after();
             return r != 0;
@@ -503,7 +505,7 @@ lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_const
 
     fence_before();
     __syncthreads();
-    if (threadIdx.x == 0 && *abort_flag) atomicExch(P.status, 1);
+    if (threadIdx.x == 0 && *abort_flag && P.fail) *reinterpret_cast<volatile int*>(P.fail) = 1;
     if (warp == 5) {
         fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem));
@@ -624,9 +626,8 @@ namespace {
 
 int ldm_of(int nbf) { return (nbf + 7) / 8 * 8; }
 
-// Scratch of the mixed form inside the job: [status | Cs | n32 | cj32 | ck32 | d | y_part | k_part | tmp/bpq out]
+// Scratch of the mixed form inside the job: [Cs | n32 | cj32 | ck32 | d | y_part | k_part | tmp/bpq out]
 struct MixedScratch {
-    int* status;
     __nv_bfloat16* cs;
     float *n32, *cj32, *ck32, *d, *ypart, *kpart;
     double *Y, *Kd, *dd;
@@ -638,7 +639,6 @@ int mixed_prepare(donof_job* job, cudaStream_t st, const double* C, int nbf5, Mi
     const int ldk = ldm_of(nbf);
     size_t off = 0;
     auto take = [&](size_t bytes) { size_t o = off; off += (bytes + 255) / 256 * 256; return o; };
-    const size_t o_status = take(sizeof(int) * 4);
     const size_t o_cs = take(sizeof(__nv_bfloat16) * (size_t)ldk * 128);
     const size_t o_n = take(sizeof(float) * 64);
     const size_t o_cj = take(sizeof(float) * 64 * 64);
@@ -651,7 +651,6 @@ int mixed_prepare(donof_job* job, cudaStream_t st, const double* C, int nbf5, Mi
     const size_t o_dd = take(sizeof(double) * (size_t)nbf5 * naux);
     DONOF_CHECK(job->W.ensure(ctx, off));  // the FP64 form's W buffer doubles as the mixed scratch
     char* base = job->W.as<char>();
-    S->status = reinterpret_cast<int*>(base + o_status);
     S->cs = reinterpret_cast<__nv_bfloat16*>(base + o_cs);
     S->n32 = reinterpret_cast<float*>(base + o_n);
     S->cj32 = reinterpret_cast<float*>(base + o_cj);
@@ -662,7 +661,6 @@ int mixed_prepare(donof_job* job, cudaStream_t st, const double* C, int nbf5, Mi
     S->Y = reinterpret_cast<double*>(base + o_Y);
     S->Kd = reinterpret_cast<double*>(base + o_K);
     S->dd = reinterpret_cast<double*>(base + o_dd);
-    DONOF_CUDA(ctx, cudaMemsetAsync(S->status, 0, sizeof(int) * 4, st));
     // the kernel accumulates its K_MO partial sums into these
     DONOF_CUDA(ctx, cudaMemsetAsync(S->kpart, 0, sizeof(float) * (size_t)grid * nbf5 * nbf5, st));
     mx::split_c_kernel<<<(ldk * 128 + 255) / 256, 256, 0, st>>>(C, nbf, nbf5, ldk, S->cs); count_launch();
@@ -699,7 +697,8 @@ int launch_mixed(donof_job* job, cudaStream_t st, int nbf5, int nalpha, int nbet
     P.mode = mode;
     P.n32 = S.n32; P.cj32 = S.cj32; P.ck32t = S.ck32;
     P.tmp_out = tmp_out; P.bpq_out = bpq_out; P.d_out = S.d; P.y_part = S.ypart; P.k_part = S.kpart;
-    P.status = S.status;
+    P.fail = ctx->fail_dev ? ctx->fail_dev + FAIL_MBAR : nullptr;
+    P.wait = sm100::wait_budget(ctx->wait_limit);
     static std::atomic<unsigned long long> attr_mask{0};
     const unsigned long long bit = 1ull << (ctx->device & 63);
     if (!(attr_mask.load(std::memory_order_acquire) & bit)) {
@@ -783,12 +782,6 @@ int mixed_t1_debug(donof_job* job, cudaStream_t st, const double* C, int nbf5, f
     MixedScratch S;
     DONOF_CHECK(mixed_prepare(job, st, C, nbf5, &S, grid));
     return launch_mixed(job, st, nbf5, nbf5, nbf5, 1, S, tmp_out, nullptr, grid);
-}
-
-int mixed_status(donof_job* job, int* out) {
-    if (job->W.ptr == nullptr) { *out = 0; return DONOF_OK; }
-    DONOF_CUDA(job->ctx, cudaMemcpy(out, job->W.ptr, sizeof(int), cudaMemcpyDeviceToHost));
-    return DONOF_OK;
 }
 
 int lagrange2_mixed(donof_job* job, cudaStream_t st, const double* C, const double* n, const double* H,

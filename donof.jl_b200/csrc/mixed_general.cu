@@ -34,7 +34,7 @@
 // TMA producer, warp 5 TMEM allocator + MMA issuer.  Every mbarrier wait is
 // bounded (sm100.cuh); a wait that runs out sets the CTA's abort flag, the
 // roles stop, in-flight copies and MMAs are drained with bounded waits, TMEM is
-// freed and the status word records the failure.
+// freed and the context's failure word records the failure.
 #include <atomic>
 #include <cuda.h>
 #include <cuda_bf16.h>
@@ -88,7 +88,8 @@ struct Params {
     __nv_bfloat16* tq_hi;  // T1 out: tmpQ[m + ldm q + ldm nbf5 l]
     __nv_bfloat16* tq_lo;
     float* out;            // T2: b_pq[p + nbf5 q + nbf5^2 l]; Y: part[m + nbf b + nbf nbf5 chunk]
-    int* status;
+    int* fail;             // the context's failure word for mbarrier waits (set to 1 on a timeout)
+    long long wait;        // cycle budget of every bounded wait (drains excepted)
 };
 
 struct Item {
@@ -156,7 +157,7 @@ mg_gemm_kernel(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant_
                 for (int l = w.l0; l < w.l1 && ok; ++l) {
                     for (int kbi = 0; kbi < P.kb; ++kbi, ++it) {
                         const int s = it % RING;
-                        if (!mbar_wait(bar(B_EMPTY + s), (uint32_t)(((it / RING) & 1) ^ 1), abort_flag)) {
+                        if (!mbar_wait(bar(B_EMPTY + s), (uint32_t)(((it / RING) & 1) ^ 1), abort_flag, P.wait)) {
                             ok = false;
                             break;
                         }
@@ -206,7 +207,7 @@ mg_gemm_kernel(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant_
             for (int k = 0; k < my_count && ok; ++k) {
                 const Item w = decode(P, (int)blockIdx.x + k * G);
                 const int buf = k & 1;
-                if (!mbar_wait(bar(B_ACCFREE + buf), (uint32_t)(((k >> 1) & 1) ^ 1), abort_flag)) break;
+                if (!mbar_wait(bar(B_ACCFREE + buf), (uint32_t)(((k >> 1) & 1) ^ 1), abort_flag, P.wait)) break;
                 fence_after();
                 const uint32_t d = tmem + (uint32_t)(BN * buf);
                 const uint32_t id = idesc(BM, mma_n(P, w.ncol), 0, b_mn);
@@ -214,7 +215,7 @@ mg_gemm_kernel(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant_
                 for (int l = w.l0; l < w.l1 && ok; ++l) {
                     for (int kbi = 0; kbi < P.kb; ++kbi, ++it) {
                         const int s = it % RING;
-                        if (!mbar_wait(bar(B_FULL + s), (uint32_t)((it / RING) & 1), abort_flag)) {
+                        if (!mbar_wait(bar(B_FULL + s), (uint32_t)((it / RING) & 1), abort_flag, P.wait)) {
                             ok = false;
                             break;
                         }
@@ -254,7 +255,7 @@ mg_gemm_kernel(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant_
             const Item w = decode(P, (int)blockIdx.x + k * G);
             const int buf = k & 1;
             int r = 1;
-            if (lane == 0) r = mbar_wait(bar(B_ACC + buf), (uint32_t)((k >> 1) & 1), abort_flag) ? 1 : 0;
+            if (lane == 0) r = mbar_wait(bar(B_ACC + buf), (uint32_t)((k >> 1) & 1), abort_flag, P.wait) ? 1 : 0;
             r = __shfl_sync(0xffffffffu, r, 0);
             if (!r) break;
             fence_after();
@@ -315,7 +316,7 @@ mg_gemm_kernel(const __grid_constant__ CUtensorMap ma_hi, const __grid_constant_
 
     fence_before();
     __syncthreads();
-    if (threadIdx.x == 0 && *abort_flag) atomicExch(P.status, 1);
+    if (threadIdx.x == 0 && *abort_flag && P.fail) *reinterpret_cast<volatile int*>(P.fail) = 1;
     if (warp == 5) {
         fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem));
@@ -440,10 +441,9 @@ namespace {
 
 int round8(int x) { return (x + 7) / 8 * 8; }
 
-// Scratch of the general mixed form.  job->tmp: tmpQ hi | lo; job->W: status |
+// Scratch of the general mixed form.  job->tmp: tmpQ hi | lo; job->W:
 // Cs hi | Cs lo | n32 | cj32 | ckT | b_pq (FP32) | W hi | W lo | Y partials.
 struct GenScratch {
-    int* status;
     __nv_bfloat16 *cs_hi, *cs_lo, *tq_hi, *tq_lo, *w_hi, *w_lo;
     float *n32, *cj32, *ckT, *bpq, *ypart, *tv;
     int ldm, ldq, nchunks, lchunk;
@@ -472,7 +472,6 @@ int gen_prepare(donof_job* job, cudaStream_t st, const double* C, const double* 
     S->tq_lo = S->tq_hi + tq;
     size_t off = 0;
     auto take = [&](size_t bytes) { size_t o = off; off += (bytes + 255) / 256 * 256; return o; };
-    const size_t o_status = take(sizeof(int) * 4);
     const size_t o_cs = take(2 * sizeof(__nv_bfloat16) * (size_t)S->ldm * nbf5);
     const size_t o_n = take(sizeof(float) * (size_t)nbf5);
     const size_t o_cj = take(sizeof(float) * (size_t)nbf5 * nbf5);
@@ -484,7 +483,6 @@ int gen_prepare(donof_job* job, cudaStream_t st, const double* C, const double* 
     const size_t o_tv = take(with_w ? sizeof(float) * (size_t)nbf5 * naux : 0);
     DONOF_CHECK(job->W.ensure(ctx, off));
     char* base = job->W.as<char>();
-    S->status = reinterpret_cast<int*>(base + o_status);
     S->cs_hi = reinterpret_cast<__nv_bfloat16*>(base + o_cs);
     S->cs_lo = S->cs_hi + (size_t)S->ldm * nbf5;
     S->n32 = reinterpret_cast<float*>(base + o_n);
@@ -495,7 +493,6 @@ int gen_prepare(donof_job* job, cudaStream_t st, const double* C, const double* 
     S->w_lo = S->w_hi + wsz;
     S->ypart = reinterpret_cast<float*>(base + o_y);
     S->tv = reinterpret_cast<float*>(base + o_tv);
-    DONOF_CUDA(ctx, cudaMemsetAsync(S->status, 0, sizeof(int) * 4, st));
     const long long work = (long long)S->ldm * nbf5 > (long long)nbf5 * nbf5 ? (long long)S->ldm * nbf5
                                                                              : (long long)nbf5 * nbf5;
     long long blocks = (work + 255) / 256;
@@ -529,7 +526,8 @@ mg::Params base_params(donof_job* job, int nbf5, const GenScratch& S) {
     P.nbf = job->nbf;
     P.nbf5 = nbf5;
     P.ldm = S.ldm;
-    P.status = S.status;
+    P.fail = job->ctx->fail_dev ? job->ctx->fail_dev + FAIL_MBAR : nullptr;
+    P.wait = sm100::wait_budget(job->ctx->wait_limit);
     P.lchunk = 1;
     P.nchunks = job->naux;
     return P;

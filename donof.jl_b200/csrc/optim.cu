@@ -232,6 +232,7 @@ int orbopt_run(donof_job* job, int method, const double* n, const double* cj12, 
     OrbState hs{};
     DONOF_CUDA(ctx, cudaMemcpyAsync(&hs, S, sizeof(OrbState), cudaMemcpyDeviceToHost, st));
     DONOF_CUDA(ctx, cudaStreamSynchronize(st));
+    DONOF_CHECK(failure_status(ctx));
     const double E0 = hs.E;
     hs.bestE = E0;
     hs.alpha = *alpha;
@@ -304,6 +305,7 @@ int orbopt_run(donof_job* job, int method, const double* n, const double* cj12, 
         DONOF_CUDA(ctx, cudaGraphLaunch(job->orb_exec, st));
         DONOF_CUDA(ctx, cudaMemcpyAsync(&hs, S, sizeof(OrbState), cudaMemcpyDeviceToHost, st));
         DONOF_CUDA(ctx, cudaStreamSynchronize(st));
+        DONOF_CHECK(failure_status(ctx));
         g_launch_adjust((long long)job->orb_per_iter * hs.it);
     }
     if (!hs.improved) {
@@ -362,6 +364,7 @@ int orbopt_run_host(donof_job* job, int method, const double* n, const double* c
         double h[2];
         DONOF_CUDA(ctx, cudaMemcpyAsync(h, stat, sizeof(h), cudaMemcpyDeviceToHost, st));
         DONOF_CUDA(ctx, cudaStreamSynchronize(st));
+        DONOF_CHECK(failure_status(ctx));
         *E = h[0];
         *gmax = h[1];
         return DONOF_OK;

@@ -216,6 +216,7 @@ struct CoopArgs {
     double* Cnew;
     double *Y, *X2, *X3, *X4, *P, *E1, *bufs;
     CoopState* cs;
+    dtile::WaitCtl wc;
 };
 
 __device__ __forceinline__ dtile::Gemm sq_gemm(int n, const double* A, const double* B, double* C, double alpha,
@@ -262,7 +263,7 @@ __device__ __forceinline__ void rotate_body(const CoopArgs& a, int cta, int G, d
         }
         __syncthreads();
     }
-    if (!dtile::grid_barrier(gs, epoch, G)) return;
+    if (!dtile::grid_barrier(gs, epoch, G, a.wc)) return;
     const double norm = __longlong_as_double((long long)cs->norm_bits);
     int s = 0;
     if (norm > 0.25) s = (int)ceil(log2(norm / 0.25));
@@ -270,7 +271,7 @@ __device__ __forceinline__ void rotate_body(const CoopArgs& a, int cta, int G, d
     const double sc = ldexp(1.0, -s);  // X = sc * Y (a power of two: exact)
     // S1: X2 = X X
     run_tiles(sq_gemm(n, a.Y, a.Y, a.X2, sc * sc, false), sm, cta, G);
-    if (!dtile::grid_barrier(gs, epoch, G)) return;
+    if (!dtile::grid_barrier(gs, epoch, G, a.wc)) return;
     // S2: X3 = X2 X, X4 = X2 X2
     {
         const dtile::Gemm g3 = sq_gemm(n, a.X2, a.Y, a.X3, sc, false);
@@ -281,7 +282,7 @@ __device__ __forceinline__ void rotate_body(const CoopArgs& a, int cta, int G, d
             else dtile::tile<RT_TN>(g4, w - nt, sm);
         }
     }
-    if (!dtile::grid_barrier(gs, epoch, G)) return;
+    if (!dtile::grid_barrier(gs, epoch, G, a.wc)) return;
     // S3: the three polynomial blocks of the degree-12 Taylor sum (1/k! coefficients)
     {
         double c[13];
@@ -312,16 +313,16 @@ __device__ __forceinline__ void rotate_body(const CoopArgs& a, int cta, int G, d
             }
         }
     }
-    if (!dtile::grid_barrier(gs, epoch, G)) return;
+    if (!dtile::grid_barrier(gs, epoch, G, a.wc)) return;
     // S4: E1 += P X4;  S5: E0 = bufs[0] += E1 X4
     run_tiles(sq_gemm(n, a.P, a.X4, a.E1, 1.0, true), sm, cta, G);
-    if (!dtile::grid_barrier(gs, epoch, G)) return;
+    if (!dtile::grid_barrier(gs, epoch, G, a.wc)) return;
     run_tiles(sq_gemm(n, a.E1, a.X4, a.bufs, 1.0, true), sm, cta, G);
-    if (!dtile::grid_barrier(gs, epoch, G)) return;
+    if (!dtile::grid_barrier(gs, epoch, G, a.wc)) return;
     // squarings: bufs[k+1] = bufs[k]^2
     for (int k = 0; k < s; ++k) {
         run_tiles(sq_gemm(n, a.bufs + k * nn, a.bufs + k * nn, a.bufs + (k + 1) * nn, 1.0, false), sm, cta, G);
-        if (!dtile::grid_barrier(gs, epoch, G)) return;
+        if (!dtile::grid_barrier(gs, epoch, G, a.wc)) return;
     }
     // C_new = C E^(2^s)
     run_tiles(sq_gemm(n, a.C, a.bufs + s * nn, a.Cnew, 1.0, false), sm, cta, G);
@@ -337,7 +338,8 @@ static_assert(sizeof(CoopState) <= GROUP_STATE_BYTES, "rotation state slot too s
 // Grouped form: the rotations of several jobs in one cooperative launch, job j
 // on CTAs [cta0, cta0 + ctas) with its own barrier state.  A CTA that lies in
 // several jobs' ranges (only jobs with ctas == 1 share CTAs) runs them in order.
-__global__ void __launch_bounds__(dtile::THREADS) rotate_grouped_kernel(const RotJob* __restrict__ jobs, int njobs) {
+__global__ void __launch_bounds__(dtile::THREADS) rotate_grouped_kernel(const RotJob* __restrict__ jobs, int njobs,
+                                                                        const dtile::WaitCtl wc) {
     extern __shared__ __align__(16) double sm[];
     const int cta = blockIdx.x;
     for (int j = 0; j < njobs; ++j) {
@@ -353,6 +355,7 @@ __global__ void __launch_bounds__(dtile::THREADS) rotate_grouped_kernel(const Ro
         a.X2 = a.Y + nn; a.X3 = a.Y + 2 * nn; a.X4 = a.Y + 3 * nn; a.P = a.Y + 4 * nn;
         a.bufs = a.Y + 5 * nn;
         a.E1 = a.bufs + (SMAX + 1) * nn;
+        a.wc = wc;
         rotate_body(a, cta - c0, cn, sm);
         __syncthreads();
     }
@@ -385,7 +388,7 @@ int rotate_grouped(donof_ctx* ctx, cudaStream_t st, const RotJob* jobs, int njob
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    DONOF_CUDA(ctx, cudaLaunchKernelEx(&cfg, rotate_grouped_kernel, jobs, njobs));
+    DONOF_CUDA(ctx, cudaLaunchKernelEx(&cfg, rotate_grouped_kernel, jobs, njobs, dtile::wait_ctl(ctx)));
     count_launch();
     return DONOF_OK;
 }
@@ -408,6 +411,7 @@ int rotate_f64(donof_ctx* ctx, cudaStream_t st, const double* y, int nbf, int nb
     a.X2 = a.Y + nn; a.X3 = a.Y + 2 * nn; a.X4 = a.Y + 3 * nn; a.P = a.Y + 4 * nn;
     a.bufs = a.Y + 5 * nn;           // E^(2^k), k = 0..SMAX
     a.E1 = a.bufs + (SMAX + 1) * nn;  // extra slot
+    a.wc = dtile::wait_ctl(ctx);
     const int smem = (int)sizeof(double) * dtile::smem_doubles<RT_TN>();
     static std::atomic<unsigned long long> attr_mask{0};
     const unsigned long long bit = 1ull << (ctx->device & 63);

@@ -18,15 +18,17 @@
 #include <math.h>
 #include <string.h>
 
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
+#include <algorithm>
 #include <deque>
 #include <map>
 #include <mutex>
 #include <thread>
 #include <vector>
 
-#include "common.cuh"
+#include "kernels.cuh"
 
 namespace {
 
@@ -72,7 +74,16 @@ struct Job {
     donof_result res;
     bool done = false;
     double t_submit = 0.0;
+    std::atomic<int> cancel{0};  // set by donof_server_cancel; the energy loop reads it
 };
+
+void mark_cancelled(Job* j, double t) {
+    j->res.status = DONOF_ERR_STATE;
+    snprintf(j->res.error, sizeof(j->res.error), "cancelled");
+    j->res.queue_s = t - j->t_submit;
+    j->res.latency_s = t - j->t_submit;
+    j->done = true;
+}
 
 }  // namespace
 
@@ -83,6 +94,7 @@ struct donof_server {
     int cta_share = 0;
     size_t budget = 0, used = 0;
     int inflight = 0;
+    int waiters = 0;  // callers blocked in donof_server_wait
     int head_bypassed = 0;
     bool closing = false;
     unsigned long long next_ticket = 1;
@@ -112,6 +124,7 @@ struct donof_server {
 namespace {
 
 int run_job(donof_ctx* ctx, int cta_share, Job* j) {
+    using donof::energy_run;
     const donof_request& r = j->req;
     donof_energy_params prm = r.params;
     const int nbf = r.nbf, nbf5 = prm.occ.nbf5;
@@ -137,12 +150,13 @@ int run_job(donof_ctx* ctx, int cta_share, Job* j) {
         pm.stop_rel_de = 1e-6;
         s = donof_job_set_precision(job, DONOF_PREC_MIXED);
         if (s == DONOF_OK)
-            s = donof_energy(job, &pm, r.H, j->C_out, gamma.data(), nullptr, nullptr, nullptr, &er);
+            s = energy_run(job, &pm, r.H, j->C_out, gamma.data(), nullptr, nullptr, nullptr, &er, &j->cancel);
         prm.maxloop = pm.maxloop;
         prm.alpha = pm.alpha;
         if (s == DONOF_OK) s = donof_job_set_precision(job, DONOF_PREC_FP64);
     }
-    if (s == DONOF_OK) s = donof_energy(job, &prm, r.H, j->C_out, gamma.data(), j->n_out, nullptr, nullptr, &er);
+    if (s == DONOF_OK)
+        s = energy_run(job, &prm, r.H, j->C_out, gamma.data(), j->n_out, nullptr, nullptr, &er, &j->cancel);
     donof_job_free(job);
     if (s != DONOF_OK) return s;
     j->res.E_elec = er.E_elec;
@@ -169,7 +183,7 @@ void worker_main(donof_server* S) {
         const double t0 = now_s();
         j->res.status = (cs == DONOF_OK) ? run_job(ctx, S->cta_share, j) : cs;
         if (j->res.status != DONOF_OK) {
-            const char* msg = donof_last_error(ctx);
+            const char* msg = (cs == DONOF_OK) ? donof_last_error(ctx) : donof_last_error(nullptr);
             snprintf(j->res.error, sizeof(j->res.error), "%s", msg ? msg : "");
         }
         const double t1 = now_s();
@@ -277,10 +291,35 @@ int donof_server_wait(donof_server* S, unsigned long long ticket, donof_result* 
     auto it = S->jobs.find(ticket);
     if (it == S->jobs.end()) return DONOF_ERR_ARG;
     Job* j = it->second;
+    ++S->waiters;
     S->cv_done.wait(lk, [&] { return j->done; });
     *res = j->res;
     delete j;
     S->jobs.erase(ticket);
+    --S->waiters;
+    lk.unlock();
+    S->cv_done.notify_all();  // donof_server_destroy waits for the waiters to leave
+    return DONOF_OK;
+}
+
+int donof_server_cancel(donof_server* S, unsigned long long ticket) {
+    if (!S) return DONOF_ERR_ARG;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        auto it = S->jobs.find(ticket);
+        if (it == S->jobs.end()) return DONOF_ERR_ARG;
+        Job* j = it->second;
+        if (j->done) return DONOF_OK;
+        auto q = std::find(S->queue.begin(), S->queue.end(), j);
+        if (q == S->queue.end()) {  // in flight: the energy loop stops at its next outer iteration
+            j->cancel.store(1, std::memory_order_relaxed);
+            return DONOF_OK;
+        }
+        S->queue.erase(q);
+        mark_cancelled(j, now_s());
+    }
+    S->cv_done.notify_all();
+    S->cv_work.notify_all();  // the queue's head may have changed
     return DONOF_OK;
 }
 
@@ -289,14 +328,17 @@ int donof_server_destroy(donof_server* S) {
     {
         std::lock_guard<std::mutex> lk(S->mu);
         S->closing = true;
-        for (Job* j : S->queue) {  // not started: reported as cancelled if collected later
-            j->res.status = DONOF_ERR_STATE;
-            j->done = true;
-        }
+        const double t = now_s();
+        for (Job* j : S->queue) mark_cancelled(j, t);  // not started
         S->queue.clear();
     }
+    S->cv_done.notify_all();  // waiters on queued jobs return their cancelled result
     S->cv_work.notify_all();
-    for (std::thread& t : S->workers) t.join();  // jobs in flight finish
+    for (std::thread& t : S->workers) t.join();  // jobs in flight finish (and notify)
+    {
+        std::unique_lock<std::mutex> lk(S->mu);
+        S->cv_done.wait(lk, [&] { return S->waiters == 0; });
+    }
     for (auto& kv : S->jobs) delete kv.second;
     delete S;
     return DONOF_OK;

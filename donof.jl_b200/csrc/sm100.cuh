@@ -3,8 +3,10 @@
 // loads (no multicast), UMMA shared-memory and instruction descriptors for
 // bf16 x bf16 -> f32, TMEM loads and the bf16 hi/lo split.
 //
-// Every wait is bounded by WAIT_CYCLES of SM clock: a wait that runs out sets
-// the CTA's abort flag, so that the other roles stop too, and returns false.
+// Every wait is bounded (WAIT_CYCLES of SM clock unless the launch gives a
+// smaller budget): a wait that runs out sets the CTA's abort flag, so that the
+// other roles stop too, and returns false.  The drains that let a CTA free its
+// resources always keep the full WAIT_CYCLES.
 #pragma once
 
 #include <cuda.h>
@@ -53,13 +55,16 @@ __device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
+// Budget of a launch's waits: the caller's value if positive, else WAIT_CYCLES.
+__host__ __device__ constexpr long long wait_budget(long long cycles) { return cycles > 0 ? cycles : WAIT_CYCLES; }
+
 // Bounded wait: false (and the abort flag set) if the phase does not complete
-// within WAIT_CYCLES or another role aborted.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
+// within `budget` cycles or another role aborted.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag, long long budget) {
     const long long t0 = clock64();
     while (!mbar_try(bar, parity)) {
         if (*abort_flag) return false;
-        if (clock64() - t0 > WAIT_CYCLES) {
+        if (clock64() - t0 > budget) {
             *abort_flag = 1;
             return false;
         }

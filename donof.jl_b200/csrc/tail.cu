@@ -41,6 +41,7 @@ struct TailArgs {
     double *Y, *HC, *Bp;  // scratch, nbf x nbf5 each
     double *Hmat, *elag, *E;
     TailState* ts;
+    dtile::WaitCtl wc;
 };
 
 // The whole tail of one job on CTAs cta = 0..G-1 (of a cooperative launch).
@@ -147,12 +148,12 @@ __device__ __forceinline__ void tail_body(const TailArgs& a, int cta, int G, dou
         for (long long i = z0 + (long long)cta * dtile::THREADS + tid; i < zn; i += (long long)G * dtile::THREADS)
             a.elag[i] = 0.0;
     }
-    if (!dtile::grid_barrier(gs, epoch, G)) return;
+    if (!dtile::grid_barrier(gs, epoch, G, a.wc)) return;
 
     // ---- stage 2: Bp = HC diag(n) + Y
     for (long long i = (long long)cta * dtile::THREADS + tid; i < ny; i += (long long)G * dtile::THREADS)
         a.Bp[i] = a.HC[i] * a.n[i / nbf] + a.Y[i];
-    if (!dtile::grid_barrier(gs, epoch, G)) return;
+    if (!dtile::grid_barrier(gs, epoch, G, a.wc)) return;
 
     // ---- stage 3: H_mat = C^T HC, elag[:, :nbf5] = C^T Bp
     dtile::Gemm gh;
@@ -206,7 +207,8 @@ static_assert(sizeof(TailState) <= GROUP_STATE_BYTES, "tail state slot too small
 
 // Grouped form: the tails of several jobs in one cooperative launch, job j on
 // CTAs [cta0, cta0 + ctas) with its own barrier state (as rotate_grouped_kernel).
-__global__ void __launch_bounds__(dtile::THREADS) tail_grouped_kernel(const TailJob* __restrict__ jobs, int njobs) {
+__global__ void __launch_bounds__(dtile::THREADS) tail_grouped_kernel(const TailJob* __restrict__ jobs, int njobs,
+                                                                      const dtile::WaitCtl wc) {
     extern __shared__ __align__(16) double sm[];
     const int cta = blockIdx.x;
     for (int j = 0; j < njobs; ++j) {
@@ -222,6 +224,7 @@ __global__ void __launch_bounds__(dtile::THREADS) tail_grouped_kernel(const Tail
         a.ts = static_cast<TailState*>(t.state);
         a.Y = t.work; a.HC = a.Y + ny; a.Bp = a.HC + ny;
         a.Hmat = t.Hmat; a.elag = t.elag; a.E = t.E;
+        a.wc = wc;
         tail_body(a, cta - c0, cn, sm);
         __syncthreads();
     }
@@ -252,7 +255,7 @@ int tail_grouped(donof_ctx* ctx, cudaStream_t st, const TailJob* jobs, int njobs
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    DONOF_CUDA(ctx, cudaLaunchKernelEx(&cfg, tail_grouped_kernel, jobs, njobs));
+    DONOF_CUDA(ctx, cudaLaunchKernelEx(&cfg, tail_grouped_kernel, jobs, njobs, dtile::wait_ctl(ctx)));
     count_launch();
     return DONOF_OK;
 }
@@ -274,6 +277,7 @@ int elag_tail_f64(donof_job* job, cudaStream_t st, const double* C, const double
     a.HC = a.Y + ny;
     a.Bp = a.HC + ny;
     a.Hmat = Hmat; a.elag = elag; a.E = E;
+    a.wc = dtile::wait_ctl(ctx);
     const int smem = (int)sizeof(double) * dtile::smem_doubles<TL_TN>();
     static std::atomic<unsigned long long> attr_mask{0};
     const unsigned long long bit = 1ull << (ctx->device & 63);

@@ -18,6 +18,12 @@ ERR_CUDA = 2
 ERR_OOM = 3
 ERR_STATE = 4
 ERR_NOT_CONVERGED = 5
+ERR_TIMEOUT = 6
+
+# bits of donof_error_flags
+FAIL_MBAR = 1
+FAIL_BARRIER = 2
+FAIL_NONFINITE = 4
 
 PREC_FP64 = 0
 PREC_MIXED = 1
@@ -57,6 +63,7 @@ SIGNATURES = {
     "donof_server_submit": (_i, [_vp, _vp, _vp, _vp, ct.POINTER(ct.c_ulonglong)]),
     "donof_server_poll": (_i, [_vp, ct.c_ulonglong, _vp, _ip]),
     "donof_server_wait": (_i, [_vp, ct.c_ulonglong, _vp]),
+    "donof_server_cancel": (_i, [_vp, ct.c_ulonglong]),
     "donof_server_destroy": (_i, [_vp]),
     "donof_lagrange2": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp, _vp]),
     "donof_lagrange2_dev": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp, _vp]),
@@ -74,6 +81,8 @@ SIGNATURES = {
     "donof_launch_count": (ct.c_ulonglong, []),
     "donof_autotune_entries": (_i, []),
     "donof_job_error_flag": (_i, [_vp, _ip]),
+    "donof_error_flags": (_i, [_vp, _ip]),
+    "donof_set_wait_limit": (_i, [_vp, ct.c_longlong]),
     "donof_profile_enable": (_i, [_vp, _i]),
     "donof_profile_last_ms": (_i, [_vp, ct.POINTER(ct.c_float)]),
     "donof_mixed_tmp_dev": (_i, [_vp, _vp, _i, _vp]),

@@ -78,6 +78,19 @@ class Context:
     def check(self, status: int) -> None:
         _lib.check(status, self.handle)
 
+    def error_flags(self) -> int:
+        """Failures the context's kernels recorded since the last read (bit mask:
+        _lib.FAIL_MBAR, FAIL_BARRIER, FAIL_NONFINITE), cleared by the read;
+        synchronises the context stream."""
+        f = ct.c_int()
+        self.check(self.lib.donof_error_flags(self.handle, ct.byref(f)))
+        return f.value
+
+    def set_wait_limit(self, cycles: int) -> None:
+        """Cycle budget of every bounded wait in the kernels launched from now
+        on (0: the built-in one); a tiny budget drives the failure path."""
+        self.check(self.lib.donof_set_wait_limit(self.handle, int(cycles)))
+
     def synchronize(self) -> None:
         self.check(self.lib.donof_synchronize(self.handle))
 

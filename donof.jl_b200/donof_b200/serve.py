@@ -145,6 +145,16 @@ class Admission:
         self.used -= nbytes
         self.inflight -= 1
 
+    def remove(self, ticket: int) -> bool:
+        """Drops a queued ticket (a cancelled job); False if it is not queued."""
+        for i, (t, _) in enumerate(self.queue):
+            if t == ticket:
+                del self.queue[i]
+                if i == 0:
+                    self._head_bypassed = 0
+                return True
+        return False
+
     def take_group(self, eligible: Callable[[int], bool], max_group: int, min_group: int = 2,
                    scale: float = 2.0) -> List[tuple]:
         """Queued tickets to run together as one group on one slot: when the head
@@ -154,6 +164,7 @@ class Admission:
         Fewer than min_group: nothing (the single-job path takes them)."""
         if self.inflight >= self.max_inflight or not self.queue or not eligible(self.queue[0][0]):
             return []
+        head = self.queue[0][0]
         room = self.budget - self.used
         group = []
         for t, nb in self.queue:
@@ -166,8 +177,13 @@ class Admission:
         if len(group) < min_group:
             return []
         picked = {t for t, _ in group}
+        if head in picked:
+            self._head_bypassed = 0
+        else:  # the head does not fit: the group passes it over, as take() counts it
+            if self._head_bypassed >= self.max_bypass:
+                return []
+            self._head_bypassed += 1
         self.queue = deque(q for q in self.queue if q[0] not in picked)
-        self._head_bypassed = 0
         self.used += sum(nb for _, nb in group)
         self.inflight += 1
         return group
@@ -326,6 +342,22 @@ class Server:
                 self._lock.wait(rem)
             return self._results[ticket]
 
+    def cancel(self, ticket: int) -> bool:
+        """Cancels a job that has not started: its result (error "cancelled")
+        is available at once.  A job already running or done is left alone
+        (False)."""
+        with self._lock:
+            if not self.admission.remove(ticket):
+                return False
+            req = self._pending.pop(ticket)
+            now = time.perf_counter()
+            self._bytes.pop(ticket)
+            self._results[ticket] = Result(ticket=ticket, error="cancelled", t_submit=self._submit_t.pop(ticket),
+                                           t_start=now, t_done=now, tag=req.tag)
+            self._admit_locked()
+            self._lock.notify_all()
+            return True
+
     def shutdown(self, wait: bool = True) -> None:
         with self._lock:
             self._closed = True
@@ -436,15 +468,33 @@ class NativeServer:
         self._keep[t.value] = (H, b, C, gamma, r, C_out, n_out, req.tag)
         return t.value
 
+    def _result(self, ticket: int, res) -> Result:
+        H, b, C, gamma, r, C_out, n_out, tag = self._keep.pop(ticket)
+        err = (res.error.decode() or f"status {res.status}") if res.status != 0 else None
+        return Result(ticket=ticket, E_elec=res.E_elec, E_tot=res.E_tot, converged=bool(res.converged),
+                      iterations=res.iterations, C=C_out, n=n_out, error=err, t_submit=0.0,
+                      t_start=res.queue_s, t_done=res.latency_s, tag=tag)
+
     def wait(self, ticket: int) -> Result:
         from . import _lib
         res = _NativeResult()
         _lib.check(self.lib.donof_server_wait(self.handle, self._ct.c_ulonglong(ticket), self._ct.byref(res)))
-        H, b, C, gamma, r, C_out, n_out, tag = self._keep.pop(ticket)
-        err = res.error.decode() if res.status != 0 else None
-        return Result(ticket=ticket, E_elec=res.E_elec, E_tot=res.E_tot, converged=bool(res.converged),
-                      iterations=res.iterations, C=C_out, n=n_out, error=err, t_submit=0.0,
-                      t_start=res.queue_s, t_done=res.latency_s, tag=tag)
+        return self._result(ticket, res)
+
+    def poll(self, ticket: int) -> Optional[Result]:
+        """The result if the job has ended (it is then collected), else None."""
+        from . import _lib
+        res = _NativeResult()
+        done = self._ct.c_int()
+        _lib.check(self.lib.donof_server_poll(self.handle, self._ct.c_ulonglong(ticket), self._ct.byref(res),
+                                              self._ct.byref(done)))
+        return self._result(ticket, res) if done.value else None
+
+    def cancel(self, ticket: int) -> None:
+        """Cancels a job: a queued one ends at once, a running one at its next
+        outer iteration; its result then carries the error "cancelled"."""
+        from . import _lib
+        _lib.check(self.lib.donof_server_cancel(self.handle, self._ct.c_ulonglong(ticket)))
 
     def close(self) -> None:
         if self.handle:

@@ -40,6 +40,7 @@ extern "C" {
 #define DONOF_ERR_OOM 3       /* device allocation failed */
 #define DONOF_ERR_STATE 4     /* object in the wrong state for this call */
 #define DONOF_ERR_NOT_CONVERGED 5
+#define DONOF_ERR_TIMEOUT 6   /* a kernel gave up on a bounded wait; its outputs are not valid */
 
 /* precision of the b tensor held by a job and of the bulk contractions */
 #define DONOF_PREC_FP64 0   /* all contractions in FP64 (plain form) */
@@ -73,10 +74,12 @@ int donof_version(void);
  * donof_b_upload replaces eris_to_gpu (ext/DoNOFGPUExt.jl:36-50, called at
  * src/integrals.jl:59-62): copies the host RI tensor b[m,n,l] (nbf x nbf x
  * naux, FP64) to the device once per job.  precision = DONOF_PREC_MIXED also
- * keeps an FP32 copy for the mixed-precision form (the FP64 copy stays, for
- * refinement steps).
+ * keeps a bf16 hi/lo split copy for the mixed-precision form (the FP64 copy
+ * stays, for refinement steps).
  * donof_b_attach wraps an existing device buffer without copying (the job
- * does not own it and it must outlive the job).                            */
+ * does not own it and it must outlive the job).
+ * Both scan b once on the device and reject a tensor holding a NaN or an
+ * infinity with DONOF_ERR_ARG (no job is created).                          */
 int donof_b_upload(donof_ctx* ctx, const double* b_host, int nbf, int naux, int precision,
                    donof_job** job);
 /* donof_iaux replaces Iaux / Iaux_gpu (src/integrals.jl:68-91,
@@ -347,7 +350,14 @@ int donof_server_submit(donof_server* server, const donof_request* request, doub
 /* done = 1 (and the result filled, the ticket released) once the job has ended */
 int donof_server_poll(donof_server* server, unsigned long long ticket, donof_result* result, int* done);
 int donof_server_wait(donof_server* server, unsigned long long ticket, donof_result* result);
-/* Cancels the jobs not started, waits for those in flight, frees the server. */
+/* Cancels a job: one still queued ends at once, one in flight at its next
+ * outer iteration; either is then collected with status DONOF_ERR_STATE and
+ * the error text "cancelled".  A job already done keeps its result.          */
+int donof_server_cancel(donof_server* server, unsigned long long ticket);
+/* Cancels the jobs not started, waits for those in flight and for callers
+ * blocked in donof_server_wait (they return the job's result, or a cancelled
+ * one), then frees the server and every job not collected.  No call on the
+ * server may start once donof_server_destroy has begun.                      */
 int donof_server_destroy(donof_server* server);
 
 /* --- diagnostics -------------------------------------------------------------
@@ -362,10 +372,26 @@ int donof_profile_last_ms(donof_ctx* ctx, float* ms);
 /* Number of GEMM shapes whose configuration the autotuner has chosen in this
  * process (each is timed once, at its first call outside stream capture).   */
 int donof_autotune_entries(void);
-/* Reads (synchronising the context stream) the job's device error flag: 1 if
- * a mixed-precision kernel gave up on a bounded wait since the last call that
- * reset it (each mixed-precision call resets it).                            */
+/* Failure detection.  Every wait inside the library's kernels is bounded (an
+ * mbarrier of the tensor-core pipelines, the grid barrier of a cooperative
+ * kernel): a wait that runs out makes the kernel stop without touching its
+ * outputs further and record the failure in its context's failure words
+ * (page-locked host memory mapped into the device), with no fault and no hang.
+ * The calls that synchronise (the host-buffer entry points, the optimiser and
+ * energy loops, the batch calls) then return DONOF_ERR_TIMEOUT; the _dev entry
+ * points only enqueue work, so their caller reads the words here.
+ * donof_error_flags synchronises the context stream and returns the recorded
+ * failures as a bit mask (1: mbarrier wait of a mixed-form kernel, 2: grid
+ * barrier of a cooperative kernel, 4: a finiteness scan met NaN or infinity)
+ * and clears them.  donof_job_error_flag does the same for the job's context
+ * and reports 1 if any bit was set.                                           */
+int donof_error_flags(donof_ctx* ctx, int* flags);
 int donof_job_error_flag(donof_job* job, int* flag);
+/* Cycle budget of every bounded wait in the context's kernels launched from now
+ * on (0, the default: about one to two seconds of clock).  A tiny budget makes
+ * the waits run out, so that a test can drive the failure path above; a
+ * captured optimiser graph keeps the budget it was captured with.            */
+int donof_set_wait_limit(donof_ctx* ctx, long long cycles);
 /* First contraction of the mixed form alone, for checking it:
  * tmp[m + nbf*q + nbf*nbf5*l] = sum_n b[m,n,l] C[n,q] (FP32, device).        */
 int donof_mixed_tmp_dev(donof_job* job, const double* C, int nbf5, float* tmp);

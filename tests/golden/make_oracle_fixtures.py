@@ -1,11 +1,14 @@
-"""Writes the golden fixtures of this folder from the CPU oracle.
+"""Writes the oracle fixtures of this folder from the CPU oracle.
 
-The reference (Julia) cannot run here and ships no fixtures, so these vectors
-come from the oracle restatement (itself pinned by tests/test_oracle.py).
+These are NOT reference outputs: the reference (Julia) cannot run here and
+ships no fixtures or golden vectors, so these vectors come from the oracle
+restatement (itself pinned only by identities and a second restatement,
+tests/test_oracle.py).  Parity against the reference stays unpinned; the
+fixtures freeze the oracle's answers so that a change to either side shows.
 Inputs are regenerated from the seed by donof_b200.workload (numpy PCG64),
 so only sizes, seed and outputs are stored.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_oracle_fixtures.py
 """
 import sys
 from pathlib import Path

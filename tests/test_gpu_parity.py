@@ -13,7 +13,7 @@ from donof_b200 import Param, _lib, gnof, workload
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-10
-GOLDEN = Path(__file__).resolve().parent / "golden"
+FIXTURES = Path(__file__).resolve().parent / "golden"  # oracle fixtures (not reference outputs)
 
 
 def rel(a, b):
@@ -154,8 +154,11 @@ def test_energy_identity_at_full_size(cuda_ctx):
 
 
 @pytest.mark.parametrize("name", ["water_surrogate", "open_shell_small"])
-def test_golden_fixtures(cuda_ctx, name):
-    g = np.load(GOLDEN / f"{name}.npz")
+def test_oracle_fixtures(cuda_ctx, name):
+    """The CUDA path against the committed fixtures written by the oracle
+    (tests/golden/make_oracle_fixtures.py); the reference itself could not be
+    run, so these pin the oracle's answers, not the reference's."""
+    g = np.load(FIXTURES / f"{name}.npz")
     nbf, naux, nbeta, nalpha, ncwo, seed = (int(g[k]) for k in ("nbf", "naux", "nbeta", "nalpha", "ncwo", "seed"))
     wl = workload.synthetic(nbf=nbf, naux=naux, nbeta=nbeta, ncwo=ncwo, seed=seed)
     bt = d.eris_to_gpu(wl.b, "fp64", cuda_ctx)

@@ -1,11 +1,13 @@
 """CPU checks of the oracle itself.
 
 The reference ships no tests or golden vectors and Julia is not available, so
-the oracle is pinned by (1) a second, literal einsum restatement of the
-reference formulas, (2) the identities the reference code implies
-(calce == computeE_elec at the same C, finite-difference orbital and
-occupation gradients, orthogonality of the rotation, occupation sum rules),
-and (3) the committed golden fixtures.
+parity with the reference is unpinned: the oracle is checked by (1) a second,
+literal einsum restatement of the reference formulas, (2) the identities the
+reference code implies (calce == computeE_elec at the same C, finite-
+difference orbital and occupation gradients, orthogonality of the rotation,
+occupation sum rules), and (3) the committed oracle fixtures (written by the
+oracle itself, tests/golden/make_oracle_fixtures.py: they freeze its answers,
+they do not come from the reference).
 """
 import numpy as np
 import pytest

@@ -147,3 +147,64 @@ def test_server_runs_small_fp64_jobs_as_groups_and_the_rest_alone():
     assert sum(len(g) for g in groups) + len(singles) == 6
     assert any(len(g) >= 2 for g in groups)
     assert all(len(g) <= 4 for g in groups)
+
+
+def test_take_group_counts_a_passed_over_head_and_stops_at_max_bypass():
+    a = Admission(budget_bytes=100, max_inflight=8, max_bypass=2)
+    a.push(1, 40)                                      # eligible head that does not fit (2 x 40 > room)
+    for t in range(2, 10):
+        a.push(t, 5)
+    a.used = 30                                        # 70 bytes free
+    every = lambda t: True
+    g1 = a.take_group(every, max_group=2)
+    assert [t for t, _ in g1] == [2, 3]                # the head is passed over once
+    g2 = a.take_group(every, max_group=2)
+    assert [t for t, _ in g2] == [4, 5]                # twice
+    assert a.take_group(every, max_group=2) == []      # max_bypass reached: the head waits for memory
+    assert a.take() == []                              # and take() does not pass it either
+    a.used = 0
+    a.inflight = 0
+    g = a.take_group(every, max_group=2)
+    assert g[0][0] == 1                                # the head goes first once it fits
+    assert a._head_bypassed == 0
+
+
+def test_cancel_of_a_queued_job_returns_a_cancelled_result_and_frees_its_place():
+    started = []
+    gate = threading.Event()
+
+    def fake(req, device):
+        started.append(req.tag)
+        gate.wait(5)
+        return Result(ticket=-1, E_elec=1.0, converged=True)
+
+    with Server(budget_bytes=10**12, max_inflight=1, executor=fake) as s:
+        t1 = s.submit(_req(8, tag="running"))
+        t2 = s.submit(_req(8, tag="queued"))
+        t3 = s.submit(_req(8, tag="next"))
+        assert s.cancel(t2) is True
+        r2 = s.wait(t2, timeout=1)
+        assert r2.error == "cancelled" and r2.tag == "queued"
+        assert s.cancel(t1) is False                   # already running: not cancelled here
+        gate.set()
+        r1, r3 = s.wait(t1, timeout=10), s.wait(t3, timeout=10)
+    assert r1.error is None and r3.error is None
+    assert started == ["running", "next"]              # the cancelled job never ran
+
+
+def test_server_refuses_a_job_larger_than_its_budget():
+    with Server(budget_bytes=1000, max_inflight=1, executor=lambda r, d: Result(ticket=-1)) as s:
+        with pytest.raises(ValueError, match="budget"):
+            s.submit(_req(16, tag=0))
+
+
+def test_a_failing_job_reports_its_error_and_the_server_goes_on():
+    def fake(req, device):
+        if req.tag == "bad":
+            raise RuntimeError("b holds a NaN or an infinity")
+        return Result(ticket=-1, E_elec=2.0, converged=True)
+
+    with Server(budget_bytes=10**12, max_inflight=2, executor=fake) as s:
+        tb, tg = s.submit(_req(8, tag="bad")), s.submit(_req(8, tag="good"))
+        rb, rg = s.wait(tb, timeout=10), s.wait(tg, timeout=10)
+    assert "NaN" in rb.error and rg.error is None and rg.E_elec == 2.0

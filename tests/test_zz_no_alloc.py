@@ -20,6 +20,7 @@ from donof_b200 import _lib, workload
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-10
+SCRATCH_BYTES = 32 << 20  # the fixed scratch array inside the library
 
 
 def rel(a, b):
@@ -57,7 +58,9 @@ def test_noalloc_lagrange2_matches_existing_entry_point():
     outs = [outputs() for _ in orbitals]
     torch.cuda.synchronize()
 
-    free_after_first = None
+    # free device memory before the first allocation-free call, and after each one
+    free_before = torch.cuda.mem_get_info()[0]
+    free_after = []
     for call, (tC, (el, hm, E), (rel_, rhm, rE)) in enumerate(zip(orbitals, outs, refs)):
         st = lib.donof_lagrange2_noalloc_dev(job_na.handle, tC.data_ptr(), tn.data_ptr(), tH.data_ptr(),
                                              tcj.data_ptr(), tck.data_ptr(), p.nbf5, p.nalpha, p.nbeta,
@@ -67,10 +70,13 @@ def test_noalloc_lagrange2_matches_existing_entry_point():
         assert rel(el, rel_) <= TOL, f"call {call}: elag"
         assert rel(hm, rhm) <= TOL, f"call {call}: H_mat"
         assert abs(float(E) - float(rE)) <= TOL * max(1.0, abs(float(rE))), f"call {call}: E"
-        if call == 0:
-            free_after_first = torch.cuda.mem_get_info()[0]
-    # the second call allocated no device memory
-    assert torch.cuda.mem_get_info()[0] == free_after_first
+        free_after.append(torch.cuda.mem_get_info()[0])
+    # Neither call allocated device memory.  The only device memory the entry point
+    # may bring in is the library's own fixed scratch array, mapped when the code
+    # module holding it is first loaded (already done here by the existing path,
+    # which lives in the same module; allowed for in case a loader defers it).
+    assert 0 <= free_before - free_after[0] <= SCRATCH_BYTES + (2 << 20), (free_before, free_after)
+    assert free_after[1] == free_after[0], free_after
     job_ref.free()
     job_na.free()
     ctx.close()
@@ -83,7 +89,7 @@ def test_noalloc_rejects_sizes_beyond_the_fixed_scratch():
         pytest.skip("no CUDA device")
     ctx = d.Context(0)
     lib = _lib.load()
-    nbf, naux, nbf5 = 128, 512, 64          # (nbf*nbf5 + 2*nbf5^2)*naux doubles = 48 MiB > 32 MiB
+    nbf, naux, nbf5 = 128, 512, 64          # (nbf*nbf5 + 2*nbf5^2)*naux doubles = 64 MiB > 32 MiB
     b = torch.zeros(naux, nbf, nbf, dtype=torch.float64, device="cuda")
     job = d.eris_to_gpu(b, "fp64", ctx)
     C = torch.eye(nbf, dtype=torch.float64, device="cuda")
