@@ -30,8 +30,10 @@ FP64) exceeds the 126 MB L2, so no flush is needed between steps.
   batched_energies  converged energies/s of 16 molecule surrogates through the
           batched energy loop against donof_energy per job (|dE| = 0: the
           grouped path is bit-for-bit the single-job one)
-  --impl reference   the CPU restatement of the reference path (C/OpenMP FP64
-          oracle, all host threads) on the same workload
+  --impl reference   the CPU restatement of the reference path on the same
+          workload: the reference contraction order as threaded FP64 BLAS GEMMs
+          on all host threads (oracle/blas_mirror.py), with the scalar C/OpenMP
+          oracle beside it
 
 Multi-GPU: the optimiser loop of one job does not shard without a collective
 per step; --gpus N runs N independent replicas (one job per GPU, weak scaling).
@@ -226,12 +228,17 @@ def pack(elag, nbf5):
     return 4.0 * (elag[i, j] - elag[j, i])
 
 
-def run_cpu_steps(wl, steps, budget_s, threads=None):
-    """Orbital steps on the CPU oracle (C/OpenMP FP64): host update + rotate + Lagrangian."""
-    from oracle import native
+def run_cpu_steps(wl, steps, budget_s, threads=None, impl="blas"):
+    """Orbital steps on the CPU (FP64): host update + rotate + Lagrangian, with
+    impl "blas" (oracle/blas_mirror.py: the reference contraction order as
+    threaded BLAS GEMMs) or "port" (the scalar C/OpenMP oracle)."""
+    if impl == "blas":
+        from oracle import blas_mirror as native
+    else:
+        from oracle import native
 
-    if threads:
-        native.set_threads(threads)
+        if threads:
+            native.set_threads(threads)
     p = wl.p
     C = wl.C.copy(order="F")
     elag, _ = native.lagrange2(C, wl.n, wl.H, wl.b, wl.cj12, wl.ck12, p.nalpha, p.nbeta)
@@ -246,7 +253,7 @@ def run_cpu_steps(wl, steps, budget_s, threads=None):
         if time.perf_counter() - t0 > budget_s:
             break
     dt = time.perf_counter() - t0
-    return done, dt, native.num_threads()
+    return done, dt, (native.threads() if impl == "blas" else native.num_threads())
 
 
 def reference_arm(args, rank, world):
@@ -258,13 +265,17 @@ def reference_arm(args, rank, world):
     run_cpu_steps(wl, max(1, min(args.warmup, 1)), 60.0)  # warm caches / thread pool
     done, dt, cores = run_cpu_steps(wl, args.steps, 150.0)
     v = done / dt
+    pdone, pdt, pcores = run_cpu_steps(wl, 3, 20.0, impl="port")
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * dt / done, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
             "config": config(args, world),
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": f"{done} of {args.steps} orbital steps (C/OpenMP FP64 restatement of "
-                                       "rotate_orbital + compute_Lagrange2, reference contraction order)"},
+                             "sample": f"{done} of {args.steps} orbital steps: rotate_orbital + compute_Lagrange2 "
+                                       "in the reference contraction order as threaded FP64 BLAS GEMMs "
+                                       "(oracle/blas_mirror.py; the reference's Tullio loops cannot run here)",
+                             "scalar_port": {"value": pdone / pdt, "unit": UNIT, "cores": pcores,
+                                             "sample": f"{pdone} orbital steps on the scalar C/OpenMP oracle"}},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     return line
 
@@ -721,9 +732,14 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        done, dt, cores = run_cpu_steps(wl, 6, 20.0)
+        run_cpu_steps(wl, 1, 20.0)  # warm the thread pool
+        done, dt, cores = run_cpu_steps(wl, 20, 15.0)
+        pdone, pdt, pcores = run_cpu_steps(wl, 6, 15.0, impl="port")
         cpu = {"value": done / dt, "unit": UNIT, "cores": cores, "kind": "port",
-               "sample": f"{done} orbital steps of the same workload on the C/OpenMP FP64 oracle"}
+               "sample": f"{done} orbital steps of the same workload: rotate_orbital + compute_Lagrange2 in the "
+                         "reference contraction order as threaded FP64 BLAS GEMMs (oracle/blas_mirror.py)",
+               "scalar_port": {"value": pdone / pdt, "unit": UNIT, "cores": pcores,
+                               "sample": f"{pdone} orbital steps on the scalar C/OpenMP oracle"}}
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

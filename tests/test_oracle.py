@@ -179,3 +179,20 @@ def test_b_symmetrisation_invariance():
     e1, _ = native.lagrange2(C, n, H, b, cj, ck, p.nalpha, p.nbeta)
     e2, _ = native.lagrange2(C, n, H, np.asfortranarray(b.transpose(1, 0, 2)), cj, ck, p.nalpha, p.nbeta)
     assert rel(e1, e2) < 1e-13
+
+
+@pytest.mark.parametrize("sym,nalpha_extra", [(True, 0), (False, 0), (True, 2)])
+def test_blas_mirror_matches_the_c_oracle(sym, nalpha_extra):
+    """The BLAS mirror (the CPU baseline) computes what the C oracle computes."""
+    from oracle import blas_mirror
+    p, b, C, H, gamma, n, dn, cj, ck = make_case(nbf=21, naux=33, nbeta=3, ncwo=3, nalpha=3 + nalpha_extra,
+                                                 seed=4, sym=sym)
+    e1, h1 = native.lagrange2(C, n, H, b, cj, ck, p.nalpha, p.nbeta)
+    e2, h2 = blas_mirror.lagrange2(C, n, H, b, cj, ck, p.nalpha, p.nbeta)
+    assert np.max(np.abs(e1 - e2)) <= 1e-12 * np.max(np.abs(e1))
+    assert np.max(np.abs(h1 - h2)) <= 1e-12 * np.max(np.abs(h1))
+    nbf5 = n.shape[0]
+    for x1, x2 in zip(native.jkh_mo(C, H, b, nbf5), blas_mirror.jkh_mo(C, H, b, nbf5)):
+        assert np.max(np.abs(x1 - x2)) <= 1e-12 * max(1.0, np.max(np.abs(x1)))
+    y = np.random.default_rng(3).standard_normal(nbf5 * p.nbf - nbf5 * (nbf5 + 1) // 2) * 0.1
+    assert np.max(np.abs(native.rotate(y, C, nbf5) - blas_mirror.rotate(y, C, nbf5))) <= 1e-12
