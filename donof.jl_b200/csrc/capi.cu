@@ -682,6 +682,26 @@ int donof_lagrange2(donof_job* job, const double* C, const double* n, const doub
     return DONOF_OK;
 }
 
+int donof_lagrange2_partial_dev(donof_job* job, const double* C, const double* n, const double* cj12,
+                                const double* ck12, int nbf5, int nalpha, int nbeta, double* Y) {
+    if (!job) return DONOF_ERR_ARG;
+    donof_ctx* ctx = job->ctx;
+    DONOF_CHECK(check_sizes(ctx, job->nbf, nbf5, nalpha, nbeta));
+    REQUIRE(ctx, C && n && cj12 && ck12 && Y, "null array argument");
+    DONOF_CHECK(use_device(ctx));
+    return lagrange2_partial_f64(job, ctx->stream, C, n, cj12, ck12, nbf5, nalpha, nbeta, Y);
+}
+
+int donof_lagrange2_finish_dev(donof_job* job, const double* C, const double* n, const double* H, int nbf5,
+                               const double* Y, double* elag, double* H_mat, double* E_elec) {
+    if (!job) return DONOF_ERR_ARG;
+    donof_ctx* ctx = job->ctx;
+    REQUIRE(ctx, nbf5 > 0 && nbf5 <= job->nbf, "invalid nbf5");
+    REQUIRE(ctx, C && n && H && Y && elag && H_mat, "null array argument");
+    DONOF_CHECK(use_device(ctx));
+    return lagrange2_finish_f64(job, ctx->stream, C, n, H, nbf5, Y, elag, H_mat, E_elec);
+}
+
 int donof_jkh_mo_prec_dev(donof_job* job, int precision, const double* C, const double* H, int nbf5,
                           double* J_MO, double* K_MO, double* H_core) {
     if (!job) return DONOF_ERR_ARG;

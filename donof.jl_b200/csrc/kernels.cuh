@@ -85,6 +85,13 @@ int lagrange2_f64(donof_job* job, cudaStream_t st, const double* C, const double
 int jkh_mo_f64(donof_job* job, cudaStream_t st, const double* C, const double* H, int nbf5,
                double* J, double* K, double* Hcore);
 
+// Aux-index slices (lagrange.cu): Y of the job's slice of b (nbf x nbf5, FP64),
+// and the Lagrangian from the Y summed over every slice.
+int lagrange2_partial_f64(donof_job* job, cudaStream_t st, const double* C, const double* n, const double* cj12,
+                          const double* ck12, int nbf5, int nalpha, int nbeta, double* Y);
+int lagrange2_finish_f64(donof_job* job, cudaStream_t st, const double* C, const double* n, const double* H,
+                         int nbf5, const double* Y, double* elag, double* Hmat, double* E);
+
 // H_core from HC = H C5 (lagrange.cu).
 int hcore_f64(donof_job* job, cudaStream_t st, const double* C, const double* HC, int nbf5, double* Hcore);
 

@@ -180,6 +180,44 @@ int lagrange2_f64(donof_job* job, cudaStream_t st, const double* C, const double
     return elag_tail_f64(job, st, C, H, n, nbf5, ypart, false, nparts, (long long)nbf * nbf5, Hmat, elag, E);
 }
 
+// The Lagrangian of a slice of the aux index (the job's b holds naux_r aux
+// indices of a larger tensor): Y_r = sum_{q, l in slice} tmp_l[m, q] W[q, l, b],
+// reduced to one nbf x nbf5 FP64 matrix.  Every term of Y is a sum over l, so the
+// Y of the whole tensor is the sum of the slices' Y (an all-reduce across the
+// ranks that hold the slices); lagrange2_finish_f64 then gives elag, H_mat, E.
+int lagrange2_partial_f64(donof_job* job, cudaStream_t st, const double* C, const double* n, const double* cj12,
+                          const double* ck12, int nbf5, int nalpha, int nbeta, double* Y) {
+    donof_ctx* ctx = job->ctx;
+    const int nbf = job->nbf, naux = job->naux;
+    const long long Kt = (long long)nbf5 * naux;
+    DONOF_CHECK(transforms_f64(job, st, C, nbf5));
+    DONOF_CHECK(job->W.ensure(ctx, sizeof(double) * (size_t)Kt * (nbf5 + 1)));
+    double* W = job->W.as<double>();
+    double* tv = W + (size_t)Kt * nbf5;
+    {
+        const double* bpq = job->bpq.as<double>();
+        long long blocks = wbuild::diag_units(nbf5, naux);
+        if (blocks > 8LL * ctx->sm_count) blocks = 8LL * ctx->sm_count;
+        w_diag_kernel<<<(int)blocks, 256, 0, st>>>(bpq, n, cj12, nbf5, naux, nalpha, nbeta, tv); count_launch();
+        blocks = wbuild::tiles(nbf5, naux);
+        if (blocks > 16LL * ctx->sm_count) blocks = 16LL * ctx->sm_count;
+        build_w_kernel<<<(int)blocks, 256, 0, st>>>(bpq, ck12, tv, nbf5, naux, W); count_launch();
+        DONOF_CUDA(ctx, cudaGetLastError());
+    }
+    const double* ypart = nullptr;
+    int nparts = 1;
+    DONOF_CHECK(gemm_f64_partials(ctx, st, false, true, nbf, nbf5, (int)Kt, job->tmp.as<double>(), nbf, W, Kt,
+                                  &job->part, &ypart, &nparts));
+    const long long ny = (long long)nbf * nbf5;
+    return splitk_reduce(ctx, st, ypart, ny, nparts, ny, Y, 0.0);
+}
+
+// elag, H_mat and E_elec from the Y of the whole aux range (the fused tail).
+int lagrange2_finish_f64(donof_job* job, cudaStream_t st, const double* C, const double* n, const double* H,
+                         int nbf5, const double* Y, double* elag, double* Hmat, double* E) {
+    return elag_tail_f64(job, st, C, H, n, nbf5, Y, false, 1, (long long)job->nbf * nbf5, Hmat, elag, E);
+}
+
 int hcore_f64(donof_job* job, cudaStream_t st, const double* C, const double* HC, int nbf5, double* Hcore) {
     hcore_kernel<<<(nbf5 * 32 + 255) / 256, 256, 0, st>>>(C, HC, job->nbf, nbf5, Hcore); count_launch();
     DONOF_CUDA(job->ctx, cudaGetLastError());

@@ -69,6 +69,8 @@ SIGNATURES = {
     "donof_lagrange2_dev": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp, _vp]),
     "donof_lagrange2_prec_dev": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp, _vp]),
     "donof_lagrange2_noalloc_dev": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp, _vp]),
+    "donof_lagrange2_partial_dev": (_i, [_vp, _vp, _vp, _vp, _vp, _i, _i, _i, _vp]),
+    "donof_lagrange2_finish_dev": (_i, [_vp, _vp, _vp, _vp, _i, _vp, _vp, _vp, _vp]),
     "donof_jkh_mo": (_i, [_vp, _vp, _vp, _i, _vp, _vp, _vp]),
     "donof_jkh_mo_dev": (_i, [_vp, _vp, _vp, _i, _vp, _vp, _vp]),
     "donof_jkh_mo_prec_dev": (_i, [_vp, _i, _vp, _vp, _i, _vp, _vp, _vp]),

@@ -136,6 +136,23 @@ int donof_lagrange2_noalloc_dev(donof_job* job, const double* C, const double* n
                                 const double* cj12, const double* ck12, int nbf5, int nalpha,
                                 int nbeta, double* elag, double* H_mat, double* E_elec);
 
+/* --- the aux index split across GPUs -----------------------------------------
+ * compute_Lagrange2 (src/utils.jl:1-59) with b[:, :, l] split into contiguous
+ * slices of the aux index, one per GPU (each job holds its slice: nbf x nbf x
+ * naux_r).  Every elag term of the reference is a sum over l; in the
+ * restructured form elag[:, :nbf5] = n o H_mat + C^T Y with
+ * Y = sum_l tmp_l W_l, so each GPU computes the Y of its slice
+ * (donof_lagrange2_partial_dev, Y nbf x nbf5 FP64, device), the ranks sum
+ * their Y with one all-reduce (nbf * nbf5 doubles, e.g. NCCL), and
+ * donof_lagrange2_finish_dev gives elag, H_mat and E_elec from the summed Y.
+ * J_MO and K_MO of JKH_MO are sums over l the same way (all-reduce the
+ * outputs of donof_jkh_mo_dev of each slice; H_core is the same on every
+ * rank).  Plain FP64 form.                                                 */
+int donof_lagrange2_partial_dev(donof_job* job, const double* C, const double* n, const double* cj12,
+                                const double* ck12, int nbf5, int nalpha, int nbeta, double* Y);
+int donof_lagrange2_finish_dev(donof_job* job, const double* C, const double* n, const double* H, int nbf5,
+                               const double* Y, double* elag, double* H_mat, double* E_elec);
+
 /* --- JKH_MO, RI method ----------------------------------------------------
  * Replaces computeJKH_MO / JKH_MO(C,H,b::CuArray{T,3},nbf,nbf5,nbfaux)
  * (ext/DoNOFGPUExt.jl:52-94); CPU definition src/integrals.jl:131-172.
