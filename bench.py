@@ -261,7 +261,16 @@ def reference_arm(args, rank, world):
 
     if rank != 0:
         return None
-    wl = workload.synthetic(**WORKLOAD, seed=SEED)
+    # the inputs' occupations and couplings from the oracle's restatement, so that
+    # this arm runs nothing of the library
+    from oracle import gnof as ognof
+
+    def sizes(p):
+        return ognof.Sizes(nbf=p.nbf, nbeta=p.nbeta, nalpha=p.nalpha, ncwo=p.ncwo, naux=p.nbfaux, no1=p.no1,
+                           ista=p.ista, HighSpin=p.HighSpin, h_cut=p.h_cut, occ_method=p.occ_method)
+
+    layer = (lambda g, p: ognof.ocupacion(g, sizes(p)), lambda n, p: ognof.PNOFi_selector(n, sizes(p)))
+    wl = workload.synthetic(**WORKLOAD, seed=SEED, layer=layer)
     run_cpu_steps(wl, max(1, min(args.warmup, 1)), 60.0)  # warm caches / thread pool
     done, dt, cores = run_cpu_steps(wl, args.steps, 150.0)
     v = done / dt

@@ -738,6 +738,30 @@ int donof_occ_energy(const donof_occ_params* prm, const double* gamma, const dou
     return DONOF_OK;
 }
 
+int donof_occupations(const donof_occ_params* prm, const double* gamma, double* n, double* dn_dgamma) {
+    Occ o;
+    if (!setup(prm, o) || !gamma || !n) {
+        donof::set_error(nullptr, "donof_occupations: invalid sizes or null pointer");
+        return DONOF_ERR_ARG;
+    }
+    std::vector<double> dn((size_t)o.N * (o.nv > 0 ? o.nv : 1), 0.0);  // dn[i * nv + k]
+    donof::occ::occupations(o, gamma, n, dn.data());
+    if (dn_dgamma)  // column-major N x nv (Julia's layout)
+        for (int i = 0; i < o.N; ++i)
+            for (int k = 0; k < o.nv; ++k) dn_dgamma[i + (size_t)o.N * k] = dn[(size_t)i * o.nv + k];
+    return DONOF_OK;
+}
+
+int donof_coupling(const donof_occ_params* prm, const double* n, double* cj12, double* ck12) {
+    Occ o;
+    if (!setup(prm, o) || !n || !cj12 || !ck12) {
+        donof::set_error(nullptr, "donof_coupling: invalid sizes or null pointer");
+        return DONOF_ERR_ARG;
+    }
+    donof::occ::coupling(o, n, cj12, ck12);
+    return DONOF_OK;
+}
+
 int donof_occ_cg(const donof_occ_params* prm, const double* J_MO, const double* K_MO, const double* H_core,
                  double* gamma, double g_abstol, int max_iter, double* E, int* nit, int* converged) {
     Occ o;

@@ -56,6 +56,8 @@ SIGNATURES = {
     "donof_job_free": (_i, [_vp]),
     "donof_job_set_precision": (_i, [_vp, _i]),
     "donof_job_device_bytes": (ct.c_size_t, [_vp]),
+    "donof_occupations": (_i, [_vp, _vp, _vp, _vp]),
+    "donof_coupling": (_i, [_vp, _vp, _vp, _vp]),
     "donof_occ_energy": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "donof_occ_cg": (_i, [_vp, _vp, _vp, _vp, _vp, ct.c_double, _i, _vp, _vp, _vp]),
     "donof_energy": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),

@@ -40,7 +40,10 @@ def make_b(nbf: int, naux: int, rng: np.random.Generator) -> np.ndarray:
 
 
 def synthetic(nbf: int = 256, naux: int = 1024, nbeta: int = 16, ncwo: int = 3, seed: int = 1234,
-              occ_method: str = "Softmax", with_b: bool = True, **param_kw) -> Workload:
+              occ_method: str = "Softmax", with_b: bool = True, layer=None, **param_kw) -> Workload:
+    """layer: (occupations, coupling) functions of (gamma | n, Param) giving n and
+    cj12/ck12 (default: this package's, i.e. the library's native host code)."""
+    occupations, coupling = layer or (gnof.occupations, gnof.coupling)
     rng = np.random.default_rng(seed)
     p = Param(nbf=nbf, nbfaux=naux, nalpha=nbeta, nbeta=nbeta, ncwo=ncwo, occ_method=occ_method, **param_kw)
     if p.nbf5 > nbf:
@@ -53,8 +56,8 @@ def synthetic(nbf: int = 256, naux: int = 1024, nbeta: int = 16, ncwo: int = 3, 
     gamma = rng.standard_normal(p.nv)
     if occ_method == "Softmax":
         C, gamma = gnof.order_occupations_softmax(C, gamma, p)
-    n, _ = gnof.occupations(gamma, p)
-    cj12, ck12 = gnof.coupling(n, p)
+    n, _ = occupations(gamma, p)
+    cj12, ck12 = coupling(n, p)
     return Workload(p, b, C, H, gamma, n, np.asfortranarray(cj12), np.asfortranarray(ck12))
 
 

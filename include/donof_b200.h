@@ -266,6 +266,13 @@ typedef struct {
     int nbf5, no1, nbeta, nalpha, ncwo, ista, high_spin, occ_method;
     double h_cut;
 } donof_occ_params;
+/* Occupations n (nbf5) of ocupacion_softmax / _trigonometric (src/pnof.jl:
+ * 1024-1163) at gamma (nv), and, if dn_dgamma != NULL, dn/dgamma (nbf5 x nv,
+ * column-major).                                                            */
+int donof_occupations(const donof_occ_params* p, const double* gamma, double* n, double* dn_dgamma);
+/* GNOF coupling coefficients cj12, ck12 (nbf5 x nbf5, column-major, zero
+ * diagonal) of PNOFi_selector / CJCKD8 (src/pnof.jl:1-53, 488-601) at n.     */
+int donof_coupling(const donof_occ_params* p, const double* n, double* cj12, double* ck12);
 /* Occupation energy at gamma from cached J_MO, K_MO (nbf5 x nbf5, column-
  * major) and H_core (nbf5): calce / calcocce (src/pnof.jl:1273-1322) with the
  * occupations of ocupacion_softmax / _trigonometric (:1047-1163) and the GNOF

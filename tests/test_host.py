@@ -1,5 +1,5 @@
-"""CPU tests of the host side: the package's occupation/functional layer
-against the oracle, the synthetic workloads, and the C ABI library (loads and
+"""CPU tests of the host side: the package's occupation/functional layer (the
+library's native host code) against the oracle, the synthetic workloads, and the C ABI library (loads and
 exports every symbol the header declares; no compute calls without a GPU)."""
 import ctypes as ct
 import re
@@ -40,9 +40,6 @@ def test_gnof_layer_matches_oracle(case, ista, occ):
     cj1, ck1 = gnof.coupling(n1, p)
     cj2, ck2 = ognof.PNOFi_selector(n2, s)
     assert np.max(np.abs(cj1 - cj2)) < 1e-15 and np.max(np.abs(ck1 - ck2)) < 1e-14
-    D1 = gnof.coupling_derivatives(n1, dn1, p)
-    D2 = ognof.der_PNOFi_selector(n2, dn2, s)
-    assert np.max(np.abs(D1[0] - D2[0])) < 1e-14 and np.max(np.abs(D1[1] - D2[1])) < 1e-12
     J = rng.standard_normal((p.nbf5, p.nbf5)); J = J + J.T
     K = rng.standard_normal((p.nbf5, p.nbf5)); K = K + K.T
     Hc = rng.standard_normal(p.nbf5)
