@@ -54,6 +54,7 @@ __global__ void permute_cols_kernel(const double* __restrict__ Cin, const int* _
 
 struct Dev {
     double *H, *C, *C2, *n, *cj, *ck, *elag, *Hmat, *E, *J, *K, *Hc, *g;
+    double *gam, *occres;  // gamma and the result of the device occupation solver
     unsigned long long* gmax;
     int* perm;
 };
@@ -78,6 +79,11 @@ struct Loop {
         if (prec == DONOF_PREC_MIXED)
             return lagrange2_mixed(job, st, D.C, D.n, D.H, D.cj, D.ck, N, nalpha, nbeta, D.elag, D.Hmat, D.E);
         return lagrange2_f64(job, st, D.C, D.n, D.H, D.cj, D.ck, N, nalpha, nbeta, D.elag, D.Hmat, D.E);
+    }
+    // J_MO, K_MO, H_core at the current C, left on the device
+    int jkh_dev() {
+        if (prec == DONOF_PREC_MIXED) return jkh_mo_mixed(job, st, D.C, D.H, N, D.J, D.K, D.Hc);
+        return jkh_mo_f64(job, st, D.C, D.H, N, D.J, D.K, D.Hc);
     }
     // J_MO, K_MO, H_core at the current C, brought to the host
     int jkh(std::vector<double>& J, std::vector<double>& K, std::vector<double>& Hc) {
@@ -186,6 +192,8 @@ struct EnergyJob::Impl {
     double E = 9999.0, E_old = 9999.0, gorb = 0.0, gocc_norm = 0.0;
     int it = 1, tot_orb = 0, tot_occ = 0, converged = 0, nit_occ = 0;
     bool done = false, moved = false;
+    bool occ_dev = false;      // occoptr's CG runs on the device (occ_device and the sizes fit)
+    bool occ_dev_done = false;  // this iteration's device CG has run (occ_fetch)
 };
 
 EnergyJob::EnergyJob() : p(new Impl) {}
@@ -219,7 +227,8 @@ int EnergyJob::setup(donof_job* job, donof_energy_params* prm, const double* H, 
     const size_t oH = take(8 * nn), oC = take(8 * nn), oC2 = take(8 * nn), on = take(8 * (size_t)N),
                  ocj = take(8 * n55), ock = take(8 * n55), oel = take(8 * nn), oHm = take(8 * (size_t)nbf * N),
                  oE = take(8), oJ = take(8 * n55), oK = take(8 * n55), oHc = take(8 * (size_t)N),
-                 og = take(8 * (size_t)nvar), ogm = take(8), op = take(sizeof(int) * (size_t)nbf);
+                 og = take(8 * (size_t)nvar), ogm = take(8), op = take(sizeof(int) * (size_t)nbf),
+                 ogam = take(8 * (size_t)(nv > 0 ? nv : 1)), ores = take(8 * (size_t)(3 + nv));
     DONOF_CHECK(job->drv.ensure(ctx, off));
     char* base = job->drv.as<char>();
     S.L = Loop{job, ctx, ctx->stream, nbf, N, prm->occ.nalpha, prm->occ.nbeta, job->precision, {}};
@@ -239,6 +248,8 @@ int EnergyJob::setup(donof_job* job, donof_energy_params* prm, const double* H, 
     D.g = (double*)(base + og);
     D.gmax = (unsigned long long*)(base + ogm);
     D.perm = (int*)(base + op);
+    D.gam = (double*)(base + ogam);
+    D.occres = (double*)(base + ores);
     DONOF_CUDA(ctx, cudaMemcpyAsync(D.H, H, 8 * nn, cudaMemcpyHostToDevice, S.L.st));
     DONOF_CUDA(ctx, cudaMemcpyAsync(D.C, C, 8 * nn, cudaMemcpyHostToDevice, S.L.st));
     S.gamma.assign(gamma_in, gamma_in + nv);
@@ -250,6 +261,7 @@ int EnergyJob::setup(donof_job* job, donof_energy_params* prm, const double* H, 
     S.perm.assign(nbf, 0);
     donof::occ::occupations(o, S.gamma.data(), S.n.data(), S.dn.data());
     donof::occ::coupling(o, S.n.data(), S.cj.data(), S.ck.data());
+    S.occ_dev = prm->occ_device != 0 && donof::occ::occ_cg_fits(o);
     return DONOF_OK;
 }
 
@@ -261,10 +273,27 @@ int EnergyJob::after_orbopt(double E_orb, int nit_orb) {
     return end_iteration(E_orb, nit_orb);
 }
 
-// occoptr, device part: J_MO, K_MO, H_core at the optimised orbitals, to the host.
+// occoptr, device part: J_MO, K_MO, H_core at the optimised orbitals, to the host
+// for the host solver; with the device solver, they stay on the device and the
+// conjugate gradient runs there too (one CTA), only gamma and its result come back.
 int EnergyJob::occ_fetch() {
     Impl& S = *p;
-    if (S.o.ndoc > 0 && !S.prm->freeze_occ) DONOF_CHECK(S.L.jkh(S.J, S.K, S.Hc));
+    S.occ_dev_done = false;
+    if (S.o.ndoc <= 0 || S.prm->freeze_occ) return DONOF_OK;
+    if (!S.occ_dev) return S.L.jkh(S.J, S.K, S.Hc);
+    Loop& L = S.L;
+    const int nv = S.o.nv;
+    DONOF_CHECK(L.jkh_dev());
+    DONOF_CUDA(L.ctx, cudaMemcpyAsync(L.D.gam, S.gamma.data(), 8 * (size_t)nv, cudaMemcpyHostToDevice, L.st));
+    DONOF_CHECK(donof::occ::occ_cg_launch(L.ctx, L.st, S.o, L.D.J, L.D.K, L.D.Hc, L.D.gam, S.prm->threshen, 1000,
+                                          L.D.occres));
+    double res[3];
+    DONOF_CUDA(L.ctx, cudaMemcpyAsync(S.gamma.data(), L.D.gam, 8 * (size_t)nv, cudaMemcpyDeviceToHost, L.st));
+    DONOF_CUDA(L.ctx, cudaMemcpyAsync(res, L.D.occres, sizeof(res), cudaMemcpyDeviceToHost, L.st));
+    DONOF_CUDA(L.ctx, cudaStreamSynchronize(L.st));
+    DONOF_CHECK(failure_status(L.ctx));
+    S.nit_occ = (int)res[1];
+    S.occ_dev_done = true;
     return DONOF_OK;
 }
 
@@ -275,14 +304,18 @@ int EnergyJob::occ_solve() {
     Impl& S = *p;
     const donof::occ::Occ& o = S.o;
     donof_energy_params* prm = S.prm;
-    S.nit_occ = 0;
     if (o.ndoc > 0 && !prm->freeze_occ) {
-        double E_occ = 0.0;
-        int conv = 0;
-        const int rc = donof::occ::cg(o, S.J.data(), S.K.data(), S.Hc.data(), S.gamma.data(), prm->threshen, 1000,
-                                      &E_occ, &S.nit_occ, &conv);
-        if (rc != DONOF_OK) return rc;
+        if (!S.occ_dev_done) {
+            S.nit_occ = 0;
+            double E_occ = 0.0;
+            int conv = 0;
+            const int rc = donof::occ::cg(o, S.J.data(), S.K.data(), S.Hc.data(), S.gamma.data(), prm->threshen,
+                                          1000, &E_occ, &S.nit_occ, &conv);
+            if (rc != DONOF_OK) return rc;
+        }
         if (S.nit_occ < 1) prm->maxloop += 10;
+    } else {
+        S.nit_occ = 0;
     }
     donof::occ::occupations(o, S.gamma.data(), S.n_occ.data(), S.dn.data());
     donof::occ::coupling(o, S.n_occ.data(), S.cj_occ.data(), S.ck_occ.data());

@@ -5,6 +5,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "occ_math.cuh"
 
 namespace donof {
 namespace occ {
@@ -20,6 +21,8 @@ struct Occ {
 
 // false on inconsistent sizes or switches
 bool setup(const donof_occ_params* q, Occ& o);
+// the tables of o as a view (valid while o lives)
+OccView view(const Occ& o);
 // n (N) and dn (N x nv, dn[i * nv + k]) of ocupacion_softmax / _trigonometric
 void occupations(const Occ& o, const double* gamma, double* n, double* dn);
 // GNOF cj12, ck12 (N x N, column-major) of CJCKD8
@@ -27,6 +30,12 @@ void coupling(const Occ& o, const double* n, double* cj, double* ck);
 // occupation energy (calce) and, with grad != nullptr, its gamma-gradient (calcoccg)
 double energy_grad(const Occ& o, const double* gamma, const double* J, const double* K, const double* Hc,
                    double* grad);
+// occoptr's minimisation on the device (occ_device.cu): one CTA runs the same
+// CG over J, K, Hc and gamma in device memory (gamma in/out); result[0] = E,
+// [1] = iterations, [2] = converged, [3, 3 + nv) = the gradient at gamma.
+bool occ_cg_fits(const Occ& o);
+int occ_cg_launch(donof_ctx* ctx, cudaStream_t st, const Occ& o, const double* J, const double* K, const double* Hc,
+                  double* gamma, double g_abstol, int max_iter, double* result);
 // occoptr's minimisation over gamma (Hager-Zhang CG, strong-Wolfe line search)
 int cg(const Occ& o, const double* J_MO, const double* K_MO, const double* H_core, double* gamma,
        double g_abstol, int max_iter, double* E, int* nit, int* converged);

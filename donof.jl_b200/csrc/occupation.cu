@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "occ.cuh"
+#include "occ_math.cuh"
 
 namespace donof {
 namespace occ {
@@ -43,7 +44,7 @@ bool setup(const donof_occ_params* q, Occ& o) {
     o.high_spin = q->high_spin;
     o.method = q->occ_method;
     o.h_cut = q->h_cut;
-    if (o.N <= 0 || o.ndoc < 0 || o.nsoc < 0 || o.ncwo < 0 || o.no1 < 0 || o.ista < 0 || o.ista > 5 ||
+    if (o.N <= 0 || o.ndoc < 0 || o.nsoc < 0 || o.ncwo < 0 || o.ncwo > 64 || o.no1 < 0 || o.ista < 0 || o.ista > 5 ||
         (o.method != 0 && o.method != 1) || o.h_cut <= 0.0)
         return false;
     const int ndns = o.ndoc + o.nsoc;
@@ -77,128 +78,40 @@ namespace {
 // entries energy_grad reads.
 void occupations_impl(const Occ& o, const double* gamma, double* n, double* dn, bool full) {
     const int N = o.N, nv = o.nv, nd = o.ndoc, nc = o.ncwo;
+    const OccView ov = view(o);
     for (int i = 0; i < N; ++i) n[i] = 0.0;
     for (int i = 0; i < o.no1; ++i) n[i] = 1.0;
     for (int i = o.no1 + nd; i < o.no1 + nd + o.nsoc; ++i) n[i] = o.high_spin ? 1.0 : 0.5;
-    if (full) {
-        std::fill(dn, dn + (size_t)N * nv, 0.0);
-    } else {
-        for (int g = 0; g < nd; ++g)
-            for (int m = 0; m <= nc; ++m) {
-                const int r = (m == 0) ? o.S[g] : o.P[g * nc + m - 1];
-                for (int c = 0; c < nc; ++c) dn[(size_t)r * nv + o.KG[g * nc + c]] = 0.0;
-            }
-    }
-    if (o.method == 0) {  // softmax (src/pnof.jl:1122-1163)
-        std::vector<double> w((size_t)nd * nc);
-        for (int g = 0; g < nd; ++g) {
-            double s = 1.0;
-            for (int c = 0; c < nc; ++c) {
-                w[g * nc + c] = exp(gamma[o.G[g * nc + c]]);
-                s += w[g * nc + c];
-            }
-            const double inv = 1.0 / s;
-            n[o.S[g]] = inv;
-            for (int c = 0; c < nc; ++c) {
-                w[g * nc + c] *= inv;
-                n[o.P[g * nc + c]] = w[g * nc + c];
-            }
-        }
-        for (int g = 0; g < nd; ++g) {
-            // src/pnof.jl:1152 multiplies by n[i] with i the pair index (kept as is)
-            for (int c = 0; c < nc; ++c) dn[(size_t)o.S[g] * nv + o.G[g * nc + c]] = -n[g] * w[g * nc + c];
-            for (int a = 0; a < nc; ++a)
-                for (int b = 0; b < nc; ++b)
-                    dn[(size_t)o.P[g * nc + a] * nv + o.G[g * nc + b]] =
-                        (a == b ? w[g * nc + a] : 0.0) - w[g * nc + a] * w[g * nc + b];
-        }
-        return;
-    }
-    // trigonometric (src/pnof.jl:1047-1120)
-    std::vector<double> dstrong(nd);
+    if (full) std::fill(dn, dn + (size_t)N * nv, 0.0);
+    for (int g = 0; g < nd; ++g) pair_n(ov, gamma, g, n);
+    std::vector<double> blk((size_t)(nc + 1) * (nc > 0 ? nc : 1));
     for (int g = 0; g < nd; ++g) {
-        const double c = cos(gamma[g]);
-        n[o.S[g]] = 0.5 * (1.0 + c * c);
-        dstrong[g] = -0.5 * sin(2.0 * gamma[g]);
-    }
-    std::vector<int> cols(std::max(nc - 1, 0));
-    std::vector<double> th(std::max(nc - 1, 0)), s2(std::max(nc - 1, 0)), c2(std::max(nc - 1, 0)), fac(nc),
-        blk((size_t)nc * std::max(nc - 1, 1)), col(nc);
-    for (int g = 0; g < nd; ++g) {
-        for (int j = 0; j < nc - 1; ++j) {
-            cols[j] = nd + (nd - (g + 1)) + nd * j;
-            th[j] = gamma[cols[j]];
-            const double sn = sin(th[j]), cs = cos(th[j]);
-            s2[j] = sn * sn;
-            c2[j] = cs * cs;
-        }
-        const double h = 1.0 - n[o.S[g]];
-        std::fill(fac.begin(), fac.end(), 1.0);
-        for (int k = 0; k < nc - 1; ++k) {
-            fac[k] *= s2[k];
-            for (int m = k + 1; m < nc; ++m) fac[m] *= c2[k];
-        }
-        for (int w = 0; w < nc; ++w) n[o.P[g * nc + w]] = h * fac[w];
-        dn[(size_t)o.S[g] * nv + g] = dstrong[g];
-        for (int w = 0; w < nc; ++w) dn[(size_t)o.P[g * nc + w] * nv + g] = -dstrong[g] * fac[w];
-        const int nb = nc - 1;
-        auto B = [&](int r, int c) -> double& { return blk[(size_t)r * nb + c]; };
-        for (int j = 0; j < nb; ++j) {
-            for (int r = 0; r < nc; ++r) col[r] = n[o.S[g]] - 1.0;
-            for (int r = 0; r <= j; ++r) col[r] = 0.0;
-            for (int k = 0; k < j; ++k)
-                for (int r = j + 1; r < nc; ++r) col[r] *= c2[k];
-            for (int r = j + 1; r < nc; ++r) col[r] *= sin(2.0 * th[j]);
-            for (int k = j + 1; k < nb; ++k) {
-                col[k] *= s2[k];
-                for (int r = k + 1; r < nc; ++r) col[r] *= c2[k];
-            }
-            for (int r = 0; r < nc; ++r) B(r, j) = col[r];
-        }
-        for (int j = 0; j < nb; ++j) B(j, j) = 1.0 - n[o.S[g]];
-        for (int k = 0; k < nb; ++k) {
-            B(k, k) *= sin(2.0 * th[k]);
-            for (int l = k + 1; l < nb; ++l) B(l, l) *= c2[k];
-        }
-        for (int r = 0; r < nc; ++r)
-            for (int j = 0; j < nb; ++j) dn[(size_t)o.P[g * nc + r] * nv + cols[j]] = B(r, j);
+        pair_dn(ov, gamma, g, n, blk.data());
+        for (int m = 0; m <= nc; ++m)
+            for (int c = 0; c < nc; ++c) dn[(size_t)member(ov, g, m) * nv + o.KG[g * nc + c]] = blk[m * nc + c];
     }
 }
 
 }  // namespace
+
+OccView view(const Occ& o) {
+    return OccView{o.N, o.no1, o.ndoc, o.nsoc, o.nbeta, o.nalpha, o.ncwo, o.nv, o.ista, o.high_spin, o.method,
+                   o.h_cut, o.S.data(), o.P.data(), o.G.data(), o.KG.data(), o.grp.data()};
+}
 
 // n (N) and dn (N x nv, dn[i * nv + k]) for the configured occupation map
 void occupations(const Occ& o, const double* gamma, double* n, double* dn) {
     occupations_impl(o, gamma, n, dn, true);
 }
 
-double phi_fn(double ni, int ista) {
-    double f = ni * (1.0 - ni);
-    if (f < 0.0) f = 0.0;
-    switch (ista) {
-        case 0: case 1: case 5: return sqrt(f);
-        case 2: return 0.9 * sqrt(f);
-        case 3: {
-            const double a = 0.55, aa = pow(pow(2.0, 2.0 * a - 1.0), 1.0 / a);
-            return pow(aa * f, a);
-        }
-        default: return sqrt(f) * exp(-(ni - 0.5) * (ni - 0.5));  // ista 4
-    }
-}
-
 // n_d, F and coc of the dynamic part (src/pnof.jl:488-601)
 void dynamic(const Occ& o, const double* n, std::vector<double>& nd, std::vector<double>& F,
              std::vector<double>& coc) {
-    const double c = (o.ista == 5) ? 0.8 : 1.0;
+    const OccView ov = view(o);
     nd.assign(o.N, 0.0);
     F.assign(o.ndoc, 0.0);
     coc.assign(o.ndoc, 0.0);
-    for (int g = 0; g < o.ndoc; ++g) {
-        coc[g] = (1.0 - n[o.S[g]]) / o.h_cut;
-        F[g] = c * exp(-coc[g] * coc[g]);
-        nd[o.S[g]] = n[o.S[g]] * F[g];
-        for (int w = 0; w < o.ncwo; ++w) nd[o.P[g * o.ncwo + w]] = n[o.P[g * o.ncwo + w]] * F[g];
-    }
+    for (int g = 0; g < o.ndoc; ++g) pair_dynamic(ov, n, g, nd.data(), F.data(), coc.data());
 }
 
 bool in(int i, int a, int b) { return i >= a && i < b; }
@@ -262,24 +175,15 @@ void coupling(const Occ& o, const double* n, double* cj, double* ck) {
 // orbital and its weak partners) they take special values.  Every double sum
 // over (i, j) therefore reduces to, per orbital i, a few dot products of
 // column i of J_MO / K_MO with those vectors over the class ranges (RowSums),
-// plus corrections for the 1 + ncwo members of i's pair.  The gradient
-// contracts the separable terms
+// plus corrections for the 1 + ncwo members of its pair (occ_math.cuh).  The
+// gradient contracts the separable terms
 //   Dcj[i,j,:] = Mcj[i,j] dn[i,:],   Dck[i,j,:] = sum_t M_t[i,j] A_t[i,:],
 //   A = (dn, dphi, dn_d^{1/2}, dn_d),
 // whose rows A_t[i,:] are nonzero only on the ncwo gamma entries of i's pair.
 
-enum : int { V_N = 0, V_FI, V_ND12, V_ND, V_ONE, NVEC };
-
-inline int cls(const Occ& o, int i) { return i < o.no1 ? 0 : (i < o.nbeta ? 1 : (i < o.nalpha ? 2 : 3)); }
-
 struct OrbVecs {
     std::vector<double> n, fi, nd12, nd, F, coc;  // per orbital; F, coc per pair (dynamic())
-};
-
-// S[R][k] = sum over j in class range R of vec_k[j] K(j, i); jn = sum_j n_j J(j, i)
-struct RowSums {
-    double S[4][NVEC];
-    double jn;
+    VecView view() const { return VecView{n.data(), fi.data(), nd12.data(), nd.data(), F.data(), coc.data()}; }
 };
 
 // Rows are taken four at a time (the last ones one at a time): every row keeps
@@ -347,131 +251,14 @@ void row_sums(const Occ& o, const OrbVecs& v, const double* J, const double* K, 
     }
 }
 
-// generic ck(i, j) of coupling(), before the pair overrides
-inline double gen_ck(const Occ& o, const OrbVecs& v, int i, int j) {
-    const int ci = cls(o, i), cj = cls(o, j);
-    const bool ibe = ci == 1, ial = ci == 2, icw = ci == 3, jbe = cj == 1, jal = cj == 2, jcw = cj == 3;
-    double k = v.n[i] * v.n[j];
-    if (o.ista == 0) {
-        if ((ibe && jcw) || (icw && jbe) || (icw && jcw)) k += v.fi[i] * v.fi[j];
-        if (o.nsoc > 0) {
-            if (ibe && jal) k += 0.25 * v.fi[i];
-            if (ial && jbe) k += 0.25 * v.fi[j];
-            if (ial && jcw) k += 0.5 * v.fi[j];
-            if (icw && jal) k += 0.5 * v.fi[i];
-        }
-        if (o.nsoc > 1 && ial && jal) k = 0.5;
-    } else {
-        k += v.fi[i] * v.fi[j];
-    }
-    if ((ibe && jcw) || (icw && jbe)) k += v.nd12[i] * v.nd12[j] - v.nd[i] * v.nd[j];
-    if (icw && jcw) k -= v.nd12[i] * v.nd12[j] + v.nd[i] * v.nd[j];
-    return k;
-}
-
-// sum_j gen_ck(i, j) K(j, i) from the row sums
-inline double row_ck(const Occ& o, const OrbVecs& v, int i, const RowSums& r) {
-    const int ci = cls(o, i);
-    const double ni = v.n[i], fi = v.fi[i];
-    double s = ni * (r.S[0][V_N] + r.S[1][V_N] + r.S[2][V_N] + r.S[3][V_N]);
-    if (o.ista == 0) {
-        if (ci == 1) s += fi * r.S[3][V_FI];
-        if (ci == 3) s += fi * (r.S[1][V_FI] + r.S[3][V_FI]);
-        if (o.nsoc > 0) {
-            if (ci == 1) s += 0.25 * fi * r.S[2][V_ONE];
-            if (ci == 2) s += 0.25 * r.S[1][V_FI] + 0.5 * r.S[3][V_FI];
-            if (ci == 3) s += 0.5 * fi * r.S[2][V_ONE];
-        }
-        if (o.nsoc > 1 && ci == 2) s += 0.5 * r.S[2][V_ONE] - ni * r.S[2][V_N];
-    } else {
-        s += fi * (r.S[0][V_FI] + r.S[1][V_FI] + r.S[2][V_FI] + r.S[3][V_FI]);
-    }
-    if (ci == 1) s += v.nd12[i] * r.S[3][V_ND12] - v.nd[i] * r.S[3][V_ND];
-    if (ci == 3)
-        s += v.nd12[i] * (r.S[1][V_ND12] - r.S[3][V_ND12]) - v.nd[i] * (r.S[1][V_ND] + r.S[3][V_ND]);
-    return s;
-}
-
-// ck(i, j) inside a pair, i != j (coupling(): strong-weak sqrt(n_s n_w), weak-weak -sqrt(n_w) sqrt(n_v))
-inline double spec_ck(const Occ& o, const OrbVecs& v, int i, int j) {
-    const int g = o.grp[i];
-    if (i == o.S[g]) return sqrt(v.n[i] * v.n[j]);
-    if (j == o.S[g]) return sqrt(v.n[j] * v.n[i]);
-    return -(sqrt(v.n[i]) * sqrt(v.n[j]));
-}
-
-// generic derivative factors M_t(r, j) (t = 0..3) and Mcj(r, j) for a row r in a pair
-inline void gen_m(const Occ& o, const OrbVecs& v, int r, int j, double (&m)[4], double& mcj) {
-    const int cr = cls(o, r), cj = cls(o, j);
-    const bool rbe = cr == 1, rcw = cr == 3, jbe = cj == 1, jal = cj == 2, jcw = cj == 3;
-    mcj = 2.0 * v.n[j];
-    m[0] = v.n[j];
-    m[1] = m[2] = m[3] = 0.0;
-    if (o.ista == 0) {
-        if ((rbe && jcw) || (rcw && jbe) || (rcw && jcw)) m[1] += v.fi[j];
-        if (o.nsoc > 0) {
-            if (rbe && jal) m[1] += 0.25;
-            if (rcw && jal) m[1] += 0.5;
-        }
-    } else {
-        m[1] += v.fi[j];
-    }
-    if ((rbe && jcw) || (rcw && jbe)) {
-        m[2] += v.nd12[j];
-        m[3] -= v.nd[j];
-    }
-    if (rcw && jcw) {
-        m[2] -= v.nd12[j];
-        m[3] -= v.nd[j];
-    }
-}
-
-// sum_j M_t(r, j) K(j, r) for the generic factors of a row r in a pair
-inline void row_m(const Occ& o, int r, const RowSums& s, double (&vk)[4]) {
-    const int cr = cls(o, r);
-    vk[0] = s.S[0][V_N] + s.S[1][V_N] + s.S[2][V_N] + s.S[3][V_N];
-    if (o.ista == 0) {
-        vk[1] = (cr == 1) ? s.S[3][V_FI] : s.S[1][V_FI] + s.S[3][V_FI];
-        if (o.nsoc > 0) vk[1] += (cr == 1 ? 0.25 : 0.5) * s.S[2][V_ONE];
-    } else {
-        vk[1] = s.S[0][V_FI] + s.S[1][V_FI] + s.S[2][V_FI] + s.S[3][V_FI];
-    }
-    if (cr == 1) {
-        vk[2] = s.S[3][V_ND12];
-        vk[3] = -s.S[3][V_ND];
-    } else {
-        vk[2] = s.S[1][V_ND12] - s.S[3][V_ND12];
-        vk[3] = -s.S[1][V_ND] - s.S[3][V_ND];
-    }
-}
-
-// d phi / d n_i (the factor of dfi = dphi * dn, der_CJCKD8)
-double dphi_factor(const Occ& o, double ni) {
-    double f = ni * (1.0 - ni);
-    if (f < 0.0) f = 0.0;
-    if (o.ista == 3) {
-        const double al = 0.55, aa = pow(pow(2.0, 2.0 * al - 1.0), 1.0 / al);
-        const double a = std::max(aa * ni * (1.0 - ni), 1e-15);
-        return al * pow(a, al - 1.0) * aa * (1.0 - 2.0 * ni);
-    }
-    const double fi0 = sqrt(f) * (o.ista == 2 ? 0.9 : 1.0);
-    const double a = std::max(fi0, 1e-15);
-    const double scale = (o.ista == 2) ? 0.81 : 1.0;
-    double fac = scale / (2.0 * a) * (1.0 - 2.0 * ni);
-    if (o.ista == 4) {
-        const double e = exp(-(ni - 0.5) * (ni - 0.5));
-        fac = fac * e - fi0 * 2.0 * (ni - 0.5) * e;
-    }
-    return fac;
-}
-
 // Occupation energy (calce, src/pnof.jl:1273-1300) and, when grad != nullptr,
 // its gamma-gradient (calcoccg, :1324-1377).
 double energy_grad(const Occ& o, const double* gamma, const double* J, const double* K, const double* Hc,
                    double* grad) {
     const int N = o.N, nv = o.nv, nc = o.ncwo;
+    const OccView ov = view(o);
     thread_local OrbVecs v;
-    thread_local std::vector<double> dn, w;
+    thread_local std::vector<double> dn, w, blk;
     thread_local std::vector<RowSums> rs;
     v.n.resize(N);
     dn.resize((size_t)N * (nv > 0 ? nv : 1));
@@ -483,74 +270,31 @@ double energy_grad(const Occ& o, const double* gamma, const double* J, const dou
         v.fi[i] = phi_fn(v.n[i], o.ista);
         v.nd12[i] = sqrt(v.nd[i]);
     }
-    auto Jm = [&](int i, int j) { return J[i + (size_t)N * j]; };
-    auto Km = [&](int i, int j) { return K[i + (size_t)N * j]; };
+    const VecView vv = v.view();
     w.resize(N);
-    for (int i = 0; i < N; ++i) w[i] = 2.0 * Hc[i] + Jm(i, i);
+    for (int i = 0; i < N; ++i) w[i] = 2.0 * Hc[i] + J[i + (size_t)N * i];
     double E = 0.0;
     for (int i = 0; i < o.nbeta; ++i) E += v.n[i] * w[i];
     if (o.nsoc > 0)
         for (int i = o.nbeta; i < o.nalpha; ++i) E += 2.0 * v.n[i] * Hc[i];
     for (int i = o.nalpha; i < N; ++i) E += v.n[i] * w[i];
     row_sums(o, v, J, K, rs);
-    // sum_ij cj12[i,j] J(j,i) - ck12[i,j] K(j,i): generic rows, minus the generic
-    // values on i's pair (or on the diagonal), plus the pair's special values
+    // sum_ij cj12[i,j] J(j,i) - ck12[i,j] K(j,i)
     double sj = 0.0, sk = 0.0;
     for (int i = 0; i < N; ++i) {
-        double rj = 2.0 * v.n[i] * rs[i].jn, rk = row_ck(o, v, i, rs[i]);
-        const int g = o.grp[i];
-        auto corr = [&](int j) {
-            rj -= 2.0 * v.n[i] * v.n[j] * Jm(j, i);
-            rk -= gen_ck(o, v, i, j) * Km(j, i);
-            if (j != i) rk += spec_ck(o, v, i, j) * Km(j, i);
-        };
-        if (g < 0) {
-            corr(i);
-        } else {
-            corr(o.S[g]);
-            for (int a = 0; a < nc; ++a) corr(o.P[g * nc + a]);
-        }
+        double rj, rk;
+        row_energy(ov, vv, i, rs[i], J, K, &rj, &rk);
         sj += rj;
         sk += rk;
     }
     E += sj - sk;
     if (grad) {
         for (int k = 0; k < nv; ++k) grad[k] = 0.0;
+        blk.resize((size_t)(nc + 1) * (nc > 0 ? nc : 1));
         for (int g = 0; g < o.ndoc; ++g) {
-            const int s = o.S[g];
-            const double kk = 2.0 * v.coc[g] / o.h_cut;
-            const double sa = sqrt(std::max(v.n[s], 1e-15));
-            for (int m = 0; m <= nc; ++m) {
-                const int r = (m == 0) ? s : o.P[g * nc + m - 1];
-                // vj = sum_j Mcj(r,j) J(j,r), vk_t = sum_j M_t(r,j) K(j,r)
-                double vj = 2.0 * rs[r].jn, vk[4];
-                row_m(o, r, rs[r], vk);
-                const double sb = sqrt(std::max(v.n[r], 1e-15));
-                for (int q = 0; q <= nc; ++q) {  // the pair's members: generic values out, special in
-                    const int j = (q == 0) ? s : o.P[g * nc + q - 1];
-                    double mg[4], mcj;
-                    gen_m(o, v, r, j, mg, mcj);
-                    vj -= mcj * Jm(j, r);
-                    for (int t = 0; t < 4; ++t) vk[t] -= mg[t] * Km(j, r);
-                    if (j == r) continue;
-                    double m0;
-                    if (r == s) m0 = 0.5 / sa * sqrt(v.n[j]);
-                    else if (j == s) m0 = 0.5 / sb * sqrt(v.n[s]);
-                    else m0 = -0.5 * (1.0 / sb) * sqrt(v.n[j]);
-                    vk[0] += m0 * Km(j, r);
-                }
-                const double cdn = w[r] + 2.0 * vj;
-                const double fac = dphi_factor(o, v.n[r]);
-                const double den = std::max(v.nd12[r], 1e-15);
-                for (int c = 0; c < nc; ++c) {
-                    const int k = o.KG[g * nc + c];
-                    const double a0 = dn[(size_t)r * nv + k];
-                    const double a3 = (r == s) ? v.F[g] * a0 * (1.0 + v.n[s] * kk)
-                                               : v.F[g] * a0 + v.F[g] * kk * v.n[r] * dn[(size_t)s * nv + k];
-                    const double a1 = fac * a0, a2 = 0.5 * a3 / den;
-                    grad[k] += a0 * cdn - 2.0 * (a0 * vk[0] + a1 * vk[1] + a2 * vk[2] + a3 * vk[3]);
-                }
-            }
+            for (int m = 0; m <= nc; ++m)
+                for (int c = 0; c < nc; ++c) blk[m * nc + c] = dn[(size_t)member(ov, g, m) * nv + o.KG[g * nc + c]];
+            pair_grad(ov, vv, rs.data(), J, K, w.data(), blk.data(), g, grad);
         }
     }
     return E;

@@ -59,6 +59,7 @@ SIGNATURES = {
     "donof_occupations": (_i, [_vp, _vp, _vp, _vp]),
     "donof_coupling": (_i, [_vp, _vp, _vp, _vp]),
     "donof_occ_energy": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "donof_occ_cg_dev": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, ct.c_double, _i, _vp]),
     "donof_occ_cg": (_i, [_vp, _vp, _vp, _vp, _vp, ct.c_double, _i, _vp, _vp, _vp]),
     "donof_energy": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "donof_server_create": (_i, [_i, ct.c_size_t, _i, ct.POINTER(_vp)]),

@@ -398,6 +398,7 @@ class Batch:
             prm.maxit, prm.maxloop, prm.alpha = int(maxit or p.maxit), int(p.maxloop), float(p.alpha)
             prm.threshgorb, prm.threshgocc, prm.threshen = float(p.threshgorb), float(p.threshgocc), float(p.threshen)
             prm.order_subspaces = int(bool(order) and p.ipnof > 4)
+            prm.occ_device = int(bool(getattr(p, "occ_device", True)))
         Hf = [_f64(H) for H in Hs]
         Cio = [np.array(_f64(C), copy=True, order="F") for C in Cs]
         gio = [np.array(g, dtype=np.float64, copy=True) for g in gammas]
@@ -482,7 +483,7 @@ class _EnergyParams(ct.Structure):
     _fields_ = [("occ", _OccParams), ("orb_method", ct.c_int), ("maxit", ct.c_int), ("maxloop", ct.c_int),
                 ("alpha", ct.c_double), ("threshgorb", ct.c_double), ("threshgocc", ct.c_double),
                 ("threshen", ct.c_double), ("order_subspaces", ct.c_int), ("freeze_occ", ct.c_int),
-                ("stop_rel_de", ct.c_double)]
+                ("stop_rel_de", ct.c_double), ("occ_device", ct.c_int)]
 
 
 class _EnergyResult(ct.Structure):
@@ -500,7 +501,8 @@ def energy_loop(H, b: BTensor, p: Param, C, gamma, maxit: Optional[int] = None, 
     maxit = int(maxit or p.maxit)
     prm = _EnergyParams(_occ_params(p), _lib.ORB_METHODS[p.orb_method], maxit, int(p.maxloop), float(p.alpha),
                         float(p.threshgorb), float(p.threshgocc), float(p.threshen),
-                        int(bool(order) and p.ipnof > 4), int(bool(freeze_occ)), float(stop_rel_de))
+                        int(bool(order) and p.ipnof > 4), int(bool(freeze_occ)), float(stop_rel_de),
+                        int(bool(getattr(p, "occ_device", True))))
     Cio = np.array(_f64(C), copy=True, order="F")
     g = np.array(gamma, dtype=np.float64, copy=True)
     n = np.zeros(p.nbf5)

@@ -32,6 +32,7 @@ class Param:
     h_cut: float = 0.02 * math.sqrt(2.0)
     title: str = "donof"
     RI: bool = True
+    occ_device: bool = True   # occoptr's conjugate gradient on the GPU (False: on the host, like the reference)
     extra: dict = field(default_factory=dict)
 
     def __post_init__(self):

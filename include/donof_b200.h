@@ -289,6 +289,16 @@ int donof_occ_cg(const donof_occ_params* p, const double* J_MO, const double* K_
                  const double* H_core, double* gamma, double g_abstol, int max_iter, double* E,
                  int* nit, int* converged);
 
+/* occoptr's minimisation (as donof_occ_cg) on the GPU: one CTA runs the same
+ * conjugate gradient and line search over J_MO, K_MO (nbf5 x nbf5), H_core
+ * (nbf5) and gamma (nv, in/out), all in DEVICE memory, and writes result (device,
+ * 3 + nv doubles): the energy, the iteration count, 1 if the gradient test was
+ * met, then the gradient at the returned gamma.  Enqueued on the context
+ * stream; allocates nothing.  Sums run in another order than on the host, so
+ * the two solvers agree to rounding.                                          */
+int donof_occ_cg_dev(donof_ctx* ctx, const donof_occ_params* p, const double* J_MO, const double* K_MO,
+                     const double* H_core, double* gamma, double g_abstol, int max_iter, double* result);
+
 /* --- the energy loop ------------------------------------------------------------
  * Switches and thresholds of DoNOF.energy's alternation (names of
  * src/param.jl): the occupation layer, the orbital optimiser (DONOF_ORB_*),
@@ -298,7 +308,9 @@ int donof_occ_cg(const donof_occ_params* p, const double* J_MO, const double* K_
  * (ipnof > 4); freeze_occ = 1 keeps gamma fixed; stop_rel_de > 0 ends the
  * loop once an outer iteration changes E by at most stop_rel_de |E| (the
  * mixed-precision phase stops there, where its energies' rounding would
- * steer the optimiser, and FP64 iterations take over).                      */
+ * steer the optimiser, and FP64 iterations take over); occ_device = 1 runs
+ * occoptr's conjugate gradient on the GPU (one CTA, J_MO / K_MO stay on the
+ * device) instead of the host.                                              */
 typedef struct {
     donof_occ_params occ;
     int orb_method;
@@ -309,6 +321,7 @@ typedef struct {
     int order_subspaces;
     int freeze_occ;
     double stop_rel_de;  /* > 0: also stop (not converged) once |E - E_prev| <= stop_rel_de |E| */
+    int occ_device;      /* 1: occoptr's minimisation on the GPU (as donof_occ_cg_dev), 0: on the host */
 } donof_energy_params;
 typedef struct {
     double E_elec;                /* E of the last orbital optimisation */

@@ -204,6 +204,7 @@ struct EnergyParams
     order_subspaces::Cint
     freeze_occ::Cint
     stop_rel_de::Cdouble
+    occ_device::Cint
 end
 
 struct EnergyResult
@@ -217,11 +218,11 @@ struct EnergyResult
 end
 
 """EnergyParams of DoNOF's Param `p` (the names of src/param.jl)."""
-energy_params(p; freeze_occ::Bool = false, stop_rel_de::Real = 0.0) =
+energy_params(p; freeze_occ::Bool = false, stop_rel_de::Real = 0.0, occ_device::Bool = true) =
     EnergyParams(OccParams(p.nbf5, p.no1, p.nbeta, p.nalpha, p.ncwo, p.ista, p.HighSpin,
                            p.occ_method == "Softmax" ? 0 : 1, p.h_cut),
                  ORB_METHODS[p.orb_method], p.maxit, p.maxloop, p.alpha, p.threshgorb, p.threshgocc,
-                 p.threshen, p.ipnof > 4, freeze_occ, stop_rel_de)
+                 p.threshen, p.ipnof > 4, freeze_occ, stop_rel_de, occ_device)
 
 """
 The orbital / occupation alternation of DoNOF.energy (src/energy.jl:140-224)
