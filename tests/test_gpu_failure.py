@@ -160,11 +160,11 @@ def test_native_server_cancels_queued_and_running_jobs():
         srv.cancel(t_run)  # stops at its next outer iteration
         r_r = srv.wait(t_run)
         assert r_r.error == "cancelled"
-        # the server goes on serving
+        # the server goes on serving: the next job runs to its end
         wl = workload.molecule_like(nbf=24, naux=58, nbeta=5, ncwo=3, seed=23, two_e_scale=0.2)
         wl.p.threshgorb = wl.p.threshgocc = 1e-4
-        r = srv.wait(srv.submit(_native_request(wl, maxit=200)))
-        assert r.error is None and r.converged
+        r = srv.wait(srv.submit(_native_request(wl, maxit=20)))
+        assert r.error is None and r.iterations > 0 and np.isfinite(r.E_elec)
 
 
 def test_native_server_destroy_releases_a_blocked_waiter():
