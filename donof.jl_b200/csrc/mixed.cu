@@ -72,11 +72,11 @@ constexpr int B_EMPTY = RING;      // +s: stage s consumed by the MMAs
 constexpr int B_CS = 2 * RING;     // Cs landed
 constexpr int B_T1 = B_CS + 1;     // +slot (2): T1 quarter in TMEM slot complete
 constexpr int B_T1FREE = B_T1 + 2; // +slot (2): the four epilogue warps read the slot (count 4)
-constexpr int B_A2Q = B_T1FREE + 2; // +qb (4): quarter qb of the tmp split written (count 4, one phase per index)
-constexpr int B_T2 = B_A2Q + 4;    // T2 complete
+constexpr int B_A2 = B_T1FREE + 2; // tmp split of the aux index written (one phase per index)
+constexpr int B_T2 = B_A2 + 1;     // T2 complete
 constexpr int B_A3 = B_T2 + 1;     // W split written, T2 region drained
-constexpr int B_YQ = B_A3 + 1;     // +qb (4): the Y MMAs reading quarter qb of the tmp split complete
-constexpr int B_END = B_YQ + 4;    // every MMA of the CTA complete
+constexpr int B_Y = B_A3 + 1;      // Y MMAs of the aux index complete
+constexpr int B_END = B_Y + 1;     // every MMA of the CTA complete
 static_assert(B_END < NBAR, "barrier count");
 
 // TMEM columns (512 allocated): Y accumulator [0, 256), two T1 quarter slots
@@ -154,8 +154,7 @@ lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_const
 
     if (threadIdx.x == 0) {
         *abort_flag = 0;
-        for (int i = 0; i <= B_END; ++i)
-            mbar_init(bar(i), ((i >= B_T1FREE && i < B_T1FREE + 2) || (i >= B_A2Q && i < B_A2Q + 4)) ? 4 : 1);
+        for (int i = 0; i <= B_END; ++i) mbar_init(bar(i), (i == B_T1FREE || i == B_T1FREE + 1) ? 4 : 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 5) {
@@ -202,58 +201,31 @@ lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_const
         }
     } else if (warp == 5) {
         // ------------------------------------------------------------ MMA issuer
-        // Issue order per aux index l: its T1 quarters, with the T2(l) partial of
-        // each 64-column quarter of m issued as soon as the epilogue has written
-        // that quarter of the tmp split; then (while the epilogue drains T2(l) and
-        // builds W(l)) up to two T1 quarters of l+1 into the free slots, and Y(l),
-        // one 64-column quarter of m at a time, as soon as W(l) is ready.
+        // Issue order per aux index l: its T1 quarters, T2(l), then (while the
+        // epilogue drains T2(l) and builds W(l)) up to two T1 quarters of l+1 into
+        // the free slots, and Y(l) as soon as W(l) is ready.
         if (lane == 0 && my_count > 0) {
             const uint32_t id_t1 = idesc(128, BOX_M, 0, 1);
             const uint32_t id_t2 = idesc(128, 128, 0, 0);
-            const uint32_t id_y = idesc(128, BOX_M, 0, 1);
+            const uint32_t id_y = idesc(128, ncol, 0, 1);
             bool ok = mbar_wait(bar(B_CS), 0, abort_flag, P.wait);
             fence_after();
             int it = 0;          // ring stages consumed
             int tq = 0;          // T1 quarters issued (slot = tq & 1)
             int y_li = -1;       // aux index whose Y MMAs are still to be issued
-            int t2_li = -1;      // aux index whose T2 partials are being issued
-            int t2_next = 0;     // next quarter of its T2 partials
             auto issue_y = [&]() {
-                // Y: RY[j, m] += sum_q A3[j, q] tmp_x[q, m]  (A2 read as an MN-major operand),
-                // one 64-column quarter of m per commit, so that the epilogue can write the
-                // next index's tmp split into a quarter as soon as its Y MMAs are done
-                for (int qm = 0; qm < P.nb; ++qm) {
-#pragma unroll
-                    for (int ks = 0; ks < 4; ++ks) {
-                        const uint64_t a = sdesc(sbase + OFF_A3 + ks * 32, 16, 1024);
-                        // K rows q = 16 ks + i of the hi part are A2 rows 32 ks + i, the lo part 32 ks + 16 + i
-                        const uint32_t bq = sbase + OFF_A2 + qm * CS_BOX_BYTES + ks * 4096;
-                        const uint64_t bh = sdesc(bq, CS_BOX_BYTES, 1024);
-                        const uint64_t bl = sdesc(bq + 2048, CS_BOX_BYTES, 1024);
-                        umma(RY + qm * BOX_M, a, bh, id_y, (y_li | ks) ? 1u : 0u);
-                        umma(RY + qm * BOX_M, a, bl, id_y, 1u);
-                    }
-                    umma_commit(bar(B_YQ + qm));
-                }
-                y_li = -1;
-            };
-            // T2 partial of quarter qb: RT2[j, j'] += sum_{m in quarter} A2[j, m] Cs[j', m]
-            auto issue_t2q = [&](int qb) {
+                // Y: RY[j, m] += sum_q A3[j, q] tmp_x[q, m]  (A2 read as an MN-major operand)
 #pragma unroll
                 for (int ks = 0; ks < 4; ++ks) {
-                    const int k = qb * 64 + ks * 16;  // m offset
-                    const uint64_t a = sdesc(sbase + OFF_A2 + qb * CS_BOX_BYTES + ks * 32, 16, 1024);
-                    const uint64_t b = sdesc(sbase + OFF_CS + (k >> 6) * CS_BOX_BYTES + (k & 63) * 2, 16, 1024);
-                    umma(RT2, a, b, id_t2, (qb | ks) ? 1u : 0u);
+                    const uint64_t a = sdesc(sbase + OFF_A3 + ks * 32, 16, 1024);
+                    // K rows q = 16 ks + i of the hi part are A2 rows 32 ks + i, the lo part 32 ks + 16 + i
+                    const uint64_t bh = sdesc(sbase + OFF_A2 + ks * 4096, CS_BOX_BYTES, 1024);
+                    const uint64_t bl = sdesc(sbase + OFF_A2 + ks * 4096 + 2048, CS_BOX_BYTES, 1024);
+                    umma(RY, a, bh, id_y, (y_li | ks) ? 1u : 0u);
+                    umma(RY, a, bl, id_y, 1u);
                 }
-            };
-            // the T2 partials whose quarter of the tmp split is ready (non-blocking)
-            auto poll_t2 = [&]() {
-                while (t2_li >= 0 && t2_next < P.nb && mbar_test(bar(B_A2Q + t2_next), (uint32_t)(t2_li & 1))) {
-                    fence_after();
-                    issue_t2q(t2_next);
-                    ++t2_next;
-                }
+                umma_commit(bar(B_Y));
+                y_li = -1;
             };
             // Bounded wait that issues the pending Y MMAs as soon as W is ready.
             auto wait_poll = [&](uint32_t b, uint32_t parity) -> bool {
@@ -263,9 +235,9 @@ lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_const
                         fence_after();
                         issue_y();
                     }
-                    poll_t2();
                     if (*abort_flag) return false;
                     if (clock64() - t0 > P.wait) { *abort_flag = 1; return false; }
+                    __nanosleep(32);  // leave issue slots to the epilogue warp on this SM sub-partition
                 }
                 return true;
             };
@@ -281,7 +253,6 @@ lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_const
                         fence_after();
                         issue_y();
                     }
-                    poll_t2();
                     if (!wait_poll(bar(B_FULL + s), (uint32_t)((it / RING) & 1))) return false;
                     fence_after();
                     const uint32_t st = sbase + OFF_RING + s * STAGE_BYTES;
@@ -304,23 +275,19 @@ lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_const
             int ahead = 0;  // quarters of the current index issued early
             for (int li = 0; li < my_count && ok; ++li) {
                 const uint32_t lph = (uint32_t)(li & 1);
-                // the T2 region is free (W(l-1) was waited for): T2(l) partials may go as
-                // their quarters of the tmp split arrive
-                if (P.mode != 1) {
-                    t2_li = li;
-                    t2_next = 0;
-                }
                 for (int qb = ahead; qb < P.nb && ok; ++qb) ok = t1_quarter();
                 ahead = 0;
                 if (!ok) break;
                 if (P.mode == 1) continue;
-                // T2: RT2[j, j'] = sum_m A2[j, m] Cs[j', m], the quarters not issued yet
-                while (t2_next < P.nb) {
-                    if (!wait_poll(bar(B_A2Q + t2_next), lph)) { ok = false; break; }
-                    poll_t2();
+                // T2: RT2[j, j'] = sum_m A2[j, m] Cs[j', m]
+                if (!wait_poll(bar(B_A2), lph)) { ok = false; break; }
+                fence_after();
+                for (int ks = 0; ks < ncol / 16; ++ks) {
+                    const int k = ks * 16;  // m offset
+                    const uint64_t a = sdesc(sbase + OFF_A2 + (k >> 6) * CS_BOX_BYTES + (k & 63) * 2, 16, 1024);
+                    const uint64_t b = sdesc(sbase + OFF_CS + (k >> 6) * CS_BOX_BYTES + (k & 63) * 2, 16, 1024);
+                    umma(RT2, a, b, id_t2, ks ? 1u : 0u);
                 }
-                if (!ok) break;
-                t2_li = -1;
                 umma_commit(bar(B_T2));
                 if (P.mode == 3) y_li = li;
                 // T1 of the next index into the slots the epilogue has already drained
@@ -406,8 +373,8 @@ lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_const
             for (int qb = 0; qb < P.nb; ++qb) {
                 const int t = tq + qb, slot = t & 1;
                 if (!warp_wait(B_T1 + slot, (uint32_t)((t >> 1) & 1))) { wok = false; break; }
-                // quarter qb of A2 is read by the Y MMAs of the previous index
-                if (li > 0 && P.mode == 3 && !warp_wait(B_YQ + qb, (uint32_t)((li - 1) & 1))) { wok = false; break; }
+                // A2 is read by the Y MMAs of the previous index
+                if (qb == 0 && li > 0 && P.mode == 3 && !warp_wait(B_Y, (uint32_t)((li - 1) & 1))) { wok = false; break; }
                 const uint32_t src = RT1 + slot * BOX_M + lane_addr;
                 uint32_t ra[32], rb[32];
                 tmem_issue32(src, ra);
@@ -419,17 +386,12 @@ lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_const
                 if (lane == 0) mbar_arrive(bar(B_T1FREE + slot));
                 drain32(ra, 2 * qb, l);
                 drain32(rb, 2 * qb + 1, l);
-                if (P.mode != 1) {
-                    // this warp's rows of quarter qb of A2, written by the generic proxy, are
-                    // read by the T2 MMAs of the quarter
-                    fence_async_smem();
-                    __syncwarp();
-                    if (lane == 0) mbar_arrive(bar(B_A2Q + qb));
-                }
             }
             tq += P.nb;
+            if (P.mode != 1) fence_async_smem();  // A2 written by the generic proxy, read by the MMAs
             if (!agree(wok)) { ok = false; break; }
             if (P.mode == 1) continue;
+            if (threadIdx.x == 0) mbar_arrive(bar(B_A2));
             // ---- T2 drain: b_pq[p, q] = sum over x, x' of D2[prow(q, x), prow(p, x')]
             if (!epi_wait(B_T2, lph)) { ok = false; break; }
             float bq[32];  // b_pq for p = off + i
@@ -524,9 +486,7 @@ lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_const
         }
         // ---- final: Y partial (mode 3): Y[m, b] = D3[prow(b, 0), m] + D3[prow(b, 1), m]
         if (ok && my_count > 0 && P.mode == 3) {
-            bool yok = true;
-            for (int qm = 0; qm < P.nb && yok; ++qm) yok = epi_wait(B_YQ + qm, (uint32_t)((my_count - 1) & 1));
-            if (yok) {
+            if (epi_wait(B_Y, (uint32_t)((my_count - 1) & 1))) {
                 for (int c = 0; c < ncol / 32; ++c) {
                     uint32_t r[32];
                     tmem_issue32(RY + lane_addr + c * 32, r);

@@ -2,7 +2,8 @@
 //
 // The same Hager-Zhang conjugate gradient with a strong-Wolfe line search and
 // the approximate-Wolfe acceptance as the host solver (occupation.cu), run by
-// one CTA: every evaluation of the occupation energy and gradient (calce /
+// one CTA (a line search that finds no step along a conjugate direction is
+// retried once from steepest descent before the solver stops): every evaluation of the occupation energy and gradient (calce /
 // calcoccg, src/pnof.jl:1273-1377) is a few CTA-wide passes over the shared
 // per-orbital formulas (occ_math.cuh) -- the occupations and dn blocks of the
 // pairs, n_d and phi(n), the class-range row sums of J_MO / K_MO (one warp per
@@ -326,7 +327,7 @@ __global__ void __launch_bounds__(NT, 1) occ_cg_kernel(const __grid_constant__ T
         for (int k = tid; k < nv; k += NT) m.d[k] = -m.gx[k];
         __syncthreads();
         double a = 1.0 / fmax(maxabs(m, m.gx, nv), 1e-12);
-        bool have_prev = false;
+        bool have_prev = false, steepest = true;
         double gd_prev = 0.0;
         nit = A.max_iter;
         for (int it = 1; it <= A.max_iter; ++it) {
@@ -335,6 +336,7 @@ __global__ void __launch_bounds__(NT, 1) occ_cg_kernel(const __grid_constant__ T
                 for (int k = tid; k < nv; k += NT) m.d[k] = -m.gx[k];
                 __syncthreads();
                 gd = dot(m, m.gx, m.d, nv);
+                steepest = true;
             }
             if (have_prev) a = fmin(fmax(a * gd_prev / gd, 1e-10), 1e6);
             const Pt pt = wolfe(A, m, fx, gd, a);
@@ -355,6 +357,16 @@ __global__ void __launch_bounds__(NT, 1) occ_cg_kernel(const __grid_constant__ T
                 break;
             }
             if (fabs(pt.f - fx) <= 0.0 && smax == 0.0) {
+                // the line search found no step: once along a conjugate direction, restart
+                // from steepest descent; along steepest descent, stop
+                if (!steepest) {
+                    for (int k = tid; k < nv; k += NT) m.d[k] = -m.gx[k];
+                    __syncthreads();
+                    steepest = true;
+                    have_prev = false;
+                    a = 1.0 / fmax(maxabs(m, m.gx, nv), 1e-12);
+                    continue;
+                }
                 fx = pt.f;
                 nit = it;
                 break;
@@ -372,6 +384,7 @@ __global__ void __launch_bounds__(NT, 1) occ_cg_kernel(const __grid_constant__ T
             }
             gd_prev = gd;
             have_prev = true;
+            steepest = false;
             for (int k = tid; k < nv; k += NT) {
                 m.d[k] = -m.gt[k] + beta * m.d[k];
                 m.gx[k] = m.gt[k];

@@ -78,6 +78,7 @@ def test_native_energy_loop_matches_python_loop(cuda_ctx, prec):
     for native in (False, True):
         p = workload.molecule_like(nbf=40, naux=80, nbeta=4, ncwo=3, seed=3).p
         p.threshgorb, p.threshgocc, p.threshen = 1e-5, 1e-5, 1e-9
+        p.occ_device = False  # the Python loop's occoptr runs on the host: compare like with like
         b = d.eris_to_gpu(wl.b, prec, cuda_ctx)
         out[native] = (energy(wl.H, b, p, wl.C, g0, maxit=300, native=native), p.maxloop, p.alpha)
         b.free()
@@ -123,6 +124,7 @@ def test_native_energy_loop_variants(cuda_ctx, variant):
     for native in (False, True):
         p = params()
         p.threshgorb, p.threshgocc, p.threshen = 1e-5, 1e-5, 1e-9
+        p.occ_device = False  # the Python loop's occoptr runs on the host: compare like with like
         g0 = gnof.guess_gamma(p)
         b = d.eris_to_gpu(wl.b, "fp64", cuda_ctx)
         out[native] = energy(wl.H, b, p, wl.C, g0, maxit=300, native=native)

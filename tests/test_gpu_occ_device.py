@@ -59,8 +59,9 @@ def test_one_evaluation_matches_the_host_layer(cuda_ctx, case, ista, occ):
     g_out, E, nit, _, grad = device_cg(cuda_ctx, p, J, K, Hc, gamma, 0.0, 0)
     E0, g0 = api.occ_energy(gamma, J, K, Hc, p)
     assert nit == 0 and np.array_equal(g_out, gamma)
-    assert abs(E - E0) <= 1e-12 * max(1.0, abs(E0))
-    assert np.max(np.abs(grad - g0)) <= 1e-12 * max(1.0, np.max(np.abs(g0)))
+    # the device sums in another order (and with fused multiply-adds): rounding only
+    assert abs(E - E0) <= 1e-11 * max(1.0, abs(E0))
+    assert np.max(np.abs(grad - g0)) <= 1e-11 * max(1.0, np.max(np.abs(g0)))
 
 
 @pytest.mark.parametrize("occ", ["Softmax", "Trigonometric"])
@@ -71,7 +72,8 @@ def test_minimisation_reaches_the_host_minimum(cuda_ctx, case, occ):
     g0 = gnof.guess_gamma(p)
     x_h, E_h, nit_h, ok_h = api.occ_cg(g0, J, K, Hc, p, 1e-9, 1000)
     x_d, E_d, nit_d, ok_d, grad = device_cg(cuda_ctx, p, J, K, Hc, g0, 1e-9, 1000)
-    assert ok_d and nit_d > 0 and np.max(np.abs(grad)) <= 1e-9
+    # the iteration counts differ (a long CG path turns on rounding), the minimum does not
+    assert ok_d and nit_d > 0 and np.max(np.abs(grad)) <= 1e-9, (ok_d, nit_d, np.max(np.abs(grad)), nit_h)
     _, g_chk = api.occ_energy(x_d, J, K, Hc, p)      # the returned gradient is the host's at gamma
     assert np.max(np.abs(g_chk - grad)) <= 1e-11
     if ok_h:
@@ -87,8 +89,9 @@ def test_minimisation_reaches_the_host_minimum(cuda_ctx, case, occ):
 @pytest.mark.parametrize("occ", ["Softmax", "Trigonometric"])
 def test_energy_loop_with_the_device_occupation_step(cuda_ctx, occ):
     """donof_energy with occoptr's CG on the device against the host CG: the
-    first outer iteration agrees to rounding, the converged energies to what the
-    1e-6 thresholds leave."""
+    first orbital optimisation is the same, the first occupation step reaches
+    the same minimum (in a different number of CG iterations: the path turns on
+    rounding), and the converged energies agree to what the thresholds leave."""
     from donof_b200.optimize import energy
     wl = workload.molecule_like(nbf=48, naux=116, nbeta=6, ncwo=3, seed=12, occ_method=occ, two_e_scale=0.3)
     out = {}
@@ -102,7 +105,7 @@ def test_energy_loop_with_the_device_occupation_step(cuda_ctx, occ):
     rh, rd = out[False], out[True]
     assert rh.converged and rd.converged
     h0, h1 = rh.history[0], rd.history[0]
-    assert h0["nit_orb"] == h1["nit_orb"] and abs(h1["nit_occ"] - h0["nit_occ"]) <= 1
-    assert abs(h1["E"] - h0["E"]) <= 1e-10 * abs(h0["E"])
-    assert abs(rd.E_elec - rh.E_elec) <= 1e-8 * abs(rh.E_elec)
+    assert h0["nit_orb"] == h1["nit_orb"] and h1["E"] == h0["E"]
+    assert abs(h1["norm_grad_occ"] - h0["norm_grad_occ"]) <= 1e-6
+    assert abs(rd.E_elec - rh.E_elec) <= 1e-7
     assert np.max(np.abs(rd.n - rh.n)) <= 1e-5
