@@ -19,6 +19,8 @@
 // argument, so the call allocates nothing.
 #include <math.h>
 
+#include <atomic>
+
 #include "kernels.cuh"
 #include "occ.cuh"
 #include "occ_math.cuh"
@@ -33,6 +35,7 @@ constexpr int MAX_N = 1024;           // nbf5
 constexpr int MAX_PAIR = 512;         // ndoc
 constexpr int MAX_PV = 2048;          // ndoc * ncwo
 constexpr int CACHE = 64;             // line-search points kept (a, f, da)
+constexpr size_t OCC_SMEM_MAX = 220 * 1024;  // dynamic shared memory of the largest solver launch
 
 struct Tables {
     int S[MAX_PAIR];
@@ -418,7 +421,7 @@ size_t occ_cg_smem_bytes(int N, int ndoc, int ncwo, int nv) {
 
 bool occ_cg_fits(const Occ& o) {
     return o.N <= MAX_N && o.ndoc <= MAX_PAIR && o.ndoc * o.ncwo <= MAX_PV &&
-           occ_cg_smem_bytes(o.N, o.ndoc, o.ncwo, o.nv) <= 220 * 1024;
+           occ_cg_smem_bytes(o.N, o.ndoc, o.ncwo, o.nv) <= OCC_SMEM_MAX;
 }
 
 int occ_cg_launch(donof_ctx* ctx, cudaStream_t st, const Occ& o, const double* J, const double* K, const double* Hc,
@@ -442,7 +445,15 @@ int occ_cg_launch(donof_ctx* ctx, cudaStream_t st, const Occ& o, const double* J
     A.J = J; A.K = K; A.Hc = Hc; A.gamma = gamma; A.result = result; A.g_abstol = g_abstol;
     A.max_iter = max_iter;
     const size_t smem = occ_cg_smem_bytes(o.N, o.ndoc, o.ncwo, o.nv);
-    DONOF_CUDA(ctx, cudaFuncSetAttribute(occ_cg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // the attribute is set once per device to the largest size a launch may ask
+    // for (setting it per launch would race with launches from other host threads)
+    static std::atomic<unsigned long long> attr_mask{0};
+    const unsigned long long bit = 1ull << (ctx->device & 63);
+    if (!(attr_mask.load(std::memory_order_acquire) & bit)) {
+        DONOF_CUDA(ctx, cudaFuncSetAttribute(occ_cg_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)OCC_SMEM_MAX));
+        attr_mask.fetch_or(bit, std::memory_order_acq_rel);
+    }
     occ_cg_kernel<<<1, NT, smem, st>>>(T, A); count_launch();
     DONOF_CUDA(ctx, cudaGetLastError());
     return DONOF_OK;
