@@ -392,11 +392,11 @@ def serving_bench(d, torch):
         b.free()
     ctx.close()
 
-    def run(precision, inflight, group_max=0):
+    def run(precision, inflight, group_max=0, rate_scale=1.0):
         with Server(max_inflight=inflight, group_max=group_max) as srv:
             t0 = time.perf_counter()
             tickets = []
-            for wl, t_arr in zip(jobs, arrivals):
+            for wl, t_arr in zip(jobs, arrivals * rate_scale):
                 delay = t0 + t_arr - time.perf_counter()
                 if delay > 0:
                     time.sleep(delay)
@@ -412,6 +412,12 @@ def serving_bench(d, torch):
     ref, seq = run("fp64", 1)
     res, served = run("auto", SERVE["inflight"])
     res_g, served_g = run("auto", SERVE["inflight"], group_max=SERVE["group_max"])
+    # the arrival rate swept: the same stream twice as fast, and all requests at once
+    sweep = [{"rate_per_s": SERVE["rate_per_s"], "value": served["value"], "latency_s": served["latency_s"]}]
+    for scale, label in ((0.5, 2 * SERVE["rate_per_s"]), (0.0, "all at t=0")):
+        _, sv = run("auto", SERVE["inflight"], rate_scale=scale)
+        sweep.append({"rate_per_s": label, "value": sv["value"], "latency_s": sv["latency_s"],
+                      "speedup_vs_fp64_one_at_a_time": sv["value"] / seq["value"]})
     dE = np.array([abs(a.E_elec - b.E_elec) for a, b in zip(res, ref)])
     dE_g = np.array([abs(a.E_elec - b.E_elec) for a, b in zip(res_g, ref)])
     return {"unit": "energies/s",
@@ -427,6 +433,7 @@ def serving_bench(d, torch):
                                        "grouped batch (donof_batch_energy)",
                                "abs_dE_Eh_vs_fp64": {"max": float(dE_g.max()), "median": float(np.median(dE_g)),
                                                      "within_1uEh": int(np.sum(dE_g <= 1e-6))}},
+            "served_rate_sweep": sweep,
             "fp64_one_at_a_time": seq,
             "speedup": served["value"] / seq["value"],
             "speedup_grouped": served_g["value"] / seq["value"],

@@ -29,7 +29,7 @@ namespace donof {
 namespace occ {
 namespace {
 
-constexpr int NT = 512;               // threads of the solver's CTA
+constexpr int NT = 256;               // threads of the solver's CTA
 constexpr int NW = NT / 32;
 constexpr int MAX_N = 1024;           // nbf5
 constexpr int MAX_PAIR = 512;         // ndoc
@@ -57,76 +57,87 @@ struct Smem {
     OccView o;
     double *n, *fi, *nd12, *nd, *w, *F, *coc, *blk, *x, *d, *gx, *gt, *xa;
     RowSums* rs;
-    double* red;    // NW partial sums
-    double* bcast;  // broadcast slot
+    double* red;    // 2 x NW x 3 per-warp partials (two buffers, used in turn)
     double *ca, *cf, *cd;  // line-search cache
     int* ncache;
+    int rbuf;       // the red buffer of the next reduction (the same in every thread)
 };
 
-__device__ __forceinline__ double warp_sum(double v) {
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    return v;  // valid in lane 0
+// Butterfly sum over a warp: every lane ends with the same value (each step
+// adds two values that are each other's mirror, and a + b == b + a).
+__device__ __forceinline__ double warp_allsum(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ double warp_allmax(double v) {
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
 }
 
-// Sum over the CTA in a fixed order, returned to every thread.
-__device__ double block_sum(const Smem& m, double v) {
-    v = warp_sum(v);
+// Sums (or maxima) of up to three values over the CTA with one barrier: each
+// warp's partials go to the current buffer, and every thread adds the warps'
+// partials in the same order, so every thread gets the same result.  The two
+// buffers alternate, so a buffer is written again only after the barrier of
+// the next reduction, by which time every thread has read it.
+template <int NVAL, bool MAX>
+__device__ __forceinline__ void block_reduce(Smem& m, double (&v)[NVAL]) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (lane == 0) m.red[warp] = v;
+    double* buf = m.red + m.rbuf * (NW * 3);
+#pragma unroll
+    for (int k = 0; k < NVAL; ++k) v[k] = MAX ? warp_allmax(v[k]) : warp_allsum(v[k]);
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < NVAL; ++k) buf[warp * 3 + k] = v[k];
     __syncthreads();
-    if (threadIdx.x == 0) {
-        double t = 0.0;
-        for (int i = 0; i < NW; ++i) t += m.red[i];
-        *m.bcast = t;
+#pragma unroll
+    for (int k = 0; k < NVAL; ++k) {
+        double t = MAX ? buf[k] : 0.0;
+        for (int i = MAX ? 1 : 0; i < NW; ++i) t = MAX ? fmax(t, buf[i * 3 + k]) : t + buf[i * 3 + k];
+        v[k] = t;
     }
-    __syncthreads();
-    const double r = *m.bcast;
-    __syncthreads();
-    return r;
+    m.rbuf ^= 1;
 }
 
-__device__ double block_max(const Smem& m, double v) {
-    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (lane == 0) m.red[warp] = v;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double t = 0.0;
-        for (int i = 0; i < NW; ++i) t = fmax(t, m.red[i]);
-        *m.bcast = t;
-    }
-    __syncthreads();
-    const double r = *m.bcast;
-    __syncthreads();
-    return r;
+__device__ __forceinline__ double block_sum(Smem& m, double v) {
+    double a[1] = {v};
+    block_reduce<1, false>(m, a);
+    return a[0];
 }
 
-__device__ double dot(const Smem& m, const double* a, const double* b, int nv) {
+__device__ __forceinline__ double block_max(Smem& m, double v) {
+    double a[1] = {v};
+    block_reduce<1, true>(m, a);
+    return a[0];
+}
+
+__device__ double dot(Smem& m, const double* a, const double* b, int nv) {
     double s = 0.0;
     for (int k = threadIdx.x; k < nv; k += NT) s += a[k] * b[k];
     return block_sum(m, s);
 }
 
-__device__ double maxabs(const Smem& m, const double* a, int nv) {
+__device__ double maxabs(Smem& m, const double* a, int nv) {
     double s = 0.0;
     for (int k = threadIdx.x; k < nv; k += NT) s = fmax(s, fabs(a[k]));
     return block_max(m, s);
 }
 
 // Occupation energy at gamma = xa and, with g != nullptr, its gradient (every thread gets E).
-__device__ double eval(const CgArgs& A, const Smem& m, const double* xa, double* g) {
+__device__ double eval(const CgArgs& A, Smem& m, const double* xa, double* g) {
     const OccView& o = m.o;
     const int N = o.N, nc = o.ncwo, nd = o.ndoc, tid = threadIdx.x;
     const double *J = A.J, *K = A.K;
-    // occupations: fixed entries, then each pair (pass 1), then the dn blocks and n_d (pass 2)
+    // occupations: orbitals outside the pairs, then each pair (pass 1); the dn
+    // blocks and n_d (pass 2, which reads n of every pair)
     for (int i = tid; i < N; i += NT) {
-        double v = 0.0;
-        if (i < o.no1) v = 1.0;
-        else if (i >= o.no1 + nd && i < o.no1 + nd + o.nsoc) v = o.high_spin ? 1.0 : 0.5;
-        m.n[i] = v;
-        m.nd[i] = 0.0;
+        if (o.grp[i] < 0) {
+            double v = 0.0;
+            if (i < o.no1) v = 1.0;
+            else if (i >= o.no1 + nd && i < o.no1 + nd + o.nsoc) v = o.high_spin ? 1.0 : 0.5;
+            m.n[i] = v;
+            m.nd[i] = 0.0;
+        }
     }
-    __syncthreads();
     for (int gi = tid; gi < nd; gi += NT) pair_n(o, xa, gi, m.n);
     __syncthreads();
     for (int gi = tid; gi < nd; gi += NT) {
@@ -134,70 +145,53 @@ __device__ double eval(const CgArgs& A, const Smem& m, const double* xa, double*
         pair_dynamic(o, m.n, gi, m.nd, m.F, m.coc);
     }
     __syncthreads();
-    double e = 0.0;
+    double part[3] = {0.0, 0.0, 0.0};  // linear terms, sum of the J rows, sum of the K rows
     for (int i = tid; i < N; i += NT) {
         m.fi[i] = phi_fn(m.n[i], o.ista);
         m.nd12[i] = sqrt(m.nd[i]);
         const double wi = 2.0 * A.Hc[i] + J[i + (size_t)N * i];
         m.w[i] = wi;
-        if (i < o.nbeta || i >= o.nalpha) e += m.n[i] * wi;
-        else e += 2.0 * m.n[i] * A.Hc[i];
+        if (i < o.nbeta || i >= o.nalpha) part[0] += m.n[i] * wi;
+        else part[0] += 2.0 * m.n[i] * A.Hc[i];
     }
     __syncthreads();
-    // class-range row sums, one warp per orbital
+    // class-range row sums and the row's energy terms, one thread per orbital
+    const VecView vv{m.n, m.fi, m.nd12, m.nd, m.F, m.coc};
     {
-        const int lane = tid & 31, warp = tid >> 5;
-        const int b1 = o.no1, b2 = o.nbeta, b3 = o.nalpha;
-        for (int i = warp; i < N; i += NW) {
-            double acc[4][NVEC], jn = 0.0;
-#pragma unroll
-            for (int R = 0; R < 4; ++R)
-#pragma unroll
-                for (int k = 0; k < NVEC; ++k) acc[R][k] = 0.0;
+        const int bnd[5] = {0, o.no1, o.nbeta, o.nalpha, N};
+        for (int i = tid; i < N; i += NT) {
             const double* Kc = K + (size_t)N * i;
             const double* Jc = J + (size_t)N * i;
-            for (int j = lane; j < N; j += 32) {
-                const double kj = Kc[j];
-                const double nj = m.n[j];
-                const int R = j < b1 ? 0 : (j < b2 ? 1 : (j < b3 ? 2 : 3));
-                const double vals[NVEC] = {nj * kj, m.fi[j] * kj, m.nd12[j] * kj, m.nd[j] * kj, kj};
-#pragma unroll
-                for (int RR = 0; RR < 4; ++RR)
-                    if (RR == R)
-#pragma unroll
-                        for (int k = 0; k < NVEC; ++k) acc[RR][k] += vals[k];
-                jn += nj * Jc[j];
+            RowSums& r = m.rs[i];
+            for (int R = 0; R < 4; ++R) {
+                double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0, a4 = 0.0;
+                for (int j = bnd[R]; j < bnd[R + 1]; ++j) {
+                    const double kj = Kc[j];
+                    a0 += m.n[j] * kj;
+                    a1 += m.fi[j] * kj;
+                    a2 += m.nd12[j] * kj;
+                    a3 += m.nd[j] * kj;
+                    a4 += kj;
+                }
+                r.S[R][V_N] = a0; r.S[R][V_FI] = a1; r.S[R][V_ND12] = a2; r.S[R][V_ND] = a3; r.S[R][V_ONE] = a4;
             }
-#pragma unroll
-            for (int R = 0; R < 4; ++R)
-#pragma unroll
-                for (int k = 0; k < NVEC; ++k) acc[R][k] = warp_sum(acc[R][k]);
-            jn = warp_sum(jn);
-            if (lane == 0) {
-                RowSums& r = m.rs[i];
-#pragma unroll
-                for (int R = 0; R < 4; ++R)
-#pragma unroll
-                    for (int k = 0; k < NVEC; ++k) r.S[R][k] = acc[R][k];
-                r.jn = jn;
-            }
+            double jn = 0.0;
+            for (int j = 0; j < N; ++j) jn += m.n[j] * Jc[j];
+            r.jn = jn;
+            double rj, rk;
+            row_energy(o, vv, i, r, J, K, &rj, &rk);
+            part[1] += rj;
+            part[2] += rk;
         }
     }
-    __syncthreads();
-    const VecView vv{m.n, m.fi, m.nd12, m.nd, m.F, m.coc};
-    double sj = 0.0, sk = 0.0;
-    for (int i = tid; i < N; i += NT) {
-        double rj, rk;
-        row_energy(o, vv, i, m.rs[i], J, K, &rj, &rk);
-        sj += rj;
-        sk += rk;
-    }
-    const double E = block_sum(m, e) + (block_sum(m, sj) - block_sum(m, sk));
+    block_reduce<3, false>(m, part);  // its barrier also publishes every row's sums
+    const double E = part[0] + (part[1] - part[2]);
     if (g != nullptr) {
-        for (int k = tid; k < o.nv; k += NT) g[k] = 0.0;
-        __syncthreads();
-        for (int gi = tid; gi < nd; gi += NT)
+        // each gamma entry belongs to exactly one pair: the pair's thread sets it
+        for (int gi = tid; gi < nd; gi += NT) {
+            for (int c = 0; c < nc; ++c) g[o.KG[gi * nc + c]] = 0.0;
             pair_grad(o, vv, m.rs, J, K, m.w, m.blk + (size_t)gi * (nc + 1) * nc, gi, g);
+        }
         __syncthreads();
     }
     return E;
@@ -210,7 +204,7 @@ struct Pt {
 // phi(a) = E(x + a d) with its gradient in m.gt (every call evaluates, so the
 // point returned by the line search is always the last one evaluated and m.gt
 // holds its gradient); the scalars are also kept for phi_f.
-__device__ Pt phi(const CgArgs& A, const Smem& m, double a) {
+__device__ Pt phi(const CgArgs& A, Smem& m, double a) {
     const int nv = m.o.nv;
     for (int k = threadIdx.x; k < nv; k += NT) m.xa[k] = m.x[k] + a * m.d[k];
     __syncthreads();
@@ -229,7 +223,7 @@ __device__ Pt phi(const CgArgs& A, const Smem& m, double a) {
 }
 
 // E(x + a d) only: from the points of this line search when a was evaluated
-__device__ double phi_f(const CgArgs& A, const Smem& m, double a) {
+__device__ double phi_f(const CgArgs& A, Smem& m, double a) {
     const int nc = *m.ncache;
     for (int i = 0; i < nc; ++i)
         if (m.ca[i] == a) return m.cf[i];
@@ -241,7 +235,7 @@ __device__ bool decrease_ok(double fa, double da, double a, double f0, double d0
     return fa <= f0 + 1e-6 * fabs(f0) && da <= (2 * 0.1 - 1.0) * d0;
 }
 
-__device__ Pt zoom(const CgArgs& A, const Smem& m, double a_lo, double a_hi, double f_lo, double d_lo, double f0,
+__device__ Pt zoom(const CgArgs& A, Smem& m, double a_lo, double a_hi, double f_lo, double d_lo, double f0,
                    double d0, double c1, double c2) {
     double f_hi = phi_f(A, m, a_hi);
     for (int it = 0; it < 30; ++it) {
@@ -267,7 +261,7 @@ __device__ Pt zoom(const CgArgs& A, const Smem& m, double a_lo, double a_hi, dou
     return phi(A, m, a_lo);
 }
 
-__device__ Pt wolfe(const CgArgs& A, const Smem& m, double fx, double d0, double a1) {
+__device__ Pt wolfe(const CgArgs& A, Smem& m, double fx, double d0, double a1) {
     const double c1 = 1e-4, c2 = 0.1, a_max = 1e6;
     if (threadIdx.x == 0) *m.ncache = 0;
     __syncthreads();
@@ -300,7 +294,8 @@ __global__ void __launch_bounds__(NT, 1) occ_cg_kernel(const __grid_constant__ T
     m.blk = take((size_t)nd * (nc + 1) * nc);
     m.x = take(nv); m.d = take(nv); m.gx = take(nv); m.gt = take(nv); m.xa = take(nv);
     m.rs = reinterpret_cast<RowSums*>(take((size_t)N * sizeof(RowSums) / sizeof(double)));
-    m.red = take(NW); m.bcast = take(2);
+    m.red = take(2 * NW * 3);
+    m.rbuf = 0;
     m.ca = take(CACHE); m.cf = take(CACHE); m.cd = take(CACHE);
     m.ncache = reinterpret_cast<int*>(take(2));
     int* tab = reinterpret_cast<int*>(p);
@@ -414,7 +409,7 @@ __global__ void __launch_bounds__(NT, 1) occ_cg_kernel(const __grid_constant__ T
 size_t occ_cg_smem_bytes(int N, int ndoc, int ncwo, int nv) {
     auto r2 = [](size_t c) { return (c + 1) & ~size_t(1); };
     size_t d = 5 * r2(N) + 2 * r2(ndoc) + r2((size_t)ndoc * (ncwo + 1) * ncwo) + 5 * r2(nv) +
-               r2((size_t)N * sizeof(RowSums) / sizeof(double)) + r2(NW) + r2(2) + 3 * r2(CACHE) + r2(2);
+               r2((size_t)N * sizeof(RowSums) / sizeof(double)) + r2(2 * NW * 3) + 3 * r2(CACHE) + r2(2);
     const size_t ints = (size_t)ndoc + 3 * (size_t)ndoc * ncwo + N;
     return d * sizeof(double) + ints * sizeof(int);
 }
