@@ -398,7 +398,7 @@ class Batch:
             prm.maxit, prm.maxloop, prm.alpha = int(maxit or p.maxit), int(p.maxloop), float(p.alpha)
             prm.threshgorb, prm.threshgocc, prm.threshen = float(p.threshgorb), float(p.threshgocc), float(p.threshen)
             prm.order_subspaces = int(bool(order) and p.ipnof > 4)
-            prm.occ_device = int(bool(getattr(p, "occ_device", True)))
+            prm.occ_device = int(bool(getattr(p, "occ_device", False)))
         Hf = [_f64(H) for H in Hs]
         Cio = [np.array(_f64(C), copy=True, order="F") for C in Cs]
         gio = [np.array(g, dtype=np.float64, copy=True) for g in gammas]
@@ -502,7 +502,7 @@ def energy_loop(H, b: BTensor, p: Param, C, gamma, maxit: Optional[int] = None, 
     prm = _EnergyParams(_occ_params(p), _lib.ORB_METHODS[p.orb_method], maxit, int(p.maxloop), float(p.alpha),
                         float(p.threshgorb), float(p.threshgocc), float(p.threshen),
                         int(bool(order) and p.ipnof > 4), int(bool(freeze_occ)), float(stop_rel_de),
-                        int(bool(getattr(p, "occ_device", True))))
+                        int(bool(getattr(p, "occ_device", False))))
     Cio = np.array(_f64(C), copy=True, order="F")
     g = np.array(gamma, dtype=np.float64, copy=True)
     n = np.zeros(p.nbf5)

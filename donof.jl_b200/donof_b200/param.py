@@ -32,7 +32,9 @@ class Param:
     h_cut: float = 0.02 * math.sqrt(2.0)
     title: str = "donof"
     RI: bool = True
-    occ_device: bool = True   # occoptr's conjugate gradient on the GPU (False: on the host, like the reference)
+    # occoptr's conjugate gradient on the GPU (one CTA) instead of the host: measured
+    # slower than the host solver at nbf5 = 20-198, so off by default
+    occ_device: bool = False
     extra: dict = field(default_factory=dict)
 
     def __post_init__(self):

@@ -457,7 +457,7 @@ class NativeServer:
         prm = api._EnergyParams(api._occ_params(p), _lib.ORB_METHODS[p.orb_method], int(req.maxit or p.maxit),
                                 int(p.maxloop), float(p.alpha), float(p.threshgorb), float(p.threshgocc),
                                 float(p.threshen), int(p.ipnof > 4), 0, 0.0,
-                                int(bool(getattr(p, "occ_device", True))))
+                                int(bool(getattr(p, "occ_device", False))))
         prec = {"fp64": 0, "mixed": 1, "mixed_refined": 1, "auto": 2}[req.precision]
         r = _NativeRequest(H.ctypes.data, b.ctypes.data, C.ctypes.data, gamma.ctypes.data, p.nbf, p.nbfaux, prm,
                            prec, float(req.E_nuc))

@@ -218,7 +218,7 @@ struct EnergyResult
 end
 
 """EnergyParams of DoNOF's Param `p` (the names of src/param.jl)."""
-energy_params(p; freeze_occ::Bool = false, stop_rel_de::Real = 0.0, occ_device::Bool = true) =
+energy_params(p; freeze_occ::Bool = false, stop_rel_de::Real = 0.0, occ_device::Bool = false) =
     EnergyParams(OccParams(p.nbf5, p.no1, p.nbeta, p.nalpha, p.ncwo, p.ista, p.HighSpin,
                            p.occ_method == "Softmax" ? 0 : 1, p.h_cut),
                  ORB_METHODS[p.orb_method], p.maxit, p.maxloop, p.alpha, p.threshgorb, p.threshgocc,
