@@ -71,6 +71,9 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--method", default="ADAM")
+    ap.add_argument("--no-fp64-tc", action="store_true",
+                    help="FP64 form with its first contraction on the DMMA GEMM instead of the tensor cores "
+                         "(int8 digit slices, exact integer products)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-energies", action="store_true")
@@ -89,6 +92,8 @@ def config(args, world):
     return {"workload": "synthetic-256 GNOF orbital step (nbf=256, naux=1024, nbf5=64)",
             "nbf": WORKLOAD["nbf"], "naux": WORKLOAD["naux"], "nbf5": 64, "ndoc": 16, "ncwo": 3,
             "orb_method": args.method, "precision": args.precision,
+            "fp64_t1": ("DMMA GEMM" if getattr(args, "no_fp64_tc", False) else
+                        "tensor cores: 7 int8 digit slices of b and C5, exact int32 products, FP64 recombination"),
             "parallelism": f"replicas x{world}", "l2": "inputs > L2 (b = 512 MiB FP64)"}
 
 
@@ -570,7 +575,8 @@ def batched_energies_bench(d, torch, ctx):
 
 
 def profile_case(d, torch, wl, ctx):
-    """Three calls each of the mixed and FP64 Lagrangian and of the rotation."""
+    """Three calls each of the mixed and FP64 Lagrangian and of the rotation, then
+    three of the FP64 Lagrangian with its first contraction on the tensor cores."""
     import numpy as np
     p = wl.p
     bt = d.eris_to_gpu(wl.b, "mixed", ctx)
@@ -584,6 +590,9 @@ def profile_case(d, torch, wl, ctx):
         d.compute_Lagrange2_dev(tC, tn, tH, bt, tcj, tck, p.nalpha, p.nbeta, el, hm, E, precision="mixed")
         d.compute_Lagrange2_dev(tC, tn, tH, bt, tcj, tck, p.nalpha, p.nbeta, el, hm, E, precision="fp64")
         d.rotate_orbital_dev(y, tC, Cn, p.nbf, p.nbf5, ctx)
+    bt.set_fp64_tc(True)
+    for _ in range(3):
+        d.compute_Lagrange2_dev(tC, tn, tH, bt, tcj, tck, p.nalpha, p.nbeta, el, hm, E, precision="fp64")
     torch.cuda.synchronize()
     bt.free()
 
@@ -632,6 +641,8 @@ def main():
         return
     bt = d.eris_to_gpu(wl.b, "mixed", ctx)   # FP64 b and its bf16 split: both forms are timed
     bt.set_precision(args.precision)
+    if not args.no_fp64_tc:
+        bt.set_fp64_tc(True)                  # and b's int8 digit slices for the FP64 form's T1
     tC0, tH, tn, tcj, tck = (d.to_device(x, dev) for x in (wl.C, wl.H, wl.n, wl.cj12, wl.ck12))
 
     def barrier():
@@ -679,6 +690,27 @@ def main():
     bt.set_precision(args.precision)
     tC.copy_(tC0)
 
+    # ---- the FP64 form with its first contraction on the DMMA GEMM (same step count)
+    fp64_gemm = None
+    if bt.fp64_tc:
+        bt.set_fp64_tc(False)
+        bt.set_precision("fp64")
+        d.orbopt_dev(args.method, tn, tcj, tck, tH, tC, bt, p, 0.01, args.warmup, 0.0)
+        tC.copy_(tC0)
+        torch.cuda.synchronize()
+        barrier()
+        ev0.record()
+        E3, nit3, _, _, _ = d.orbopt_dev(args.method, tn, tcj, tck, tH, tC, bt, p, 0.01, args.steps, 0.0)
+        ev1.record()
+        torch.cuda.synchronize()
+        t3 = max_over_ranks(ev0.elapsed_time(ev1) / 1e3, dist, dev)
+        fp64_gemm = {"value": world * nit3 / t3, "unit": UNIT, "ms_per_step": 1e3 * t3 / nit3,
+                     "t1": "DMMA GEMM (mma.sync f64)", "final_E": E3,
+                     "abs_dE_vs_tensor_cores": abs(E3 - E)}
+        bt.set_fp64_tc(True)
+        bt.set_precision(args.precision)
+        tC.copy_(tC0)
+
     # ---- roofline of the dominant kernel, timed by the library's events on the launching stream
     nbf, naux, nbf5 = p.nbf, p.nbfaux, p.nbf5
     lib = ctx.lib
@@ -696,7 +728,20 @@ def main():
     ctx.check(lib.donof_profile_enable(ctx.handle, 0))
     tr = statistics.mean(durs)
     peaks = load_peaks()
-    if args.precision == "fp64":
+    if args.precision == "fp64" and bt.fp64_tc:
+        ldn = (nbf + 15) // 16 * 16
+        byts = 7.0 * nbf * ldn * naux + 8.0 * nbf * nbf5 * naux
+        macs = 28.0 * nbf * nbf * nbf5 * naux
+        roof = {"bound": "hbm", "achieved": byts / tr / 1e9, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": byts / tr / 1e9 / peaks["hbm_gbs"], "traffic": traffic_from_profiles("t1_oz"),
+                "kernel": "ozaki_t1_kernel (T1 tmp_l = b_l C5 on tcgen05 kind::i8: 28 digit products, "
+                          "int32 TMEM accumulators, FP64 recombination)",
+                "algorithmic": f"int8 slices of b read once + tmp written = 7*nbf*ldn*naux + 8*nbf*nbf5*naux "
+                               f"= {byts:.4e} bytes per launch",
+                "int8_tops": 2.0 * macs / tr / 1e12, "fp64_equivalent_tflops": 2.0 * nbf * nbf * nbf5 * naux / tr / 1e12,
+                "ms": tr * 1e3,
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs, of measured" + (" (fallback)" if peaks.get("fallback") else "")}
+    elif args.precision == "fp64":
         flops = 2.0 * nbf * nbf * nbf5 * naux
         peak = measured_dgemm_tflops(torch, dev)
         roof = {"bound": "tensor", "achieved": flops / tr / 1e12, "peak": peak, "unit": "TFLOP/s",
@@ -782,7 +827,7 @@ def main():
                 "dtype": "f64" if args.precision == "fp64" else "bf16x2-split+f64", "data": "synthetic",
                 "config": config(args, world), "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": int(launches), "clocks": clk.summary(), "final_E": E,
-                "other_form": other_form}
+                "other_form": other_form, "fp64_dmma_t1": fp64_gemm}
         if energies is not None:
             line["energies"] = energies
         if serving is not None:

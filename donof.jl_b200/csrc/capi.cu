@@ -328,6 +328,29 @@ int donof_mixed_tmp_dev(donof_job* job, const double* C, int nbf5, float* tmp) {
     return mixed_t1_debug(job, job->ctx->stream, C, nbf5, tmp);
 }
 
+int donof_job_set_fp64_tc(donof_job* job, int enable) {
+    if (!job) return DONOF_ERR_ARG;
+    DONOF_CHECK(use_device(job->ctx));
+    if (enable) return ozaki_build(job);
+    ozaki_free(job);
+    return DONOF_OK;
+}
+
+int donof_job_fp64_tc(const donof_job* job) { return job && job->oz_b ? 1 : 0; }
+
+int donof_t1_dev(donof_job* job, const double* C, int nbf5, double* tmp) {
+    if (!job) return DONOF_ERR_ARG;
+    donof_ctx* ctx = job->ctx;
+    REQUIRE(ctx, C != nullptr && tmp != nullptr, "null pointer");
+    REQUIRE(ctx, nbf5 > 0 && nbf5 <= job->nbf, "invalid nbf5");
+    DONOF_CHECK(use_device(ctx));
+    if (job->oz_b) return t1_ozaki(job, ctx->stream, C, nbf5, tmp);
+    DONOF_CHECK(transforms_f64(job, ctx->stream, C, nbf5));
+    DONOF_CUDA(ctx, cudaMemcpyAsync(tmp, job->tmp.ptr, sizeof(double) * (size_t)job->nbf * nbf5 * job->naux,
+                                    cudaMemcpyDeviceToDevice, ctx->stream));
+    return DONOF_OK;
+}
+
 int donof_transform_dev(donof_job* job, int precision, const double* C, int nbf5, double* b_pq) {
     if (!job) return DONOF_ERR_ARG;
     donof_ctx* ctx = job->ctx;
@@ -594,6 +617,7 @@ int donof_job_free(donof_job* job) {
     if (job->own_b) dev_free(ctx, job->b);
     dev_free(ctx, job->b16hi);
     dev_free(ctx, job->b16lo);
+    ozaki_free(job);
     job->tmp.release(ctx);
     job->bpq.release(ctx);
     job->W.release(ctx);
@@ -622,6 +646,7 @@ size_t donof_job_device_bytes(const donof_job* job) {
                job->orb.bytes + job->io.bytes;
     if (job->own_b) s += sizeof(double) * (size_t)job->nbf * job->nbf * job->naux;
     if (job->b16hi) s += 4 * (size_t)64 * ((job->nbf + 63) / 64) * job->nbf * job->naux;
+    if (job->oz_b) s += ozaki_bytes(job->nbf, job->naux) + job->oz_c.bytes;
     return s;
 }
 

@@ -130,6 +130,13 @@ struct donof_job {
     // layout [mi + 64*n + 64*nbf*qb + 64*nbf*nb*l] with m = 64*qb + mi, nb = ceil(nbf/64)
     void* b16hi = nullptr;
     void* b16lo = nullptr;
+    // int8 digit slices of b for the FP64 form's T1 on the tensor cores
+    // (ozaki.cu): oz_b[n + ldn*(m + nbf*(i + S*l))] with row scales oz_sa[m + nbf*l];
+    // oz_c holds the per-call slices of C5; oz_gen counts enable/disable switches
+    void* oz_b = nullptr;
+    double* oz_sa = nullptr;
+    donof::DevBuf oz_c;
+    unsigned oz_gen = 0;
     // per-call scratch, sized for the largest nbf5 seen
     donof::DevBuf tmp, bpq, W, part, small;
     // device-resident orbital-optimiser state

@@ -3,6 +3,8 @@
 
 #include <atomic>
 
+#include <cuda.h>
+
 #include "common.cuh"
 #include "gemm_f64.cuh"
 
@@ -76,6 +78,22 @@ int elag_tail_f64(donof_job* job, cudaStream_t st, const double* C, const double
 // (iaux.cu); part is scratch for the products.
 int iaux_f64(donof_ctx* ctx, cudaStream_t st, const double* G_host, const double* I_host, int nbf, int naux,
              double* b, DevBuf* part);
+
+// FP64-accurate T1 on the tensor cores from int8 digit slices (ozaki.cu):
+// ozaki_build makes the slices of the job's b (once), t1_ozaki computes
+// tmp[m + nbf*q + nbf*nbf5*l] = (B_l C5)[m, q]; transforms_f64 uses it whenever
+// the job holds the slices.
+bool ozaki_shape_ok(int nbf);
+size_t ozaki_bytes(int nbf, int naux);
+int ozaki_build(donof_job* job);
+void ozaki_free(donof_job* job);
+int t1_ozaki(donof_job* job, cudaStream_t st, const double* C, int nbf5, double* tmp);
+
+// Tensor maps with 128-byte swizzle and zero fill (mixed.cu)
+int make_tmap_bf16(donof_ctx* ctx, CUtensorMap* map, const void* base, int rank, const cuuint64_t* dims,
+                   const cuuint64_t* strides_bytes, const cuuint32_t* box);
+int make_tmap_u8(donof_ctx* ctx, CUtensorMap* map, const void* base, int rank, const cuuint64_t* dims,
+                 const cuuint64_t* strides_bytes, const cuuint32_t* box);
 
 // FP64 pipelines (lagrange.cu)
 int transforms_f64(donof_job* job, cudaStream_t st, const double* C, int nbf5);

@@ -123,8 +123,11 @@ int transforms_f64(donof_job* job, cudaStream_t st, const double* C, int nbf5) {
     DONOF_CHECK(job->bpq.ensure(ctx, sizeof(double) * (size_t)nbf5 * nbf5 * naux));
     double* tmp = job->tmp.as<double>();
     double* bpq = job->bpq.as<double>();
-    // T1: tmp_l(m,q) = sum_n b[m,n,l] C[n,q]; A(i=m,k=n) = b[m + nbf*n] (M-contiguous)
-    {
+    // T1: tmp_l(m,q) = sum_n b[m,n,l] C[n,q]; A(i=m,k=n) = b[m + nbf*n] (M-contiguous).
+    // With b's digit slices on the device it runs on the tensor cores (ozaki.cu).
+    if (job->oz_b) {
+        DONOF_CHECK(t1_ozaki(job, st, C, nbf5, tmp));
+    } else {
         GemmF64Args p{};
         p.M = nbf; p.N = nbf5; p.K = nbf;
         p.A = job->b; p.lda = nbf; p.strideA = (long long)nbf * nbf;

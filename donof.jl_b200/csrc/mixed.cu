@@ -603,17 +603,31 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 
 }  // namespace
 
-// bf16 tensor map with 128-byte swizzle and zero fill outside the tensor (no
-// interleave); used by the mixed kernels of this file and mixed_general.cu.
+// Tensor map with 128-byte swizzle and zero fill outside the tensor (no
+// interleave): bf16 for the mixed kernels of this file and mixed_general.cu,
+// 8-bit for the digit slices of ozaki.cu.
+static int make_tmap(donof_ctx* ctx, CUtensorMap* map, CUtensorMapDataType dtype, const void* base, int rank,
+                     const cuuint64_t* dims, const cuuint64_t* strides_bytes, const cuuint32_t* box);
+
 int make_tmap_bf16(donof_ctx* ctx, CUtensorMap* map, const void* base, int rank, const cuuint64_t* dims,
              const cuuint64_t* strides_bytes, const cuuint32_t* box) {
+    return make_tmap(ctx, map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, base, rank, dims, strides_bytes, box);
+}
+
+int make_tmap_u8(donof_ctx* ctx, CUtensorMap* map, const void* base, int rank, const cuuint64_t* dims,
+                 const cuuint64_t* strides_bytes, const cuuint32_t* box) {
+    return make_tmap(ctx, map, CU_TENSOR_MAP_DATA_TYPE_UINT8, base, rank, dims, strides_bytes, box);
+}
+
+static int make_tmap(donof_ctx* ctx, CUtensorMap* map, CUtensorMapDataType dtype, const void* base, int rank,
+                     const cuuint64_t* dims, const cuuint64_t* strides_bytes, const cuuint32_t* box) {
     auto fn = encode_fn();
     if (!fn) {
         set_error(ctx, "cuTensorMapEncodeTiled is not available");
         return DONOF_ERR_CUDA;
     }
     cuuint32_t es[5] = {1, 1, 1, 1, 1};
-    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, rank, const_cast<void*>(base), dims, strides_bytes, box, es,
+    CUresult r = fn(map, dtype, rank, const_cast<void*>(base), dims, strides_bytes, box, es,
                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {

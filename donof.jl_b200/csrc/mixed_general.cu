@@ -44,9 +44,6 @@
 
 namespace donof {
 
-int make_tmap_bf16(donof_ctx* ctx, CUtensorMap* map, const void* base, int rank, const cuuint64_t* dims,
-                   const cuuint64_t* strides_bytes, const cuuint32_t* box);
-
 namespace mg {
 
 using namespace sm100;

@@ -246,7 +246,8 @@ int orbopt_run(donof_job* job, int method, const double* n, const double* cj12, 
     if (*maxloop >= 1) {
         // (re)build the graph when its inputs or any buffer it references changed
         const unsigned long long gens = (unsigned long long)job->tmp.gen + job->bpq.gen + job->W.gen + job->part.gen +
-                                        job->small.gen + job->orb.gen + ctx->rot.gen;
+                                        job->small.gen + job->orb.gen + ctx->rot.gen + job->oz_c.gen +
+                                        ((unsigned long long)job->oz_gen << 32);
         const unsigned long long key[10] = {(unsigned long long)(uintptr_t)n, (unsigned long long)(uintptr_t)cj12,
                                             (unsigned long long)(uintptr_t)ck12, (unsigned long long)(uintptr_t)H,
                                             (unsigned long long)nbf5 | ((unsigned long long)nalpha << 20) |

@@ -1,7 +1,7 @@
 // Device helpers for sm_100a kernels built on TMA, mbarriers and the
 // 5th-generation tensor cores (tcgen05): bounded mbarrier waits, tiled TMA
 // loads (no multicast), UMMA shared-memory and instruction descriptors for
-// bf16 x bf16 -> f32, TMEM loads and the bf16 hi/lo split.
+// bf16 x bf16 -> f32 and s8 x s8 -> s32, TMEM loads and the bf16 hi/lo split.
 //
 // Every wait is bounded (WAIT_CYCLES of SM clock unless the launch gives a
 // smaller budget): a wait that runs out sets the CTA's abort flag, so that the
@@ -122,6 +122,19 @@ __device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t a, uint64_t b, ui
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
         "l"(a), "l"(b), "r"(id), "r"(accum));
 }
+// instruction descriptor: s8 x s8 -> s32 (kind::i8), both operands K-major
+__host__ __device__ constexpr uint32_t idesc_i8(int M, int N) {
+    return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+// D (s32, TMEM) (+)= A (s8) x B (s8): exact integer products and sums
+__device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t id, uint32_t accum) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(a), "l"(b), "r"(id), "r"(accum));
+}
 __device__ __forceinline__ void umma_commit(uint32_t bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
 }
@@ -157,6 +170,23 @@ __device__ __forceinline__ void tmem_issue32(uint32_t taddr, uint32_t (&r)[32]) 
           "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
         : "r"(taddr));
 }
+// Issue a 16-column TMEM load without waiting (valid after tmem_wait_ld()).
+__device__ __forceinline__ void tmem_issue16(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+}
+// Store zeros to 32 TMEM columns of the warp's 32 lanes (valid after tmem_wait_st()).
+__device__ __forceinline__ void tmem_zero32(uint32_t taddr) {
+    const uint32_t z = 0;
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,"
+        "%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1};" ::"r"(taddr), "r"(z)
+        : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 // Byte offset of bf16 element k (0..63) of row r inside a K-major 128B-swizzled

@@ -91,6 +91,9 @@ SIGNATURES = {
     "donof_profile_enable": (_i, [_vp, _i]),
     "donof_profile_last_ms": (_i, [_vp, ct.POINTER(ct.c_float)]),
     "donof_mixed_tmp_dev": (_i, [_vp, _vp, _i, _vp]),
+    "donof_job_set_fp64_tc": (_i, [_vp, _i]),
+    "donof_job_fp64_tc": (_i, [_vp]),
+    "donof_t1_dev": (_i, [_vp, _vp, _i, _vp]),
     "donof_orbopt": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _i, _i, _i, _dp, _ip, ct.c_double, _vp, _dp,
                           _ip, _ip]),
     "donof_batch_create": (_i, [_vp, _i, _vp, ct.POINTER(_vp)]),

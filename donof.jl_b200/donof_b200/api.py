@@ -146,6 +146,16 @@ class BTensor:
         self.ctx.check(self.ctx.lib.donof_job_set_precision(self.handle, prec))
         self.precision = prec
 
+    def set_fp64_tc(self, enable: bool = True) -> None:
+        """Run the FP64 form's first contraction (tmp_l = b_l C5) on the tensor
+        cores from int8 digit slices of b (made now, 7/8 of b's FP64 size), or
+        back on the FP64 GEMM (enable=False frees the slices)."""
+        self.ctx.check(self.ctx.lib.donof_job_set_fp64_tc(self.handle, 1 if enable else 0))
+
+    @property
+    def fp64_tc(self) -> bool:
+        return bool(self.ctx.lib.donof_job_fp64_tc(self.handle))
+
     def device_bytes(self) -> int:
         return int(self.ctx.lib.donof_job_device_bytes(self.handle))
 
@@ -428,6 +438,12 @@ def transform_dev(C, b: BTensor, nbf5: int, out=None, precision=None):
     """b_pq^l = C5^T b_l C5 on the device (out: CUDA tensor or None)."""
     prec = b.precision if precision is None else _prec(precision)
     b.ctx.check(b.ctx.lib.donof_transform_dev(b.handle, prec, _ptr(C), int(nbf5), _ptr(out)))
+
+
+def t1_dev(C, b: BTensor, nbf5: int, out):
+    """tmp[m + nbf*q + nbf*nbf5*l] = sum_n b[m,n,l] C[n,q] of the FP64 form on the
+    device (C and out: CUDA tensors; out holds nbf*nbf5*naux doubles)."""
+    b.ctx.check(b.ctx.lib.donof_t1_dev(b.handle, _ptr(C), int(nbf5), _ptr(out)))
 
 
 def launch_count() -> int:

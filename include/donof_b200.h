@@ -172,6 +172,21 @@ int donof_jkh_mo_prec_dev(donof_job* job, int precision, const double* C, const 
  * b_pq[p + nbf5*q + nbf5*nbf5*l].                                            */
 int donof_transform_dev(donof_job* job, int precision, const double* C, int nbf5, double* b_pq);
 
+/* --- FP64 form on the tensor cores ----------------------------------------
+ * enable != 0 makes the int8 digit slices of the job's b (7 slices of 7 bits
+ * per row, scaled by a power of two; 7/8 of b's FP64 size) and from then on
+ * runs the FP64 form's first contraction tmp_l = b_l C5 (src/utils.jl:19,
+ * src/integrals.jl:150) as exact int8 x int8 -> int32 tensor-core products
+ * recombined in FP64 (Ozaki scheme): within ~1e-13 of the largest |tmp| of
+ * an FP64 GEMM, inside the form's 1e-10 parity.  enable = 0 frees the slices
+ * (the DMMA GEMM runs again).  Needs nbf <= 16384.  donof_job_fp64_tc tells
+ * whether the slices are present.                                            */
+int donof_job_set_fp64_tc(donof_job* job, int enable);
+int donof_job_fp64_tc(const donof_job* job);
+/* FP64 form's first contraction alone: tmp[m + nbf*q + nbf*nbf5*l] =
+ * sum_n b[m,n,l] C[n,q] (device, FP64), by whichever engine the job uses.   */
+int donof_t1_dev(donof_job* job, const double* C, int nbf5, double* tmp);
+
 /* --- rotate_orbital ------------------------------------------------------
  * Replaces rotate_orbital(y,C,p) (ext/DoNOFGPUExt.jl:355-382, which runs in
  * FP32); CPU definition src/utils.jl:499-521, followed here in FP64:

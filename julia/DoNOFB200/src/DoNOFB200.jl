@@ -112,6 +112,12 @@ end
 set_precision!(b::B200Tensor, precision::Integer) =
     check(ccall((:donof_job_set_precision, libdonof), Cint, (Ptr{Cvoid}, Cint), b.job, precision))
 
+"""FP64 form: run the first contraction (b_l C5) on the tensor cores from int8 digit
+slices of b (exact integer products, within ~1e-13 of the FP64 GEMM), or back on the
+FP64 GEMM with `enable = false`."""
+set_fp64_tc!(b::B200Tensor, enable::Bool=true) =
+    check(ccall((:donof_job_set_fp64_tc, libdonof), Cint, (Ptr{Cvoid}, Cint), b.job, enable ? 1 : 0))
+
 # ---------------------------------------------------------------- the hot path
 """compute_Lagrange2 (src/utils.jl:1-59): (elag, H_mat, E_elec)."""
 function lagrange2(C, n, H, b::B200Tensor, cj12, ck12, nalpha, nbeta)
