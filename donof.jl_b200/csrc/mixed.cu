@@ -213,16 +213,19 @@ lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_const
             int it = 0;          // ring stages consumed
             int tq = 0;          // T1 quarters issued (slot = tq & 1)
             int y_li = -1;       // aux index whose Y MMAs are still to be issued
+            // Shared-memory descriptors are linear in the address (addr >> 4 in the low 14
+            // bits, no carry below 256 KB): the fixed bases are built once, offsets are adds.
+            const uint64_t dA3 = sdesc(sbase + OFF_A3, 16, 1024);
+            const uint64_t dA2k = sdesc(sbase + OFF_A2, 16, 1024);            // A2 as a K-major operand
+            const uint64_t dA2m = sdesc(sbase + OFF_A2, CS_BOX_BYTES, 1024);  // A2 as an MN-major operand
+            const uint64_t dCS = sdesc(sbase + OFF_CS, 16, 1024);
             auto issue_y = [&]() {
                 // Y: RY[j, m] += sum_q A3[j, q] tmp_x[q, m]  (A2 read as an MN-major operand)
+                // K rows q = 16 ks + i of the hi part are A2 rows 32 ks + i, the lo part 32 ks + 16 + i
 #pragma unroll
                 for (int ks = 0; ks < 4; ++ks) {
-                    const uint64_t a = sdesc(sbase + OFF_A3 + ks * 32, 16, 1024);
-                    // K rows q = 16 ks + i of the hi part are A2 rows 32 ks + i, the lo part 32 ks + 16 + i
-                    const uint64_t bh = sdesc(sbase + OFF_A2 + ks * 4096, CS_BOX_BYTES, 1024);
-                    const uint64_t bl = sdesc(sbase + OFF_A2 + ks * 4096 + 2048, CS_BOX_BYTES, 1024);
-                    umma(RY, a, bh, id_y, (y_li | ks) ? 1u : 0u);
-                    umma(RY, a, bl, id_y, 1u);
+                    umma(RY, dA3 + (uint64_t)(2 * ks), dA2m + (uint64_t)(256 * ks), id_y, (y_li | ks) ? 1u : 0u);
+                    umma(RY, dA3 + (uint64_t)(2 * ks), dA2m + (uint64_t)(256 * ks + 128), id_y, 1u);
                 }
                 umma_commit(bar(B_Y));
                 y_li = -1;
@@ -255,15 +258,14 @@ lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_const
                     }
                     if (!wait_poll(bar(B_FULL + s), (uint32_t)((it / RING) & 1))) return false;
                     fence_after();
-                    const uint32_t st = sbase + OFF_RING + s * STAGE_BYTES;
+                    // n rows kb*64 + 16 ks of Cs: box kb (KB = 64 = one box), 32 bytes per ks
+                    const uint64_t a0 = dCS + (uint64_t)((kb * CS_BOX_BYTES) >> 4);
+                    const uint64_t bh0 = sdesc(sbase + OFF_RING + s * STAGE_BYTES, BOX_BYTES, 1024);
+                    const uint64_t bl0 = bh0 + (uint64_t)(BOX_BYTES >> 4);
 #pragma unroll
                     for (int ks = 0; ks < KB / 16; ++ks) {
-                        const int k = kb * KB + ks * 16;  // n offset
-                        const uint64_t a = sdesc(sbase + OFF_CS + (k >> 6) * CS_BOX_BYTES + (k & 63) * 2, 16, 1024);
-                        const uint64_t bh = sdesc(st + ks * 2048, BOX_BYTES, 1024);
-                        const uint64_t bl = sdesc(st + BOX_BYTES + ks * 2048, BOX_BYTES, 1024);
-                        umma(d, a, bh, id_t1, (kb | ks) ? 1u : 0u);
-                        umma(d, a, bl, id_t1, 1u);
+                        umma(d, a0 + (uint64_t)(2 * ks), bh0 + (uint64_t)(128 * ks), id_t1, (kb | ks) ? 1u : 0u);
+                        umma(d, a0 + (uint64_t)(2 * ks), bl0 + (uint64_t)(128 * ks), id_t1, 1u);
                     }
                     umma_commit(bar(B_EMPTY + s));
                 }
@@ -283,10 +285,9 @@ lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_const
                 if (!wait_poll(bar(B_A2), lph)) { ok = false; break; }
                 fence_after();
                 for (int ks = 0; ks < ncol / 16; ++ks) {
-                    const int k = ks * 16;  // m offset
-                    const uint64_t a = sdesc(sbase + OFF_A2 + (k >> 6) * CS_BOX_BYTES + (k & 63) * 2, 16, 1024);
-                    const uint64_t b = sdesc(sbase + OFF_CS + (k >> 6) * CS_BOX_BYTES + (k & 63) * 2, 16, 1024);
-                    umma(RT2, a, b, id_t2, ks ? 1u : 0u);
+                    // m offset 16 ks: box ks / 4, 32 bytes per ks inside it
+                    const uint64_t off = (uint64_t)((ks >> 2) * (CS_BOX_BYTES >> 4) + 2 * (ks & 3));
+                    umma(RT2, dA2k + off, dCS + off, id_t2, ks ? 1u : 0u);
                 }
                 umma_commit(bar(B_T2));
                 if (P.mode == 3) y_li = li;
