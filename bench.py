@@ -305,9 +305,11 @@ ENERGY_OCTANE = dict(nbf=202, naux=974, nbeta=33, ncwo=5)
 def energies_case(d, torch, ctx, shape, scale, seed):
     from donof_b200 import workload
     from donof_b200.optimize import energy, energy_mixed_refined
+    from donof_b200.serve import use_fp64_tc
     out = {"workload": f"molecule-like surrogate (nbf={shape['nbf']}, naux={shape['naux']}, nbeta={shape['nbeta']}, "
                        f"ncwo={shape['ncwo']}, two_e_scale={scale}, seed {seed}), max|g_orb|, |g_occ| < 1e-6",
-           "unit": "energies/s"}
+           "unit": "energies/s",
+           "fp64_t1": "tensor cores" if use_fp64_tc(None, shape["nbf"]) else "DMMA GEMM"}
     res = {}
     for form in ("fp64", "mixed_refined"):
         wl = workload.molecule_like(**shape, seed=seed, two_e_scale=scale)
@@ -315,6 +317,8 @@ def energies_case(d, torch, ctx, shape, scale, seed):
         p.threshgorb = p.threshgocc = 1e-6
         p.threshen = 1e-10  # occupations solved tightly each iteration: both forms reach the same minimum
         b = d.eris_to_gpu(wl.b, "fp64" if form == "fp64" else "mixed", ctx)
+        if use_fp64_tc(None, p.nbf):
+            b.set_fp64_tc(True)   # both forms' FP64 iterations, as the server runs them
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         if form == "fp64":
@@ -367,7 +371,7 @@ def serving_bench(d, torch):
     serving the same stream one job at a time; per-job |dE| between the two."""
     import copy
     from donof_b200 import workload
-    from donof_b200.serve import Request, Server, resolve_precision
+    from donof_b200.serve import Request, Server, resolve_precision, use_fp64_tc
     rng = np.random.default_rng(SERVE["seed"])
     shapes = [SERVE_SHAPES[i] for i in rng.integers(len(SERVE_SHAPES), size=SERVE["jobs"])]
     for pos in rng.choice(len(shapes) + SERVE["large"], size=SERVE["large"], replace=False):
@@ -390,6 +394,8 @@ def serving_bench(d, torch):
         p = wl.p
         prec = resolve_precision("auto", p.nbf, p.nbf5, p.nbfaux)
         b = d.eris_to_gpu(wl.b, "fp64" if prec == "fp64" else "mixed", ctx)
+        if use_fp64_tc(None, p.nbf):
+            b.set_fp64_tc(True)
         for form in (("fp64",) if prec == "fp64" else ("fp64", "mixed")):
             b.set_precision(form)
             d.compute_Lagrange2(wl.C, wl.n, wl.H, b, wl.cj12, wl.ck12, p.nalpha, p.nbeta)
@@ -431,6 +437,7 @@ def serving_bench(d, torch):
                         f"{SERVE['large']} n-octane-sized jobs (nbf 24-202); max|g_orb|, |g_occ| < "
                         f"{SERVE['thresh']:g} ({SERVE_LARGE_JOB['thresh']:g} for the n-octane-sized jobs, "
                         f"two_e_scale {SERVE_LARGE_JOB['two_e_scale']})",
+            "fp64_t1": "tensor cores for nbf >= 128 (both arms), DMMA GEMM below",
             "served": {**served, "precision": "auto (mixed + closing FP64 for nbf*nbf5*naux >= 2e7, else FP64)",
                        "max_inflight": SERVE["inflight"]},
             "served_grouped": {**served_g, "group_max": SERVE["group_max"],

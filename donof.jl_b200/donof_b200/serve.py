@@ -42,6 +42,18 @@ PRECISIONS = ("fp64", "mixed", "mixed_refined", "auto")
 AUTO_MIXED_MIN_WORK = 2.0e7
 
 
+# The FP64 form's first contraction runs on the tensor cores from int8 digit
+# slices of b (ozaki.cu) for jobs of at least this many basis functions: there
+# it is faster than the DMMA GEMM (nbf = 202: 450 against 746 us per call,
+# nbf = 256: 130 against 290 us); below, the contraction is a few microseconds
+# either way and the slices would only cost memory.
+FP64_TC_MIN_NBF = 128
+
+
+def use_fp64_tc(fp64_tc: Optional[bool], nbf: int) -> bool:
+    return nbf >= FP64_TC_MIN_NBF if fp64_tc is None else bool(fp64_tc)
+
+
 def resolve_precision(precision: str, nbf: int, nbf5: int, naux: int) -> str:
     if precision != "auto":
         return precision
@@ -62,6 +74,7 @@ class Request:
     E_nuc: float = 0.0
     maxit: Optional[int] = None
     tag: object = None
+    fp64_tc: Optional[bool] = None  # FP64 contraction on the tensor cores (None: nbf >= FP64_TC_MIN_NBF)
 
 
 @dataclass
@@ -85,9 +98,11 @@ class Result:
         return self.t_done - self.t_submit
 
 
-def footprint(nbf: int, naux: int, nbf5: int, precision: str) -> int:
+def footprint(nbf: int, naux: int, nbf5: int, precision: str, fp64_tc: bool = False) -> int:
     """Device bytes a job holds while it runs (upper estimate)."""
     b = 8 * nbf * nbf * naux
+    if fp64_tc:  # b's int8 digit slices (7 per element, rows padded to 16 bytes) and row scales
+        b += 7 * nbf * (-(-nbf // 16) * 16) * naux + 8 * nbf * naux
     nb = (nbf + 63) // 64
     split = 4 * 64 * nb * nbf * naux if precision != "fp64" else 0
     # FP64 transforms: tmp (nbf nbf5 naux), b_pq and W (nbf5^2 naux each)
@@ -209,6 +224,8 @@ def run_energy(req: Request, device: int, cta_limit: int = 0) -> Result:
         prec = resolve_precision(req.precision, req.p.nbf, req.p.nbf5, req.p.nbfaux)
         up = "fp64" if prec == "fp64" else "mixed"
         b = api.eris_to_gpu(req.b, up, ctx)
+        if use_fp64_tc(req.fp64_tc, p.nbf):
+            b.set_fp64_tc(True)
         if prec == "mixed_refined":
             r, _ = energy_mixed_refined(req.H, b, req.p, req.C, req.gamma, E_nuc=req.E_nuc, maxit=req.maxit)
         else:
@@ -316,7 +333,8 @@ class Server:
         if req.precision not in PRECISIONS:
             raise ValueError(f"precision must be one of {PRECISIONS}")
         nbf, naux = req.p.nbf, req.p.nbfaux
-        nb = footprint(nbf, naux, req.p.nbf5, resolve_precision(req.precision, nbf, req.p.nbf5, naux))
+        nb = footprint(nbf, naux, req.p.nbf5, resolve_precision(req.precision, nbf, req.p.nbf5, naux),
+                       use_fp64_tc(req.fp64_tc, nbf))
         with self._lock:
             if self._closed:
                 raise RuntimeError("server is shut down")

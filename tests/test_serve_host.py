@@ -208,3 +208,12 @@ def test_a_failing_job_reports_its_error_and_the_server_goes_on():
         tb, tg = s.submit(_req(8, tag="bad")), s.submit(_req(8, tag="good"))
         rb, rg = s.wait(tb, timeout=10), s.wait(tg, timeout=10)
     assert "NaN" in rb.error and rg.error is None and rg.E_elec == 2.0
+
+
+def test_fp64_tensor_core_policy_and_footprint():
+    from donof_b200.serve import FP64_TC_MIN_NBF, footprint, use_fp64_tc
+    assert not use_fp64_tc(None, FP64_TC_MIN_NBF - 1) and use_fp64_tc(None, FP64_TC_MIN_NBF)
+    assert use_fp64_tc(True, 24) and not use_fp64_tc(False, 512)
+    # the digit slices: 7 bytes per element of b with rows padded to 16 bytes, plus the row scales
+    extra = footprint(202, 974, 198, "fp64", True) - footprint(202, 974, 198, "fp64")
+    assert extra == 7 * 202 * 208 * 974 + 8 * 202 * 974
