@@ -136,8 +136,10 @@ ozaki_t1_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant
 
     if (warp == PRODUCER) {
         // ------------------------------------------------------------ producer
-        // per unit, per q tile, per n chunk: the C5 stage (unless resident), then
-        // the S slices of b in the order the MMAs consume them (i = S-1 .. 0)
+        // b's slices in the order the MMAs consume them: with C5 resident, slice
+        // i of every n chunk before slice i-1 (i = S-1 .. 0), so that a round
+        // needs accumulator 0 only for its last nkc stages; with C5 streamed, per
+        // q tile and n chunk the C5 stage, then the slices i = S-1 .. 0
         if (lane == 0 && my_units > 0) {
             int it = 0, bs = 0;
             bool ok = true;
@@ -152,6 +154,19 @@ ozaki_t1_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant
                 const int w = (int)blockIdx.x + u * G;
                 const int l = w / P.nmt, mt = w - l * P.nmt;
                 for (int qt = 0; qt < P.nqt && ok; ++qt) {
+                    if (P.resident) {
+                        for (int i = S - 1; i >= 0 && ok; --i)
+                            for (int kc = 0; kc < P.nkc; ++kc, ++it) {
+                                const int s = it % RING;
+                                if (!mbar_wait(bar(A_EMPTY + s), (uint32_t)(((it / RING) & 1) ^ 1), abort_flag, P.wait)) {
+                                    ok = false;
+                                    break;
+                                }
+                                mbar_expect_tx(bar(A_FULL + s), (uint32_t)A_BYTES);
+                                tma_load_4d(sbase + OFF_RING + s * A_BYTES, &map_a, bar(A_FULL + s), kc * KC, mt * MT, i, l);
+                            }
+                        continue;
+                    }
                     for (int kc = 0; kc < P.nkc && ok; ++kc) {
                         if (!P.resident) {
                             const int slot = bs & 1;
@@ -197,6 +212,48 @@ ozaki_t1_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant
             bool ok = true;
             for (int u = 0; u < my_units && ok; ++u) {
                 for (int qt = 0; qt < P.nqt && ok; ++qt, ++rnd) {
+                    if (P.resident) {
+                        const uint64_t bq = sdesc(sbase + OFF_B + qt * P.nkc * B_BYTES, 16, 1024);
+                        if (rnd == 0)
+                            for (int b = 0; b < nbst && ok; ++b) ok = mbar_wait(bar(B_FULL + b), 0, abort_flag, P.wait);
+                        fence_after();
+#pragma unroll
+                        for (int ii = 0; ii < S; ++ii) {
+                            const int i = S - 1 - ii;
+                            for (int kc = 0; kc < P.nkc && ok; ++kc) {
+                                const uint64_t bd = bq + (uint64_t)((kc * B_BYTES) >> 4);
+                                if (kc == 0 && !mbar_wait(bar(GFREE + i), (uint32_t)(rnd & 1), abort_flag, P.wait)) {
+                                    ok = false;
+                                    break;
+                                }
+                                if (!mbar_wait(bar(A_FULL + s), aph, abort_flag, P.wait)) {
+                                    ok = false;
+                                    break;
+                                }
+                                fence_after();
+                                const uint64_t ad = sdesc(sbase + OFF_RING + s * A_BYTES, 16, 1024);
+#pragma unroll
+                                for (int k4 = 0; k4 < KC / 32; ++k4) {
+#pragma unroll
+                                    for (int j0 = 0; j0 < S - i; j0 += 4) {
+                                        constexpr int kMax = 4;
+                                        const int cnt = (S - i - j0) < kMax ? (S - i - j0) : kMax;
+                                        umma_i8(tmem + (uint32_t)((i + j0) * QT), ad + (uint64_t)(2 * k4),
+                                                bd + (uint64_t)((j0 * BS_BYTES + k4 * 32) >> 4), idesc_i8(MT, QT * cnt), 1u);
+                                    }
+                                }
+                                umma_commit(bar(A_EMPTY + s));
+                                if (++s == RING) {
+                                    s = 0;
+                                    aph ^= 1u;
+                                }
+                            }
+                            if (!ok) break;
+                        }
+                        if (!ok) break;
+                        umma_commit(bar(ACC_FULL));
+                        continue;
+                    }
                     for (int kc = 0; kc < P.nkc && ok; ++kc) {
                         const int bslot = P.resident ? qt * P.nkc + kc : (bs & 1);
                         const uint32_t bpar = P.resident ? 0u : (uint32_t)((bs >> 1) & 1);
