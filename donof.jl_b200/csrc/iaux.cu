@@ -6,10 +6,8 @@
 // the contraction as one GEMM of I seen as an (nbf^2 x naux) column-major
 // matrix, whose product is b in the layout of the rest of the library.
 //
-// The symmetric eigensolver is cuSOLVER's dsyevd (a one-time set-up step of a
-// job, like a library GEMM); the two products run on the library's FP64
-// tensor-core GEMM.
-#include <cusolverDn.h>
+// The symmetric eigensolver is the library's own parallel Jacobi kernel
+// (eigh.cu); the two products run on the library's FP64 tensor-core GEMM.
 #include <math.h>
 
 #include "kernels.cuh"
@@ -33,12 +31,16 @@ __global__ void gmsqrt_factors_kernel(const double* __restrict__ V, const double
 }
 
 struct DeviceScratch {
-    void* p[8] = {};
+    void* p[16] = {};
     int n = 0;
     donof_ctx* ctx;
     explicit DeviceScratch(donof_ctx* c) : ctx(c) {}
     template <class T>
     int alloc(T** out, size_t count) {
+        if (n >= 16) {
+            set_error(ctx, "Iaux scratch: too many buffers");
+            return DONOF_ERR_STATE;
+        }
         void* d = nullptr;
         DONOF_CHECK(dev_alloc(ctx, &d, sizeof(T) * count));
         p[n++] = d;
@@ -57,51 +59,25 @@ int iaux_f64(donof_ctx* ctx, cudaStream_t st, const double* G_host, const double
     const size_t nn = (size_t)nbf * nbf, na2 = (size_t)naux * naux;
     DeviceScratch s(ctx);
     double *dI = nullptr, *dG = nullptr, *dw = nullptr, *dVs = nullptr, *dVT = nullptr, *dGm = nullptr,
-           *work = nullptr;
-    int* dinfo = nullptr;
+           *dA = nullptr, *dV = nullptr;
+    unsigned char* escr = nullptr;
     DONOF_CHECK(s.alloc(&dI, nn * naux));
     DONOF_CHECK(s.alloc(&dG, na2));
     DONOF_CHECK(s.alloc(&dw, (size_t)naux));
     DONOF_CHECK(s.alloc(&dVs, na2));
     DONOF_CHECK(s.alloc(&dVT, na2));
     DONOF_CHECK(s.alloc(&dGm, na2));
-    DONOF_CHECK(s.alloc(&dinfo, 1));
+    DONOF_CHECK(s.alloc(&dA, na2));
+    DONOF_CHECK(s.alloc(&dV, na2));
+    DONOF_CHECK(s.alloc(&escr, eigh_scratch_bytes(naux)));
     DONOF_CUDA(ctx, cudaMemcpyAsync(dI, I_host, sizeof(double) * nn * naux, cudaMemcpyHostToDevice, st));
     DONOF_CUDA(ctx, cudaMemcpyAsync(dG, G_host, sizeof(double) * na2, cudaMemcpyHostToDevice, st));
-
-    cusolverDnHandle_t h = nullptr;
-    if (cusolverDnCreate(&h) != CUSOLVER_STATUS_SUCCESS) {
-        set_error(ctx, "cusolverDnCreate failed");
-        return DONOF_ERR_CUDA;
-    }
-    struct HandleGuard {
-        cusolverDnHandle_t h;
-        ~HandleGuard() { cusolverDnDestroy(h); }
-    } guard{h};
-    int lwork = 0;
-    if (cusolverDnSetStream(h, st) != CUSOLVER_STATUS_SUCCESS ||
-        cusolverDnDsyevd_bufferSize(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, naux, dG, naux, dw,
-                                    &lwork) != CUSOLVER_STATUS_SUCCESS) {
-        set_error(ctx, "cusolverDnDsyevd_bufferSize failed");
-        return DONOF_ERR_CUDA;
-    }
-    DONOF_CHECK(s.alloc(&work, (size_t)(lwork > 0 ? lwork : 1)));
-    if (cusolverDnDsyevd(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, naux, dG, naux, dw, work, lwork,
-                         dinfo) != CUSOLVER_STATUS_SUCCESS) {
-        set_error(ctx, "cusolverDnDsyevd failed");
-        return DONOF_ERR_CUDA;
-    }
-    int info = 0;
-    DONOF_CUDA(ctx, cudaMemcpyAsync(&info, dinfo, sizeof(int), cudaMemcpyDeviceToHost, st));
-    DONOF_CUDA(ctx, cudaStreamSynchronize(st));
-    if (info != 0) {
-        set_error(ctx, "eigen-decomposition of G did not converge (info = %d)", info);
-        return DONOF_ERR_CUDA;
-    }
+    // eigen-decomposition of Symmetric(G) (its upper triangle)
+    DONOF_CHECK(eigh_jacobi(ctx, st, dG, naux, dA, dV, dw, escr));
     {
         long long blocks = ((long long)na2 + 255) / 256;
         if (blocks > 8LL * ctx->sm_count) blocks = 8LL * ctx->sm_count;
-        gmsqrt_factors_kernel<<<(int)blocks, 256, 0, st>>>(dG, dw, naux, dVs, dVT); count_launch();
+        gmsqrt_factors_kernel<<<(int)blocks, 256, 0, st>>>(dV, dw, naux, dVs, dVT); count_launch();
         DONOF_CUDA(ctx, cudaGetLastError());
     }
     // G^{-1/2} = Vs V^T (A: Vs, M-contiguous; B: V^T stored K-contiguous)

@@ -74,6 +74,13 @@ int elag_tail_f64(donof_job* job, cudaStream_t st, const double* C, const double
                   const void* part, bool part_f32, int nparts, long long pstride, double* Hmat, double* elag,
                   double* E);
 
+// Eigenvalues w and eigenvectors V (columns) of Symmetric(G) on the device by
+// the parallel cyclic Jacobi method (eigh.cu); A: n x n scratch, scratch:
+// eigh_scratch_bytes(n).  Synchronises the stream.
+size_t eigh_scratch_bytes(int n);
+int eigh_jacobi(donof_ctx* ctx, cudaStream_t st, const double* G, int n, double* A, double* V, double* w,
+                void* scratch);
+
 // b = I G^{-1/2} on the device from host G (naux x naux) and I (nbf x nbf x naux)
 // (iaux.cu); part is scratch for the products.
 int iaux_f64(donof_ctx* ctx, cudaStream_t st, const double* G_host, const double* I_host, int nbf, int naux,

@@ -40,7 +40,8 @@ def _download_b(bt, nbf, naux):
 
 
 @pytest.mark.parametrize("nbf,naux,negative,asym", [(13, 29, 0, False), (24, 116, 3, False), (40, 64, 0, True),
-                                                     (96, 200, 5, True)])
+                                                     (96, 200, 5, True), (16, 1, 0, False), (20, 333, 2, True),
+                                                     (24, 1024, 0, False)])
 def test_iaux_matches_oracle(cuda_ctx, nbf, naux, negative, asym):
     G, I = _inputs(nbf, naux, nbf + naux, negative, asym)
     bt = d.Iaux_gpu(G, I, "fp64", cuda_ctx)
@@ -70,3 +71,18 @@ def test_iaux_feeds_the_lagrangian(cuda_ctx):
 def test_iaux_rejects_bad_shapes(cuda_ctx):
     with pytest.raises(ValueError):
         d.Iaux_gpu(np.eye(5), np.zeros((4, 4, 6)), "fp64", cuda_ctx)
+
+
+def test_iaux_with_repeated_eigenvalues(cuda_ctx):
+    """Degenerate eigenvalues (a multiple of the identity plus a low-rank term):
+    G^{-1/2} is unique even though the eigenvectors are not."""
+    nbf, naux = 12, 80
+    rng = np.random.default_rng(11)
+    U = np.linalg.qr(rng.standard_normal((naux, 3)))[0]
+    G = np.asfortranarray(2.0 * np.eye(naux) + (U * np.array([1.0, 1.0, 3.0])) @ U.T)
+    I = rng.standard_normal((nbf, nbf, naux))
+    I = np.asfortranarray(0.5 * (I + I.transpose(1, 0, 2)))
+    bt = d.Iaux_gpu(G, I, "fp64", cuda_ctx)
+    b = _download_b(bt, nbf, naux)
+    assert rel(b, integrals.iaux(G, I)) <= 1e-10
+    bt.free()
