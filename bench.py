@@ -357,7 +357,7 @@ SERVE_SHAPES = [(24 * k, 116 * k, 5 * k, 3) for k in (1, 2, 3, 4)] + \
                [(24 * n + 10, int(4.8 * (24 * n + 10)), 4 * n + 1, 5) for n in (1, 2, 3)]
 SERVE_LARGE = (202, 974, 33, 5)   # n-octane shape
 SERVE = dict(jobs=64, large=4, rate_per_s=20.0, seed=7, thresh=1e-5, threshen=1e-6, inflight=8,
-             group_max=16)  # threshen = thresh / 10
+             group_max=16, continuous_slots=8)  # threshen = thresh / 10
 # the n-octane-sized jobs (the ones auto runs mixed + closing FP64): a weak
 # two-electron part (one GNOF minimum) and gradients to 1e-6, where the energy is
 # pinned well below 1 uEh (at 1e-5 two FP64 paths still differ by ~1e-5 Eh)
@@ -403,8 +403,8 @@ def serving_bench(d, torch):
         b.free()
     ctx.close()
 
-    def run(precision, inflight, group_max=0, rate_scale=1.0):
-        with Server(max_inflight=inflight, group_max=group_max) as srv:
+    def run(precision, inflight, group_max=0, rate_scale=1.0, continuous=0):
+        with Server(max_inflight=inflight, group_max=group_max, continuous_slots=continuous) as srv:
             t0 = time.perf_counter()
             tickets = []
             for wl, t_arr in zip(jobs, arrivals * rate_scale):
@@ -423,6 +423,7 @@ def serving_bench(d, torch):
     ref, seq = run("fp64", 1)
     res, served = run("auto", SERVE["inflight"])
     res_g, served_g = run("auto", SERVE["inflight"], group_max=SERVE["group_max"])
+    res_c, served_c = run("auto", SERVE["inflight"], continuous=SERVE["continuous_slots"])
     # the arrival rate swept: the same stream twice as fast, and all requests at once
     sweep = [{"rate_per_s": SERVE["rate_per_s"], "value": served["value"], "latency_s": served["latency_s"]}]
     for scale, label in ((0.5, 2 * SERVE["rate_per_s"]), (0.0, "all at t=0")):
@@ -431,6 +432,7 @@ def serving_bench(d, torch):
                       "speedup_vs_fp64_one_at_a_time": sv["value"] / seq["value"]})
     dE = np.array([abs(a.E_elec - b.E_elec) for a, b in zip(res, ref)])
     dE_g = np.array([abs(a.E_elec - b.E_elec) for a, b in zip(res_g, ref)])
+    dE_c = np.array([abs(a.E_elec - b.E_elec) for a, b in zip(res_c, ref)])
     return {"unit": "energies/s",
             "workload": f"{len(jobs)} jobs, Poisson arrivals at {SERVE['rate_per_s']:g}/s (seed {SERVE['seed']}): "
                         "molecule-shaped surrogates of (H2O)_k k=1..4, CnH2n+2 n=1..3 and "
@@ -445,6 +447,13 @@ def serving_bench(d, torch):
                                        "grouped batch (donof_batch_energy)",
                                "abs_dE_Eh_vs_fp64": {"max": float(dE_g.max()), "median": float(np.median(dE_g)),
                                                      "within_1uEh": int(np.sum(dE_g <= 1e-6))}},
+            "served_continuous": {**served_c, "slots_per_shape": SERVE["continuous_slots"],
+                                  "path": "as served, and the FP64 jobs of each shape share one batch whose slots are "
+                                          "refilled as jobs converge (donof_batch_serve: every outer iteration "
+                                          "advances all running jobs of the shape as grouped launches)",
+                                  "abs_dE_Eh_vs_fp64": {"max": float(dE_c.max()), "median": float(np.median(dE_c)),
+                                                        "within_1uEh": int(np.sum(dE_c <= 1e-6))}},
+            "speedup_continuous": served_c["value"] / seq["value"],
             "served_rate_sweep": sweep,
             "fp64_one_at_a_time": seq,
             "speedup": served["value"] / seq["value"],

@@ -27,6 +27,11 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <memory>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -254,7 +259,8 @@ struct donof_batch {
     donof_ctx* ctx = nullptr;
     int nj = 0;
     struct Shape {
-        donof_job* job;
+        donof_job* job;       // the job bound to the slot (not dereferenced once bound: it may be freed)
+        const double* b;      // its RI tensor, read by T1 while the slot runs
         int nbf, naux, nbf5, nalpha, nbeta;
         long long nvar, nn;
         int splits, kchunk;
@@ -312,7 +318,7 @@ GemmF64Args stage_args(const donof_batch* B, int s, int j) {
     GemmF64Args a{};
     if (s == ST_T1) {  // tmp_l(m, q) = sum_n b[m, n, l] C[n, q]
         a.M = h.nbf; a.N = h.nbf5; a.K = h.nbf;
-        a.A = h.job->b; a.lda = h.nbf; a.strideA = (long long)h.nbf * h.nbf;
+        a.A = h.b; a.lda = h.nbf; a.strideA = (long long)h.nbf * h.nbf;
         a.B = p.Cnew; a.ldb = h.nbf; a.strideB = 0;
         a.C = p.tmp; a.ldc = h.nbf; a.strideC = (long long)h.nbf * h.nbf5;
         a.batch = h.naux; a.splits = 1; a.kchunk = h.nbf;
@@ -652,6 +658,7 @@ int donof_batch_create(donof_ctx* ctx, int count, const donof_batch_shape* shape
     for (int j = 0; j < count; ++j) {
         donof_batch::Shape& h = B->sh[j];
         h.job = shapes[j].job;
+        h.b = h.job->b;
         h.nbf = h.job->nbf; h.naux = h.job->naux; h.nbf5 = shapes[j].nbf5;
         h.nalpha = shapes[j].nalpha; h.nbeta = shapes[j].nbeta;
         h.nvar = nvar_of(h.nbf, h.nbf5);
@@ -992,6 +999,77 @@ int donof_batch_orbopt(donof_batch* B, int method, donof_batch_item* items) {
     return DONOF_OK;
 }
 
+struct donof_batch_queue {
+    struct Req {
+        donof_batch_request r;
+        unsigned long long ticket;
+        bool taken = false, done = false;
+        int status = DONOF_OK;
+        donof_energy_result res{};
+    };
+    std::mutex mu;
+    std::condition_variable cv;       // serve loop: new request or close
+    std::condition_variable cv_done;  // pollers: a request finished
+    std::deque<std::shared_ptr<Req>> all;
+    unsigned long long next = 1;
+    bool closed = false;
+    int method = -1;
+    std::shared_ptr<Req> find(unsigned long long t) {
+        for (auto& q : all)
+            if (q->ticket == t) return q;
+        return nullptr;
+    }
+};
+
+int donof_batch_queue_create(donof_batch_queue** q) {
+    if (!q) return DONOF_ERR_ARG;
+    *q = new (std::nothrow) donof_batch_queue();
+    return *q ? DONOF_OK : DONOF_ERR_OOM;
+}
+
+int donof_batch_queue_push(donof_batch_queue* q, const donof_batch_request* r, unsigned long long* ticket) {
+    if (!q || !r || !ticket || !r->job || !r->H || !r->C_inout || !r->gamma_inout) return DONOF_ERR_ARG;
+    std::lock_guard<std::mutex> lk(q->mu);
+    if (q->closed) return DONOF_ERR_STATE;
+    if (q->method < 0) q->method = r->params.orb_method;
+    if (r->params.orb_method != q->method) return DONOF_ERR_ARG;  // one optimiser per queue
+    auto req = std::make_shared<donof_batch_queue::Req>();
+    req->r = *r;
+    req->ticket = q->next++;
+    q->all.push_back(req);
+    *ticket = req->ticket;
+    q->cv.notify_all();
+    return DONOF_OK;
+}
+
+int donof_batch_queue_close(donof_batch_queue* q) {
+    if (!q) return DONOF_ERR_ARG;
+    std::lock_guard<std::mutex> lk(q->mu);
+    q->closed = true;
+    q->cv.notify_all();
+    return DONOF_OK;
+}
+
+int donof_batch_queue_poll(donof_batch_queue* q, unsigned long long ticket, int wait, int* done, int* status,
+                           donof_energy_result* res) {
+    if (!q || !done) return DONOF_ERR_ARG;
+    std::unique_lock<std::mutex> lk(q->mu);
+    auto req = q->find(ticket);
+    if (!req) return DONOF_ERR_ARG;
+    if (wait) q->cv_done.wait(lk, [&] { return req->done; });
+    *done = req->done ? 1 : 0;
+    if (req->done) {
+        if (status) *status = req->status;
+        if (res) *res = req->res;
+    }
+    return DONOF_OK;
+}
+
+int donof_batch_queue_destroy(donof_batch_queue* q) {
+    delete q;
+    return DONOF_OK;
+}
+
 int donof_batch_energy(donof_batch* B, donof_energy_params* params, const double* const* H, double* const* C_inout,
                        double* const* gamma_inout, double* const* n_out, donof_energy_result* results) {
     if (!B) return DONOF_ERR_ARG;
@@ -1074,6 +1152,194 @@ int donof_batch_energy(donof_batch* B, donof_energy_params* params, const double
     for (int j = 0; j < nj; ++j)
         DONOF_CHECK(E[j].finish(C_inout[j], gamma_inout[j], n_out ? n_out[j] : nullptr, nullptr, &results[j]));
     return DONOF_OK;
+}
+
+int donof_batch_serve(donof_batch* B, donof_batch_queue* q) {
+    if (!B || !q) return DONOF_ERR_ARG;
+    donof_ctx* ctx = B->ctx;
+    DONOF_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t bst = batch_stream(B);
+    if (!bst) {
+        set_error(ctx, "donof_batch_serve: no stream");
+        return DONOF_ERR_CUDA;
+    }
+    using Req = donof_batch_queue::Req;
+    const int nj = B->nj;
+    std::vector<std::shared_ptr<Req>> slot(nj);
+    std::vector<std::unique_ptr<EnergyJob>> E(nj);
+    std::vector<donof_energy_params> prm(nj);
+    std::vector<donof_batch_item> items(nj);
+    // zero device arrays standing in for an idle slot's inputs (the grouped step skips the slot)
+    DevBuf idle;
+    std::vector<size_t> ioff(nj);
+    size_t per = 0;
+    for (int j = 0; j < nj; ++j) {
+        const donof_batch::Shape& h = B->sh[j];
+        ioff[j] = per;
+        per += al32((size_t)h.nbf5 + 2 * (size_t)h.nbf5 * h.nbf5 + 2 * (size_t)h.nn);
+    }
+    DONOF_CHECK(idle.ensure(ctx, sizeof(double) * per));
+    DONOF_CUDA(ctx, cudaMemsetAsync(idle.ptr, 0, sizeof(double) * per, bst));
+    struct Release {
+        donof_ctx* c;
+        DevBuf* b;
+        cudaStream_t s;
+        ~Release() {
+            cudaStreamSynchronize(s);
+            b->release(c);
+        }
+    } release{ctx, &idle, bst};
+    auto fits = [&](const Req& r, int j) {
+        const donof_batch::Shape& h = B->sh[j];
+        const donof_job* jb = r.r.job;
+        return jb->ctx != nullptr && jb->ctx->device == ctx->device && jb->b != nullptr &&
+               jb->precision == DONOF_PREC_FP64 && jb->nbf == h.nbf && jb->naux == h.naux &&
+               r.r.params.occ.nbf5 == h.nbf5 && r.r.params.occ.nalpha == h.nalpha && r.r.params.occ.nbeta == h.nbeta;
+    };
+    auto complete = [&](const std::shared_ptr<Req>& r, int status, const donof_energy_result* res) {
+        std::lock_guard<std::mutex> lk(q->mu);
+        r->status = status;
+        if (res) r->res = *res;
+        r->done = true;
+        q->cv_done.notify_all();
+    };
+    auto retire = [&](int j, int status) {
+        donof_energy_result res{};
+        int s = status;
+        if (s == DONOF_OK)
+            s = E[j]->finish(slot[j]->r.C_inout, slot[j]->r.gamma_inout, slot[j]->r.n_out, nullptr, &res);
+        complete(slot[j], s, s == DONOF_OK ? &res : nullptr);
+        slot[j].reset();
+        E[j].reset();
+    };
+    auto fail_all = [&](int status) {
+        for (int j = 0; j < nj; ++j)
+            if (slot[j]) {
+                complete(slot[j], status, nullptr);
+                slot[j].reset();
+                E[j].reset();
+            }
+        return status;
+    };
+    int method = -1;
+    for (;;) {
+        // ---- free slots take the oldest waiting request of their shape
+        std::vector<int> fresh;
+        {
+            std::unique_lock<std::mutex> lk(q->mu);
+            for (;;) {
+                method = q->method;
+                for (auto& r : q->all) {
+                    if (r->taken) continue;
+                    bool some = false;
+                    for (int j = 0; j < nj && !some; ++j) some = fits(*r, j);
+                    if (!some) {  // no slot of the batch has this request's shape
+                        r->taken = r->done = true;
+                        r->status = DONOF_ERR_ARG;
+                        q->cv_done.notify_all();
+                    }
+                }
+                for (int j = 0; j < nj; ++j) {
+                    if (slot[j]) continue;
+                    for (auto& r : q->all)
+                        if (!r->taken && fits(*r, j)) {
+                            r->taken = true;
+                            slot[j] = r;
+                            fresh.push_back(j);
+                            break;
+                        }
+                }
+                bool active = false, pending = false;
+                for (int j = 0; j < nj; ++j) active = active || (bool)slot[j];
+                for (auto& r : q->all) pending = pending || !r->taken;
+                if (active) break;
+                if (q->closed && !pending) return DONOF_OK;
+                q->cv.wait_for(lk, std::chrono::milliseconds(20));
+            }
+        }
+        // ---- bind the new requests' RI tensors and start their energy loops
+        bool rebound = false;
+        for (int j : fresh) {
+            // always rebind: a freed job's address may have been reused by this one
+            B->sh[j].job = slot[j]->r.job;
+            B->sh[j].b = slot[j]->r.job->b;
+            rebound = true;
+            prm[j] = slot[j]->r.params;
+            E[j].reset(new (std::nothrow) EnergyJob());
+            const int s = E[j] ? E[j]->setup(slot[j]->r.job, &prm[j], slot[j]->r.H, slot[j]->r.C_inout,
+                                             slot[j]->r.gamma_inout, nullptr)
+                               : DONOF_ERR_OOM;
+            if (s != DONOF_OK) retire(j, s);
+        }
+        if (rebound) {
+            const int s = upload_gemm_tables(B, bst);
+            if (s != DONOF_OK) return fail_all(s);
+        }
+        // ---- one outer iteration of every running request, the orbital steps grouped
+        bool any = false;
+        for (int j = 0; j < nj; ++j) {
+            donof_batch_item& it = items[j];
+            it.maxloop = 0;  // left out unless running
+            if (E[j] && !E[j]->done()) {
+                int s = E[j]->begin();
+                if (s == DONOF_OK && cudaStreamSynchronize(slot[j]->r.job->ctx->stream) != cudaSuccess) s = DONOF_ERR_CUDA;
+                if (s != DONOF_OK) {
+                    retire(j, s);
+                } else {
+                    it.n = E[j]->dev_n(); it.cj12 = E[j]->dev_cj(); it.ck12 = E[j]->dev_ck(); it.H = E[j]->dev_H();
+                    it.C = E[j]->dev_C();
+                    it.alpha = prm[j].alpha;
+                    it.threshgorb = prm[j].threshgorb;
+                    it.maxloop = prm[j].maxloop;
+                    any = true;
+                    continue;
+                }
+            }
+            const donof_batch::Shape& h = B->sh[j];
+            double* z = idle.as<double>() + ioff[j];
+            it.n = z; it.cj12 = z + h.nbf5; it.ck12 = z + h.nbf5 + (size_t)h.nbf5 * h.nbf5;
+            it.H = z + h.nbf5 + 2 * (size_t)h.nbf5 * h.nbf5;
+            it.C = const_cast<double*>(it.H) + h.nn;
+            it.alpha = 0.01;
+            it.threshgorb = 1.0;
+        }
+        if (any) {
+            int s = donof_batch_orbopt(B, method, items.data());
+            if (s != DONOF_OK) return fail_all(s);
+            std::vector<int> run;
+            for (int j = 0; j < nj; ++j) {
+                if (items[j].maxloop == 0 || !E[j]) continue;
+                prm[j].alpha = items[j].alpha;
+                prm[j].maxloop = items[j].maxloop;
+                s = E[j]->occ_fetch();
+                if (s != DONOF_OK) retire(j, s);
+                else run.push_back(j);
+            }
+            std::vector<int> st(run.size(), DONOF_OK);
+            {
+                std::atomic<size_t> next{0};
+                auto work = [&]() {
+                    for (size_t i = next.fetch_add(1); i < run.size(); i = next.fetch_add(1))
+                        st[i] = E[run[i]]->occ_solve();
+                };
+                const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+                const size_t nt = std::min<size_t>(run.size(), hw);
+                std::vector<std::thread> pool;
+                for (size_t k = 1; k < nt; ++k) pool.emplace_back(work);
+                work();
+                for (std::thread& th : pool) th.join();
+            }
+            for (size_t i = 0; i < run.size(); ++i) {
+                const int j = run[i];
+                s = st[i];
+                if (s == DONOF_OK) s = E[j]->end_iteration(items[j].E, items[j].nit);
+                if (s != DONOF_OK) retire(j, s);
+            }
+        }
+        // ---- converged (or out of iterations) requests return now; their slots free up
+        for (int j = 0; j < nj; ++j)
+            if (E[j] && E[j]->done()) retire(j, DONOF_OK);
+    }
 }
 
 }  // extern "C"

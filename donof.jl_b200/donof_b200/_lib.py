@@ -102,6 +102,12 @@ SIGNATURES = {
     "donof_batch_orbopt": (_i, [_vp, _i, _vp]),
     "donof_batch_lagrange2": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "donof_batch_energy": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "donof_batch_queue_create": (_i, [_vp]),
+    "donof_batch_queue_push": (_i, [_vp, _vp, _vp]),
+    "donof_batch_queue_close": (_i, [_vp]),
+    "donof_batch_queue_poll": (_i, [_vp, ct.c_ulonglong, _i, _vp, _vp, _vp]),
+    "donof_batch_queue_destroy": (_i, [_vp]),
+    "donof_batch_serve": (_i, [_vp, _vp]),
 }
 
 

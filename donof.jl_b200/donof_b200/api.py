@@ -422,6 +422,15 @@ class Batch:
             out.append((Cio[j], gio[j], ns[j], {f: getattr(res[j], f) for f, _ in _EnergyResult._fields_}))
         return out
 
+    def serve(self, queue: "BatchQueue") -> None:
+        """Continuous batching (donof_batch_serve): the batch's jobs are slots of
+        their shapes; requests pushed into ``queue`` (also from other threads while
+        this runs) take a free slot of their shape, every outer iteration advances
+        all running requests as grouped launches, and a request returns as soon as
+        it converges.  Returns once the queue is closed and every request has
+        finished."""
+        self.ctx.check(self.ctx.lib.donof_batch_serve(self.handle, queue.handle))
+
     def free(self) -> None:
         if getattr(self, "handle", None) and getattr(self.ctx, "handle", None):
             self.ctx.lib.donof_batch_destroy(self.handle)
@@ -546,3 +555,68 @@ def occ_cg(gamma, J_MO, K_MO, H_core, p: Param, g_abstol: float, max_iter: int =
     _lib.check(lib.donof_occ_cg(ct.byref(prm), _ptr(J), _ptr(K), _ptr(Hc), _ptr(x), float(g_abstol), int(max_iter),
                                 ct.byref(E), ct.byref(nit), ct.byref(ok)))
     return x, E.value, nit.value, bool(ok.value)
+
+
+class _BatchRequest(ct.Structure):
+    _fields_ = [("job", ct.c_void_p), ("params", _EnergyParams), ("H", ct.c_void_p), ("C_inout", ct.c_void_p),
+                ("gamma_inout", ct.c_void_p), ("n_out", ct.c_void_p)]
+
+
+class BatchQueue:
+    """Requests for ``Batch.serve`` (donof_batch_queue_*).  ``push`` copies the
+    inputs into arrays the queue owns until the request is collected."""
+
+    def __init__(self):
+        self.lib = _lib.load()
+        h = ct.c_void_p()
+        _lib.check(self.lib.donof_batch_queue_create(ct.byref(h)), None)
+        self.handle = h
+        self._keep = {}
+
+    def push(self, b: BTensor, H, C, gamma, p: Param, maxit: Optional[int] = None, order: bool = True) -> int:
+        prm = _EnergyParams()
+        prm.occ = _occ_params(p)
+        prm.orb_method = _lib.ORB_METHODS[p.orb_method]
+        prm.maxit, prm.maxloop, prm.alpha = int(maxit or p.maxit), int(p.maxloop), float(p.alpha)
+        prm.threshgorb, prm.threshgocc, prm.threshen = float(p.threshgorb), float(p.threshgocc), float(p.threshen)
+        prm.order_subspaces = int(bool(order) and p.ipnof > 4)
+        prm.occ_device = int(bool(getattr(p, "occ_device", False)))
+        Hf = _f64(H)
+        Cio = np.array(_f64(C), copy=True, order="F")
+        gio = np.array(gamma, dtype=np.float64, copy=True)
+        n = np.zeros(p.nbf5)
+        req = _BatchRequest(b.handle, prm, _ptr(Hf), _ptr(Cio), _ptr(gio), _ptr(n))
+        t = ct.c_ulonglong()
+        _lib.check(self.lib.donof_batch_queue_push(self.handle, ct.byref(req), ct.byref(t)), None)
+        self._keep[t.value] = (b, Hf, Cio, gio, n)
+        return t.value
+
+    def close(self) -> None:
+        _lib.check(self.lib.donof_batch_queue_close(self.handle), None)
+
+    def poll(self, ticket: int, wait: bool = False):
+        """None while running; else (C, gamma, n, result fields) -- or raises the
+        request's error."""
+        done, status, res = ct.c_int(), ct.c_int(), _EnergyResult()
+        _lib.check(self.lib.donof_batch_queue_poll(self.handle, ct.c_ulonglong(ticket), 1 if wait else 0,
+                                                   ct.byref(done), ct.byref(status), ct.byref(res)), None)
+        if not done.value:
+            return None
+        _, _, Cio, gio, n = self._keep[ticket]
+        if status.value != 0:
+            raise _lib.DonofError(status.value, f"batch request {ticket} failed")
+        return Cio, gio, n, {f: getattr(res, f) for f, _ in _EnergyResult._fields_}
+
+    def wait(self, ticket: int):
+        return self.poll(ticket, wait=True)
+
+    def free(self) -> None:
+        if getattr(self, "handle", None):
+            self.lib.donof_batch_queue_destroy(self.handle)
+        self.handle = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.free()
+        except Exception:
+            pass

@@ -20,6 +20,7 @@ orbital state and the partial sums (see ``footprint``).
 """
 from __future__ import annotations
 
+import copy
 import functools
 import itertools
 import threading
@@ -304,7 +305,8 @@ class Server:
     def __init__(self, device: int = 0, budget_bytes: Optional[int] = None, max_inflight: int = 8,
                  max_bypass: int = 4, executor: Callable[[Request, int], Result] = run_energy,
                  cta_share: Optional[int] = None, group_max: int = 0,
-                 group_executor: Callable[[List[Request], int], List[Result]] = run_energy_group):
+                 group_executor: Callable[[List[Request], int], List[Result]] = run_energy_group,
+                 continuous_slots: int = 0):
         if budget_bytes is None:
             import torch
             free, _ = torch.cuda.mem_get_info(device)
@@ -327,6 +329,10 @@ class Server:
         self._bytes: Dict[int, int] = {}
         self._threads: List[threading.Thread] = []
         self._closed = False
+        # continuous batching (continuous_slots > 0): the FP64 jobs go to one batch
+        # per shape, `continuous_slots` slots each, served by donof_batch_serve
+        self.continuous_slots = int(continuous_slots)
+        self._buckets: Dict[tuple, "_Bucket"] = {}
 
     # ---- client side
     def submit(self, req: Request) -> int:
@@ -339,6 +345,10 @@ class Server:
             if self._closed:
                 raise RuntimeError("server is shut down")
             t = next(self._tickets)
+            if self.continuous_slots > 0 and resolve_precision(req.precision, nbf, req.p.nbf5, naux) == "fp64":
+                self._submit_t[t] = time.perf_counter()
+                self._bucket_locked(req).submit(t, req)
+                return t
             self.admission.push(t, nb)
             self._pending[t] = req
             self._submit_t[t] = time.perf_counter()
@@ -379,9 +389,29 @@ class Server:
     def shutdown(self, wait: bool = True) -> None:
         with self._lock:
             self._closed = True
+            buckets = list(self._buckets.values())
+        for bk in buckets:
+            bk.close()
         if wait:
             for th in list(self._threads):
                 th.join()
+            for bk in buckets:
+                bk.join()
+
+    def _bucket_locked(self, req: Request) -> "_Bucket":
+        p = req.p
+        key = (p.nbf, p.nbfaux, p.nbf5, p.nalpha, p.nbeta, p.orb_method)
+        bk = self._buckets.get(key)
+        if bk is None:
+            bk = self._buckets[key] = _Bucket(self, self.continuous_slots)
+        return bk
+
+    def _finish(self, t: int, r: Result) -> None:
+        with self._lock:
+            r.ticket = t
+            r.t_submit = self._submit_t.pop(t)
+            self._results[t] = r
+            self._lock.notify_all()
 
     def __enter__(self):
         return self
@@ -443,6 +473,68 @@ class Server:
             self.admission.release(self._bytes.pop(t))
             self._admit_locked()
             self._lock.notify_all()
+
+
+class _Bucket:
+    """The FP64 jobs of one shape under continuous batching: a batch of `slots`
+    slots on its own context (stream) serves a queue (donof_batch_serve); each
+    request uploads its RI tensor on a context of its own, pushes itself and
+    waits for its result, so no context is used by two threads at once."""
+
+    def __init__(self, server: "Server", slots: int):
+        from . import api
+        self.server, self.slots = server, slots
+        self.ctx = api.Context(server.device, torch_stream=False)
+        # the batch's grouped persistent kernels take a share of the SMs, as a served job does
+        self.ctx.set_cta_limit(cta_share_for(server.admission.max_inflight, server.device))
+        self.queue = api.BatchQueue()
+        self.batch = None
+        self.ready = threading.Event()   # the batch exists (made from the first request)
+        self.lock = threading.Lock()
+        self.thread = None
+
+    def submit(self, t: int, req: Request) -> None:
+        th = threading.Thread(target=self._request, args=(t, req), daemon=True)
+        self.server._threads.append(th)
+        th.start()
+
+    def _request(self, t: int, req: Request) -> None:
+        from . import api, gnof
+        t0 = time.perf_counter()
+        ctx = b = None
+        try:
+            ctx = api.Context(self.server.device, torch_stream=False)
+            b = api.eris_to_gpu(req.b, "fp64", ctx)
+            p = copy.copy(req.p)
+            gamma = gnof.guess_gamma(p) if req.gamma is None else req.gamma
+            with self.lock:
+                if self.batch is None:  # every slot starts bound to the first request's tensor
+                    self.batch = api.Batch([b] * self.slots, [p] * self.slots, self.ctx)
+                    self.thread = threading.Thread(target=self.batch.serve, args=(self.queue,), daemon=True)
+                    self.thread.start()
+            ticket = self.queue.push(b, req.H, req.C, gamma, p, maxit=req.maxit)
+            C, g, n, f = self.queue.wait(ticket)
+            r = Result(ticket=t, E_elec=f["E_elec"], E_tot=f["E_elec"] + req.E_nuc, converged=bool(f["converged"]),
+                       iterations=f["iterations"], C=C, n=n)
+        except Exception as e:  # the job fails, the server goes on
+            r = Result(ticket=t, error=f"{type(e).__name__}: {e}")
+        finally:
+            if b is not None:
+                b.free()
+            if ctx is not None:
+                ctx.close()
+        r.t_start, r.t_done, r.tag = t0, time.perf_counter(), req.tag
+        self.server._finish(t, r)
+
+    def close(self) -> None:
+        self.queue.close()
+
+    def join(self) -> None:
+        if self.thread is not None:
+            self.thread.join()
+        if self.batch is not None:
+            self.batch.free()
+        self.ctx.close()
 
 
 def percentiles(values, qs=(50, 99)) -> dict:

@@ -363,6 +363,40 @@ int donof_batch_energy(donof_batch* batch, donof_energy_params* params, const do
                        double* const* C_inout, double* const* gamma_inout, double* const* n_out,
                        donof_energy_result* results);
 
+/* --- continuous batching at the step level ---------------------------------
+ * donof_batch_serve runs donof_batch_energy's alternation over a stream of
+ * requests: the batch's jobs are slots; a request whose job has a slot's shape
+ * (nbf, naux of its RI tensor; nbf5, nalpha, nbeta of its parameters) takes
+ * that slot when it frees, so that every outer iteration advances all running
+ * requests as grouped launches (one per stage of a gradient step) and a request
+ * that converges returns at once while the others go on.  Requests are pushed
+ * into a queue (any host thread, also while donof_batch_serve runs) and taken in
+ * arrival order, the oldest request that fits a free slot first;
+ * donof_batch_serve returns once the queue is closed and every request that a
+ * slot can take has finished (a request that fits no slot finishes with
+ * DONOF_ERR_ARG).  Each request gives bit-for-bit what donof_energy gives it
+ * alone.  Every request of one queue uses the same orb_method.  The request's
+ * host arrays must stay valid until it is done (donof_batch_queue_poll).     */
+typedef struct donof_batch_queue donof_batch_queue;
+typedef struct {
+    donof_job* job;                 /* FP64 RI tensor of this request (same device as the batch) */
+    donof_energy_params params;     /* copied at push; alpha, maxloop as for donof_energy */
+    const double* H;                /* host nbf x nbf */
+    double* C_inout;                /* host nbf x nbf */
+    double* gamma_inout;            /* host nv */
+    double* n_out;                  /* host nbf5, or NULL */
+} donof_batch_request;
+int donof_batch_queue_create(donof_batch_queue** queue);
+int donof_batch_queue_push(donof_batch_queue* queue, const donof_batch_request* request,
+                           unsigned long long* ticket);
+int donof_batch_queue_close(donof_batch_queue* queue);
+/* done = 1 once the request finished; then *status is its outcome and *result
+ * its energy result (wait != 0: block until done).                           */
+int donof_batch_queue_poll(donof_batch_queue* queue, unsigned long long ticket, int wait, int* done,
+                           int* status, donof_energy_result* result);
+int donof_batch_queue_destroy(donof_batch_queue* queue);
+int donof_batch_serve(donof_batch* batch, donof_batch_queue* queue);
+
 /* --- serving ------------------------------------------------------------------
  * Continuous batching of energy jobs on one GPU behind a thread-safe queue:
  * jobs are admitted while their device footprint fits the budget (0: 85 % of

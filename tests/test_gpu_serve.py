@@ -102,3 +102,35 @@ def test_grouped_server_gives_each_job_its_alone_result():
         assert a.converged and g.converged
         assert g.E_elec == a.E_elec and g.iterations == a.iterations
         assert np.array_equal(g.n, a.n) and np.array_equal(g.C, a.C)
+
+
+def test_continuous_server_gives_each_job_its_alone_result():
+    """continuous_slots: FP64 jobs of one shape share a batch whose slots are
+    refilled as jobs converge (donof_batch_serve), jobs of other shapes run in
+    their own batches, mixed jobs on their own streams; each FP64 job's energy,
+    occupations and orbitals are bit-for-bit those it gets served alone."""
+    import copy
+
+    shapes = [(24, 58, 5, 3), (34, 80, 5, 5), (24, 58, 5, 3), (24, 58, 5, 3), (34, 80, 5, 5), (24, 58, 5, 3)]
+    wls = [workload.molecule_like(nbf=a, naux=b, nbeta=c, ncwo=e, seed=80 + i, two_e_scale=0.2)
+           for i, (a, b, c, e) in enumerate(shapes)]
+    for wl in wls:
+        wl.p.threshgorb = wl.p.threshgocc = 1e-5
+        wl.p.threshen = 1e-6
+    req = lambda wl, i, prec="fp64": Request(H=wl.H, b=wl.b, C=wl.C, p=copy.deepcopy(wl.p), gamma=wl.gamma,
+                                             precision=prec, maxit=500, tag=i)
+    with Server(max_inflight=1) as s:
+        alone = [s.wait(s.submit(req(wl, i)), timeout=600) for i, wl in enumerate(wls)]
+    mixed = workload.molecule_like(nbf=24, naux=40, nbeta=3, ncwo=3, seed=4)
+    mixed.p.threshgorb, mixed.p.threshgocc, mixed.p.threshen = 1e-4, 1e-4, 1e-8
+    with Server(max_inflight=2, continuous_slots=2) as s:
+        tickets = [s.submit(req(wl, i)) for i, wl in enumerate(wls)]
+        tm = s.submit(req(mixed, 99, "mixed_refined"))
+        served = [s.wait(t, timeout=600) for t in tickets]
+        rm = s.wait(tm, timeout=600)
+    assert rm.error is None and rm.converged
+    for a, g in zip(alone, served):
+        assert a.error is None and g.error is None, (a.error, g.error)
+        assert a.converged and g.converged
+        assert g.E_elec == a.E_elec and g.iterations == a.iterations
+        assert np.array_equal(g.n, a.n) and np.array_equal(g.C, a.C)
