@@ -46,6 +46,92 @@ __global__ void __launch_bounds__(256, 4) build_w_kernel(const double* __restric
     for (long long t = blockIdx.x; t < tiles; t += gridDim.x) wbuild::tile(bpq, ck12, tv, nbf5, naux, W, t, tb);
 }
 
+// W in one pass for nbf5 <= FUSED_W_MAX: the tiles of build_w_kernel, where a
+// diagonal tile (b0 == q0) first computes its own n'_b d_b^l + t_b^l for its 32
+// b and LT aux indices -- one thread per (b, l), summing over q in the order of
+// wbuild::diag_unit, so W is bit-for-bit the two-kernel W (the grouped path of
+// batch.cu still builds it in two passes and must agree with this one).
+constexpr int FUSED_W_MAX = 256;
+
+__global__ void __launch_bounds__(256, 4) build_w_fused_kernel(const double* __restrict__ bpq,
+                                                            const double* __restrict__ n,
+                                                            const double* __restrict__ cj12,
+                                                            const double* __restrict__ ck12, int nbf5, int naux,
+                                                            int nalpha, int nbeta, double* __restrict__ W) {
+    __shared__ double tb[wbuild::LT][32][33];
+    __shared__ double sd[wbuild::LT * FUSED_W_MAX];
+    __shared__ double stv[wbuild::LT][32];
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const long long n55 = (long long)nbf5 * nbf5, Kt = (long long)nbf5 * naux;
+    const int nt = (nbf5 + 31) / 32;
+    const long long tiles = wbuild::tiles(nbf5, naux);
+    for (long long t = blockIdx.x; t < tiles; t += gridDim.x) {
+        const int b0 = (int)(t % nt) * 32, q0 = (int)((t / nt) % nt) * 32;
+        const long long l0 = (t / ((long long)nt * nt)) * wbuild::LT;
+        const int b = b0 + tx;
+        const bool diag = (b0 == q0);
+        if (diag) {
+            __syncthreads();  // the previous tile's reads of sd are done
+            for (int i = threadIdx.x; i < wbuild::LT * nbf5; i += blockDim.x) {
+                const int k = i / nbf5, q = i - k * nbf5;
+                const long long l = l0 + k;
+                sd[i] = (l < naux) ? bpq[n55 * l + (long long)q * (nbf5 + 1)] : 0.0;
+            }
+            __syncthreads();
+            if (threadIdx.x < 32 * wbuild::LT) {
+                const int k = threadIdx.x >> 5, bb = b0 + tx;
+                const long long l = l0 + k;
+                if (l < naux && bb < nbf5) {
+                    const double* d = sd + k * nbf5;
+                    double s = 0.0;
+                    for (int q = 0; q < nbf5; ++q) s += cj12[bb + (long long)nbf5 * q] * d[q];
+                    const bool dj = (nbeta > 0) && (bb < nbeta || bb >= nalpha);
+                    stv[k][tx] = (dj ? n[bb] * d[bb] : 0.0) + s;
+                }
+            }
+        }
+        double ck[4], v[wbuild::LT][4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const int q = q0 + ty + 8 * r;
+            ck[r] = (b < nbf5 && q < nbf5) ? ck12[b + (long long)nbf5 * q] : 0.0;
+        }
+#pragma unroll
+        for (int k = 0; k < wbuild::LT; ++k) {
+            const long long l = l0 + k;
+            const double* B = bpq + n55 * l;
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const int q = q0 + ty + 8 * r;
+                v[k][r] = (l < naux && b < nbf5 && q < nbf5) ? B[b + (long long)nbf5 * q] : 0.0;
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < wbuild::LT; ++k) {
+            const long long l = l0 + k;
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const int q = q0 + ty + 8 * r;
+                double w = -ck[r] * v[k][r];
+                if (diag && q == b && l < naux && b < nbf5) w += stv[k][tx];
+                tb[k][ty + 8 * r][tx] = w;  // [l - l0][q - q0][b - b0]
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < wbuild::LT; ++k) {
+            const long long l = l0 + k;
+            if (l >= naux) break;
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const int q = q0 + tx, bb = b0 + ty + 8 * r;
+                if (bb < nbf5 && q < nbf5) W[q + (long long)nbf5 * l + Kt * bb] = tb[k][tx][ty + 8 * r];
+            }
+        }
+    }
+}
+
 // elag[a, b] = n_b H_mat[a, b] for b < nbf5 (the 2ndH/dy_ab term,
 // src/utils.jl:39), columns >= nbf5 set to zero.
 __global__ void elag_init_kernel(const double* __restrict__ Hmat, const double* __restrict__ n,
@@ -107,6 +193,26 @@ __global__ void hcore_kernel(const double* __restrict__ C, const double* __restr
     if (lane == 0) Hcore[warp] = s;
 }
 
+// W of every aux index into W (Kt * nbf5 values; W + Kt * nbf5 holds the Kt
+// diagonal terms when they are built in a pass of their own).
+int build_w(donof_ctx* ctx, cudaStream_t st, const double* bpq, const double* n, const double* cj12,
+            const double* ck12, int nbf5, int naux, int nalpha, int nbeta, double* W) {
+    long long blocks = wbuild::tiles(nbf5, naux);
+    if (blocks > 16LL * ctx->sm_count) blocks = 16LL * ctx->sm_count;
+    if (nbf5 <= FUSED_W_MAX) {
+        build_w_fused_kernel<<<(int)blocks, 256, 0, st>>>(bpq, n, cj12, ck12, nbf5, naux, nalpha, nbeta, W);
+        count_launch();
+    } else {
+        double* tv = W + (size_t)nbf5 * naux * nbf5;  // n'_b d_b^l + t_b^l (Kt values)
+        long long dblocks = wbuild::diag_units(nbf5, naux);
+        if (dblocks > 8LL * ctx->sm_count) dblocks = 8LL * ctx->sm_count;
+        w_diag_kernel<<<(int)dblocks, 256, 0, st>>>(bpq, n, cj12, nbf5, naux, nalpha, nbeta, tv); count_launch();
+        build_w_kernel<<<(int)blocks, 256, 0, st>>>(bpq, ck12, tv, nbf5, naux, W); count_launch();
+    }
+    DONOF_CUDA(ctx, cudaGetLastError());
+    return DONOF_OK;
+}
+
 int grid_for(long long total, int threads, int sm) {
     long long b = (total + threads - 1) / threads;
     if (b > 8LL * sm) b = 8LL * sm;
@@ -162,17 +268,7 @@ int lagrange2_f64(donof_job* job, cudaStream_t st, const double* C, const double
 
     DONOF_CHECK(job->W.ensure(ctx, sizeof(double) * (size_t)Kt * (nbf5 + 1)));
     double* W = job->W.as<double>();
-    double* tv = W + (size_t)Kt * nbf5;  // n'_b d_b^l + t_b^l (Kt values)
-    {
-        const double* bpq = job->bpq.as<double>();
-        long long blocks = wbuild::diag_units(nbf5, naux);
-        if (blocks > 8LL * ctx->sm_count) blocks = 8LL * ctx->sm_count;
-        w_diag_kernel<<<(int)blocks, 256, 0, st>>>(bpq, n, cj12, nbf5, naux, nalpha, nbeta, tv); count_launch();
-        blocks = wbuild::tiles(nbf5, naux);
-        if (blocks > 16LL * ctx->sm_count) blocks = 16LL * ctx->sm_count;
-        build_w_kernel<<<(int)blocks, 256, 0, st>>>(bpq, ck12, tv, nbf5, naux, W); count_launch();
-        DONOF_CUDA(ctx, cudaGetLastError());
-    }
+    DONOF_CHECK(build_w(ctx, st, job->bpq.as<double>(), n, cj12, ck12, nbf5, naux, nalpha, nbeta, W));
 
     // Y = sum_{q,l} tmp[m, q + nbf5*l] W[q + nbf5*l, b], left as split-K partials
     const double* ypart = nullptr;
@@ -196,17 +292,7 @@ int lagrange2_partial_f64(donof_job* job, cudaStream_t st, const double* C, cons
     DONOF_CHECK(transforms_f64(job, st, C, nbf5));
     DONOF_CHECK(job->W.ensure(ctx, sizeof(double) * (size_t)Kt * (nbf5 + 1)));
     double* W = job->W.as<double>();
-    double* tv = W + (size_t)Kt * nbf5;
-    {
-        const double* bpq = job->bpq.as<double>();
-        long long blocks = wbuild::diag_units(nbf5, naux);
-        if (blocks > 8LL * ctx->sm_count) blocks = 8LL * ctx->sm_count;
-        w_diag_kernel<<<(int)blocks, 256, 0, st>>>(bpq, n, cj12, nbf5, naux, nalpha, nbeta, tv); count_launch();
-        blocks = wbuild::tiles(nbf5, naux);
-        if (blocks > 16LL * ctx->sm_count) blocks = 16LL * ctx->sm_count;
-        build_w_kernel<<<(int)blocks, 256, 0, st>>>(bpq, ck12, tv, nbf5, naux, W); count_launch();
-        DONOF_CUDA(ctx, cudaGetLastError());
-    }
+    DONOF_CHECK(build_w(ctx, st, job->bpq.as<double>(), n, cj12, ck12, nbf5, naux, nalpha, nbeta, W));
     const double* ypart = nullptr;
     int nparts = 1;
     DONOF_CHECK(gemm_f64_partials(ctx, st, false, true, nbf, nbf5, (int)Kt, job->tmp.as<double>(), nbf, W, Kt,
