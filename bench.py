@@ -465,6 +465,53 @@ def serving_bench(d, torch):
 BATCH = dict(count=64, kmax=8, seed=11)
 
 
+def batched_mixed_bench(d, torch, ctx, steps, warmup, method):
+    """The jobs of the water-cluster batch that fit the fused mixed kernel
+    ((H2O)_k with k <= 3: nbf <= 72, nbf5 <= 60) advanced together, the grouped
+    step with the FP64 Lagrangian against the grouped step with the mixed one
+    (donof_batch_set_precision: every job's fused tcgen05 kernel in one grouped
+    launch)."""
+    from donof_b200 import workload
+    jobs = [(j, k, wl) for j, (k, wl) in enumerate(workload.water_clusters(**BATCH)) if k <= 3]
+    bts, ins = [], []
+    for j, k, wl in jobs:
+        tb = workload.b_device(wl.p.nbf, wl.p.nbfaux, seed=BATCH["seed"] * 7919 + j)
+        bts.append(d.eris_to_gpu(tb, "mixed", ctx))
+        ins.append(dict(p=wl.p, C=d.to_device(wl.C), H=d.to_device(wl.H), n=d.to_device(wl.n),
+                        cj=d.to_device(wl.cj12), ck=d.to_device(wl.ck12)))
+    nj = len(jobs)
+    cols = lambda key: [x[key] for x in ins]
+    out = {"workload": f"the {nj} jobs of the 64-job water-cluster batch with k <= 3 (nbf 24-72, nbf5 20-60), "
+                       f"{steps} orbital steps each", "unit": "job orbital-gradient steps/s"}
+    Es = {}
+    for prec in ("fp64", "mixed"):
+        batch = d.Batch(bts, [x["p"] for x in ins], ctx)
+        batch.set_precision(prec)
+
+        def grouped(ml):
+            Cs = [x["C"].clone() for x in ins]
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            res = batch.orbopt(method, cols("n"), cols("cj"), cols("ck"), cols("H"), Cs, [0.01] * nj, [ml] * nj,
+                               [0.0] * nj)
+            e1.record()
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1) / 1e3, res
+
+        grouped(warmup)
+        tg, res = grouped(steps)
+        Es[prec] = [r[0] for r in res]
+        out[prec] = {"value": nj * steps / tg, "ms_per_step": 1e3 * tg / steps}
+        batch.free()
+    out["mixed"]["path"] = "donof_batch_orbopt with donof_batch_set_precision(MIXED)"
+    out["speedup_mixed_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    out["max_rel_dE_mixed_vs_fp64"] = max(abs(a - b) / max(1.0, abs(b)) for a, b in zip(Es["mixed"], Es["fp64"]))
+    for b in bts:
+        b.free()
+    return out
+
+
 def batched_bench(d, torch, ctx, steps, warmup, method, sequential_arm=True, spec=None):
     """Orbital-gradient steps/s of a batch of uneven jobs advanced together (one
     grouped launch per stage of a step, the loop as one captured graph) against
@@ -823,6 +870,7 @@ def main():
     batched = batched_e = None
     if rank == 0 and world == 1 and not args.no_batched:
         batched = batched_bench(d, torch, ctx, args.steps, args.warmup, args.method)
+        batched["mixed_subset"] = batched_mixed_bench(d, torch, ctx, args.steps, args.warmup, args.method)
         batched_e = batched_energies_bench(d, torch, ctx)
 
     cpu = None

@@ -296,6 +296,12 @@ struct donof_batch {
     };
     std::vector<Launch> launches[NSTAGE];
     bool tuned = false;
+    // mixed form (donof_batch_set_precision): the fused tcgen05 kernel over every job
+    int precision = DONOF_PREC_FP64;
+    DevBuf mix;                          // per job: Cs, n32, cj32, ck32, Y partials; the split table
+    std::vector<MixedGroupJob> mjobs;
+    MixedSplitJob* d_split = nullptr;
+    int max_ldk = 0;
     // captured loop
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -408,6 +414,13 @@ int grid_units(int total, int per_sm, int sm) {
 // The Lagrangian of every running job at C_new: T1, T2, W, Y, tail (energy into the job state).
 int lagrangian(donof_batch* B, cudaStream_t st) {
     donof_ctx* ctx = B->ctx;
+    if (B->precision == DONOF_PREC_MIXED) {
+        // every job's fused T1, T2, W, Y on its CTA range (bf16 split products, FP32 Y
+        // partials), then the grouped FP64 tail on those partials
+        DONOF_CHECK(split_c_grouped(ctx, st, B->d_split, B->nj, B->max_ldk));
+        DONOF_CHECK(launch_mixed_grouped(ctx, st, B->mjobs.data(), B->nj));
+        return tail_grouped(ctx, st, B->d_tail, B->nj, B->d_tstate, B->tail_grid);
+    }
     DONOF_CHECK(run_stage(B, st, ST_T1));
     DONOF_CHECK(run_stage(B, st, ST_T2));
     b_wdiag_kernel<<<grid_units(B->pre_total[2], 4, ctx->sm_count), 256, 0, st>>>(B->d_jobs, B->d_pre[2], B->nj);
@@ -500,6 +513,11 @@ int upload_call_tables(donof_batch* B, cudaStream_t st, const donof_batch_item* 
         T.state = static_cast<char*>(B->d_tstate) + (size_t)GROUP_STATE_BYTES * j;
         T.skip = &B->d_state[j].stopped;
         T.nbf = h.nbf; T.nbf5 = h.nbf5; T.part_f32 = 0; T.nparts = h.splits; T.cta0 = t0[j]; T.ctas = tn[j];
+        if (B->precision == DONOF_PREC_MIXED) {
+            T.part = B->mjobs[j].ypart;
+            T.part_f32 = 1;
+            T.nparts = B->mjobs[j].ctas;
+        }
     }
     DONOF_CUDA(ctx, cudaMemcpyAsync(B->d_jobs, bj.data(), sizeof(BJob) * nj, cudaMemcpyHostToDevice, st));
     DONOF_CUDA(ctx, cudaMemcpyAsync(B->d_rot, rj.data(), sizeof(RotJob) * nj, cudaMemcpyHostToDevice, st));
@@ -604,6 +622,12 @@ int start_call(donof_batch* B, cudaStream_t st, const donof_batch_item* items, c
     donof_ctx* ctx = B->ctx;
     DONOF_CHECK(upload_call_tables(B, st, items, hs, true));
     if (!B->tuned) DONOF_CHECK(autotune(B, st));
+    if (B->precision == DONOF_PREC_MIXED)
+        for (int j = 0; j < B->nj; ++j) {
+            MixedGroupJob& g = B->mjobs[j];
+            DONOF_CHECK(prep_coef(B->ctx, st, items[j].n, items[j].cj12, items[j].ck12, g.nbf5,
+                                  const_cast<float*>(g.n32), const_cast<float*>(g.cj32), const_cast<float*>(g.ck32)));
+        }
     DONOF_CUDA(ctx, cudaMemsetAsync(B->mvv, 0, sizeof(double) * B->mvv_doubles, st));
     b_copy_kernel<<<grid_units(B->pre_total[1], 4, ctx->sm_count), 256, 0, st>>>(B->d_jobs, B->d_pre[1], B->nj,
                                                                                COPY_IN_TO_NEW);
@@ -824,6 +848,84 @@ int donof_batch_create(donof_ctx* ctx, int count, const donof_batch_shape* shape
     return DONOF_OK;
 }
 
+int donof_batch_set_precision(donof_batch* B, int precision) {
+    if (!B) return DONOF_ERR_ARG;
+    donof_ctx* ctx = B->ctx;
+    if (precision == DONOF_PREC_FP64) {
+        B->precision = precision;
+        B->graph_method = -1;  // the captured loop is taken again
+        return DONOF_OK;
+    }
+    if (precision != DONOF_PREC_MIXED) {
+        set_error(ctx, "donof_batch_set_precision: unknown precision %d", precision);
+        return DONOF_ERR_ARG;
+    }
+    const int nj = B->nj;
+    for (int j = 0; j < nj; ++j) {
+        const donof_batch::Shape& h = B->sh[j];
+        if (h.job->b16hi == nullptr) {
+            set_error(ctx, "donof_batch_set_precision: job %d holds no bf16 split of b (upload it as mixed)", j);
+            return DONOF_ERR_ARG;
+        }
+        if (!mixed_fused_fits(h.nbf, h.nbf5)) {
+            set_error(ctx, "donof_batch_set_precision: job %d (nbf %d, nbf5 %d) exceeds the fused mixed kernel "
+                           "(nbf <= 256, nbf5 <= 64)", j, h.nbf, h.nbf5);
+            return DONOF_ERR_ARG;
+        }
+    }
+    DONOF_CUDA(ctx, cudaSetDevice(ctx->device));
+    // CTAs per job in proportion to its b (nbf^2 naux), at least one, about one wave in all
+    std::vector<double> w(nj);
+    double wsum = 0.0;
+    for (int j = 0; j < nj; ++j) wsum += (w[j] = (double)B->sh[j].nbf * B->sh[j].nbf * B->sh[j].naux);
+    const int G = ctx_ctas(ctx) > nj ? ctx_ctas(ctx) : nj;
+    std::vector<int> ctas(nj);
+    for (int j = 0; j < nj; ++j) {
+        int c = (int)(w[j] / wsum * (G - nj)) + 1;
+        if (c > B->sh[j].naux) c = B->sh[j].naux;
+        ctas[j] = c;
+    }
+    size_t off = 0;
+    auto take = [&](size_t bytes) { size_t o = off; off += (bytes + 255) / 256 * 256; return o; };
+    std::vector<size_t> o_cs(nj), o_n(nj), o_cj(nj), o_ck(nj), o_y(nj);
+    int max_ldk = 0;
+    for (int j = 0; j < nj; ++j) {
+        const donof_batch::Shape& h = B->sh[j];
+        const int ldk = mixed_ldk(h.nbf);
+        if (ldk > max_ldk) max_ldk = ldk;
+        o_cs[j] = take(2 * (size_t)ldk * 128);
+        o_n[j] = take(sizeof(float) * 64);
+        o_cj[j] = take(sizeof(float) * 64 * 64);
+        o_ck[j] = take(sizeof(float) * 64 * 64);
+        o_y[j] = take(sizeof(float) * (size_t)ctas[j] * h.nbf * h.nbf5);
+    }
+    const size_t o_split = take(sizeof(MixedSplitJob) * nj);
+    DONOF_CHECK(B->mix.ensure(ctx, off));
+    char* base = B->mix.as<char>();
+    B->mjobs.resize(nj);
+    std::vector<MixedSplitJob> sj(nj);
+    for (int j = 0; j < nj; ++j) {
+        const donof_batch::Shape& h = B->sh[j];
+        MixedGroupJob& g = B->mjobs[j];
+        g.job = h.job;
+        g.nbf5 = h.nbf5; g.nalpha = h.nalpha; g.nbeta = h.nbeta; g.ctas = ctas[j];
+        g.cs = base + o_cs[j];
+        g.n32 = reinterpret_cast<float*>(base + o_n[j]);
+        g.cj32 = reinterpret_cast<float*>(base + o_cj[j]);
+        g.ck32 = reinterpret_cast<float*>(base + o_ck[j]);
+        g.ypart = reinterpret_cast<float*>(base + o_y[j]);
+        sj[j] = MixedSplitJob{B->pt[j].Cnew, g.cs, h.nbf, h.nbf5, mixed_ldk(h.nbf), 0};
+    }
+    B->d_split = reinterpret_cast<MixedSplitJob*>(base + o_split);
+    B->max_ldk = max_ldk;
+    DONOF_CUDA(ctx, cudaMemcpyAsync(B->d_split, sj.data(), sizeof(MixedSplitJob) * nj, cudaMemcpyHostToDevice,
+                                    ctx->stream));
+    DONOF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    B->precision = precision;
+    B->graph_method = -1;  // the captured loop is taken again
+    return DONOF_OK;
+}
+
 int donof_batch_destroy(donof_batch* B) {
     if (!B) return DONOF_OK;
     donof_ctx* ctx = B->ctx;
@@ -835,13 +937,14 @@ int donof_batch_destroy(donof_batch* B) {
     B->tab.release(ctx);
     B->ypbuf.release(ctx);
     B->arena.release(ctx);
+    B->mix.release(ctx);
     cudaStreamSynchronize(ctx->stream);
     delete B;
     return DONOF_OK;
 }
 
 size_t donof_batch_device_bytes(const donof_batch* B) {
-    return B ? B->arena.bytes + B->tab.bytes + B->ypbuf.bytes : 0;
+    return B ? B->arena.bytes + B->tab.bytes + B->ypbuf.bytes + B->mix.bytes : 0;
 }
 
 int donof_batch_lagrange2(donof_batch* B, const donof_batch_item* items, double* const* elag, double* const* H_mat,
@@ -1157,6 +1260,10 @@ int donof_batch_energy(donof_batch* B, donof_energy_params* params, const double
 int donof_batch_serve(donof_batch* B, donof_batch_queue* q) {
     if (!B || !q) return DONOF_ERR_ARG;
     donof_ctx* ctx = B->ctx;
+    if (B->precision != DONOF_PREC_FP64) {
+        set_error(ctx, "donof_batch_serve: continuous batching runs the FP64 form");
+        return DONOF_ERR_STATE;
+    }
     DONOF_CUDA(ctx, cudaSetDevice(ctx->device));
     cudaStream_t bst = batch_stream(B);
     if (!bst) {

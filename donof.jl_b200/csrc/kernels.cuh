@@ -128,6 +128,28 @@ int lagrange2_mixed(donof_job* job, cudaStream_t st, const double* C, const doub
 int jkh_mo_mixed(donof_job* job, cudaStream_t st, const double* C, const double* H, int nbf5,
                  double* J, double* K, double* Hcore);
 
+// Grouped form of the fused mixed kernel (mixed.cu) for a batch: each job's
+// Y partials (FP32, one nbf x nbf5 block per CTA of its range) from its bf16
+// split of b and its Cs / FP32 coefficients; jobs must fit the fused kernel.
+struct MixedGroupJob {
+    donof_job* job;
+    int nbf5, nalpha, nbeta, ctas;
+    void* cs;                        // bf16 Cs (mixed_ldk(nbf) x 128)
+    const float *n32, *cj32, *ck32;  // prep_coef outputs
+    float* ypart;                    // ctas x nbf x nbf5
+};
+struct MixedSplitJob {               // device table entry of split_c_grouped
+    const double* C;
+    void* cs;
+    int nbf, nbf5, ldk, pad;
+};
+bool mixed_fused_fits(int nbf, int nbf5);
+int mixed_ldk(int nbf);
+int launch_mixed_grouped(donof_ctx* ctx, cudaStream_t st, const MixedGroupJob* jobs, int njobs);
+int split_c_grouped(donof_ctx* ctx, cudaStream_t st, const MixedSplitJob* d_jobs, int njobs, int max_ldk);
+int prep_coef(donof_ctx* ctx, cudaStream_t st, const double* n, const double* cj12, const double* ck12, int nbf5,
+              float* n32, float* cj32, float* ck32);
+
 // General-shape mixed pipeline (mixed_general.cu), used when the fused kernel's
 // shape limits (nbf <= 256, nbf5 <= 64) do not hold.
 bool mixed_general_needed(int nbf, int nbf5);

@@ -136,9 +136,13 @@ __device__ __forceinline__ void finish_tmp16(const Params& P, unsigned char* sm,
     }
 }
 
-__global__ void __launch_bounds__(NTHREADS, 1)
-lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_constant__ CUtensorMap map_blo,
-                 const __grid_constant__ CUtensorMap map_cs, const Params P) {
+// The kernel's work on CTA `cta` of `G` CTAs for one job (its aux indices
+// l = cta + k G): lag_mixed_kernel runs it for one job on the whole grid,
+// lag_mixed_grouped_kernel for each job of a batch on its own CTA range.  The
+// tensor maps and P live in the launch's parameter space (__grid_constant__).
+__device__ __forceinline__ void lag_mixed_body(const CUtensorMap& map_bhi, const CUtensorMap& map_blo,
+                                               const CUtensorMap& map_cs, const Params& P, const int cta,
+                                               const int G) {
     extern __shared__ unsigned char smem_raw[];
     unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const uint32_t sbase = saddr(sm);
@@ -148,8 +152,7 @@ lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_const
     auto bar = [&](int i) { return saddr(&bars[i]); };
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int G = gridDim.x;
-    const int my_count = (P.naux - (int)blockIdx.x + G - 1) / G;  // l = blockIdx.x + k*G
+    const int my_count = (P.naux - cta + G - 1) / G;  // l = cta + k*G
     const int ncol = 64 * P.nb;
 
     if (threadIdx.x == 0) {
@@ -178,7 +181,7 @@ lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_const
             int it = 0;
             bool ok = true;
             for (int li = 0; li < my_count && ok; ++li) {
-                const int l = blockIdx.x + li * G;
+                const int l = cta + li * G;
                 for (int qb = 0; qb < P.nb && ok; ++qb) {
                     for (int kb = 0; kb < P.nkb; ++kb, ++it) {
                         const int s = it % RING;
@@ -366,7 +369,7 @@ lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_const
         bool ok = true;
         int tq = 0;  // T1 quarters drained (slot = tq & 1)
         for (int li = 0; li < my_count && ok; ++li) {
-            const int l = blockIdx.x + li * G;
+            const int l = cta + li * G;
             const uint32_t lph = (uint32_t)(li & 1);
             // ---- T1 drain, one 64-column quarter of m at a time, each warp on its own:
             // tmp[m, q] = D1[prow(q, 0), m] + D1[prow(q, 1), m]
@@ -441,7 +444,7 @@ lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_const
                         if (off + i < P.nbf5) dst[i] = bq[i];
                     // K_MO partial sums of this CTA, stored transposed (kp[q + nbf5*p]) so that
                     // the reductions of a warp are coalesced; each address has one writer
-                    float* kp = P.k_part + (size_t)blockIdx.x * P.nbf5 * P.nbf5 + q;
+                    float* kp = P.k_part + (size_t)cta * P.nbf5 * P.nbf5 + q;
 #pragma unroll
                     for (int i = 0; i < 32; ++i)
                         if (off + i < P.nbf5) atomicAdd(kp + (size_t)P.nbf5 * (off + i), bq[i] * bq[i]);
@@ -493,7 +496,7 @@ lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_const
                     tmem_issue32(RY + lane_addr + c * 32, r);
                     tmem_wait_ld();
                     const int m0 = 32 * c + 16 * x;
-                    float* dst = P.y_part + (size_t)blockIdx.x * P.nbf * P.nbf5 + (size_t)P.nbf * q + m0;
+                    float* dst = P.y_part + (size_t)cta * P.nbf * P.nbf5 + (size_t)P.nbf * q + m0;
 #pragma unroll
                     for (int i = 0; i < 16; ++i) {
                         const float send = __uint_as_float(x ? r[i] : r[16 + i]);
@@ -512,6 +515,30 @@ lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_const
         fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem));
     }
+}
+
+__global__ void __launch_bounds__(NTHREADS, 1)
+lag_mixed_kernel(const __grid_constant__ CUtensorMap map_bhi, const __grid_constant__ CUtensorMap map_blo,
+                 const __grid_constant__ CUtensorMap map_cs, const Params P) {
+    lag_mixed_body(map_bhi, map_blo, map_cs, P, (int)blockIdx.x, (int)gridDim.x);
+}
+
+// Several jobs in one launch: job j owns the CTAs [cta0[j], cta0[j + 1]) and
+// runs lag_mixed_body on them with its own tensor maps and parameters.
+constexpr int GROUP_MAX = 48;  // 48 jobs' maps and parameters fit the 32 KB of kernel parameters
+struct GroupParams {
+    CUtensorMap maps[GROUP_MAX][3];  // b_hi, b_lo, Cs
+    Params P[GROUP_MAX];
+    int cta0[GROUP_MAX + 1];
+    int njobs;
+};
+static_assert(sizeof(GroupParams) <= 32000, "kernel parameter space");
+
+__global__ void __launch_bounds__(NTHREADS, 1) lag_mixed_grouped_kernel(const __grid_constant__ GroupParams GP) {
+    int j = 0;
+    while (j + 1 < GP.njobs && GP.cta0[j + 1] <= (int)blockIdx.x) ++j;
+    const int cta = (int)blockIdx.x - GP.cta0[j], G = GP.cta0[j + 1] - GP.cta0[j];
+    lag_mixed_body(GP.maps[j][0], GP.maps[j][1], GP.maps[j][2], GP.P[j], cta, G);
 }
 
 // ---------------------------------------------------------------- helpers
@@ -536,6 +563,19 @@ __global__ void split_b_kernel(const double* __restrict__ b, int nbf, int nb, lo
         const __nv_bfloat16 lw = __double2bfloat16(v - (double)__bfloat162float(h));
         hi[i] = h;
         lo[i] = lw;
+    }
+}
+
+// split_c_kernel for every job of a batch: job blockIdx.y, its arrays from a device table.
+__global__ void split_c_grouped_kernel(const MixedSplitJob* __restrict__ jobs) {
+    const MixedSplitJob J = jobs[blockIdx.y];
+    const int total = J.ldk * 128;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        const int k = i % J.ldk, j = i / J.ldk;
+        const int q = 16 * (j >> 5) + (j & 15), x = (j >> 4) & 1;  // j = prow(q, x)
+        double v = (k < J.nbf && q < J.nbf5) ? J.C[k + (long long)J.nbf * q] : 0.0;
+        const __nv_bfloat16 h = __double2bfloat16(v);
+        static_cast<__nv_bfloat16*>(J.cs)[i] = (x == 0) ? h : __double2bfloat16(v - (double)__bfloat162float(h));
     }
 }
 
@@ -729,6 +769,59 @@ int launch_mixed(donof_job* job, cudaStream_t st, int nbf5, int nalpha, int nbet
     return DONOF_OK;
 }
 
+// One launch of lag_mixed_grouped_kernel per GROUP_MAX jobs (mode 3: the Y
+// partials of every job's CTAs into its ypart).
+int launch_mixed_grouped_impl(donof_ctx* ctx, cudaStream_t st, const MixedGroupJob* jobs, int njobs) {
+    static std::atomic<unsigned long long> attr_mask{0};
+    const unsigned long long bit = 1ull << (ctx->device & 63);
+    if (!(attr_mask.load(std::memory_order_acquire) & bit)) {
+        DONOF_CUDA(ctx, cudaFuncSetAttribute(mx::lag_mixed_grouped_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             mx::SMEM_ALLOC));
+        attr_mask.fetch_or(bit, std::memory_order_acq_rel);
+    }
+    for (int j0 = 0; j0 < njobs; j0 += mx::GROUP_MAX) {
+        const int nj = njobs - j0 < mx::GROUP_MAX ? njobs - j0 : mx::GROUP_MAX;
+        mx::GroupParams GP;
+        memset(&GP, 0, sizeof(GP));
+        GP.njobs = nj;
+        int cta = 0;
+        for (int i = 0; i < nj; ++i) {
+            const MixedGroupJob& g = jobs[j0 + i];
+            donof_job* job = g.job;
+            const int nbf = job->nbf, naux = job->naux, ldm = ldm_of(nbf), nb = (nbf + 63) / 64;
+            {
+                cuuint64_t dims[4] = {64, (cuuint64_t)nbf, (cuuint64_t)nb, (cuuint64_t)naux};
+                cuuint64_t strides[3] = {128, (cuuint64_t)128 * nbf, (cuuint64_t)128 * nbf * nb};
+                cuuint32_t box[4] = {mx::BOX_M, mx::KB, 1, 1};
+                DONOF_CHECK(make_tmap_bf16(ctx, &GP.maps[i][0], job->b16hi, 4, dims, strides, box));
+                DONOF_CHECK(make_tmap_bf16(ctx, &GP.maps[i][1], job->b16lo, 4, dims, strides, box));
+            }
+            {
+                cuuint64_t dims[2] = {(cuuint64_t)nbf, 128};
+                cuuint64_t strides[1] = {(cuuint64_t)ldm * 2};
+                cuuint32_t box[2] = {64, 128};
+                DONOF_CHECK(make_tmap_bf16(ctx, &GP.maps[i][2], g.cs, 2, dims, strides, box));
+            }
+            mx::Params& P = GP.P[i];
+            P.nbf = nbf; P.nbf5 = g.nbf5; P.naux = naux; P.nalpha = g.nalpha; P.nbeta = g.nbeta;
+            P.nb = nb;
+            P.nkb = (nbf + mx::KB - 1) / mx::KB;
+            P.ncs = (nbf + 63) / 64;
+            P.mode = 3;
+            P.n32 = g.n32; P.cj32 = g.cj32; P.ck32t = g.ck32;
+            P.y_part = g.ypart;
+            P.fail = ctx->fail_dev ? ctx->fail_dev + FAIL_MBAR : nullptr;
+            P.wait = sm100::wait_budget(ctx->wait_limit);
+            GP.cta0[i] = cta;
+            cta += g.ctas;
+        }
+        GP.cta0[nj] = cta;
+        mx::lag_mixed_grouped_kernel<<<cta, mx::NTHREADS, mx::SMEM_ALLOC, st>>>(GP); count_launch();
+        DONOF_CUDA(ctx, cudaGetLastError());
+    }
+    return DONOF_OK;
+}
+
 int mixed_grid(donof_job* job) { return job->naux < ctx_ctas(job->ctx) ? job->naux : ctx_ctas(job->ctx); }
 
 int check_mixed(donof_job* job, int nbf5) {
@@ -744,6 +837,28 @@ int check_mixed(donof_job* job, int nbf5) {
 }
 
 }  // namespace
+
+bool mixed_fused_fits(int nbf, int nbf5) { return !mixed_general_needed(nbf, nbf5); }
+
+int launch_mixed_grouped(donof_ctx* ctx, cudaStream_t st, const MixedGroupJob* jobs, int njobs) {
+    return launch_mixed_grouped_impl(ctx, st, jobs, njobs);
+}
+
+int split_c_grouped(donof_ctx* ctx, cudaStream_t st, const MixedSplitJob* d_jobs, int njobs, int max_ldk) {
+    const int blocks = (max_ldk * 128 + 255) / 256;
+    mx::split_c_grouped_kernel<<<dim3(blocks, njobs), 256, 0, st>>>(d_jobs); count_launch();
+    DONOF_CUDA(ctx, cudaGetLastError());
+    return DONOF_OK;
+}
+
+int prep_coef(donof_ctx* ctx, cudaStream_t st, const double* n, const double* cj12, const double* ck12, int nbf5,
+              float* n32, float* cj32, float* ck32) {
+    mx::prep_coef_kernel<<<16, 256, 0, st>>>(n, cj12, ck12, nbf5, n32, cj32, ck32); count_launch();
+    DONOF_CUDA(ctx, cudaGetLastError());
+    return DONOF_OK;
+}
+
+int mixed_ldk(int nbf) { return ldm_of(nbf); }
 
 int convert_b_f32(donof_job* job) {
     // b split into bf16 hi + lo (the mixed form's copy of b)

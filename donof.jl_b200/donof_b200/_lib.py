@@ -108,6 +108,7 @@ SIGNATURES = {
     "donof_batch_queue_poll": (_i, [_vp, ct.c_ulonglong, _i, _vp, _vp, _vp]),
     "donof_batch_queue_destroy": (_i, [_vp]),
     "donof_batch_serve": (_i, [_vp, _vp]),
+    "donof_batch_set_precision": (_i, [_vp, _i]),
 }
 
 

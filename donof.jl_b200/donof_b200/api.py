@@ -422,6 +422,12 @@ class Batch:
             out.append((Cio[j], gio[j], ns[j], {f: getattr(res[j], f) for f, _ in _EnergyResult._fields_}))
         return out
 
+    def set_precision(self, precision) -> None:
+        """The form of the batch's Lagrangian: "fp64", or "mixed" (the fused
+        tcgen05 kernel for every job in one grouped launch; the jobs uploaded as
+        mixed, nbf <= 256, nbf5 <= 64)."""
+        self.ctx.check(self.ctx.lib.donof_batch_set_precision(self.handle, _prec(precision)))
+
     def serve(self, queue: "BatchQueue") -> None:
         """Continuous batching (donof_batch_serve): the batch's jobs are slots of
         their shapes; requests pushed into ``queue`` (also from other threads while

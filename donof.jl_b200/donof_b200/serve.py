@@ -485,8 +485,9 @@ class _Bucket:
         from . import api
         self.server, self.slots = server, slots
         self.ctx = api.Context(server.device, torch_stream=False)
-        # the batch's grouped persistent kernels take a share of the SMs, as a served job does
-        self.ctx.set_cta_limit(cta_share_for(server.admission.max_inflight, server.device))
+        # no CTA share: a shape's grouped launches carry every job of the shape (with
+        # the share of a single served job the benchmark stream served 2.2 against
+        # 4.2 energies/s)
         self.queue = api.BatchQueue()
         self.batch = None
         self.ready = threading.Event()   # the batch exists (made from the first request)

@@ -260,6 +260,17 @@ typedef struct {
     int nit, success;     /* out */
 } donof_batch_item;
 int donof_batch_create(donof_ctx* ctx, int count, const donof_batch_shape* shapes, donof_batch** batch);
+/* Form of the batch's Lagrangian (donof_batch_lagrange2 / _orbopt / _energy):
+ * DONOF_PREC_FP64 (default) or DONOF_PREC_MIXED -- the fused tcgen05 kernel
+ * of the mixed form for every job in one grouped launch (each job on its own
+ * CTA range, b read from its bf16 split: the jobs must be uploaded with
+ * DONOF_PREC_MIXED and have nbf <= 256, nbf5 <= 64), then the grouped FP64
+ * tail.  The rotation, optimiser and occupation steps stay FP64.  Mixed
+ * results agree with the FP64 ones to the mixed form's tolerance; they are not
+ * bit-for-bit a job's mixed result alone (the Y partials are summed over the
+ * job's CTA range, which depends on the batch).  donof_batch_serve runs FP64
+ * batches only.                                                               */
+int donof_batch_set_precision(donof_batch* batch, int precision);
 int donof_batch_destroy(donof_batch* batch);
 size_t donof_batch_device_bytes(const donof_batch* batch);
 /* Optimiser loop of every job (items[j] for shapes[j]); returns when all ended.

@@ -245,3 +245,79 @@ def test_batch_energy_variants_match_each_job_alone(cuda_ctx):
     batch.free()
     for b in bts:
         b.free()
+
+
+MIXED_TOL = 2e-4  # the mixed form's bound on elag (max-norm relative; tests/test_gpu_mixed.py)
+
+
+def test_mixed_batch_lagrangian_matches_each_job_and_the_oracle(cuda_ctx):
+    """donof_batch_set_precision(MIXED): the fused tcgen05 kernel of every job in
+    one grouped launch, each job on its own CTA range, then the grouped FP64
+    tail.  Against the single-job mixed Lagrangian (the same products, Y
+    partials summed over other CTA ranges: FP32 rounding apart) and against the
+    FP64 oracle (the mixed form's tolerance)."""
+    import torch
+
+    inputs = device_inputs([case(**kw) for kw in SHAPES])
+    bts = [d.eris_to_gpu(x["b"], "mixed", cuda_ctx) for x in inputs]
+    batch = d.Batch(bts, [x["p"] for x in inputs], cuda_ctx)
+    batch.set_precision("mixed")
+    elag = [torch.zeros(x["p"].nbf, x["p"].nbf, dtype=torch.float64, device="cuda") for x in inputs]
+    hmat = [torch.zeros(x["p"].nbf5, x["p"].nbf, dtype=torch.float64, device="cuda") for x in inputs]
+    E = batch.lagrange2([x["tn"] for x in inputs], [x["tcj"] for x in inputs], [x["tck"] for x in inputs],
+                        [x["tH"] for x in inputs], [x["tC"] for x in inputs], elag, hmat)
+    torch.cuda.synchronize()
+    for j, x in enumerate(inputs):
+        p = x["p"]
+        e_ref, h_ref = native.lagrange2(x["C"], x["n"], x["H"], x["b"], x["cj"], x["ck"], p.nalpha, p.nbeta)
+        e, h = d.from_device(elag[j]), d.from_device(hmat[j])
+        assert rel(h, h_ref) <= TOL, j          # H_mat stays FP64
+        assert rel(e, e_ref) <= MIXED_TOL, j
+        assert np.all(e[:, p.nbf5:] == 0.0)
+        bts[j].set_precision("mixed")
+        e1, h1, E1 = d.compute_Lagrange2(x["C"], x["n"], x["H"], bts[j], x["cj"], x["ck"], p.nalpha, p.nbeta,
+                                         return_energy=True)
+        assert rel(e, e1) <= 1e-5, j
+        # energies: the mixed form's bound (1e-5 relative, as tests/test_gpu_mixed.py states)
+        assert abs(E[j] - E1) <= 1e-5 * max(1.0, abs(E1)), j
+        E_ref = orbital.e_elec(h_ref, x["n"], e_ref, p.nbf5)
+        assert abs(E[j] - E_ref) <= 1e-5 * max(1.0, abs(E_ref)), j
+    # back to FP64: the grouped FP64 path again, bit-for-bit the single-job FP64 result
+    batch.set_precision("fp64")
+    E64 = batch.lagrange2([x["tn"] for x in inputs], [x["tcj"] for x in inputs], [x["tck"] for x in inputs],
+                          [x["tH"] for x in inputs], [x["tC"] for x in inputs], elag, hmat)
+    for j, x in enumerate(inputs):
+        p = x["p"]
+        bts[j].set_precision("fp64")
+        _, _, E1 = d.compute_Lagrange2(x["C"], x["n"], x["H"], bts[j], x["cj"], x["ck"], p.nalpha, p.nbeta,
+                                       return_energy=True)
+        assert E64[j] == E1, j
+    batch.free()
+
+
+def test_mixed_batch_orbital_optimiser_runs_every_job(cuda_ctx):
+    """The grouped optimiser loop on the mixed Lagrangian: every job's energy
+    within the mixed form's rounding of the FP64 batch's, and the same stopping
+    behaviour (iterations within a few steps)."""
+    import copy
+
+    import torch
+
+    inputs = device_inputs([case(**kw) for kw in SHAPES[:4]])
+    bts = [d.eris_to_gpu(x["b"], "mixed", cuda_ctx) for x in inputs]
+    out = {}
+    for prec in ("fp64", "mixed"):
+        batch = d.Batch(bts, [x["p"] for x in inputs], cuda_ctx)
+        batch.set_precision(prec)
+        Cs = [x["tC"].clone() for x in inputs]
+        res = batch.orbopt("ADAM", [x["tn"] for x in inputs], [x["tcj"] for x in inputs],
+                           [x["tck"] for x in inputs], [x["tH"] for x in inputs], Cs,
+                           [0.01] * len(inputs), [20] * len(inputs), [1e-12] * len(inputs))
+        torch.cuda.synchronize()
+        out[prec] = res
+        batch.free()
+    for j in range(len(inputs)):
+        E64, nit64 = out["fp64"][j][0], out["fp64"][j][1]
+        Em, nitm = out["mixed"][j][0], out["mixed"][j][1]
+        assert nitm > 0 and np.isfinite(Em)
+        assert abs(Em - E64) <= 1e-4 * max(1.0, abs(E64)), (j, Em, E64)
