@@ -210,27 +210,52 @@ def max_over_ranks(t, dist, device=None):
     return float(tt.item())
 
 
-def host_adam(state, g, i, alpha, beta1=0.5, beta2=0.9):
-    m, v, vmax = state
-    m[:] = beta1 * m + (1 - beta1) * g
-    v[:] = beta2 * v + (1 - beta2) * g * g
-    vmax[:] = np.maximum(vmax, v / (1 - beta2 ** i))
-    return -alpha * (m / (1 - beta1 ** i)) / np.sqrt(vmax + 1e-16)
+class HostAdam:
+    """The optimiser's host side per step: calcorbg's packing of 4 (elag - elag^T),
+    row-wise over i < nbf5, j > i (src/pnof.jl:1395-1403), and the AMSGrad form of
+    ADAM (src/minimization.jl:406-412), in arrays allocated once (``alloc``
+    makes them, e.g. page-locked).  The returned y is overwritten by the next
+    step."""
 
-
-_PACK_INDEX = {}
-
-
-def pack(elag, nbf5):
-    """calcorbg's packing of 4 (elag - elag^T), row-wise over i < nbf5, j > i
-    (src/pnof.jl:1395-1403); the index arrays are built once per size."""
-    key = (elag.shape[0], nbf5)
-    if key not in _PACK_INDEX:
-        iu = np.triu_indices(elag.shape[0], 1)
+    def __init__(self, nbf, nbf5, alpha=0.01, beta1=0.5, beta2=0.9, alloc=np.zeros):
+        iu = np.triu_indices(nbf, 1)
         sel = iu[0] < nbf5
-        _PACK_INDEX[key] = (iu[0][sel], iu[1][sel])
-    i, j = _PACK_INDEX[key]
-    return 4.0 * (elag[i, j] - elag[j, i])
+        self.ij = (iu[0][sel] + nbf * iu[1][sel]).astype(np.intp)  # elag[i, j], column-major
+        self.ji = (iu[1][sel] + nbf * iu[0][sel]).astype(np.intp)  # elag[j, i]
+        nvar = self.ij.shape[0]
+        self.m, self.v, self.vmax, self.g, self.t = (np.zeros(nvar) for _ in range(5))
+        self.y = alloc(nvar)
+        self.alpha, self.beta1, self.beta2, self.i = alpha, beta1, beta2, 0
+
+    def reset(self):
+        for a in (self.m, self.v, self.vmax):
+            a[:] = 0.0
+        self.i = 0
+
+    def step(self, elag):
+        g, t, m, v, y = self.g, self.t, self.m, self.v, self.y
+        b1, b2 = self.beta1, self.beta2
+        self.i += 1
+        f = elag.ravel(order="F")
+        np.take(f, self.ij, out=g)
+        np.take(f, self.ji, out=t)
+        np.subtract(g, t, out=g)
+        np.multiply(g, 4.0, out=g)
+        np.multiply(m, b1, out=m)
+        np.multiply(g, 1.0 - b1, out=t)
+        np.add(m, t, out=m)
+        np.multiply(v, b2, out=v)
+        np.multiply(g, g, out=t)
+        np.multiply(t, 1.0 - b2, out=t)
+        np.add(v, t, out=v)
+        np.multiply(v, 1.0 / (1.0 - b2 ** self.i), out=t)
+        np.maximum(self.vmax, t, out=self.vmax)
+        np.add(self.vmax, 1e-16, out=t)
+        np.sqrt(t, out=t)
+        np.multiply(m, 1.0 / (1.0 - b1 ** self.i), out=y)
+        np.divide(y, t, out=y)
+        np.multiply(y, -self.alpha, out=y)
+        return y
 
 
 def run_cpu_steps(wl, steps, budget_s, threads=None, impl="blas"):
@@ -247,11 +272,11 @@ def run_cpu_steps(wl, steps, budget_s, threads=None, impl="blas"):
     p = wl.p
     C = wl.C.copy(order="F")
     elag, _ = native.lagrange2(C, wl.n, wl.H, wl.b, wl.cj12, wl.ck12, p.nalpha, p.nbeta)
-    st = (np.zeros(p.nvar), np.zeros(p.nvar), np.zeros(p.nvar))
+    adam = HostAdam(p.nbf, p.nbf5)
     done = 0
     t0 = time.perf_counter()
     for i in range(1, steps + 1):
-        y = host_adam(st, pack(elag, p.nbf5), i, 0.01)
+        y = adam.step(elag)
         C = native.rotate(y, C, p.nbf5)
         elag, Hmat = native.lagrange2(C, wl.n, wl.H, wl.b, wl.cj12, wl.ck12, p.nalpha, p.nbeta)
         done += 1
@@ -826,27 +851,40 @@ def main():
     # ---- end to end through the host-buffer C ABI (what a DoNOF.jl loop does per step)
     e2e = None
     if not args.no_e2e:
-        C = wl.C.copy(order="F")
-        st = (np.zeros(p.nvar), np.zeros(p.nvar), np.zeros(p.nvar))
-        elag, Hm = d.compute_Lagrange2(C, wl.n, wl.H, bt, wl.cj12, wl.ck12, p.nalpha, p.nbeta)
+        # the caller's arrays in page-locked host memory, as a DoNOF.jl loop
+        # would hold them pinned: the entry points DMA them with no staging copy
+        def pinned_copy(a):
+            h = d.host_pinned(a.shape)
+            h[...] = a
+            return h
 
-        def host_step(i, C, elag):
-            y = host_adam(st, pack(elag, p.nbf5), i, 0.01)
-            C = d.rotate_orbital(y, C, p, ctx)
-            elag, Hm, E = d.compute_Lagrange2(C, wl.n, wl.H, bt, wl.cj12, wl.ck12, p.nalpha, p.nbeta,
-                                              return_energy=True)
-            return C, elag
+        Hh, nh, cjh, ckh = (pinned_copy(a) for a in (wl.H, wl.n, wl.cj12, wl.ck12))
+        Cs = [pinned_copy(wl.C), d.host_pinned(wl.C.shape)]
+        elag, Hm = d.host_pinned((nbf, nbf)), d.host_pinned((nbf, nbf5))
+        adam = HostAdam(nbf, nbf5, alloc=d.host_pinned)
 
-        for i in range(1, args.warmup + 1):
-            C, elag = host_step(i, C, elag)
-        C = wl.C.copy(order="F")
-        st = (np.zeros(p.nvar), np.zeros(p.nvar), np.zeros(p.nvar))
+        def host_step(k):
+            # one iteration of src/minimization.jl:387-422: update, rotate, Lagrangian + energy
+            y = adam.step(elag)
+            d.rotate_orbital(y, Cs[k % 2], p, ctx, out=Cs[(k + 1) % 2])
+            d.compute_Lagrange2(Cs[(k + 1) % 2], nh, Hh, bt, cjh, ckh, p.nalpha, p.nbeta, return_energy=True,
+                                out=(elag, Hm))
+
+        def start():
+            Cs[0][...] = wl.C
+            adam.reset()
+            d.compute_Lagrange2(Cs[0], nh, Hh, bt, cjh, ckh, p.nalpha, p.nbeta, out=(elag, Hm))
+
+        start()
+        for k in range(args.warmup):
+            host_step(k)
+        start()
         torch.cuda.synchronize()
         barrier()
         evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
         evs[0].record()
         for i in range(1, args.steps + 1):
-            C, elag = host_step(i, C, elag)
+            host_step(i - 1)
             evs[i].record()
         torch.cuda.synchronize()
         te = evs[0].elapsed_time(evs[-1]) / 1e3
@@ -856,7 +894,8 @@ def main():
         h2d = 8 * (p.nvar + nn) + 8 * (nn + nn + nbf5 + 2 * n55)
         d2h = 8 * nn + 8 * (nn + nbf * nbf5 + 1)
         e2e = {"value": world * args.steps / te, "unit": UNIT, "h2d_bytes_per_step": h2d,
-               "d2h_bytes_per_step": d2h, "path": "donof_rotate + donof_lagrange2 (host buffers), host update",
+               "d2h_bytes_per_step": d2h,
+               "path": "donof_rotate + donof_lagrange2 (page-locked host buffers), host update",
                "latency_ms": {"p50": float(np.percentile(per_step, 50)), "p99": float(np.percentile(per_step, 99)),
                               "per": "orbital step through the host-buffer C ABI"}}
 

@@ -176,7 +176,9 @@ int check_sizes(donof_ctx* ctx, int nbf, int nbf5, int nalpha, int nbeta) {
 // host and then sent by an asynchronous DMA; an output is DMA'd into it and
 // copied to the caller's array once finish() has synchronised the stream.
 // Page-locked transfers run at full PCIe speed whatever memory the caller
-// passes.  Without pin(), or when no page-locked memory can be allocated, the
+// passes.  A caller array that is itself page-locked (cudaMallocHost,
+// cudaHostRegister, a pinned torch tensor) is DMA'd directly, with no host
+// copy.  Without pin(), or when no page-locked memory can be allocated, the
 // copies use the caller's memory directly.
 struct Stager {
     donof_ctx* ctx;
@@ -194,6 +196,16 @@ struct Stager {
     int nout = 0;
 
     static size_t bytes(size_t count) { return ((count * sizeof(double) + 255) / 256) * 256; }
+
+    // the caller's array is page-locked host memory the DMA engines can reach
+    static bool page_locked(const void* h) {
+        cudaPointerAttributes a{};
+        if (cudaPointerGetAttributes(&a, h) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        return a.type == cudaMemoryTypeHost;
+    }
 
     // page-locked room for `total` bytes of inputs and outputs
     int pin(size_t total) {
@@ -223,7 +235,7 @@ struct Stager {
         const size_t b = bytes(count);
         off += b;
         if (h == nullptr) return d;
-        if (pinned && hoff + b <= pinned_bytes) {
+        if (pinned && !page_locked(h) && hoff + b <= pinned_bytes) {
             memcpy(pinned + hoff, h, count * sizeof(double));
             cudaMemcpyAsync(d, pinned + hoff, count * sizeof(double), cudaMemcpyHostToDevice, st);
             hoff += b;
@@ -236,7 +248,7 @@ struct Stager {
     // device -> caller array h, complete after finish()
     int get(double* h, const double* d, size_t count) {
         const size_t b = bytes(count);
-        if (pinned && hoff + b <= pinned_bytes && nout < 8) {
+        if (pinned && !page_locked(h) && hoff + b <= pinned_bytes && nout < 8) {
             DONOF_CUDA(ctx, cudaMemcpyAsync(pinned + hoff, d, count * sizeof(double), cudaMemcpyDeviceToHost, st));
             outs[nout++] = Out{h, pinned + hoff, count * sizeof(double)};
             hoff += b;

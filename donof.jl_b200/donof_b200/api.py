@@ -220,13 +220,33 @@ def Iaux_gpu(G, I, precision="fp64", ctx: Optional[Context] = None) -> BTensor:
 Iaux = Iaux_gpu
 
 
-def compute_Lagrange2(C, n, H, b: BTensor, cj12, ck12, nalpha: int, nbeta: int, return_energy=False):
+def host_pinned(shape) -> np.ndarray:
+    """Zeroed Fortran-ordered FP64 numpy array in page-locked host memory (the
+    storage of a pinned torch tensor, kept alive by the array).  The host-buffer
+    entry points DMA such arrays directly, without a staging copy."""
+    shape = (shape,) if np.isscalar(shape) else tuple(shape)
+    t = torch.zeros(int(np.prod(shape)), dtype=torch.float64, pin_memory=True)
+    return t.numpy().reshape(shape, order="F")
+
+
+def _out(out, shape):
+    if out is None:
+        return np.zeros(shape, order="F")
+    if out.shape != shape or out.dtype != np.float64 or not out.flags.f_contiguous:
+        raise ValueError(f"output array must be Fortran-ordered float64 of shape {shape}")
+    return out
+
+
+def compute_Lagrange2(C, n, H, b: BTensor, cj12, ck12, nalpha: int, nbeta: int, return_energy=False,
+                      out=None):
     """elag, H_mat = compute_Lagrange2(C, n, H, b, cj12, ck12, nalpha, nbeta)
-    (src/utils.jl:1-59; ext/DoNOFGPUExt.jl:150-245).  Host arrays in and out."""
+    (src/utils.jl:1-59; ext/DoNOFGPUExt.jl:150-245).  Host arrays in and out;
+    ``out=(elag, H_mat)`` writes into caller arrays (page-locked ones from
+    ``host_pinned`` skip the staging copy)."""
     C, n, H, cj12, ck12 = _f64(C), _f64(n), _f64(H), _f64(cj12), _f64(ck12)
     nbf, nbf5 = b.nbf, n.shape[0]
-    elag = np.zeros((nbf, nbf), order="F")
-    Hmat = np.zeros((nbf, nbf5), order="F")
+    elag = _out(None if out is None else out[0], (nbf, nbf))
+    Hmat = _out(None if out is None else out[1], (nbf, nbf5))
     E = np.zeros(1)
     b.ctx.check(b.ctx.lib.donof_lagrange2(b.handle, _ptr(C), _ptr(n), _ptr(H), _ptr(cj12), _ptr(ck12),
                                           nbf5, int(nalpha), int(nbeta), _ptr(elag), _ptr(Hmat), _ptr(E)))
@@ -270,13 +290,16 @@ def computeJKH_MO(C, H, b: BTensor, p: Param):
     return JKH_MO(C, H, b, p.nbf, p.nbf5, p.nbfaux)
 
 
-def rotate_orbital(y, C, p: Param, ctx: Optional[Context] = None):
-    """C exp(Y(y)) in FP64 (src/utils.jl:499-521; replaces ext/DoNOFGPUExt.jl:355-382)."""
+def rotate_orbital(y, C, p: Param, ctx: Optional[Context] = None, out=None):
+    """C exp(Y(y)) in FP64 (src/utils.jl:499-521; replaces ext/DoNOFGPUExt.jl:355-382).
+    ``out`` receives the result when given (it must not be C itself)."""
     ctx = ctx or default_context()
     y, C = _f64(y), _f64(C)
     if y.shape[0] != p.nvar:
         raise ValueError(f"y has {y.shape[0]} entries, nvar = {p.nvar}")
-    Cn = np.zeros_like(C, order="F")
+    Cn = _out(out, C.shape)
+    if Cn is C:
+        raise ValueError("rotate_orbital cannot write its result over C")
     ctx.check(ctx.lib.donof_rotate(ctx.handle, _ptr(y), p.nbf, p.nbf5, _ptr(C), _ptr(Cn)))
     return Cn
 

@@ -181,3 +181,68 @@ def test_native_server_destroy_releases_a_blocked_waiter():
     th.join(60)
     assert not th.is_alive()
     assert got["r"].error == "cancelled"
+
+
+def test_eigensolver_barrier_timeout_returns_timeout_and_recovers(ctx):
+    """The Jacobi eigensolver of Iaux waits on bounded grid barriers: a one-cycle
+    budget makes them run out; Iaux returns DONOF_ERR_TIMEOUT and the next call
+    gives the same b as before.  naux = 200 gives 100 x 101 / 2 rotation pairs
+    per round, so the solver runs on 20 CTAs and its barriers really wait (one
+    CTA alone never waits)."""
+    import torch
+    rng = np.random.default_rng(3)
+    nbf, naux = 8, 200
+    Q, _ = np.linalg.qr(rng.standard_normal((naux, naux)))
+    G = np.asfortranarray((Q * np.linspace(0.5, 2.0, naux)) @ Q.T)
+    I = np.asfortranarray(rng.standard_normal((nbf, nbf, naux)))
+
+    def download(bt):
+        C = d.to_device(np.asfortranarray(np.eye(nbf)))
+        out = torch.zeros(nbf * nbf * naux, dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()  # the fill runs on torch's stream, the transform on the context's
+        d.transform_dev(C, bt, nbf, out=out)
+        ctx.synchronize()
+        return out.cpu().numpy()
+
+    b0 = d.Iaux_gpu(G, I, "fp64", ctx)
+    before = download(b0)
+    b0.free()
+    ctx.set_wait_limit(1)
+    try:
+        with pytest.raises(_lib.DonofError) as e:
+            d.Iaux_gpu(G, I, "fp64", ctx)
+    finally:
+        ctx.set_wait_limit(0)
+    assert e.value.status == _lib.ERR_TIMEOUT
+    b1 = d.Iaux_gpu(G, I, "fp64", ctx)
+    np.testing.assert_array_equal(download(b1), before)
+    b1.free()
+
+
+def test_grouped_mixed_kernel_timeout_returns_timeout_and_recovers(ctx):
+    """The grouped mixed Lagrangian of a batch (one launch over every job's CTA
+    range) with a one-cycle wait budget: DONOF_ERR_TIMEOUT, then the same
+    result as before with the normal budget."""
+    import torch
+    jobs = [workload.synthetic(nbf=48, naux=60, nbeta=4, ncwo=3, seed=s) for s in (1, 2)]
+    bts = [d.eris_to_gpu(wl.b, "mixed", ctx) for wl in jobs]
+    batch = d.Batch(bts, [wl.p for wl in jobs], ctx)
+    batch.set_precision("mixed")
+    dev = [{k: d.to_device(getattr(wl, k)) for k in ("C", "n", "H", "cj12", "ck12")} for wl in jobs]
+    elag = [torch.zeros(wl.p.nbf, wl.p.nbf, dtype=torch.float64, device="cuda") for wl in jobs]
+    hmat = [torch.zeros(wl.p.nbf5, wl.p.nbf, dtype=torch.float64, device="cuda") for wl in jobs]
+    torch.cuda.synchronize()  # torch's copies and fills before the context's stream reads them
+    call = lambda: batch.lagrange2([x["n"] for x in dev], [x["cj12"] for x in dev], [x["ck12"] for x in dev],
+                                   [x["H"] for x in dev], [x["C"] for x in dev], elag, hmat)
+    before = call()
+    ctx.set_wait_limit(1)
+    try:
+        with pytest.raises(_lib.DonofError) as e:
+            call()
+    finally:
+        ctx.set_wait_limit(0)
+    assert e.value.status == _lib.ERR_TIMEOUT
+    assert call() == before
+    batch.free()
+    for bt in bts:
+        bt.free()

@@ -140,6 +140,35 @@ def test_device_entry_points_match_host(cuda_ctx):
     bt2.free()
 
 
+def test_page_locked_caller_arrays_match_pageable(cuda_ctx):
+    """Caller arrays in page-locked memory are DMA'd directly (no staging copy):
+    rotate_orbital and compute_Lagrange2 give the same bits as with ordinary
+    arrays, for inputs and outputs, mixed pinned and pageable in one call."""
+    p, b, C, H, n, cj, ck = case(nbf=64, naux=40, nbeta=4, ncwo=3, seed=11)
+    bt = d.eris_to_gpu(b, "fp64", cuda_ctx)
+    y = 0.02 * np.random.default_rng(2).standard_normal(p.nvar)
+
+    def pinned(a):
+        h = d.host_pinned(a.shape)
+        h[...] = a
+        return h
+
+    C1 = d.rotate_orbital(y, C, p, cuda_ctx)
+    e1, h1, E1 = d.compute_Lagrange2(C1, n, H, bt, cj, ck, p.nalpha, p.nbeta, return_energy=True)
+    Cp = d.host_pinned(C.shape)
+    d.rotate_orbital(pinned(y), pinned(C), p, cuda_ctx, out=Cp)
+    assert np.array_equal(Cp, C1)
+    ep, hp = d.host_pinned((p.nbf, p.nbf)), d.host_pinned((p.nbf, p.nbf5))
+    _, _, Ep = d.compute_Lagrange2(Cp, pinned(n), H, bt, pinned(cj), ck, p.nalpha, p.nbeta, return_energy=True,
+                                   out=(ep, hp))
+    assert np.array_equal(ep, e1) and np.array_equal(hp, h1) and Ep == E1
+    with pytest.raises(ValueError):
+        d.compute_Lagrange2(C, n, H, bt, cj, ck, p.nalpha, p.nbeta, out=(np.zeros((p.nbf, p.nbf)), hp))
+    with pytest.raises(ValueError):
+        d.rotate_orbital(y, Cp, p, cuda_ctx, out=Cp)
+    bt.free()
+
+
 def test_energy_identity_at_full_size(cuda_ctx):
     """Size-independent check at the benchmark size: computeE_elec(Lagrangian) ==
     calce(JKH_MO) at the same C, both from the device."""
