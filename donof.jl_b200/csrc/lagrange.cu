@@ -84,9 +84,9 @@ __global__ void __launch_bounds__(256, 4) build_w_fused_kernel(const double* __r
                 if (l < naux && bb < nbf5) {
                     const double* d = sd + k * nbf5;
                     double s = 0.0;
-                    for (int q = 0; q < nbf5; ++q) s += cj12[bb + (long long)nbf5 * q] * d[q];
+                    for (int q = 0; q < nbf5; ++q) s = wbuild::tv_step(s, cj12[bb + (long long)nbf5 * q], d[q]);
                     const bool dj = (nbeta > 0) && (bb < nbeta || bb >= nalpha);
-                    stv[k][tx] = (dj ? n[bb] * d[bb] : 0.0) + s;
+                    stv[k][tx] = wbuild::tv_value(dj, n[bb], d[bb], s);
                 }
             }
         }
@@ -113,8 +113,8 @@ __global__ void __launch_bounds__(256, 4) build_w_fused_kernel(const double* __r
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
                 const int q = q0 + ty + 8 * r;
-                double w = -ck[r] * v[k][r];
-                if (diag && q == b && l < naux && b < nbf5) w += stv[k][tx];
+                double w = wbuild::w_value(ck[r], v[k][r]);
+                if (diag && q == b && l < naux && b < nbf5) w = wbuild::w_diag(w, stv[k][tx]);
                 tb[k][ty + 8 * r][tx] = w;  // [l - l0][q - q0][b - b0]
             }
         }

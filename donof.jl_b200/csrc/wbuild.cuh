@@ -9,6 +9,20 @@
 namespace donof {
 namespace wbuild {
 
+// The arithmetic of W with explicit rounding (no multiply-add contraction left
+// to the compiler's choice), so that every kernel that builds W -- single job,
+// grouped, fused into T2 or not -- writes the same bits.
+// t_b^l accumulation: s + cj12[b, q] d_q^l, one rounding
+__device__ __forceinline__ double tv_step(double s, double cj, double d) { return __fma_rn(cj, d, s); }
+// n'_b d_b^l + t_b^l
+__device__ __forceinline__ double tv_value(bool dj, double nb, double db, double s) {
+    return __dadd_rn(dj ? __dmul_rn(nb, db) : 0.0, s);
+}
+// -ck12[b, q] b_pq^l[b, q]
+__device__ __forceinline__ double w_value(double ck, double v) { return __dmul_rn(-ck, v); }
+// the diagonal element adds n'_b d_b^l + t_b^l
+__device__ __forceinline__ double w_diag(double w, double tv) { return __dadd_rn(w, tv); }
+
 // n'_b d_b^l + t_b^l for element i = b + nbf5 l.
 __device__ __forceinline__ double diag_value(const double* __restrict__ bpq, const double* __restrict__ n,
                                              const double* __restrict__ cj12, int nbf5, int nalpha, int nbeta,
@@ -18,9 +32,9 @@ __device__ __forceinline__ double diag_value(const double* __restrict__ bpq, con
     const long long l = i / nbf5;
     const double* B = bpq + n55 * l;
     double s = 0.0;
-    for (int q = 0; q < nbf5; ++q) s += cj12[b + (long long)nbf5 * q] * B[(long long)q * (nbf5 + 1)];
+    for (int q = 0; q < nbf5; ++q) s = tv_step(s, cj12[b + (long long)nbf5 * q], B[(long long)q * (nbf5 + 1)]);
     const bool dj = (nbeta > 0) && (b < nbeta || b >= nalpha);
-    return (dj ? n[b] * B[(long long)b * (nbf5 + 1)] : 0.0) + s;
+    return tv_value(dj, n[b], B[(long long)b * (nbf5 + 1)], s);
 }
 
 // The diagonal terms for a group of aux indices at a time: their diagonals
@@ -72,9 +86,9 @@ __device__ __forceinline__ void diag_unit(const double* __restrict__ bpq, const 
         if (l >= naux) continue;
         const double* d = sd + li * nbf5;
         double s = 0.0;
-        for (int q = 0; q < nbf5; ++q) s += cj12[b + (long long)nbf5 * q] * d[q];
+        for (int q = 0; q < nbf5; ++q) s = tv_step(s, cj12[b + (long long)nbf5 * q], d[q]);
         const bool dj = (nbeta > 0) && (b < nbeta || b >= nalpha);
-        tv[b + (long long)nbf5 * l] = (dj ? n[b] * d[b] : 0.0) + s;
+        tv[b + (long long)nbf5 * l] = tv_value(dj, n[b], d[b], s);
     }
 }
 
@@ -125,8 +139,8 @@ __device__ __forceinline__ void tile(const double* __restrict__ bpq, const doubl
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
             const int q = q0 + ty + 8 * r;
-            double w = -ck[r] * v[k][r];
-            if (q == b && l < naux && b < nbf5) w += tv[b + (long long)nbf5 * l];
+            double w = w_value(ck[r], v[k][r]);
+            if (q == b && l < naux && b < nbf5) w = w_diag(w, tv[b + (long long)nbf5 * l]);
             tb[k][ty + 8 * r][tx] = w;  // [l - l0][q - q0][b - b0]
         }
     }

@@ -35,6 +35,8 @@ SHAPES = [
     dict(nbf=20, naux=17, nbeta=3, ncwo=3, nalpha=5, seed=4),
     dict(nbf=96, naux=120, nbeta=6, ncwo=3, seed=5),
     dict(nbf=72, naux=348, nbeta=15, ncwo=3, seed=6),
+    dict(nbf=128, naux=200, nbeta=16, ncwo=3, seed=7),      # nbf5 = 64: the fused mixed kernel's largest
+    dict(nbf=40, naux=64, nbeta=5, ncwo=2, seed=8),         # odd nbf5 = 15 with even nbf
 ]
 
 
@@ -99,9 +101,10 @@ def test_batch_orbopt_matches_each_job_alone(cuda_ctx, method):
     k = len(inputs)
     # different step sizes, loop lengths and thresholds per job: the jobs stop at
     # different iterations, some on the gradient rule, some on maxloop
-    alpha = [0.01, 0.02, 0.01, 0.005, 0.01, 0.02]
-    maxloop = [6, 9, 3, 12, 5, 8]
-    thresh = [1e-4, 1e-1, 1e-4, 1.0, 1e-4, 1e-4]
+    alpha = [0.01, 0.02, 0.01, 0.005, 0.01, 0.02, 0.01, 0.02]
+    maxloop = [6, 9, 3, 12, 5, 8, 7, 4]
+    thresh = [1e-4, 1e-1, 1e-4, 1.0, 1e-4, 1e-4, 1e-4, 1e-4]
+    assert len(alpha) == k
     Cs = [x["tC"].clone() for x in inputs]
     res = batch.orbopt(method, [x["tn"] for x in inputs], [x["tcj"] for x in inputs], [x["tck"] for x in inputs],
                        [x["tH"] for x in inputs], Cs, alpha, maxloop, thresh)
