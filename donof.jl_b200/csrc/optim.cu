@@ -116,11 +116,14 @@ struct OrbState {
 };
 
 // update of the AMSGrad family with the iteration count and step size read
-// from the device state (src/minimization.jl:307-316, 406-411, 503-508, 598-603)
-__global__ void orb_update_kernel(const OrbState* __restrict__ s, long long nvar, const double* __restrict__ g,
+// from the device state (src/minimization.jl:307-316, 406-411, 503-508, 598-603);
+// it also clears max|g| for the gradient this iteration reduces (the first
+// node of the iteration, so no memset node is needed)
+__global__ void orb_update_kernel(OrbState* __restrict__ s, long long nvar, const double* __restrict__ g,
                                   double* __restrict__ m, double* __restrict__ v, double* __restrict__ vmax,
                                   double* __restrict__ y) {
     const orbupd::Coef c = orbupd::coef(s->method, s->it + 1, s->maxloop, s->alpha);
+    if (blockIdx.x == 0 && threadIdx.x == 0) s->gmax_bits = 0ull;
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nvar;
          k += (long long)gridDim.x * blockDim.x)
         orbupd::step(c, k, g, m, v, vmax, y);
@@ -152,12 +155,17 @@ __global__ void orb_end_kernel(OrbState* s, cudaGraphConditionalHandle h) {
     cudaGraphSetConditional(h, stop ? 0u : 1u);
 }
 
-__global__ void copy_if_kernel(const double* __restrict__ src, double* __restrict__ dst, long long count,
-                               const int* flag) {
-    if (*flag == 0) return;
+// The rotated orbitals become the current ones, and the best ones when this
+// iteration improved E (one pass over C_new for both copies).
+__global__ void copy_step_kernel(const double* __restrict__ src, double* __restrict__ cur, double* __restrict__ best,
+                                 long long count, const int* flag) {
+    const bool improved = *flag != 0;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
-         i += (long long)gridDim.x * blockDim.x)
-        dst[i] = src[i];
+         i += (long long)gridDim.x * blockDim.x) {
+        const double v = src[i];
+        cur[i] = v;
+        if (improved) best[i] = v;
+    }
 }
 
 }  // namespace
@@ -283,10 +291,11 @@ int orbopt_run(donof_job* job, int method, const double* n, const double* cj12, 
                 orb_update_kernel<<<nblocks(nvar, ctx->sm_count), 256, 0, st>>>(S, nvar, g, m, v, vm, y); count_launch();
                 if ((rc = rotate_f64(ctx, st, y, nbf, nbf5, Ccur, Cnew)) != DONOF_OK) break;
                 if ((rc = lagr(Cnew)) != DONOF_OK) break;
-                if ((rc = grad()) != DONOF_OK) break;
+                // max|g| was cleared by orb_update_kernel
+                if ((rc = pack_grad(ctx, st, elag, nbf, nbf5, g, &S->gmax_bits)) != DONOF_OK) break;
                 orb_end_kernel<<<1, 1, 0, st>>>(S, handle); count_launch();
-                copy_if_kernel<<<nblocks(nn, ctx->sm_count), 256, 0, st>>>(Cnew, Cbest, nn, &S->improved_now); count_launch();
-                if (cudaMemcpyAsync(Ccur, Cnew, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st) != cudaSuccess) rc = DONOF_ERR_CUDA;
+                copy_step_kernel<<<nblocks(nn, ctx->sm_count), 256, 0, st>>>(Cnew, Ccur, Cbest, nn, &S->improved_now);
+                count_launch();
             } while (false);
             cudaGraph_t captured = nullptr;
             const cudaError_t ce = cudaStreamEndCapture(st, &captured);
