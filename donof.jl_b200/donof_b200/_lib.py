@@ -91,6 +91,15 @@ SIGNATURES = {
     "donof_profile_enable": (_i, [_vp, _i]),
     "donof_profile_last_ms": (_i, [_vp, ct.POINTER(ct.c_float)]),
     "donof_mixed_tmp_dev": (_i, [_vp, _vp, _i, _vp]),
+    # integral front end
+    "donof_basis_create": (_i, [_i, _vp, _vp, _vp, _vp, _vp, _i, ct.POINTER(_vp)]),
+    "donof_basis_nbf": (_i, [_vp]),
+    "donof_basis_free": (_i, [_vp]),
+    "donof_int1e": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp]),
+    "donof_int2c2e": (_i, [_vp, _vp]),
+    "donof_int3c2e": (_i, [_vp, _vp, _vp]),
+    "donof_int3c2e_dev": (_i, [_vp, _vp, _vp, _vp]),
+    "donof_int4c2e": (_i, [_vp, _vp]),
     "donof_job_set_fp64_tc": (_i, [_vp, _i]),
     "donof_job_fp64_tc": (_i, [_vp]),
     "donof_t1_dev": (_i, [_vp, _vp, _i, _vp]),

@@ -493,6 +493,39 @@ int donof_set_wait_limit(donof_ctx* ctx, long long cycles);
  * tmp[m + nbf*q + nbf*nbf5*l] = sum_n b[m,n,l] C[n,q] (FP32, device).        */
 int donof_mixed_tmp_dev(donof_job* job, const double* C, int nbf5, float* tmp);
 
+/* ---- Integral front end (replaces GaussianBasis.jl/libcint as called by
+ * compute_integrals, src/integrals.jl:1-49: overlap, kinetic, nuclear,
+ * ERI_2e2c, ERI_2e3c, ERI_2e4c).  McMurchie-Davidson over contracted shells
+ * with l <= 5.  A basis is a list of shells: angular momentum l[s], centre
+ * (bohr) centre[3s..3s+2], nprim[s] primitives whose exponents and contraction
+ * coefficients follow in exps/coefs (as printed in a basis-set file; the
+ * library normalises primitives like x^l and each contraction to unit
+ * self-overlap).  spherical: real solid harmonics (p as x, y, z; l >= 2 as
+ * m = -l..l), else Cartesian components (xx..x, xx..y, ..., zz..z).  Every
+ * output is column-major and FP64.                                          */
+typedef struct donof_basis donof_basis;
+int donof_basis_create(int nshell, const int* l, const double* centre, const int* nprim, const double* exps,
+                       const double* coefs, int spherical, donof_basis** basis);
+int donof_basis_nbf(const donof_basis* basis);
+int donof_basis_free(donof_basis* basis);
+/* S, T and V (nbf x nbf; T or V may be null; V sums -Z_k/|r - R_k| over the
+ * natom nuclei of charge Z[k] at xyz[3k..3k+2] bohr).  Replaces overlap,
+ * kinetic, nuclear (src/integrals.jl:4-9).                                   */
+int donof_int1e(const donof_basis* basis, int natom, const double* Z, const double* xyz, double* S, double* T,
+                double* V);
+/* G[P,Q] = (P|Q) over the auxiliary basis (naux x naux): ERI_2e2c
+ * (src/integrals.jl:47).                                                     */
+int donof_int2c2e(const donof_basis* aux, double* G);
+/* I[m + nbf (n + nbf P)] = (mn|P) (nbf x nbf x naux): ERI_2e3c
+ * (src/integrals.jl:49), host threads; donof_int3c2e_dev computes the same on
+ * the context's device into device memory (orbital shells l <= 3, auxiliary
+ * l <= 4).                                                                   */
+int donof_int3c2e(const donof_basis* orb, const donof_basis* aux, double* I);
+int donof_int3c2e_dev(donof_ctx* ctx, const donof_basis* orb, const donof_basis* aux, double* I_dev);
+/* I[m + nbf (n + nbf (l + nbf s))] = (mn|ls) (nbf^4): ERI_2e4c
+ * (src/integrals.jl:16), for small bases.                                    */
+int donof_int4c2e(const donof_basis* basis, double* I);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif
