@@ -238,18 +238,22 @@ def molecule(mol: str, basis_text: str, spherical: bool = False, name: str = "ba
 
 def compute_integrals(bset: BasisSet, aux: BasisSet, p: Param, ctx=None, precision: str = "fp64",
                       device_3c: bool = True):
-    """S, T, V, H, b = compute_integrals(bset, aux, p) (src/integrals.jl:1-66,
-    RI branch): the one-electron matrices symmetrised as the reference does,
+    """S, T, V, H, b = compute_integrals(bset, aux, p) (src/integrals.jl:1-66):
+    the one-electron matrices symmetrised as the reference does; with p.RI,
     G = (P|Q) symmetrised, (mn|P) (on the B200 when its shells fit the device
     kernel and device_3c, else on host threads), then b = I G^{-1/2} built on
-    the device (Iaux_gpu) and kept there as the job's RI tensor.  Sets
-    p.nbfaux."""
+    the device (Iaux_gpu) and kept there as the job's RI tensor, and p.nbfaux
+    set; without p.RI the four-index (mn|ls) array (ERI_2e4c, host) in place
+    of b."""
     from . import api
 
-    ctx = ctx or api.default_context()
     S, T, V = one_electron(bset)
     S, T, V = (S + S.T) / 2, (T + T.T) / 2, (V + V.T) / 2
     H = T + V
+    if not p.RI:
+        return (np.asfortranarray(S), np.asfortranarray(T), np.asfortranarray(V), np.asfortranarray(H),
+                ERI_2e4c(bset))
+    ctx = ctx or api.default_context()
     G = ERI_2e2c(aux)
     G = (G + G.T) / 2
     lmax_orb = int(bset.shell_l.max()) if len(bset.shell_l) else 0

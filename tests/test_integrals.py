@@ -223,3 +223,27 @@ def test_ri_diagonal_is_a_lower_bound():
             assert err < prev
         prev = err
     assert prev < 5e-3
+
+
+def test_invalid_shells_are_refused():
+    from donof_b200 import _lib
+
+    good = {"H": H_STO3G}
+    with pytest.raises(_lib.DonofError) as e:
+        basis([("H", (0, 0, 0))], {"H": [(6, np.array([1.0]), np.array([1.0]))]})
+    assert e.value.status == _lib.ERR_ARG
+    with pytest.raises(_lib.DonofError):
+        basis([("H", (0, 0, 0))], {"H": [(0, np.array([-1.0]), np.array([1.0]))]})
+    with pytest.raises(ValueError):
+        basis([("C", (0, 0, 0))], good)  # no shells for C
+    with pytest.raises(ValueError):
+        it.parse_gbs("H 0\nQ 1 1.0\n 1.0 1.0\n****")
+
+
+def test_compute_integrals_without_ri_returns_the_four_index_array():
+    bset, p = it.molecule(f"H 0 0 0\nH 0 0 {1.4 * B2A:.12f}", "H 0\nS 3 1.00\n 3.42525091 0.15432897\n"
+                          " 0.62391373 0.53532814\n 0.16885540 0.44463454\n****", spherical=True)
+    p.RI = False
+    S, T, V, H, I = it.compute_integrals(bset, None, p)
+    assert np.allclose(H, T + V) and I.shape == (2, 2, 2, 2)
+    assert abs(I[0, 0, 0, 0] - 0.7746) < 1e-4
