@@ -167,11 +167,9 @@ void parallel_for(long long count, Body body) {
 }
 
 // ---- the three-centre integrals on the device
-constexpr int DEV_LORB = 2;  // orbital shells up to d
-constexpr int DEV_LAUX = 3;  // auxiliary shells up to f
-constexpr int DEV_BLOCK = 6 * 6 * 10;                            // ncart(2)^2 ncart(3)
-constexpr int DEV_SCRATCH = 3 * 45 + 3 * 16 + 3 * 120 + 35;      // coulomb_scratch(2, 2, 3, 0)
-constexpr int SPH_DOUBLES = 1 + 9 + 30 + 70;                     // ncart(l) (2l + 1), l <= 3
+constexpr int DEV_LORB = 3;  // orbital shells up to f
+constexpr int DEV_LAUX = 4;  // auxiliary shells up to g
+constexpr int SPH_DOUBLES = 1 + 9 + 30 + 70 + 135;  // ncart(l) (2l + 1), l <= 4
 
 struct DevBasis {
     int nshell, nbf, spherical, pad;
@@ -181,13 +179,17 @@ struct DevBasis {
 
 __constant__ double c_sph[SPH_DOUBLES];
 
-__host__ __device__ inline int sph_off(int l) { return l == 0 ? 0 : (l == 1 ? 1 : (l == 2 ? 10 : 40)); }
+__host__ __device__ inline int sph_off(int l) { return l == 0 ? 0 : (l == 1 ? 1 : (l == 2 ? 10 : (l == 3 ? 40 : 110))); }
 
 // One thread per (orbital shell pair, auxiliary shell): the Cartesian block
 // over all primitive triples, then the spherical (or Cartesian) values
-// written to I[m + nbf (n + nbf P)] and I[n + nbf (m + nbf P)].
+// written to I[m + nbf (n + nbf P)] and I[n + nbf (m + nbf P)].  LO and LX
+// bound the orbital and auxiliary l (they size the per-thread arrays).
+template <int LO, int LX>
 __global__ void __launch_bounds__(128) int3c2e_kernel(const DevBasis orb, const DevBasis aux, long long npair,
                                                       double* __restrict__ I) {
+    constexpr int DEV_BLOCK = ints::ncart(LO) * ints::ncart(LO) * ints::ncart(LX);
+    constexpr int DEV_SCRATCH = ints::coulomb_scratch(LO, LO, LX, 0);
     const long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (w >= npair * aux.nshell) return;
     const long long pw = w / aux.nshell;
@@ -599,7 +601,13 @@ int donof_int3c2e_dev(donof_ctx* ctx, const donof_basis* orb, const donof_basis*
     const long long npair = (long long)orb->nshell * (orb->nshell + 1) / 2;
     const long long work = npair * aux->nshell;
     const long long blocks = (work + 127) / 128;
-    int3c2e_kernel<<<(unsigned)blocks, 128, 0, ctx->stream>>>(dorb, daux, npair, I_dev);
+    // the smallest per-thread arrays that hold the bases' shells
+    if (orb->lmax <= 2 && aux->lmax <= 3)
+        int3c2e_kernel<2, 3><<<(unsigned)blocks, 128, 0, ctx->stream>>>(dorb, daux, npair, I_dev);
+    else if (orb->lmax <= 2)
+        int3c2e_kernel<2, 4><<<(unsigned)blocks, 128, 0, ctx->stream>>>(dorb, daux, npair, I_dev);
+    else
+        int3c2e_kernel<3, 4><<<(unsigned)blocks, 128, 0, ctx->stream>>>(dorb, daux, npair, I_dev);
     count_launch();
     DONOF_CUDA(ctx, cudaGetLastError());
     return DONOF_OK;

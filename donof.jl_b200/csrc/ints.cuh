@@ -72,7 +72,7 @@ __host__ __device__ inline void boys(int nmax, double T, double* F) {
 //   E^{i+1,j}_t = E^{ij}_{t-1} / (2p) + X_PA E^{ij}_t + (t+1) E^{ij}_{t+1}  (and j alike),
 // stored E[e_index(la, lb, i, j, t)] ((la+1)(lb+1)(la+lb+1) doubles); b = 0 with
 // XAB = 0 gives the expansion of a single Gaussian (an auxiliary function).
-__host__ __device__ inline int e_size(int la, int lb) { return (la + 1) * (lb + 1) * (la + lb + 1); }
+__host__ __device__ constexpr int e_size(int la, int lb) { return (la + 1) * (lb + 1) * (la + lb + 1); }
 __host__ __device__ inline int e_index(int la, int lb, int i, int j, int t) {
     return (i * (lb + 1) + j) * (la + lb + 1) + t;
 }
@@ -147,7 +147,7 @@ __host__ __device__ inline void hermite_r(int L, double alpha, double X, double 
 }
 
 // Scratch doubles coulomb_prim needs for angular momenta la, lb, lc, ld.
-__host__ __device__ inline int coulomb_scratch(int la, int lb, int lc, int ld) {
+__host__ __device__ constexpr int coulomb_scratch(int la, int lb, int lc, int ld) {
     return 3 * e_size(la, lb) + 3 * e_size(lc, ld) + 3 * tri_size(la + lb + lc + ld) + tri_size(la + lb);
 }
 

@@ -193,8 +193,8 @@ def ERI_2e3c(bset: BasisSet, aux: BasisSet) -> np.ndarray:
 
 def ERI_2e3c_dev(bset: BasisSet, aux: BasisSet, ctx):
     """(mn|P) computed on the context's B200 into a CUDA tensor holding the
-    column-major nbf x nbf x naux array (orbital shells up to d, auxiliary up
-    to f)."""
+    column-major nbf x nbf x naux array (orbital shells up to f, auxiliary up
+    to g)."""
     import torch
 
     out = torch.empty(bset.nbas * bset.nbas * aux.nbas, dtype=torch.float64, device=f"cuda:{ctx.device}")
@@ -258,7 +258,7 @@ def compute_integrals(bset: BasisSet, aux: BasisSet, p: Param, ctx=None, precisi
     G = (G + G.T) / 2
     lmax_orb = int(bset.shell_l.max()) if len(bset.shell_l) else 0
     lmax_aux = int(aux.shell_l.max()) if len(aux.shell_l) else 0
-    if device_3c and lmax_orb <= 2 and lmax_aux <= 3:
+    if device_3c and lmax_orb <= 3 and lmax_aux <= 4:
         I = ERI_2e3c_dev(bset, aux, ctx).cpu().numpy().reshape((bset.nbas, bset.nbas, aux.nbas), order="F")
     else:
         I = ERI_2e3c(bset, aux)

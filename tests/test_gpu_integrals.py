@@ -31,8 +31,16 @@ def test_device_three_centre_matches_host(cuda_ctx, spherical):
     assert np.max(np.abs(dev - host)) <= 1e-13 * np.max(np.abs(host))
 
 
-def test_device_three_centre_refuses_shells_beyond_its_limits(cuda_ctx):
+def test_device_three_centre_with_f_orbital_and_g_auxiliary_shells(cuda_ctx):
     b = basis(GEOM, {**ORB, "C": ORB["C"] + [(3, np.array([0.7]), np.array([1.0]))]})
+    aux = basis(GEOM, {**AUX, "C": AUX["C"] + [(4, np.array([0.9]), np.array([1.0]))]})
+    host = it.ERI_2e3c(b, aux)
+    dev = it.ERI_2e3c_dev(b, aux, cuda_ctx).cpu().numpy().reshape(host.shape, order="F")
+    assert np.max(np.abs(dev - host)) <= 1e-13 * np.max(np.abs(host))
+
+
+def test_device_three_centre_refuses_shells_beyond_its_limits(cuda_ctx):
+    b = basis(GEOM, {**ORB, "C": ORB["C"] + [(4, np.array([0.7]), np.array([1.0]))]})
     aux = basis(GEOM, AUX)
     with pytest.raises(_lib.DonofError) as e:
         it.ERI_2e3c_dev(b, aux, cuda_ctx)
