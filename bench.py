@@ -861,7 +861,9 @@ def main():
         Hh, nh, cjh, ckh = (pinned_copy(a) for a in (wl.H, wl.n, wl.cj12, wl.ck12))
         Cs = [pinned_copy(wl.C), d.host_pinned(wl.C.shape)]
         elag, Hm = d.host_pinned((nbf, nbf)), d.host_pinned((nbf, nbf5))
-        adam = HostAdam(nbf, nbf5, alloc=d.host_pinned)
+        # the host side of each iteration (gradient packing, AMSGrad update) in the
+        # library's compiled helper, as a compiled Julia loop would run it
+        adam = d.OrbStepHost(nbf, nbf5, "ADAM", alpha=0.01, maxloop=p.maxloop, alloc=d.host_pinned)
 
         def host_step(k):
             # one iteration of src/minimization.jl:387-422: update, rotate, Lagrangian + energy
@@ -895,7 +897,8 @@ def main():
         d2h = 8 * nn + 8 * (nn + nbf * nbf5 + 1)
         e2e = {"value": world * args.steps / te, "unit": UNIT, "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h,
-               "path": "donof_rotate + donof_lagrange2 (page-locked host buffers), host update",
+               "path": "donof_rotate + donof_lagrange2 (page-locked host buffers), "
+                       "host update by donof_orb_step_host",
                "latency_ms": {"p50": float(np.percentile(per_step, 50)), "p99": float(np.percentile(per_step, 99)),
                               "per": "orbital step through the host-buffer C ABI"}}
 

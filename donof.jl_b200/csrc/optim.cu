@@ -7,6 +7,8 @@
 #include <vector>
 
 #include "kernels.cuh"
+#include <type_traits>
+
 #include "orbupd.cuh"
 
 namespace donof {
@@ -429,3 +431,74 @@ int orbopt_run_host(donof_job* job, int method, const double* n, const double* c
 }
 
 }  // namespace donof
+
+// The host side of one optimiser iteration (src/minimization.jl:390-412, which
+// the reference runs on the host between its GPU calls): calcorbg's packing of
+// 4 (elag - elag^T) and the update of the AMSGrad family, with the same
+// per-element arithmetic as the device loop (orbupd.cuh).
+extern "C" int donof_orb_step_host(int method, int it, int maxloop, double alpha, const double* elag, int nbf,
+                                   int nbf5, double* g, double* m, double* v, double* vmax, double* y,
+                                   double* gmax) {
+    if (!elag || !g || !m || !v || !vmax || !y || nbf < 1 || nbf5 < 1 || nbf5 > nbf || it < 1 ||
+        method < DONOF_ORB_ADAM || method > DONOF_ORB_DEMON || (method == DONOF_ORB_DEMON && maxloop < 2)) {
+        donof::set_error(nullptr, "donof_orb_step_host: invalid arguments");
+        return DONOF_ERR_ARG;
+    }
+    // rows i of the packing in groups of 8: for each column j the group's
+    // elag[i + nbf j] share a cache line and elag[j + nbf i], g run along j
+    double mx = 0.0;
+    auto start = [nbf](long long i) { return i * (nbf - 1) - i * (i - 1) / 2; };  // first k of row i
+    for (int i0 = 0; i0 < nbf5; i0 += 8) {
+        const int i1 = i0 + 8 < nbf5 ? i0 + 8 : nbf5;
+        for (int j = i0 + 1; j < nbf; ++j) {
+            const double* col = elag + (long long)nbf * j;
+            for (int i = i0; i < i1 && i < j; ++i) {
+                const double val = 4.0 * col[i] - 4.0 * elag[j + (long long)nbf * i];
+                g[start(i) + (j - i - 1)] = val;
+                mx = fmax(mx, fabs(val));
+            }
+        }
+    }
+    const long long nvar = start(nbf5);
+    const donof::orbupd::Coef c = donof::orbupd::coef(method, it, maxloop, alpha);
+    // one loop per method, so that the per-element branch on it folds away; the
+    // bias corrections as reciprocals (one division and one square root per
+    // element; within an ulp of orbupd::step)
+    auto run = [&](auto tag) {
+        constexpr int M = decltype(tag)::value;
+        const double b1 = c.beta1, b2 = c.beta2, ib1 = 1.0 / c.bc1, ib2 = 1.0 / c.bc2, a = c.alpha;
+        double* __restrict__ mm = m;
+        double* __restrict__ vv = v;
+        double* __restrict__ vx = vmax;
+        double* __restrict__ yy = y;
+        const double* __restrict__ gg = g;
+        for (long long q = 0; q < nvar; ++q) {
+            const double gk = gg[q];
+            const double mk = b1 * mm[q] + (1.0 - b1) * gk;
+            double vk;
+            if (M == DONOF_ORB_ADABELIEF) {
+                const double dd = gk - mk;
+                vk = b2 * vv[q] + (1.0 - b2) * (dd * dd);
+            } else if (M == DONOF_ORB_YOGI) {
+                const double g2 = gk * gk, dv = vv[q] - g2;
+                vk = vv[q] - (1.0 - b2) * ((dv > 0.0) ? g2 : ((dv < 0.0) ? -g2 : 0.0));
+            } else {
+                vk = b2 * vv[q] + (1.0 - b2) * (gk * gk);
+            }
+            const double vh = vk * ib2, vo = vx[q];
+            const double vm = (vo > vh) ? vo : vh;
+            mm[q] = mk;
+            vv[q] = vk;
+            vx[q] = vm;
+            yy[q] = -a * (mk * ib1) / sqrt(vm + 1e-16);
+        }
+    };
+    switch (method) {
+        case DONOF_ORB_ADABELIEF: run(std::integral_constant<int, DONOF_ORB_ADABELIEF>{}); break;
+        case DONOF_ORB_YOGI: run(std::integral_constant<int, DONOF_ORB_YOGI>{}); break;
+        case DONOF_ORB_DEMON: run(std::integral_constant<int, DONOF_ORB_DEMON>{}); break;
+        default: run(std::integral_constant<int, DONOF_ORB_ADAM>{}); break;
+    }
+    if (gmax) *gmax = mx;
+    return DONOF_OK;
+}

@@ -16,7 +16,7 @@ struct Coef {
     double beta1, beta2, bc1, bc2, alpha;  // bc = 1 - beta^i
 };
 
-__device__ __forceinline__ Coef coef(int method, int i, int maxloop, double alpha) {
+__host__ __device__ __forceinline__ Coef coef(int method, int i, int maxloop, double alpha) {
     Coef c;
     c.method = method;
     c.beta1 = (method == DONOF_ORB_DEMON) ? 0.6 : 0.5;
@@ -32,7 +32,7 @@ __device__ __forceinline__ Coef coef(int method, int i, int maxloop, double alph
     return c;
 }
 
-__device__ __forceinline__ void step(const Coef& c, long long k, const double* __restrict__ g, double* __restrict__ m,
+__host__ __device__ __forceinline__ void step(const Coef& c, long long k, const double* __restrict__ g, double* __restrict__ m,
                                      double* __restrict__ v, double* __restrict__ vmax, double* __restrict__ y) {
     const double gk = g[k];
     const double mk = c.beta1 * m[k] + (1.0 - c.beta1) * gk;

@@ -91,6 +91,7 @@ SIGNATURES = {
     "donof_profile_enable": (_i, [_vp, _i]),
     "donof_profile_last_ms": (_i, [_vp, ct.POINTER(ct.c_float)]),
     "donof_mixed_tmp_dev": (_i, [_vp, _vp, _i, _vp]),
+    "donof_orb_step_host": (_i, [_i, _i, _i, ct.c_double, _vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp]),
     # integral front end
     "donof_basis_create": (_i, [_i, _vp, _vp, _vp, _vp, _vp, _i, ct.POINTER(_vp)]),
     "donof_basis_nbf": (_i, [_vp]),

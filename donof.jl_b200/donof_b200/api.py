@@ -319,6 +319,41 @@ def calcorbg(y, n, cj12, ck12, C, H, b: BTensor, p: Param):
     return g
 
 
+class OrbStepHost:
+    """The host side of the reference's optimiser loop (src/minimization.jl:390-412)
+    for a caller that drives it through rotate_orbital + compute_Lagrange2:
+    ``y = step(elag)`` packs calcorbg's gradient and applies the update of the
+    next iteration in compiled code (donof_orb_step_host), keeping m, v, vmax.
+    ``alloc`` makes the arrays (e.g. host_pinned, so that y is DMA'd directly);
+    y is overwritten by the next step; ``gmax`` holds max|g| of the last one."""
+
+    def __init__(self, nbf: int, nbf5: int, method: str = "ADAM", alpha: float = 0.01, maxloop: int = 10,
+                 alloc=np.zeros):
+        self.lib = _lib.load()
+        self.nbf, self.nbf5, self.method = nbf, nbf5, _lib.ORB_METHODS[method]
+        self.alpha, self.maxloop = alpha, maxloop
+        nvar = nbf5 * nbf - nbf5 * (nbf5 + 1) // 2
+        self.g, self.m, self.v, self.vmax = (np.zeros(nvar) for _ in range(4))
+        self.y = alloc(nvar)
+        self.it = 0
+        self.gmax = ct.c_double()
+
+    def reset(self) -> None:
+        for a in (self.m, self.v, self.vmax):
+            a[:] = 0.0
+        self.it = 0
+
+    def step(self, elag) -> np.ndarray:
+        elag = _f64(elag)
+        if elag.shape != (self.nbf, self.nbf):
+            raise ValueError(f"elag must be {self.nbf} x {self.nbf}")
+        self.it += 1
+        _lib.check(self.lib.donof_orb_step_host(self.method, self.it, self.maxloop, float(self.alpha), _ptr(elag),
+                                                self.nbf, self.nbf5, _ptr(self.g), _ptr(self.m), _ptr(self.v),
+                                                _ptr(self.vmax), _ptr(self.y), ct.byref(self.gmax)))
+        return self.y
+
+
 def orbopt(gamma, C, H, b: BTensor, p: Param, method: Optional[str] = None):
     """One orbital-optimiser call, device resident (src/minimization.jl:242-630).
     Returns (E, C, nit, success) and updates p.alpha / p.maxloop like the reference."""

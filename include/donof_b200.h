@@ -204,6 +204,16 @@ int donof_rotate_dev(donof_ctx* ctx, const double* y, int nbf, int nbf5, const d
 int donof_orbgrad(donof_job* job, const double* y, const double* C, const double* n,
                   const double* H, const double* cj12, const double* ck12, int nbf5, int nalpha,
                   int nbeta, double* grad);
+/* The host side of one iteration of the reference's optimiser loop
+ * (src/minimization.jl:390-412), for a caller that drives the loop itself
+ * through donof_rotate + donof_lagrange2: g = 4 elag - 4 elag^T packed over
+ * i < nbf5, j > i (nvar values), then the update of iteration it (1-based) of
+ * method (DONOF_ORB_*; Demon's beta1 decays over maxloop) with step alpha into
+ * the caller's state m, v, vmax and the rotation y (nvar doubles each, zero
+ * before iteration 1); *gmax = max|g| (may be NULL).  Host arrays, no device
+ * work.                                                                     */
+int donof_orb_step_host(int method, int it, int maxloop, double alpha, const double* elag, int nbf, int nbf5,
+                        double* g, double* m, double* v, double* vmax, double* y, double* gmax);
 
 /* --- orbital optimiser -----------------------------------------------------
  * One call of orbopt_adam / orbopt_adabelief / orbopt_yogi / orbopt_demon
