@@ -167,6 +167,67 @@ function orbgrad(y, n, cj12, ck12, C, H, b::B200Tensor, nalpha, nbeta)
 end
 
 """
+The host side of one iteration of the optimiser loop (src/minimization.jl:390-412)
+for a caller that drives it through `rotate` and `lagrange2`: packs calcorbg's
+gradient from `elag` into `g` and updates `m`, `v`, `vmax` and `y` in place
+(donof_orb_step_host, compiled code).  Returns max|g|.
+"""
+function orb_step_host!(method::AbstractString, it::Integer, maxloop::Integer, alpha::Real,
+                        elag::Matrix{Float64}, nbf5::Integer, g, m, v, vmax, y)
+    gmax = Ref{Float64}(0.0)
+    check(ccall((:donof_orb_step_host, libdonof), Cint,
+                (Cint, Cint, Cint, Cdouble, Ptr{Float64}, Cint, Cint, Ptr{Float64}, Ptr{Float64}, Ptr{Float64},
+                 Ptr{Float64}, Ptr{Float64}, Ref{Float64}),
+                ORB_METHODS[method], it, maxloop, alpha, elag, size(elag, 1), nbf5, g, m, v, vmax, y, gmax),
+          Ptr{Cvoid}(C_NULL))
+    return gmax[]
+end
+
+# --- integral front end (in place of GaussianBasis.jl in compute_integrals,
+# src/integrals.jl:1-49): shells as flat arrays (l, centre in bohr, primitive
+# counts, exponents, contraction coefficients as a basis-set file prints them).
+mutable struct B200Basis
+    handle::Ptr{Cvoid}
+    nbas::Int
+end
+
+function basis(l::Vector{Cint}, centre::Vector{Float64}, nprim::Vector{Cint}, exps::Vector{Float64},
+               coefs::Vector{Float64}; spherical::Bool = true)
+    h = Ref{Ptr{Cvoid}}(C_NULL)
+    check(ccall((:donof_basis_create, libdonof), Cint,
+                (Cint, Ptr{Cint}, Ptr{Float64}, Ptr{Cint}, Ptr{Float64}, Ptr{Float64}, Cint, Ref{Ptr{Cvoid}}),
+                length(l), l, centre, nprim, exps, coefs, spherical, h), Ptr{Cvoid}(C_NULL))
+    nb = ccall((:donof_basis_nbf, libdonof), Cint, (Ptr{Cvoid},), h[])
+    bs = B200Basis(h[], nb)
+    finalizer(x -> ccall((:donof_basis_free, libdonof), Cint, (Ptr{Cvoid},), x.handle), bs)
+    return bs
+end
+
+"""S, T, V (overlap, kinetic, nuclear with the nuclei Z at xyz, bohr, 3 x natom)."""
+function int1e(b::B200Basis, Z::Vector{Float64}, xyz::Matrix{Float64})
+    S, T, V = zeros(b.nbas, b.nbas), zeros(b.nbas, b.nbas), zeros(b.nbas, b.nbas)
+    check(ccall((:donof_int1e, libdonof), Cint,
+                (Ptr{Cvoid}, Cint, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}),
+                b.handle, length(Z), Z, xyz, S, T, V), Ptr{Cvoid}(C_NULL))
+    return S, T, V
+end
+
+"""ERI_2e2c: G[P, Q] = (P|Q) over the auxiliary basis."""
+function int2c2e(aux::B200Basis)
+    G = zeros(aux.nbas, aux.nbas)
+    check(ccall((:donof_int2c2e, libdonof), Cint, (Ptr{Cvoid}, Ptr{Float64}), aux.handle, G), Ptr{Cvoid}(C_NULL))
+    return G
+end
+
+"""ERI_2e3c: I[m, n, P] = (mn|P) (host threads); `iaux(int2c2e(aux), int3c2e(b, aux))` then gives the job's b."""
+function int3c2e(b::B200Basis, aux::B200Basis)
+    I = zeros(b.nbas, b.nbas, aux.nbas)
+    check(ccall((:donof_int3c2e, libdonof), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Float64}),
+                b.handle, aux.handle, I), Ptr{Cvoid}(C_NULL))
+    return I
+end
+
+"""
 One orbopt_adam / _adabelief / _yogi / _demon call (src/minimization.jl:242-630)
 with the whole loop on the device.  `alpha` and `maxloop` are read and updated
 like p.alpha and p.maxloop.  Returns (E, C, nit, success).
