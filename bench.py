@@ -80,11 +80,13 @@ def parse():
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--profile-case", nargs="?", const="synthetic256",
-                    choices=["synthetic256", "octane600", "batch64", "batch8"],
+                    choices=["synthetic256", "octane600", "batch64", "batch8", "ints3c"],
                     help="run the mixed and FP64 Lagrangian and the rotation three times each and exit (the "
                          "cases the committed ncu captures use): the benchmark workload, or an n-octane-shaped "
                          "job (nbf 202, nbf5 198, naux 600) on the general-shape mixed pipeline; batch64: three "
-                         "grouped orbital steps of the 64-job water-cluster batch; batch8: the same for its first 8 jobs")
+                         "grouped orbital steps of the 64-job water-cluster batch; batch8: the same for its first 8 "
+                         "jobs; ints3c: the integral front end's three-centre kernel on a cc-pVDZ-sized synthetic "
+                         "basis of (H2O)_8 (nbf 192, naux 512), three launches, timed against the host path")
     return ap.parse_args()
 
 
@@ -685,6 +687,30 @@ def profile_case(d, torch, wl, ctx):
     bt.free()
 
 
+def ints3c_case(d, torch, workload, device):
+    """(mn|P) of the integral front end on the device (three launches, CUDA
+    events on the context's stream) and on the host threads, same basis."""
+    import numpy as np
+    from donof_b200 import integrals as it
+
+    ctx = d.Context(device)
+    orb, aux = workload.water_cluster_bases(8)
+    ms = []
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        out = it.ERI_2e3c_dev(orb, aux, ctx)
+        e1.record()
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    t = time.perf_counter()
+    host = it.ERI_2e3c(orb, aux)
+    th = time.perf_counter() - t
+    dev = out.cpu().numpy().reshape(host.shape, order="F")
+    return {"case": "ints3c", "nbf": orb.nbas, "naux": aux.nbas, "device_ms": ms, "host_ms": th * 1e3,
+            "host_threads": os.cpu_count(), "max_rel_diff": float(np.max(np.abs(dev - host)) / np.max(np.abs(host)))}
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -715,6 +741,9 @@ def main():
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
+    if args.profile_case == "ints3c":
+        print(json.dumps(ints3c_case(d, torch, workload, local)), flush=True)
+        return
     wl = workload.synthetic(**WORKLOAD, seed=SEED)
     p = wl.p
     ctx = d.Context(local)

@@ -117,3 +117,35 @@ CONFIGS = {
     "synthetic-256": dict(nbf=256, naux=1024, nbeta=16, ncwo=3),
     "n-octane-ccpvdz-surrogate": dict(nbf=202, naux=974, nbeta=33, ncwo=5),
 }
+
+
+def _et(lo: float, ratio: float, count: int) -> np.ndarray:
+    return lo * ratio ** np.arange(count)[::-1]
+
+
+def water_cluster_bases(k: int = 8, seed: int = 0, spherical: bool = True):
+    """A cc-pVDZ-sized synthetic orbital basis and an s-f auxiliary basis on a
+    seeded (H2O)_k (the integral front end's workload; no basis-set data ships
+    here, so the exponents are even-tempered and the contractions seeded):
+    O 3s2p1d + H 2s1p (24 functions per water), auxiliary O 5s3p3d1f + H 3s2p1d
+    (64 per water).  Returns (orbital BasisSet, auxiliary BasisSet)."""
+    from . import integrals as it
+
+    rng = np.random.default_rng(seed)
+    prim = _et(0.25, 3.0, 8)
+    c = lambda n: np.abs(rng.standard_normal(n)) + 0.1
+    orb = {"O": [(0, prim, c(8)), (0, prim[-3:], c(3)), (0, prim[-1:], np.ones(1)),
+                 (1, _et(0.3, 3.5, 3), c(3)), (1, np.array([0.3]), np.ones(1)), (2, np.array([1.2]), np.ones(1))],
+           "H": [(0, _et(0.15, 4.0, 3), c(3)), (0, np.array([0.12]), np.ones(1)), (1, np.array([0.7]), np.ones(1))]}
+    aux = {"O": [(0, np.array([x]), np.ones(1)) for x in _et(0.3, 4.0, 5)] +
+                [(1, np.array([x]), np.ones(1)) for x in _et(0.5, 4.0, 3)] +
+                [(2, np.array([x]), np.ones(1)) for x in _et(0.4, 3.0, 3)] + [(3, np.array([1.0]), np.ones(1))],
+           "H": [(0, np.array([x]), np.ones(1)) for x in _et(0.3, 5.0, 3)] +
+                [(1, np.array([x]), np.ones(1)) for x in _et(0.5, 4.0, 2)] + [(2, np.array([1.0]), np.ones(1))]}
+    lines = []
+    for _ in range(k):
+        o = rng.uniform(-4.0, 4.0, 3)
+        lines += [f"O {o[0]} {o[1]} {o[2]}", f"H {o[0]} {o[1] + 0.757} {o[2] + 0.587}",
+                  f"H {o[0]} {o[1] - 0.757} {o[2] + 0.587}"]
+    atoms, _, _ = it.parse_molecule("\n".join(lines))
+    return it.BasisSet("synthetic-dz", atoms, orb, spherical), it.BasisSet("synthetic-dz-jk", atoms, aux, spherical)
