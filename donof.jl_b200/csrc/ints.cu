@@ -174,6 +174,7 @@ constexpr int SPH_DOUBLES = 1 + 9 + 30 + 70 + 135;  // ncart(l) (2l + 1), l <= 4
 struct DevBasis {
     int nshell, nbf, spherical, pad;
     const int *l, *nprim, *prim0, *ao0;
+    const int* order;  // shells sorted by (l, primitive count): neighbouring threads take alike shells
     const double *ctr, *ex, *co;
 };
 
@@ -193,7 +194,7 @@ __global__ void __launch_bounds__(128) int3c2e_kernel(const DevBasis orb, const 
     const long long w = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (w >= npair * aux.nshell) return;
     const long long pw = w / aux.nshell;
-    const int k = (int)(w % aux.nshell);
+    const int k = aux.order[w % aux.nshell];
     int i = (int)((sqrt(8.0 * (double)pw + 1.0) - 1.0) / 2.0);
     while ((long long)i * (i + 1) / 2 > pw) --i;
     while ((long long)(i + 1) * (i + 2) / 2 <= pw) ++i;
@@ -241,7 +242,7 @@ __global__ void __launch_bounds__(128) int3c2e_kernel(const DevBasis orb, const 
 // The basis' arrays in device memory (one allocation, made once per basis).
 int upload_basis(donof_ctx* ctx, donof_basis* b, DevBasis* d) {
     const size_t ni = (size_t)b->nshell, np = b->ex.size();
-    const size_t bytes = 4 * ni * sizeof(int) + (3 * ni + 2 * np) * sizeof(double) + 64;
+    const size_t bytes = 5 * ni * sizeof(int) + (3 * ni + 2 * np) * sizeof(double) + 64;
     if (!b->dev || b->dev_device != ctx->device) {
         if (b->dev) cudaFree(b->dev);
         b->dev = nullptr;
@@ -260,6 +261,12 @@ int upload_basis(donof_ctx* ctx, donof_basis* b, DevBasis* d) {
         put(b->nprim.data(), ni * sizeof(int));
         put(b->prim0.data(), ni * sizeof(int));
         put(b->ao0.data(), ni * sizeof(int));
+        std::vector<int> order(ni);
+        for (size_t s = 0; s < ni; ++s) order[s] = (int)s;
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+            return b->l[x] != b->l[y] ? b->l[x] < b->l[y] : b->nprim[x] < b->nprim[y];
+        });
+        put(order.data(), ni * sizeof(int));
         DONOF_CUDA(ctx, cudaMemcpy(b->dev, h.data(), bytes, cudaMemcpyHostToDevice));
     }
     char* q = static_cast<char*>(b->dev);
@@ -278,6 +285,7 @@ int upload_basis(donof_ctx* ctx, donof_basis* b, DevBasis* d) {
     d->nprim = reinterpret_cast<const int*>(take(ni * sizeof(int)));
     d->prim0 = reinterpret_cast<const int*>(take(ni * sizeof(int)));
     d->ao0 = reinterpret_cast<const int*>(take(ni * sizeof(int)));
+    d->order = reinterpret_cast<const int*>(take(ni * sizeof(int)));
     return DONOF_OK;
 }
 
