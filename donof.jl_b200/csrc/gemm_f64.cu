@@ -189,8 +189,10 @@ int gemm_f64_run(donof_ctx* ctx, cudaStream_t st, bool a_kmajor, bool b_kmajor, 
     cudaError_t e;
     if (tile == GemmTile::Large)
         e = launch_layout<128, 64, 4, 2>(p, a_kmajor, b_kmajor, vec, st, persistent);
-    else if (tile == GemmTile::Small || tile == GemmTile::SmallW8)
+    else if (tile == GemmTile::Small)
         e = launch_layout<64, 64, 2, 2>(p, a_kmajor, b_kmajor, vec, st, persistent);
+    else if (tile == GemmTile::SmallW8)
+        e = launch_layout<64, 64, 2, 4>(p, a_kmajor, b_kmajor, vec, st, persistent);
     else
         e = launch_layout<32, 32, 2, 2>(p, a_kmajor, b_kmajor, vec, st, persistent);
     if (e != cudaSuccess) {
@@ -323,8 +325,9 @@ int time_candidates(donof_ctx* ctx, cudaStream_t st, int count, Run run) {
     return best;
 }
 
-const GemmTile kTiles[3] = {GemmTile::Large, GemmTile::Small, GemmTile::Tiny};
-const int kTileBM[3] = {128, 64, 32}, kTileBN[3] = {64, 64, 32};
+constexpr int kNT = 4;
+const GemmTile kTiles[kNT] = {GemmTile::Large, GemmTile::Small, GemmTile::Tiny, GemmTile::SmallW8};
+const int kTileBM[kNT] = {128, 64, 32, 64}, kTileBN[kNT] = {64, 64, 32, 64};
 
 }  // namespace
 
@@ -338,11 +341,11 @@ int gemm_f64_tuned(donof_ctx* ctx, cudaStream_t st, bool a_kmajor, bool b_kmajor
     if (tune_lookup(key, &v)) return gemm_f64_run(ctx, st, a_kmajor, b_kmajor, p, v.tile, v.persistent);
     if (capturing(st)) return gemm_f64(ctx, st, a_kmajor, b_kmajor, p, heuristic);
     // every tile shape, one CTA per tile and persistent
-    const int best = time_candidates(ctx, st, 6, [&](int c) {
-        return gemm_f64_run(ctx, st, a_kmajor, b_kmajor, p, kTiles[c % 3], c >= 3);
+    const int best = time_candidates(ctx, st, 2 * kNT, [&](int c) {
+        return gemm_f64_run(ctx, st, a_kmajor, b_kmajor, p, kTiles[c % kNT], c >= kNT);
     });
     if (best < 0) return DONOF_ERR_CUDA;
-    tune_store(key, TuneVal{kTiles[best % 3], 1, best >= 3});
+    tune_store(key, TuneVal{kTiles[best % kNT], 1, best >= kNT});
     return DONOF_OK;  // every candidate wrote the same C
 }
 
@@ -366,7 +369,7 @@ int partials_choice(donof_ctx* ctx, cudaStream_t st, bool a_kmajor, bool b_kmajo
         const GemmTile h = pick_tile(ctx, M, N, K, true, &sp);
         cands.push_back(TuneVal{h, sp});
         const int max_splits = K / 64 > 1 ? K / 64 : 1;
-        for (int t = 0; t < 3; ++t) {
+        for (int t = 0; t < kNT; ++t) {
             const long long tiles = (long long)((M + kTileBM[t] - 1) / kTileBM[t]) * ((N + kTileBN[t] - 1) / kTileBN[t]);
             for (int f = 1; f <= 2; ++f) {
                 long long s = (f * (long long)ctx->sm_count + tiles - 1) / tiles;

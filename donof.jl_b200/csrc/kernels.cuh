@@ -10,8 +10,8 @@
 
 namespace donof {
 
-// Tile shapes of the FP64 GEMM.  SmallW8 (64 x 64 over 8 warps of 32 x 16) is
-// a grouped-kernel-only shape: more warps per SM for short-K products.
+// Tile shapes of the FP64 GEMM.  SmallW8 (64 x 64 over 8 warps of 32 x 16):
+// more warps per SM for short-K products.
 enum class GemmTile { Large /*128x64*/, Small /*64x64*/, Tiny /*32x32*/, SmallW8 /*64x64, 8 warps*/ };
 
 // C = alpha*op(A)op(B) + beta*C on stream st (see gemm_f64.cuh for addressing).
