@@ -314,7 +314,7 @@ ozaki_t1_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant
         // and columns [32 (w / 4), +32) of every accumulator = q = 64 qt + 32 (w / 4) + k
         const int quarter = warp & 3, half = warp >> 2;
         const uint32_t tl = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(half * 32);
-        // zero every accumulator and release it for round 0
+        // zero every accumulator and release it for the first work unit
 #pragma unroll
         for (int g = 0; g < S; ++g) tmem_zero32(tl + (uint32_t)(g * QT));
         tmem_wait_st();
