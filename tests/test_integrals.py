@@ -247,3 +247,23 @@ def test_compute_integrals_without_ri_returns_the_four_index_array():
     S, T, V, H, I = it.compute_integrals(bset, None, p)
     assert np.allclose(H, T + V) and I.shape == (2, 2, 2, 2)
     assert abs(I[0, 0, 0, 0] - 0.7746) < 1e-4
+
+
+@pytest.mark.parametrize("spherical_orb", [True, False])
+def test_ri_is_exact_when_the_auxiliary_basis_spans_every_product(spherical_orb):
+    """On one centre, s(a) s(a) = s(2a), s(a) p(b) = p(a+b) and p(b) p(b) lies in
+    the six Cartesian d(2b) functions, so with those as the auxiliary basis the
+    RI factorisation sum (mn|P) G^-1_PQ (Q|ls) reproduces (mn|ls) exactly: a
+    consistency check of the two-, three- and four-centre integrals together."""
+    a, b = 0.9, 0.6
+    orb = basis([("He", (0.2, -0.1, 0.3))], {"He": [(0, np.array([a]), np.array([1.0])),
+                                                    (1, np.array([b]), np.array([1.0]))]}, spherical_orb)
+    aux = basis([("He", (0.2, -0.1, 0.3))], {"He": [(0, np.array([2 * a]), np.array([1.0])),
+                                                    (1, np.array([a + b]), np.array([1.0])),
+                                                    (2, np.array([2 * b]), np.array([1.0]))]}, spherical=False)
+    n = orb.nbas
+    I4 = it.ERI_2e4c(orb).reshape(n * n, n * n)
+    I3 = it.ERI_2e3c(orb, aux).reshape(n * n, -1)
+    G = it.ERI_2e2c(aux)
+    ri = I3 @ np.linalg.solve(G, I3.T)
+    assert np.max(np.abs(ri - I4)) < 1e-11 * np.max(np.abs(I4))
