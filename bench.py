@@ -80,13 +80,15 @@ def parse():
     ap.add_argument("--no-serving", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--profile-case", nargs="?", const="synthetic256",
-                    choices=["synthetic256", "octane600", "batch64", "batch8", "ints3c"],
+                    choices=["synthetic256", "octane600", "batch64", "batch8", "ints3c", "pipeline"],
                     help="run the mixed and FP64 Lagrangian and the rotation three times each and exit (the "
                          "cases the committed ncu captures use): the benchmark workload, or an n-octane-shaped "
                          "job (nbf 202, nbf5 198, naux 600) on the general-shape mixed pipeline; batch64: three "
                          "grouped orbital steps of the 64-job water-cluster batch; batch8: the same for its first 8 "
                          "jobs; ints3c: the integral front end's three-centre kernel on a cc-pVDZ-sized synthetic "
-                         "basis of (H2O)_8 (nbf 192, naux 512), three launches, timed against the host path")
+                         "basis of (H2O)_8 (nbf 192, naux 512), three launches, timed against the host path; "
+                         "pipeline: that molecule from its basis to 20 outer iterations of the energy loop "
+                         "(integrals, RI tensor, guess, loop), timed by stage")
     return ap.parse_args()
 
 
@@ -711,6 +713,37 @@ def ints3c_case(d, torch, workload, device):
             "host_threads": os.cpu_count(), "max_rel_diff": float(np.max(np.abs(dev - host)) / np.max(np.abs(host)))}
 
 
+def pipeline_case(d, torch, workload, device, outer=20):
+    """A molecule through the whole path: integrals (one-electron and (P|Q) on
+    the host, (mn|P) on the device), b = I G^{-1/2} on the device (Iaux), the
+    core-Hamiltonian guess, then `outer` iterations of the FP64 energy loop
+    (first contraction on the tensor cores), each stage timed."""
+    from donof_b200 import integrals as it
+    from donof_b200.guess import guess
+
+    ctx = d.Context(device)
+    orb, aux = workload.water_cluster_bases(8)
+    ne = sum(a.Z for a in orb.atoms)
+    p = d.Param(nbf=orb.nbas, nbfaux=0, nalpha=ne // 2, nbeta=ne // 2)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    S, T, V, H, bt = it.compute_integrals(orb, aux, p, ctx)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    bt.set_fp64_tc(True)
+    C, gamma = guess(H, p, S)
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    _, _, _, _, r, hist = d.api.energy_loop(H, bt, p, C, gamma, maxit=outer)
+    t3 = time.perf_counter()
+    out = {"case": "pipeline", "workload": "synthetic cc-pVDZ-sized basis on (H2O)_8", "nbf": orb.nbas,
+           "naux": aux.nbas, "nbf5": p.nbf5, "electrons": ne, "integrals_and_iaux_s": t1 - t0,
+           "digit_split_and_guess_s": t2 - t1, "energy_loop_s": t3 - t2, "outer_iterations": r["iterations"],
+           "orbital_steps": r["tot_it_orb"], "E_elec": r["E_elec"], "converged": bool(r["converged"])}
+    bt.free()
+    return out
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -743,6 +776,9 @@ def main():
     torch.cuda.set_device(dev)
     if args.profile_case == "ints3c":
         print(json.dumps(ints3c_case(d, torch, workload, local)), flush=True)
+        return
+    if args.profile_case == "pipeline":
+        print(json.dumps(pipeline_case(d, torch, workload, local)), flush=True)
         return
     wl = workload.synthetic(**WORKLOAD, seed=SEED)
     p = wl.p
