@@ -236,10 +236,12 @@ def molecule(mol: str, basis_text: str, spherical: bool = False, name: str = "ba
     return bset, p
 
 
-def compute_integrals(bset: BasisSet, aux: BasisSet, p: Param, ctx=None, precision: str = "fp64",
+def compute_integrals(bset: BasisSet, aux, p: Param, ctx=None, precision: str = "fp64",
                       device_3c: bool = True):
     """S, T, V, H, b = compute_integrals(bset, aux, p) (src/integrals.jl:1-66):
-    the one-electron matrices symmetrised as the reference does; with p.RI,
+    the one-electron matrices symmetrised as the reference does (aux: a
+    BasisSet, or the auxiliary basis' Gaussian94 text, placed on bset's atoms in
+    bset's spherical or Cartesian form as the reference does); with p.RI,
     G = (P|Q) symmetrised, (mn|P) (on the B200 when its shells fit the device
     kernel and device_3c, else on host threads), then b = I G^{-1/2} built on
     the device (Iaux_gpu) and kept there as the job's RI tensor, and p.nbfaux
@@ -247,6 +249,8 @@ def compute_integrals(bset: BasisSet, aux: BasisSet, p: Param, ctx=None, precisi
     of b."""
     from . import api
 
+    if isinstance(aux, str):  # the auxiliary basis' text: on the same atoms, in the same form (src/integrals.jl:17-39)
+        aux = BasisSet.from_text(bset.name + "-jkfit", aux, bset.atoms, bset.spherical)
     S, T, V = one_electron(bset)
     S, T, V = (S + S.T) / 2, (T + T.T) / 2, (V + V.T) / 2
     H = T + V
