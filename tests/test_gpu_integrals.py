@@ -121,3 +121,20 @@ def test_h2_energy_from_computed_integrals_is_the_exact_two_electron_energy(cuda
     assert abs(E_final - E_exact) < 1e-7, (E_final, E_exact)
     assert r["E_elec"] >= E_final - 1e-9
     bt.free()
+
+
+def test_compute_integrals_takes_the_auxiliary_basis_as_text(cuda_ctx):
+    """The auxiliary basis given as Gaussian94 text is placed on the molecule in
+    the orbital basis' form and gives the same RI tensor as the BasisSet."""
+    text = ("H 0\nS 3 1.00\n 3.42525091 0.15432897\n 0.62391373 0.53532814\n 0.16885540 0.44463454\n****\n")
+    aux_text = ("H 0\nS 1 1.00\n 1.2 1.0\n****\nH 0\nS 1 1.00\n 0.35 1.0\nP 1 1.00\n 0.9 1.0\n****\n")
+    bset, p = it.molecule("H 0 0 0\nH 0 0 0.74", text, spherical=True)
+    _, _, _, H, b1 = it.compute_integrals(bset, aux_text, p, cuda_ctx)
+    aux = it.BasisSet.from_text("aux", aux_text, bset.atoms, True)
+    _, _, _, _, b2 = it.compute_integrals(bset, aux, p, cuda_ctx)
+    assert b1.naux == aux.nbas == 2 * (1 + 1 + 3)
+    J1, K1, _ = d.JKH_MO(np.eye(2), H, b1, 2, 2, b1.naux)
+    J2, K2, _ = d.JKH_MO(np.eye(2), H, b2, 2, 2, b2.naux)
+    assert np.array_equal(J1, J2) and np.array_equal(K1, K2)
+    b1.free()
+    b2.free()
